@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark: time-to-solution of the 1M-node P1 wave-equation CG solve.
+
+Workload (one step): SOLVE of A x = b on the 1001 x 1001-node mesh
+(1,002,001 nodes, 2,000,000 triangles; A = M + dt*g*h_e*K_e, smooth depth,
+b = A x_true), diagonal preconditioning, relative residual 1e-8, x0 = 0.
+`value` is the mixed-precision solve (binary32 inner CG with binary64
+refinement) in solves/s over all ranks, with the inputs resident in HBM;
+the plain binary64 GRACJG solve, the standalone EBE matvec bandwidth and
+the end-to-end (host buffers through the C ABI) time are reported beside it.
+
+Multi-GPU: each rank solves its own replica (the path does not shard in
+this build), so scaling is weak; times are the max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1M-node P1 CG time-to-1e-8 relres: mixed vs FP64 on 1 B200; matvec HBM GB/s"
+UNIT = "solves/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=1001, help="nodes per side of the mesh")
+    ap.add_argument("--eps", type=float, default=1e-8)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="target CPU time of the bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def algorithmic_bytes(npoin, nelem):
+    """Algorithmic bytes (each input read once, each output written once)."""
+    return dict(
+        # EBE matvec 'X=AY' with a full diagonal, binary64: XM 3x8 + IKLE 3x4
+        # per element; DM, Y in, X out per node
+        mv64=36 * nelem + 24 * npoin,
+        # one binary64 GRACJG iteration on the scaled system: matvec without
+        # diagonal (36/elem + 16/node) + 9 node-vector accesses (72/node)
+        it64=36 * nelem + 88 * npoin,
+        # one binary32 inner iteration: matvec 12+12 per element, row sum +
+        # p in + q out (12/node) + 9 binary32 node-vector accesses (36/node)
+        it32=24 * nelem + 48 * npoin,
+        # reliable update: binary64 matvec on x + b, r32, x and z updates
+        upd=36 * nelem + 48 * npoin,
+    )
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                p = [c.strip() for c in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def build_problem(n, device):
+    """Mesh, operator (assembled on the device), manufactured solution."""
+    import torch
+    from opentelemac_b200 import bief, meshgen as mg
+    x, y, ik = mg.square_mesh(n)
+    coef = mg.wave_coef(mg.depth_smooth(x, y, ik))
+    npoin = x.size
+    mesh = bief.Mesh(ik, npoin, device=device)
+    A = bief.Matrix(mesh)
+    t = lambda a: torch.tensor(a, device=f"cuda:{device}", dtype=torch.float64)
+    A.assemble_wave(t(x), t(y), t(coef))
+    xt = t(mg.random_solution(npoin))
+    b = torch.zeros_like(xt)
+    bief.matvec("X=AY    ", b, A, xt)
+    return dict(x=x, y=y, ik=ik, coef=coef, mesh=mesh, A=A, xt=xt, b=b, npoin=npoin,
+                nelem=ik.shape[0])
+
+
+def cpu_baseline(n, eps, nit_full, seconds, ik=None):
+    """The oracle's reference-order binary64 SOLVE on one host core, timed on
+    a bounded number of CG iterations and extrapolated to a full solve."""
+    import oracle
+    from opentelemac_b200 import meshgen as mg
+    oracle.build()
+    x, y, ik = mg.square_mesh(n)
+    coef = mg.wave_coef(mg.depth_smooth(x, y, ik))
+    dm, xm = oracle.wave_matrix(x, y, ik, coef)
+    b = oracle.matvec("X=AY    ", ik, dm, "Q", xm, "S", mg.random_solution(x.size))
+    args = (ik, dm, "Q", xm, "S", b)
+    k1 = 5
+    t0 = time.perf_counter()
+    oracle.solve(*args, nitmax=k1, eps=1e-300)
+    t1 = time.perf_counter() - t0
+    k2 = 25
+    t0 = time.perf_counter()
+    oracle.solve(*args, nitmax=k2, eps=1e-300)
+    t2 = time.perf_counter() - t0
+    per_it = max((t2 - t1) / (k2 - k1), 1e-9)
+    k3 = int(min(max(k2 + 10, seconds / per_it), nit_full))
+    t0 = time.perf_counter()
+    oracle.solve(*args, nitmax=k3, eps=1e-300)
+    t3 = time.perf_counter() - t0
+    per_it = (t3 - t1) / (k3 - k1)
+    setup = max(t1 - k1 * per_it, 0.0)
+    full = setup + per_it * nit_full
+    return {"value": 1.0 / full, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": (f"binary64 reference-order C restatement of SOLVE/GRACJG, 1 thread, "
+                       f"{k3} of {nit_full} CG iterations timed ({t3:.1f} s) on the "
+                       f"{x.size}-node mesh, extrapolated: {per_it * 1e3:.2f} ms/iteration, "
+                       f"{full:.1f} s per solve"),
+            "seconds_per_solve": full, "ms_per_iteration": per_it * 1e3}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def max_over_ranks(v, ws):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_reference(args, ws, rank):
+    """--impl reference: the reference algorithm's CPU implementation (the
+    oracle port; the Fortran cannot be compiled on these machines), one
+    bounded sample per step, rank 0 only."""
+    if rank != 0:
+        return
+    import oracle
+    from opentelemac_b200 import meshgen as mg
+    oracle.build()
+    x, y, ik = mg.square_mesh(args.n)
+    coef = mg.wave_coef(mg.depth_smooth(x, y, ik))
+    dm, xm = oracle.wave_matrix(x, y, ik, coef)
+    b = oracle.matvec("X=AY    ", ik, dm, "Q", xm, "S", mg.random_solution(x.size))
+    solve_args = (ik, dm, "Q", xm, "S", b)
+    # iteration count of the full solve: known for the standard mesh, else
+    # measured on the small mesh and scaled linearly with n (CG ~ sqrt(cond))
+    nit_full = {1001: 4315}.get(args.n)
+    if nit_full is None:
+        r = oracle.solve(*solve_args, eps=args.eps) if x.size <= 300000 else None
+        nit_full = r["nit"] if r else int(438 * args.n / 101)
+    k = 40
+    times = []
+    for s in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        oracle.solve(*solve_args, nitmax=k, eps=1e-300)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            times.append(dt)
+    per_it = statistics.median(times) / k
+    full = per_it * nit_full
+    val = 1.0 / full
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": full * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"SOLVE SLV=1 PRECON=2 EPS={args.eps:g}, {x.size}-node "
+                                   f"P1 mesh ({ik.shape[0]} triangles), binary64, CPU"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": f"{k} of {nit_full} CG iterations per step, "
+                                       f"extrapolated to a full solve"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import torch
+    from opentelemac_b200 import bief
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    P = build_problem(args.n, local)
+    A, b, mesh = P["A"], P["b"], P["mesh"]
+    npoin, nelem = P["npoin"], P["nelem"]
+    by = algorithmic_bytes(npoin, nelem)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
+    x = torch.zeros_like(b)
+    cfg = bief.SlvCfg(slv=1, nitmax=1000000, precon=2, krylov=0, eps=args.eps, zero=0.0)
+
+    def run_mixed():
+        x.zero_()
+        return bief.solve_mixed(x, A, b, precon=2, inner_tol=1e-4, outer_tol=args.eps)
+
+    def run_fp64():
+        x.zero_()
+        return bief.solve(x, A, b, cfg)
+
+    def timed(fn, steps, warmup):
+        """per-step device time (ms) with an L2 flush before each step, and
+        the library's kernel time of the solver launch."""
+        out, kern, res = [], [], None
+        for s in range(warmup + steps):
+            flush.fill_(float(s))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = fn()
+            e1.record()
+            e1.synchronize()
+            if s >= warmup:
+                out.append(e0.elapsed_time(e1))
+                kern.append(mesh.last_timing()[0])
+        return out, kern, res
+
+    # binary64 GRACJG (reported beside the headline)
+    barrier(ws)
+    f64_ms, f64_kern, f64_res = timed(run_fp64, max(2, args.steps // 2), args.warmup)
+    f64_x_err = float(torch.linalg.norm(x - P["xt"]) / torch.linalg.norm(P["xt"]))
+    x_f64 = x.clone()
+    nit64 = f64_res[1]
+
+    # standalone EBE matvec bandwidth (binary64, full diagonal)
+    y = P["xt"]
+    out = torch.zeros_like(y)
+    mv_ms = []
+    for s in range(args.warmup + 20):
+        flush.fill_(float(s))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        bief.matvec("X=AY    ", out, A, y)
+        e1.record()
+        e1.synchronize()
+        if s >= args.warmup:
+            mv_ms.append(e0.elapsed_time(e1))
+    mv_t = statistics.median(mv_ms)
+
+    # headline: mixed precision, timed steps, clocks sampled meanwhile
+    barrier(ws)
+    launches0 = mesh.kernel_launches()
+    with ClockSampler(local) as clk:
+        mx_ms, mx_kern, mx_res = timed(run_mixed, args.steps, args.warmup)
+    launches = (mesh.kernel_launches() - launches0) * args.steps // (args.steps + args.warmup)
+    st, outer, inner, relres = mx_res
+    mixed_x_err = float(torch.linalg.norm(x - P["xt"]) / torch.linalg.norm(P["xt"]))
+    mixed_vs_f64 = float(torch.linalg.norm(x - x_f64) / torch.linalg.norm(x_f64))
+    barrier(ws)
+    step_ms = max_over_ranks(sum(mx_ms) / len(mx_ms), ws)
+    f64_step_ms = max_over_ranks(sum(f64_ms) / len(f64_ms), ws)
+    kern_ms = sum(mx_kern) / len(mx_kern)
+    f64_kern_ms = sum(f64_kern) / len(f64_kern)
+
+    # end to end through the public API with pinned host buffers: matrix and
+    # right-hand side uploaded, solution read back, every step
+    dm_h, xm_h, _ = A.get()
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    dm_p, xm_p = pin(dm_h), pin(xm_h)
+    b_p = pin(b.cpu().numpy())
+    x_p = pin(np.zeros(npoin))
+    e2e = []
+    for s in range(args.warmup + args.steps):
+        x_p[:] = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        A.set(dm_p, xm_p, "Q", "S")
+        bief.solve_mixed(x_p, A, b_p, precon=2, inner_tol=1e-4, outer_tol=args.eps)
+        t1 = time.perf_counter()
+        if s >= args.warmup:
+            e2e.append((t1 - t0) * 1e3)
+    e2e_ms = max_over_ranks(sum(e2e) / len(e2e), ws)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.n, args.eps, nit64, args.cpu_seconds)
+
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except Exception:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    mixed_bytes = inner * by["it32"] + (outer + 1) * by["upd"]
+    achieved = mixed_bytes / (kern_ms * 1e-3) / 1e9
+    f64_bytes = nit64 * by["it64"]
+    mv_gbs = by["mv64"] / (mv_t * 1e-3) / 1e9
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": ws * 1000.0 / step_ms, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+            "config": {"workload": f"wave-equation SOLVE (CG, diagonal precon, relres "
+                                   f"{args.eps:g}) on the {args.n}x{args.n}-node P1 mesh",
+                       "npoin": npoin, "nelem": nelem, "parallelism": f"replicas x{ws}",
+                       "l2": "256 MiB buffer written before every timed step"},
+            "time_to_solution_ms": {"mixed": step_ms, "fp64": f64_step_ms,
+                                    "mixed_kernel": kern_ms, "fp64_kernel": f64_kern_ms},
+            "speedup_mixed_vs_fp64": f64_step_ms / step_ms,
+            "iterations": {"fp64": nit64, "mixed_inner": inner, "mixed_updates": outer},
+            "relres": {"mixed": relres, "fp64": f64_res[2]},
+            "error": {"mixed_vs_fp64": mixed_vs_f64, "mixed_vs_xtrue": mixed_x_err,
+                      "fp64_vs_xtrue": f64_x_err},
+            "matvec": {"op": "X=AY binary64 TYPDIA=Q", "ms": mv_t, "gbs": mv_gbs,
+                       "frac": mv_gbs / hbm, "bytes": by["mv64"]},
+            "fp64_cg": {"gbs": f64_bytes / (f64_kern_ms * 1e-3) / 1e9,
+                        "frac": f64_bytes / (f64_kern_ms * 1e-3) / 1e9 / hbm,
+                        "bytes_per_iteration": by["it64"]},
+            "roofline": {"bound": "hbm", "kernel": "k_mixed", "achieved": achieved,
+                         "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+                         "bytes_per_launch": mixed_bytes, "traffic": None},
+            "e2e": {"value": ws * 1000.0 / e2e_ms, "unit": UNIT,
+                    "h2d_bytes_per_step": 8 * (npoin + 3 * nelem) + 16 * npoin,
+                    "d2h_bytes_per_step": 8 * npoin, "ms_per_step": e2e_ms},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    barrier(ws)
+    mesh.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

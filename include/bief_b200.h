@@ -1,0 +1,154 @@
+/*
+ * bief_b200.h -- C ABI of the B200 (sm_100a) implementation of BIEF's
+ * element-by-element P1 conjugate-gradient solve and matrix-vector product.
+ *
+ * The entry points replace, for one mesh of 3-node triangles with EBE
+ * storage (STO=1, ELMLIN=ELMCOL=11), the reference subroutines
+ *
+ *   SOLVE(X,A,B,TB,CFG,INFOGR,MESH,AUX)   sources/utils/bief/solve.f:2-5
+ *        with CFG%SLV=1 (GRACJG, gracjg.F:2-5) and CFG%PRECON in
+ *        {0,1,2,3,5} (diagonal change of variables, precd1.f:88-158)
+ *   MATVEC(OP,X,A,Y,C,MESH,LEGO)           sources/utils/bief/matvec.f:2-5
+ *        with OP in 'X=AY', 'X=X+AY', 'X=-AY', 'X=X-AY', 'X=X+CAY',
+ *        'X=CAY', 'X=TAY', 'X=-TAY', 'X=X+TAY', 'X=X-TAY', 'X=X+CTAY'
+ *        (matvec.f:316-380 -> matvct.f:255-306 -> mv0303.f:117-630)
+ *
+ * Conventions (those of the Fortran caller):
+ *   - IKLE is the Fortran array IKLE(NELMAX,3): column-major, 1-based.
+ *   - XM is A%X%R viewed as XM(NELMAX,NDIAG): NDIAG=3 for symmetric storage
+ *     TYPEXT='S' (columns M12,M13,M23) or 6 for TYPEXT='Q' (then M21,M31,
+ *     M32), following om1111.f:43-50.  DM is A%D%R(NPOIN).
+ *   - TYPDIA is 'Q' (any diagonal), 'I' (identity) or '0' (zero).
+ *   - Host pointers unless the function name ends in _dev.
+ *   - Every function returns an int status: 0 = success; > 0 = the solve
+ *     stopped at NITMAX without converging (the value is the iteration
+ *     count); < 0 = an error (see BIEF_ERR_*).  The reference aborts with
+ *     PLANTE(1) on errors; a Fortran shim maps < 0 to PLANTE(1).
+ *   - A handle owns one CUDA stream and its device buffers; calls on one
+ *     handle must not overlap.  Different handles are independent.
+ *
+ * Floating point: the binary64 solve performs the reference's operations in
+ * the reference's order with no fused multiply-add, so the matrix-vector
+ * product, the change of variables and every vector update are bit-identical
+ * to the Fortran; only the dot products are summed in a fixed parallel tree
+ * (bief_launch_info gives its shape).
+ */
+#ifndef BIEF_B200_H
+#define BIEF_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BIEF_OK                   0
+#define BIEF_ERR_ARGS            -1  /* bad argument / unknown OP string   */
+#define BIEF_ERR_BREAKDOWN       -2  /* D.AD <= 0: matrix not SPD           */
+#define BIEF_ERR_NAN             -3  /* NaN/Inf met in the iteration         */
+#define BIEF_ERR_BAD_MESH        -4  /* IKLE entry outside 1..NPOIN          */
+#define BIEF_ERR_UNSUPPORTED     -5  /* SLV/PRECON/storage not on this path  */
+#define BIEF_ERR_CUDA            -6  /* CUDA runtime error                   */
+#define BIEF_ERR_DEVICE_TIMEOUT  -7  /* a grid barrier wait ran out          */
+#define BIEF_ERR_NO_MATRIX       -8  /* solve/matvec before set_matrix       */
+#define BIEF_ERR_SIZE            -9  /* problem larger than a fixed limit    */
+
+/* Mirror of TYPE(SLVCFG) (bief_def.f:506-532). */
+typedef struct {
+    int    slv;     /* 1 = conjugate gradient; anything else is rejected  */
+    int    nitmax;  /* maximum number of iterations                        */
+    int    precon;  /* 0/1 none, 2 diagonal, 3 (=2 for one matrix), 5 |diag| */
+    int    krylov;  /* unused by CG                                        */
+    double eps;     /* relative (or absolute, when ||B||^2 < 1) accuracy    */
+    double zero;    /* unused by CG                                        */
+    int    ok;      /* out: 1 when the accuracy was reached                */
+    int    nit;     /* out: iterations done                                */
+} bief_slvcfg;
+
+typedef struct bief_handle bief_handle;
+
+/* Solve flags */
+#define BIEF_SOLVE_MUTATE_INPUTS  1  /* leave B = D.B and the stored matrix
+                                        = D.A.D (TYPDIA 'I'), as SOLVE does */
+#define BIEF_SOLVE_INFOGR         2  /* print the GRACJG iteration message  */
+
+/* Mesh: replaces the MESH%IKLE / NPOIN / NELEM / NELMAX part of BIEF_MESH
+ * (bief_def.f:205-498).  Validates IKLE and builds the node->element
+ * gather index used instead of ASSVEC's scatter (assvec.f:88-93).  All
+ * device memory for the mesh, one matrix and the solver work vectors
+ * (SOLVE's TBB blocks, solve.f:192-209) is allocated here, once. */
+int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle,
+                     int device, bief_handle **out);
+int bief_destroy(bief_handle *h);
+
+/* Matrix A%D, A%X, A%TYPDIA, A%TYPEXT of a BIEF_OBJ with STO=1
+ * (bief_def.f:74-196): host arrays copied to the device. */
+int bief_set_matrix(bief_handle *h, const double *dm, const double *xm,
+                    char typdia, char typext);
+/* Device-array variant: dm[npoin], xm[ndiag*nelem] with leading dim nelem. */
+int bief_set_matrix_dev(bief_handle *h, const double *dm, const double *xm,
+                        char typdia, char typext);
+/* Read back the stored matrix (e.g. after a mutating solve). */
+int bief_get_matrix(bief_handle *h, double *dm, double *xm, char *typdia);
+
+/* SOLVE(X,A,B,...) for SLV=1: host X (initial guess in, solution out) and
+ * B.  relres_out receives SQRT(RMRM/XL) as printed by GRACJG. */
+int bief_solve(bief_handle *h, double *x, double *b, bief_slvcfg *cfg,
+               int flags, double *relres_out);
+/* Same with device pointers, on `stream` (cudaStream_t, NULL = handle's). */
+int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg,
+                   int flags, double *relres_out, void *stream);
+
+/* Mixed precision (no reference counterpart): binary32 copy of the scaled
+ * operator and binary32 inner CG (stopped at inner_tol relative),
+ * binary64 residual and update in an outer refinement loop stopped at
+ * outer_tol (relative to ||D.B||, absolute when that is < 1).  B is not
+ * modified.  outer_out/inner_out: outer steps and total inner iterations. */
+int bief_solve_mixed(bief_handle *h, double *x, const double *b,
+                     int precon, double inner_tol, double outer_tol,
+                     int max_outer, int max_inner, int *outer_out,
+                     int *inner_out, double *relres_out);
+int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b,
+                         int precon, double inner_tol, double outer_tol,
+                         int max_outer, int max_inner, int *outer_out,
+                         int *inner_out, double *relres_out, void *stream);
+
+/* MATVEC(OP,X,A,Y,C,MESH,LEGO=.TRUE.): OP is the reference's 8-character
+ * operation string (trailing blanks optional). */
+int bief_matvec(bief_handle *h, const char *op, double *x, const double *y,
+                double c);
+int bief_matvec_dev(bief_handle *h, const char *op, double *x,
+                    const double *y, double c, void *stream);
+
+/* Wave-equation operator A = M + coef_e K_e assembled on the device the way
+ * PROPAG assembles AM1 (propag.F:661-677,1407): MT01AA mass (mt01aa.f:82-
+ * 103) plus MT02AA P0 diffusion (mt02aa.f:106-149), diagonals assembled by
+ * ASSVEC (matrix.f:218-227) and summed by OM 'M=M+N' (om1111.f:299-312).
+ * x, y: node coordinates; coef: per-element coefficient (device arrays).
+ * Stores the result as the handle's matrix (TYPDIA 'Q', TYPEXT 'S'). */
+int bief_assemble_wave_dev(bief_handle *h, const double *x, const double *y,
+                           const double *coef, void *stream);
+/* Copy the stored matrix to device arrays dm[npoin], xm[3*nelem]. */
+int bief_get_matrix_dev(bief_handle *h, double *dm, double *xm, void *stream);
+
+/* Adjoint gradient of a loss through x = A(coef)^-1 b with
+ * A = M + coef_e K_e: grad[e] = -lambda_e^T K_e x_e (K_e from MT02AA with
+ * unit coefficient), for device arrays lambda[npoin], x[npoin],
+ * x/y coordinates; writes grad[nelem].  No reference counterpart. */
+int bief_wave_coef_grad_dev(bief_handle *h, const double *xc,
+                            const double *yc, const double *lambda,
+                            const double *x, double *grad, void *stream);
+
+/* Shape of the device dot-product tree: number of blocks and threads per
+ * block of the persistent solver kernel. */
+int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads);
+/* Kernel time (ms, CUDA events on the handle's stream) of the last solve
+ * kernel and of the last matvec kernel. */
+int bief_last_timing(bief_handle *h, float *solve_ms, float *matvec_ms);
+/* Number of device kernels the library launched since the handle was made. */
+long long bief_kernel_launches(bief_handle *h);
+
+const char *bief_strerror(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

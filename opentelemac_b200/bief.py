@@ -1,0 +1,225 @@
+"""Host-side mirror of BIEF's SOLVE / MATVEC interface over libbief_b200.
+
+    SOLVE(X,A,B,TB,CFG,INFOGR,MESH,AUX)   sources/utils/bief/solve.f:2-5
+    MATVEC(OP,X,A,Y,C,MESH,LEGO)          sources/utils/bief/matvec.f:2-5
+
+`Mesh` stands for the IKLE/NPOIN/NELEM part of BIEF_MESH, `Matrix` for a
+BIEF_OBJ matrix with EBE storage (STO=1) and `SlvCfg` for SLVCFG.  Vectors
+are numpy float64 arrays (host path: the library copies them to the device
+and back) or torch CUDA float64 tensors (device path, no copies).
+
+Errors: the reference aborts with PLANTE(1); here a negative status raises
+BiefError.  A solve that stops at NITMAX returns normally with cfg.ok = 0
+(the reference only prints a message in that case).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native
+from ._native import BiefError, SlvCfg  # noqa: F401  (re-exported)
+
+
+def _is_torch(a):
+    return type(a).__module__.startswith("torch")
+
+
+def _ptr(a):
+    if _is_torch(a):
+        if not a.is_cuda or not a.is_contiguous():
+            raise ValueError("torch tensors must be contiguous CUDA tensors")
+        return ctypes.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _stream(a):
+    import torch
+    return ctypes.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)
+
+
+def _check(st, what):
+    if st < 0:
+        raise BiefError(st, what)
+    return st
+
+
+class Mesh:
+    """Mesh connectivity on one GPU (owns the native handle).
+
+    ikle0: (nelem, 3) 0-based node numbers of each triangle, or use
+    Mesh.from_fortran for the reference's IKLE(NELMAX,3) 1-based layout."""
+
+    def __init__(self, ikle0, npoin, device=0):
+        ik = np.asarray(ikle0)
+        if ik.ndim != 2 or ik.shape[1] != 3:
+            raise ValueError("ikle0 must have shape (nelem, 3)")
+        nelem = ik.shape[0]
+        fort = np.ascontiguousarray((ik.T + 1).astype(np.int32)).ravel()
+        self._init(fort, npoin, nelem, nelem, device)
+
+    @classmethod
+    def from_fortran(cls, ikle, npoin, nelem, nelmax, device=0):
+        self = cls.__new__(cls)
+        self._init(np.ascontiguousarray(ikle, dtype=np.int32).ravel(), npoin, nelem, nelmax,
+                   device)
+        return self
+
+    def _init(self, fort, npoin, nelem, nelmax, device):
+        self.npoin, self.nelem, self.nelmax, self.device = int(npoin), int(nelem), int(nelmax), device
+        self._h = ctypes.c_void_p()
+        L = _native.lib()
+        _check(L.bief_mesh_create(self.npoin, self.nelem, self.nelmax,
+                                  fort.ctypes.data_as(ctypes.c_void_p), device,
+                                  ctypes.byref(self._h)), "bief_mesh_create")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def launch_info(self):
+        """(blocks, threads) of the persistent solver: the dot-product tree."""
+        g, t = ctypes.c_int(), ctypes.c_int()
+        _native.lib().bief_launch_info(self._h, ctypes.byref(g), ctypes.byref(t))
+        return g.value, t.value
+
+    def last_timing(self):
+        s, m = ctypes.c_float(), ctypes.c_float()
+        _native.lib().bief_last_timing(self._h, ctypes.byref(s), ctypes.byref(m))
+        return s.value, m.value
+
+    def kernel_launches(self):
+        return int(_native.lib().bief_kernel_launches(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _native.lib().bief_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Matrix:
+    """EBE matrix A (A%D, A%X, TYPDIA, TYPEXT) stored on the mesh's handle.
+
+    dm: (npoin,) diagonal; xm: (ndiag, nelem) off-diagonal terms, columns
+    M12, M13, M23 (+ M21, M31, M32 for typext 'Q').  The handle holds one
+    matrix: creating a second Matrix on the same Mesh replaces the first."""
+
+    def __init__(self, mesh, dm=None, xm=None, typdia="Q", typext="S"):
+        self.mesh = mesh
+        self.typdia, self.typext = typdia, typext
+        if dm is not None:
+            self.set(dm, xm, typdia, typext)
+
+    def set(self, dm, xm, typdia="Q", typext="S"):
+        L = _native.lib()
+        if _is_torch(dm):
+            _check(L.bief_set_matrix_dev(self.mesh.handle, _ptr(dm), _ptr(xm),
+                                         typdia.encode(), typext.encode()), "bief_set_matrix_dev")
+        else:
+            dm = np.ascontiguousarray(dm, dtype=np.float64)
+            nd = {"S": 3, "Q": 6, "0": 0}[typext]
+            xm = (np.ascontiguousarray(np.asarray(xm, dtype=np.float64).reshape(nd, -1))
+                  if nd else np.zeros(1))
+            _check(L.bief_set_matrix(self.mesh.handle, _ptr(dm), _ptr(xm), typdia.encode(),
+                                     typext.encode()), "bief_set_matrix")
+        self.typdia, self.typext = typdia, typext
+        return self
+
+    def get(self):
+        """Stored (dm, xm, typdia) as numpy arrays."""
+        nd = {"S": 3, "Q": 6, "0": 0}[self.typext]
+        dm = np.empty(self.mesh.npoin)
+        xm = np.empty((max(nd, 1), self.mesh.nelem))
+        td = ctypes.create_string_buffer(2)
+        _check(_native.lib().bief_get_matrix(self.mesh.handle, _ptr(dm), _ptr(xm), td),
+               "bief_get_matrix")
+        self.typdia = td.value.decode()
+        return dm, xm[:nd], self.typdia
+
+    def assemble_wave(self, xc, yc, coef):
+        """A = M + coef_e K_e from device coordinates and coefficients
+        (torch CUDA float64 tensors)."""
+        _check(_native.lib().bief_assemble_wave_dev(self.mesh.handle, _ptr(xc), _ptr(yc),
+                                                    _ptr(coef), _stream(xc)),
+               "bief_assemble_wave_dev")
+        self.typdia, self.typext = "Q", "S"
+        return self
+
+
+def solve(x, A, b, cfg, infogr=False, mutate=False):
+    """SOLVE(X,A,B,...,CFG,INFOGR,...) for CFG.slv = 1 (GRACJG).
+
+    x holds the initial guess and receives the solution.  With mutate=True
+    the reference's side effects are reproduced: b becomes D.b and A is
+    replaced by D.A.D (TYPDIA 'I').  Returns (status, nit, relres)."""
+    L = _native.lib()
+    flags = (_native.BIEF_SOLVE_MUTATE_INPUTS if mutate else 0) | (
+        _native.BIEF_SOLVE_INFOGR if infogr else 0)
+    relres = ctypes.c_double()
+    if _is_torch(x):
+        st = L.bief_solve_dev(A.mesh.handle, _ptr(x), _ptr(b), ctypes.byref(cfg), flags,
+                              ctypes.byref(relres), _stream(x))
+    else:
+        _host_vec(x, A.mesh.npoin)
+        _host_vec(b, A.mesh.npoin)
+        st = L.bief_solve(A.mesh.handle, _ptr(x), _ptr(b), ctypes.byref(cfg), flags,
+                          ctypes.byref(relres))
+    _check(st, "SOLVE")
+    if mutate:
+        A.typdia = A.get()[2] if not _is_torch(x) else A.typdia
+    return st, cfg.nit, relres.value
+
+
+def solve_mixed(x, A, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, max_outer=1000,
+                max_inner=1000000):
+    """Mixed-precision solve (binary32 inner CG, binary64 refinement).
+    Returns (status, outer_steps, inner_iterations, relres)."""
+    L = _native.lib()
+    o, i = ctypes.c_int(), ctypes.c_int()
+    relres = ctypes.c_double()
+    if _is_torch(x):
+        st = L.bief_solve_mixed_dev(A.mesh.handle, _ptr(x), _ptr(b), precon, inner_tol,
+                                    outer_tol, max_outer, max_inner, ctypes.byref(o),
+                                    ctypes.byref(i), ctypes.byref(relres), _stream(x))
+    else:
+        _host_vec(x, A.mesh.npoin)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        st = L.bief_solve_mixed(A.mesh.handle, _ptr(x), _ptr(b), precon, inner_tol, outer_tol,
+                                max_outer, max_inner, ctypes.byref(o), ctypes.byref(i),
+                                ctypes.byref(relres))
+    _check(st, "SOLVE (mixed)")
+    return st, o.value, i.value, relres.value
+
+
+def matvec(op, x, A, y, c=0.0):
+    """MATVEC(OP,X,A,Y,C,MESH,LEGO=.TRUE.): X updated in place."""
+    L = _native.lib()
+    opb = op.encode() if isinstance(op, str) else op
+    if _is_torch(x):
+        st = L.bief_matvec_dev(A.mesh.handle, opb, _ptr(x), _ptr(y), float(c), _stream(x))
+    else:
+        _host_vec(x, A.mesh.npoin)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        st = L.bief_matvec(A.mesh.handle, opb, _ptr(x), _ptr(y), float(c))
+    _check(st, "MATVEC")
+    return x
+
+
+def coef_grad(A, xc, yc, lam, x, grad):
+    """grad[e] = -lam_e^T K_e x_e (device tensors)."""
+    _check(_native.lib().bief_wave_coef_grad_dev(A.mesh.handle, _ptr(xc), _ptr(yc), _ptr(lam),
+                                                 _ptr(x), _ptr(grad), _stream(x)),
+           "bief_wave_coef_grad_dev")
+    return grad
+
+
+def _host_vec(a, n):
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise ValueError("host vectors must be contiguous float64 numpy arrays")
+    if a.size != n:
+        raise ValueError(f"vector of size {a.size}, expected NPOIN={n}")

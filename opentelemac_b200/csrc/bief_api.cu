@@ -1,0 +1,677 @@
+// bief_api.cu -- extern "C" entry points of libbief_b200.so (declared in
+// include/bief_b200.h).  Host side of the B200 drop-in for BIEF's
+// SOLVE(SLV=1) and MATVEC on EBE P1 matrices: argument validation with the
+// reference's semantics, the node->element gather index, device buffers,
+// and launches of the kernels in bief_kernels.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/bief_b200.h"
+#include "bief_kernels.cuh"
+
+using namespace bief;
+
+struct bief_handle {
+  int dev = 0, npoin = 0, nelem = 0, nelmax = 0, nsm = 0;
+  cudaStream_t stream = nullptr;
+  int G = 0, T = CG_THREADS;  // persistent grid shape (dot tree shape)
+  // mesh
+  int *d_ptr = nullptr, *d_ek = nullptr, *d_ik = nullptr;
+  // stored matrix (A%D, A%X)
+  double *d_dm = nullptr, *d_xm = nullptr;
+  char typdia = 'Q', typext = 'S';
+  int has_matrix = 0;
+  // working (scaled) matrix and change of variables
+  double *d_dms = nullptr, *d_xms = nullptr, *d_dsc = nullptr;
+  float *d_xm32 = nullptr, *d_dm32 = nullptr;
+  // vectors
+  double *d_x = nullptr, *d_b = nullptr, *d_bs = nullptr, *d_r = nullptr, *d_d0 = nullptr,
+         *d_d1 = nullptr, *d_ad = nullptr, *d_t = nullptr;
+  float *d_z = nullptr, *d_ri = nullptr, *d_p0 = nullptr, *d_p1 = nullptr, *d_q = nullptr;
+  double *d_part = nullptr, *d_ew = nullptr;
+  Ctl *d_ctl = nullptr, *h_ctl = nullptr;
+  int *d_err = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  float solve_ms = 0.f, matvec_ms = 0.f;
+  long long launches = 0;
+  long long timeout_ns = 2000000000LL;
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char *what, int line) {
+  fprintf(stderr, "libbief_b200: %s failed (%s) at %s:%d\n", what, cudaGetErrorString(e), __FILE__,
+          line);
+  return BIEF_ERR_CUDA;
+}
+#define CK(call)                                              \
+  do {                                                        \
+    cudaError_t e__ = (call);                                 \
+    if (e__ != cudaSuccess) return cuda_fail(e__, #call, __LINE__); \
+  } while (0)
+
+struct DevGuard {
+  int prev = -1;
+  explicit DevGuard(int d) {
+    cudaGetDevice(&prev);
+    if (prev != d) cudaSetDevice(d);
+  }
+  ~DevGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+int typdia_code(char c) {
+  switch (c) {
+    case 'Q': case 'q': return DIA_Q;
+    case 'I': case 'i': return DIA_I;
+    case '0': return DIA_0;
+    default: return -1;
+  }
+}
+
+int grid_for(int n, int nsm) {
+  int g = (n + 255) / 256;
+  return std::max(1, std::min(g, nsm * 16));
+}
+
+// Parse an 8-character MATVEC operation string (trailing blanks optional).
+int parse_op(const char *op, int *opc, bool *trans) {
+  if (!op) return BIEF_ERR_ARGS;
+  char s[9];
+  int n = 0;
+  for (; n < 8 && op[n]; ++n) s[n] = op[n];
+  while (n > 0 && s[n - 1] == ' ') --n;
+  s[n] = 0;
+  struct { const char *name; int opc; bool trans; } tab[] = {
+      {"X=AY", OP_AY, false},    {"X=X+AY", OP_XPAY, false}, {"X=-AY", OP_MAY, false},
+      {"X=X-AY", OP_XMAY, false}, {"X=X+CAY", OP_XPCAY, false}, {"X=CAY", OP_CAY, false},
+      {"X=TAY", OP_AY, true},    {"X=-TAY", OP_MAY, true},   {"X=X+TAY", OP_XPAY, true},
+      {"X=X-TAY", OP_XMAY, true}, {"X=X+CTAY", OP_XPCAY, true}};
+  for (auto &t : tab)
+    if (!strcmp(s, t.name)) {
+      *opc = t.opc;
+      *trans = t.trans;
+      return BIEF_OK;
+    }
+  return BIEF_ERR_ARGS;
+}
+
+template <int TD, bool SYM, bool TR>
+void launch_mv(bief_handle *h, const double *xm, const double *da, const double *y, double *x,
+               int opc, double c, cudaStream_t st) {
+  k_matvec<TD, SYM, TR><<<grid_for(h->npoin, h->nsm), 256, 0, st>>>(
+      h->npoin, h->nelem, h->d_ptr, h->d_ek, h->d_ik, xm, da, y, x, opc, c);
+}
+
+void dispatch_mv(bief_handle *h, int td, bool sym, bool tr, const double *xm, const double *da,
+                 const double *y, double *x, int opc, double c, cudaStream_t st) {
+#define MV_CASE(TD_, S_, T_) \
+  if (td == TD_ && sym == S_ && tr == T_) return launch_mv<TD_, S_, T_>(h, xm, da, y, x, opc, c, st);
+  MV_CASE(DIA_Q, true, false) MV_CASE(DIA_I, true, false) MV_CASE(DIA_0, true, false)
+  MV_CASE(DIA_Q, false, false) MV_CASE(DIA_I, false, false) MV_CASE(DIA_0, false, false)
+  MV_CASE(DIA_Q, true, true) MV_CASE(DIA_I, true, true) MV_CASE(DIA_0, true, true)
+  MV_CASE(DIA_Q, false, true) MV_CASE(DIA_I, false, true) MV_CASE(DIA_0, false, true)
+#undef MV_CASE
+}
+
+void *cg_kernel(int td, bool sym) {
+  if (sym) {
+    if (td == DIA_Q) return (void *)k_cg64<DIA_Q, true>;
+    if (td == DIA_I) return (void *)k_cg64<DIA_I, true>;
+    return (void *)k_cg64<DIA_0, true>;
+  }
+  if (td == DIA_Q) return (void *)k_cg64<DIA_Q, false>;
+  if (td == DIA_I) return (void *)k_cg64<DIA_I, false>;
+  return (void *)k_cg64<DIA_0, false>;
+}
+
+void *mixed_kernel(int td) {
+  if (td == DIA_Q) return (void *)k_mixed<DIA_Q>;
+  if (td == DIA_I) return (void *)k_mixed<DIA_I>;
+  return (void *)k_mixed<DIA_0>;
+}
+
+// Largest grid of the persistent kernels that is guaranteed co-resident,
+// reduced for small meshes so that each thread has at least two nodes.
+int persistent_grid(int npoin, int nsm, int *out) {
+  int best = 1 << 30;
+  void *ks[] = {cg_kernel(DIA_Q, true), cg_kernel(DIA_I, true), cg_kernel(DIA_0, true),
+                cg_kernel(DIA_Q, false), cg_kernel(DIA_I, false), cg_kernel(DIA_0, false),
+                mixed_kernel(DIA_Q), mixed_kernel(DIA_I), mixed_kernel(DIA_0)};
+  for (void *k : ks) {
+    int bps = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, CG_THREADS, 0));
+    best = std::min(best, bps);
+  }
+  if (best < 1) return BIEF_ERR_CUDA;
+  int g = best * nsm;
+  int need = (npoin + 2 * CG_THREADS - 1) / (2 * CG_THREADS);
+  *out = std::max(1, std::min(g, need));
+  return BIEF_OK;
+}
+
+template <typename T>
+int dalloc(T **p, size_t n) {
+  CK(cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(n, 1)));
+  return BIEF_OK;
+}
+
+int ensure_matrix_buffers(bief_handle *h) {
+  if (h->d_xm) return BIEF_OK;
+  size_t ne = (size_t)h->nelem;
+  int st;
+  if ((st = dalloc(&h->d_xm, 6 * ne))) return st;
+  if ((st = dalloc(&h->d_xms, 6 * ne))) return st;
+  if ((st = dalloc(&h->d_xm32, 3 * ne))) return st;
+  return BIEF_OK;
+}
+
+void print_gracjg(int status, int nit, double relres, int relat) {
+  // gracjg.F:426-435 formats 102/202 (converged), 104/204 (NITMAX)
+  if (status > 0)
+    printf(" GRACJG (BIEF) : EXCEEDING MAXIMUM ITERATIONS:%8d %s PRECISION:%16.7G\n", nit,
+           relat ? "RELATIVE" : "ABSOLUTE", relres);
+  else
+    printf(" GRACJG (BIEF) : %8d ITERATIONS, %s PRECISION:%16.7G\n", nit,
+           relat ? "RELATIVE" : "ABSOLUTE", relres);
+}
+
+int launch_coop(bief_handle *h, void *k, void *arg, cudaStream_t st) {
+  void *args[] = {arg};
+  CK(cudaLaunchCooperativeKernel(k, dim3(h->G), dim3(h->T), args, 0, st));
+  h->launches++;
+  return BIEF_OK;
+}
+
+// PRECD1 (precd1.f:88-158) into the working matrix; x scaled in place,
+// b_out = D*b_in.  Returns the working TYPDIA.
+int do_precd1(bief_handle *h, int precon, double *x, const double *b_in, double *b_out,
+              bool want32, int *td_work, cudaStream_t st) {
+  const int n = h->npoin;
+  const int td_in = typdia_code(h->typdia);
+  k_precd1_nodes<<<grid_for(n, h->nsm), 256, 0, st>>>(n, precon, td_in, h->d_dm, x, b_in, b_out,
+                                                      h->d_dsc, h->d_dms);
+  h->launches++;
+  const int ndiag = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
+  if (ndiag) {
+    k_precd1_elems<<<grid_for(h->nelem, h->nsm), 256, 0, st>>>(
+        h->nelem, ndiag, h->d_ik, h->d_dsc, h->d_xm, h->d_xms, want32 ? h->d_xm32 : nullptr);
+    h->launches++;
+  }
+  // TYPDIA after OM 'M=DMD' is 'Q' (unless '0'); PRECON divisible by 2
+  // or 3 then makes it the identity (precd1.f:137-142).
+  int td = (td_in == DIA_0) ? DIA_0 : DIA_Q;
+  if (precon % 2 == 0 || precon % 3 == 0) td = DIA_I;
+  *td_work = td;
+  CK(cudaGetLastError());
+  return BIEF_OK;
+}
+
+int check_cfg(const bief_slvcfg *cfg, int *precon) {
+  if (!cfg) return BIEF_ERR_ARGS;
+  if (cfg->slv != 1) return BIEF_ERR_UNSUPPORTED;
+  int p = cfg->precon == 0 ? 1 : cfg->precon;
+  if (p <= 0) return BIEF_ERR_ARGS;
+  if (p % 7 == 0 || p % 11 == 0 || p % 13 == 0 || p % 17 == 0) return BIEF_ERR_UNSUPPORTED;
+  *precon = p;
+  return BIEF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *bief_strerror(int s) {
+  if (s > 0) return "not converged: NITMAX reached";
+  switch (s) {
+    case BIEF_OK: return "ok";
+    case BIEF_ERR_ARGS: return "invalid argument";
+    case BIEF_ERR_BREAKDOWN: return "breakdown: D.AD <= 0 (matrix not positive definite)";
+    case BIEF_ERR_NAN: return "NaN or Inf in the iteration";
+    case BIEF_ERR_BAD_MESH: return "bad mesh: IKLE outside 1..NPOIN or non-positive element area";
+    case BIEF_ERR_UNSUPPORTED: return "unsupported solver, preconditioning or storage";
+    case BIEF_ERR_CUDA: return "CUDA runtime error";
+    case BIEF_ERR_DEVICE_TIMEOUT: return "device barrier wait timed out";
+    case BIEF_ERR_NO_MATRIX: return "no matrix set on this handle";
+    case BIEF_ERR_SIZE: return "problem size exceeds a fixed limit";
+    default: return "unknown status";
+  }
+}
+
+int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int device,
+                     bief_handle **out) {
+  if (!out || !ikle || npoin <= 0 || nelem <= 0 || nelmax < nelem) return BIEF_ERR_ARGS;
+  if (nelem > (1 << 29)) return BIEF_ERR_SIZE;
+  *out = nullptr;
+  // IKLE(NELMAX,3), 1-based -> three 0-based columns; range check.
+  std::vector<int> ik(3 * (size_t)nelem);
+  std::vector<int> deg(npoin + 1, 0);
+  for (int k = 0; k < 3; ++k)
+    for (int e = 0; e < nelem; ++e) {
+      int v = ikle[(size_t)k * nelmax + e];
+      if (v < 1 || v > npoin) return BIEF_ERR_BAD_MESH;
+      ik[(size_t)k * nelem + e] = v - 1;
+      deg[v]++;
+    }
+  // Node -> (element, local point) gather index in ASSVEC order: local
+  // point outer, element inner (assvec.f:88-93), i.e. sorted by (k, e).
+  std::vector<int> ptr(npoin + 1, 0);
+  for (int i = 0; i < npoin; ++i) ptr[i + 1] = ptr[i] + deg[i + 1];
+  std::vector<int> pos(ptr.begin(), ptr.end() - 1);
+  std::vector<int> ek(3 * (size_t)nelem);
+  for (int k = 0; k < 3; ++k)
+    for (int e = 0; e < nelem; ++e) {
+      int v = ik[(size_t)k * nelem + e];
+      ek[pos[v]++] = (e << 2) | k;
+    }
+
+  bief_handle *h = new (std::nothrow) bief_handle;
+  if (!h) return BIEF_ERR_ARGS;
+  h->dev = device;
+  h->npoin = npoin;
+  h->nelem = nelem;
+  h->nelmax = nelmax;
+  int st = BIEF_OK;
+  {
+    DevGuard g(device);
+    auto fail = [&](int s) { bief_destroy(h); return s; };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaSetDevice", __LINE__));
+    if ((e = cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+      return fail(cuda_fail(e, "cudaDeviceGetAttribute", __LINE__));
+    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess)
+      return fail(cuda_fail(e, "cudaStreamCreate", __LINE__));
+    for (auto &ev : h->ev)
+      if ((e = cudaEventCreate(&ev)) != cudaSuccess) return fail(cuda_fail(e, "cudaEventCreate", __LINE__));
+    size_t n = (size_t)npoin, ne = (size_t)nelem;
+    if ((st = dalloc(&h->d_ptr, n + 1)) || (st = dalloc(&h->d_ek, 3 * ne)) ||
+        (st = dalloc(&h->d_ik, 3 * ne)) || (st = dalloc(&h->d_dm, n)) ||
+        (st = dalloc(&h->d_dms, n)) || (st = dalloc(&h->d_dsc, n)) ||
+        (st = dalloc(&h->d_dm32, n)) || (st = dalloc(&h->d_x, n)) || (st = dalloc(&h->d_b, n)) ||
+        (st = dalloc(&h->d_bs, n)) || (st = dalloc(&h->d_r, n)) || (st = dalloc(&h->d_d0, n)) ||
+        (st = dalloc(&h->d_d1, n)) || (st = dalloc(&h->d_ad, n)) || (st = dalloc(&h->d_t, n)) ||
+        (st = dalloc(&h->d_z, n)) || (st = dalloc(&h->d_ri, n)) || (st = dalloc(&h->d_p0, n)) ||
+        (st = dalloc(&h->d_p1, n)) || (st = dalloc(&h->d_q, n)) || (st = dalloc(&h->d_err, 1)) ||
+        (st = dalloc(&h->d_ctl, 1)))
+      return fail(st);
+    if ((st = persistent_grid(npoin, h->nsm, &h->G))) return fail(st);
+    if ((st = dalloc(&h->d_part, 2 * (size_t)h->G + 2))) return fail(st);
+    if ((e = cudaMallocHost((void **)&h->h_ctl, sizeof(Ctl))) != cudaSuccess)
+      return fail(cuda_fail(e, "cudaMallocHost", __LINE__));
+    if ((e = cudaMemcpyAsync(h->d_ptr, ptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice,
+                             h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_ek, ek.data(), sizeof(int) * 3 * ne, cudaMemcpyHostToDevice,
+                             h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_ik, ik.data(), sizeof(int) * 3 * ne, cudaMemcpyHostToDevice,
+                             h->stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
+      return fail(cuda_fail(e, "mesh upload", __LINE__));
+  }
+  *out = h;
+  return BIEF_OK;
+}
+
+int bief_destroy(bief_handle *h) {
+  if (!h) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  void *bufs[] = {h->d_ptr, h->d_ek, h->d_ik, h->d_dm, h->d_xm, h->d_dms, h->d_xms, h->d_dsc,
+                  h->d_xm32, h->d_dm32, h->d_x, h->d_b, h->d_bs, h->d_r, h->d_d0, h->d_d1,
+                  h->d_ad, h->d_t, h->d_z, h->d_ri, h->d_p0, h->d_p1, h->d_q, h->d_part,
+                  h->d_ew, h->d_ctl, h->d_err};
+  for (void *p : bufs)
+    if (p) cudaFree(p);
+  if (h->h_ctl) cudaFreeHost(h->h_ctl);
+  for (auto &ev : h->ev)
+    if (ev) cudaEventDestroy(ev);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return BIEF_OK;
+}
+
+static int set_matrix_impl(bief_handle *h, const double *dm, const double *xm, char typdia,
+                           char typext, bool dev) {
+  if (!h || !dm) return BIEF_ERR_ARGS;
+  if (typdia_code(typdia) < 0) return BIEF_ERR_ARGS;
+  if (typext != 'S' && typext != 'Q' && typext != '0') return BIEF_ERR_ARGS;
+  if (typext != '0' && !xm) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  int st = ensure_matrix_buffers(h);
+  if (st) return st;
+  const size_t n = (size_t)h->npoin, ne = (size_t)h->nelem;
+  const int nd = typext == 'Q' ? 6 : (typext == 'S' ? 3 : 0);
+  if (dev) {
+    CK(cudaMemcpyAsync(h->d_dm, dm, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+    if (nd)
+      CK(cudaMemcpyAsync(h->d_xm, xm, sizeof(double) * nd * ne, cudaMemcpyDeviceToDevice,
+                         h->stream));
+  } else {
+    CK(cudaMemcpyAsync(h->d_dm, dm, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    if (nd)  // XM(NELMAX,NDIAG) -> leading dimension NELEM
+      CK(cudaMemcpy2DAsync(h->d_xm, sizeof(double) * ne, xm, sizeof(double) * h->nelmax,
+                           sizeof(double) * ne, nd, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  }
+  h->typdia = typdia == 'q' ? 'Q' : (typdia == 'i' ? 'I' : typdia);
+  h->typext = typext;
+  h->has_matrix = 1;
+  return BIEF_OK;
+}
+
+int bief_set_matrix(bief_handle *h, const double *dm, const double *xm, char typdia,
+                    char typext) {
+  return set_matrix_impl(h, dm, xm, typdia, typext, false);
+}
+
+int bief_set_matrix_dev(bief_handle *h, const double *dm, const double *xm, char typdia,
+                        char typext) {
+  return set_matrix_impl(h, dm, xm, typdia, typext, true);
+}
+
+int bief_get_matrix(bief_handle *h, double *dm, double *xm, char *typdia) {
+  if (!h || !dm) return BIEF_ERR_ARGS;
+  if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
+  DevGuard g(h->dev);
+  const size_t n = (size_t)h->npoin, ne = (size_t)h->nelem;
+  const int nd = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
+  CK(cudaMemcpyAsync(dm, h->d_dm, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+  if (nd && xm)
+    CK(cudaMemcpy2DAsync(xm, sizeof(double) * h->nelmax, h->d_xm, sizeof(double) * ne,
+                         sizeof(double) * ne, nd, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (typdia) *typdia = h->typdia;
+  return BIEF_OK;
+}
+
+int bief_get_matrix_dev(bief_handle *h, double *dm, double *xm, void *stream) {
+  if (!h || !dm || !xm) return BIEF_ERR_ARGS;
+  if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
+  DevGuard g(h->dev);
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  const size_t n = (size_t)h->npoin, ne = (size_t)h->nelem;
+  CK(cudaMemcpyAsync(dm, h->d_dm, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(xm, h->d_xm, sizeof(double) * 3 * ne, cudaMemcpyDeviceToDevice, st));
+  return BIEF_OK;
+}
+
+int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int flags,
+                   double *relres_out, void *stream) {
+  if (!h || !x || !b) return BIEF_ERR_ARGS;
+  int precon, st = check_cfg(cfg, &precon);
+  if (st) return st;
+  if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
+  DevGuard g(h->dev);
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
+  const bool sym = h->typext != 'Q';
+  int td = typdia_code(h->typdia);
+  const double *xm = h->d_xm, *da = h->d_dm;
+  const double *bw = b;
+  if (diag) {
+    if ((st = do_precd1(h, precon, x, b, h->d_bs, false, &td, s))) return st;
+    xm = h->d_xms;
+    da = h->d_dms;
+    bw = h->d_bs;
+  }
+  CgP P;
+  P.npoin = h->npoin;
+  P.nelem = h->nelem;
+  P.nitmax = cfg->nitmax;
+  P.eps = cfg->eps;
+  P.ptr = h->d_ptr;
+  P.ek = h->d_ek;
+  P.ik = h->d_ik;
+  P.xm = xm;
+  P.da = da;
+  P.dsc = diag ? h->d_dsc : nullptr;
+  P.x = x;
+  P.b = bw;
+  P.r = h->d_r;
+  P.d0 = h->d_d0;
+  P.d1 = h->d_d1;
+  P.ad = h->d_ad;
+  P.part = h->d_part;
+  P.ctl = h->d_ctl;
+  P.timeout_ns = h->timeout_ns;
+  CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
+  CK(cudaEventRecord(h->ev[0], s));
+  if ((st = launch_coop(h, cg_kernel(td, sym), &P, s))) return st;
+  CK(cudaEventRecord(h->ev[1], s));
+  CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaEventElapsedTime(&h->solve_ms, h->ev[0], h->ev[1]));
+  const Ctl &c = *h->h_ctl;
+  st = c.status;
+  cfg->nit = c.nit;
+  cfg->ok = (st == BIEF_OK) ? 1 : 0;
+  if (relres_out) *relres_out = c.relres;
+  if (st >= 0 && ((flags & BIEF_SOLVE_INFOGR) || st > 0)) print_gracjg(st, c.nit, c.relres, c.relat);
+  if (diag && (flags & BIEF_SOLVE_MUTATE_INPUTS) && st >= 0) {
+    // SOLVE leaves B = D.B and A = D.A.D with TYPDIA from PRECD1
+    CK(cudaMemcpyAsync(b, h->d_bs, sizeof(double) * h->npoin, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(h->d_dm, h->d_dms, sizeof(double) * h->npoin, cudaMemcpyDeviceToDevice, s));
+    const int nd = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
+    if (nd)
+      CK(cudaMemcpyAsync(h->d_xm, h->d_xms, sizeof(double) * nd * h->nelem,
+                         cudaMemcpyDeviceToDevice, s));
+    CK(cudaStreamSynchronize(s));
+    h->typdia = td == DIA_I ? 'I' : (td == DIA_0 ? '0' : 'Q');
+  }
+  return st;
+}
+
+int bief_solve(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int flags,
+               double *relres_out) {
+  if (!h || !x || !b) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  const size_t nb = sizeof(double) * h->npoin;
+  CK(cudaMemcpyAsync(h->d_x, x, nb, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_b, b, nb, cudaMemcpyHostToDevice, h->stream));
+  int st = bief_solve_dev(h, h->d_x, h->d_b, cfg, flags, relres_out, h->stream);
+  if (st < 0 && st != BIEF_ERR_BREAKDOWN && st != BIEF_ERR_NAN) return st;
+  CK(cudaMemcpyAsync(x, h->d_x, nb, cudaMemcpyDeviceToHost, h->stream));
+  if (flags & BIEF_SOLVE_MUTATE_INPUTS)
+    CK(cudaMemcpyAsync(b, h->d_b, nb, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return st;
+}
+
+int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b, int precon,
+                         double inner_tol, double outer_tol, int max_outer, int max_inner,
+                         int *outer_out, int *inner_out, double *relres_out, void *stream) {
+  if (!h || !x || !b || max_inner < 1 || max_outer < 0) return BIEF_ERR_ARGS;
+  if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
+  if (h->typext != 'S') return BIEF_ERR_UNSUPPORTED;
+  if (precon == 0) precon = 1;
+  if (precon < 0 || precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 || precon % 17 == 0)
+    return BIEF_ERR_UNSUPPORTED;
+  DevGuard g(h->dev);
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
+  int td = typdia_code(h->typdia), st;
+  const double *xm = h->d_xm, *da = h->d_dm, *bw = b;
+  if (diag) {
+    if ((st = do_precd1(h, precon, x, b, h->d_bs, true, &td, s))) return st;
+    xm = h->d_xms;
+    da = h->d_dms;
+    bw = h->d_bs;
+  } else {
+    k_to_f32<<<grid_for(3 * h->nelem, h->nsm), 256, 0, s>>>(3 * h->nelem, h->d_xm, h->d_xm32);
+    h->launches++;
+  }
+  // binary32 row sums of the scaled operator (difference-form diagonal)
+  {
+    const int gn = grid_for(h->npoin, h->nsm);
+    if (td == DIA_Q)
+      k_rowsum<DIA_Q><<<gn, 256, 0, s>>>(h->npoin, h->nelem, h->d_ptr, h->d_ek, h->d_ik, xm, da,
+                                         h->d_dm32);
+    else if (td == DIA_I)
+      k_rowsum<DIA_I><<<gn, 256, 0, s>>>(h->npoin, h->nelem, h->d_ptr, h->d_ek, h->d_ik, xm, da,
+                                         h->d_dm32);
+    else
+      k_rowsum<DIA_0><<<gn, 256, 0, s>>>(h->npoin, h->nelem, h->d_ptr, h->d_ek, h->d_ik, xm, da,
+                                         h->d_dm32);
+    h->launches++;
+  }
+  MixP P;
+  P.npoin = h->npoin;
+  P.nelem = h->nelem;
+  P.max_outer = max_outer;
+  P.max_inner = max_inner;
+  P.outer_tol = outer_tol;
+  P.inner_tol = inner_tol;
+  P.ptr = h->d_ptr;
+  P.ek = h->d_ek;
+  P.ik = h->d_ik;
+  P.xm = xm;
+  P.da = da;
+  P.xm32 = h->d_xm32;
+  P.s32 = h->d_dm32;
+  P.dsc = diag ? h->d_dsc : nullptr;
+  P.x = x;
+  P.b = bw;
+  P.z = h->d_z;
+  P.ri = h->d_ri;
+  P.p0 = h->d_p0;
+  P.p1 = h->d_p1;
+  P.q = h->d_q;
+  P.part = h->d_part;
+  P.ctl = h->d_ctl;
+  P.timeout_ns = h->timeout_ns;
+  CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
+  CK(cudaEventRecord(h->ev[0], s));
+  if ((st = launch_coop(h, mixed_kernel(td), &P, s))) return st;
+  CK(cudaEventRecord(h->ev[1], s));
+  CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaEventElapsedTime(&h->solve_ms, h->ev[0], h->ev[1]));
+  const Ctl &c = *h->h_ctl;
+  if (outer_out) *outer_out = c.outer;
+  if (inner_out) *inner_out = c.nit;
+  if (relres_out) *relres_out = c.relres;
+  return c.status;
+}
+
+int bief_solve_mixed(bief_handle *h, double *x, const double *b, int precon, double inner_tol,
+                     double outer_tol, int max_outer, int max_inner, int *outer_out,
+                     int *inner_out, double *relres_out) {
+  if (!h || !x || !b) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  const size_t nb = sizeof(double) * h->npoin;
+  CK(cudaMemcpyAsync(h->d_x, x, nb, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_b, b, nb, cudaMemcpyHostToDevice, h->stream));
+  int st = bief_solve_mixed_dev(h, h->d_x, h->d_b, precon, inner_tol, outer_tol, max_outer,
+                                max_inner, outer_out, inner_out, relres_out, h->stream);
+  if (st < 0 && st != BIEF_ERR_BREAKDOWN && st != BIEF_ERR_NAN) return st;
+  CK(cudaMemcpyAsync(x, h->d_x, nb, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return st;
+}
+
+int bief_matvec_dev(bief_handle *h, const char *op, double *x, const double *y, double c,
+                    void *stream) {
+  if (!h || !x || !y) return BIEF_ERR_ARGS;
+  int opc;
+  bool trans;
+  int st = parse_op(op, &opc, &trans);
+  if (st) return st;
+  if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
+  DevGuard g(h->dev);
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  const int td = typdia_code(h->typdia);
+  const bool sym = h->typext != 'Q';
+  const size_t nb = sizeof(double) * h->npoin;
+  if (x == y) {  // the reference goes through MESH%T, so X may alias Y
+    CK(cudaMemcpyAsync(h->d_t, y, nb, cudaMemcpyDeviceToDevice, s));
+    y = h->d_t;
+  }
+  const double *xm = h->d_xm;
+  if (h->typext == '0') {
+    // no off-diagonal terms: reuse the symmetric kernel on a zero operator
+    CK(cudaMemsetAsync(h->d_xms, 0, sizeof(double) * 3 * h->nelem, s));
+    xm = h->d_xms;
+  }
+  CK(cudaEventRecord(h->ev[2], s));
+  dispatch_mv(h, td, sym, trans, xm, h->d_dm, y, x, opc, c, s);
+  h->launches++;
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[3], s));
+  return BIEF_OK;
+}
+
+int bief_matvec(bief_handle *h, const char *op, double *x, const double *y, double c) {
+  if (!h || !x || !y) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  const size_t nb = sizeof(double) * h->npoin;
+  CK(cudaMemcpyAsync(h->d_x, x, nb, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_b, y, nb, cudaMemcpyHostToDevice, h->stream));
+  int st = bief_matvec_dev(h, op, h->d_x, h->d_b, c, h->stream);
+  if (st) return st;
+  CK(cudaMemcpyAsync(x, h->d_x, nb, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  CK(cudaEventElapsedTime(&h->matvec_ms, h->ev[2], h->ev[3]));
+  return BIEF_OK;
+}
+
+int bief_assemble_wave_dev(bief_handle *h, const double *xc, const double *yc,
+                           const double *coef, void *stream) {
+  if (!h || !xc || !yc || !coef) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  int st = ensure_matrix_buffers(h);
+  if (st) return st;
+  if (!h->d_ew && (st = dalloc(&h->d_ew, 4 * (size_t)h->nelem))) return st;
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  CK(cudaMemsetAsync(h->d_err, 0, sizeof(int), s));
+  k_wave_elems<<<grid_for(h->nelem, h->nsm), 256, 0, s>>>(h->nelem, h->d_ik, xc, yc, coef,
+                                                          h->d_xm, h->d_ew, h->d_err);
+  k_wave_nodes<<<grid_for(h->npoin, h->nsm), 256, 0, s>>>(h->npoin, h->d_ptr, h->d_ek, h->nelem,
+                                                          h->d_ew, h->d_dm);
+  h->launches += 2;
+  CK(cudaGetLastError());
+  int err = 0;
+  CK(cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (err) return BIEF_ERR_BAD_MESH;
+  h->typdia = 'Q';
+  h->typext = 'S';
+  h->has_matrix = 1;
+  return BIEF_OK;
+}
+
+int bief_wave_coef_grad_dev(bief_handle *h, const double *xc, const double *yc,
+                            const double *lambda, const double *x, double *grad, void *stream) {
+  if (!h || !xc || !yc || !lambda || !x || !grad) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  k_coef_grad<<<grid_for(h->nelem, h->nsm), 256, 0, s>>>(h->nelem, h->d_ik, xc, yc, lambda, x,
+                                                         grad);
+  h->launches++;
+  CK(cudaGetLastError());
+  return BIEF_OK;
+}
+
+int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads) {
+  if (!h) return BIEF_ERR_ARGS;
+  if (nblocks) *nblocks = h->G;
+  if (nthreads) *nthreads = h->T;
+  return BIEF_OK;
+}
+
+int bief_last_timing(bief_handle *h, float *solve_ms, float *matvec_ms) {
+  if (!h) return BIEF_ERR_ARGS;
+  if (solve_ms) *solve_ms = h->solve_ms;
+  if (matvec_ms) *matvec_ms = h->matvec_ms;
+  return BIEF_OK;
+}
+
+long long bief_kernel_launches(bief_handle *h) { return h ? h->launches : -1; }
+
+}  // extern "C"

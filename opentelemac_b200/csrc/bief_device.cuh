@@ -1,0 +1,243 @@
+// bief_device.cuh -- device-side building blocks shared by the BIEF kernels:
+// rounding-explicit arithmetic, the fixed dot-product tree, the bounded grid
+// barrier of the persistent solvers, and the node-centric EBE row product.
+#pragma once
+
+#include <cuda/atomic>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bief {
+
+// ---------------------------------------------------------------------------
+// Arithmetic with explicit rounding.  The reference is compiled for x86-64
+// without fused multiply-add, so every product and sum is rounded on its own;
+// using the _rn intrinsics stops nvcc from contracting a*b+c into an FMA and
+// keeps the binary64 path bit-identical to the Fortran.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+
+// Status codes (same values as include/bief_b200.h).
+enum : int {
+  ST_OK = 0,
+  ST_BREAKDOWN = -2,
+  ST_NAN = -3,
+  ST_BAD_MESH = -4,
+  ST_TIMEOUT = -7,
+};
+
+// Diagonal kinds (TYPDIA): 'Q' any, 'I' identity, '0' zero.
+enum : int { DIA_Q = 0, DIA_I = 1, DIA_0 = 2 };
+
+// ---------------------------------------------------------------------------
+// Fixed-shape block reduction: xor-butterfly inside each warp, warp totals
+// (zero-padded to 32) through a second butterfly in warp 0.  The result is
+// valid in warp 0.  `sm` holds 32 values.  The CPU oracle restates exactly
+// this tree, so dot products are reproducible bit for bit.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T block_tree(T v, T *sm) {
+  const unsigned FULL = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = add(v, __shfl_xor_sync(FULL, v, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) sm[w] = v;
+  __syncthreads();
+  T u = T(0);
+  if (w == 0) {
+    u = lane < nw ? sm[lane] : T(0);
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) u = add(u, __shfl_xor_sync(FULL, u, o));
+  }
+  __syncthreads();
+  return u;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Control block of one persistent solve (device memory, zeroed per launch).
+struct Ctl {
+  unsigned int count;  // barrier arrivals
+  unsigned int gen;    // barrier generation
+  int status;          // final status (written by block 0) or error
+  int nit;             // iterations (CG) / total inner iterations (mixed)
+  int relat;           // 1: relative test, 0: absolute (||B||^2 < 1)
+  int outer;           // mixed: outer refinement steps
+  int pad0, pad1;
+  double red[4];       // reduction results published by the last block
+  double relres;       // SQRT(RMRM/XL) at exit
+};
+
+// Grid-wide reduction + barrier.  Each block reduces its thread partials
+// with block_tree (ND binary64 values, NF binary32 values), thread 0 stores
+// them and arrives on the counter; the last block to arrive sums the block
+// partials in block order (thread t: partials t, t+T, ...; then block_tree),
+// publishes the totals and advances the generation; the other blocks wait
+// for the generation with a bounded spin (globaltimer), after which they
+// record ST_TIMEOUT and return false instead of hanging.
+template <int ND, int NF>
+__device__ __noinline__ bool grid_reduce(Ctl *ctl, double *part, long long timeout_ns,
+                                         const double *vd, const float *vf,
+                                         double *od, float *of) {
+  __shared__ double smd[32];
+  __shared__ float smf[32];
+  __shared__ int s_last, s_err;
+  __shared__ unsigned s_gen;
+  constexpr int NV = ND + NF;
+  const int G = gridDim.x, T = blockDim.x, t = threadIdx.x;
+  double bd[ND > 0 ? ND : 1];
+  float bf[NF > 0 ? NF : 1];
+#pragma unroll
+  for (int q = 0; q < ND; ++q) bd[q] = block_tree(vd[q], smd);
+#pragma unroll
+  for (int q = 0; q < NF; ++q) bf[q] = block_tree(vf[q], smf);
+  if (t == 0) {
+#pragma unroll
+    for (int q = 0; q < ND; ++q) part[(size_t)blockIdx.x * NV + q] = bd[q];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) part[(size_t)blockIdx.x * NV + ND + q] = (double)bf[q];
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(ctl->gen), cnt(ctl->count);
+    unsigned g0 = gen.load(cuda::memory_order_relaxed);
+    unsigned a = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+    s_last = (a == (unsigned)(G - 1));
+    s_gen = g0;
+    s_err = 0;
+  }
+  __syncthreads();
+  if (s_last) {
+#pragma unroll
+    for (int q = 0; q < ND; ++q) {
+      double acc = 0.0;
+      for (int k = t; k < G; k += T) acc = add(acc, __ldcg(part + (size_t)k * NV + q));
+      double tot = block_tree(acc, smd);
+      if (t == 0) ctl->red[q] = tot;
+    }
+#pragma unroll
+    for (int q = 0; q < NF; ++q) {
+      float acc = 0.0f;
+      for (int k = t; k < G; k += T) acc = add(acc, (float)__ldcg(part + (size_t)k * NV + ND + q));
+      float tot = block_tree(acc, smf);
+      if (t == 0) ctl->red[ND + q] = (double)tot;
+    }
+    if (t == 0) {
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(ctl->gen), cnt(ctl->count);
+      cnt.store(0u, cuda::memory_order_relaxed);
+      gen.fetch_add(1u, cuda::memory_order_release);
+    }
+  } else if (t == 0) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(ctl->gen);
+    const unsigned long long t0 = global_ns();
+    unsigned ns = 32;
+    while (gen.load(cuda::memory_order_acquire) == s_gen) {
+      if ((long long)(global_ns() - t0) > timeout_ns) {
+        s_err = 1;
+        atomicExch(&ctl->status, (int)ST_TIMEOUT);
+        break;
+      }
+      __nanosleep(ns);
+      if (ns < 256) ns <<= 1;
+    }
+  }
+  __syncthreads();
+  if (s_err) return false;
+#pragma unroll
+  for (int q = 0; q < ND; ++q) od[q] = __ldcg(&ctl->red[q]);
+#pragma unroll
+  for (int q = 0; q < NF; ++q) of[q] = (float)__ldcg(&ctl->red[ND + q]);
+  if (__ldcg(&ctl->status) == (int)ST_TIMEOUT) return false;
+  return true;
+}
+
+// Plain grid barrier (no values) built on grid_reduce.
+__device__ __forceinline__ bool grid_sync(Ctl *ctl, double *part, long long timeout_ns) {
+  double dummy_in = 0.0, dummy_out;
+  return grid_reduce<1, 0>(ctl, part, timeout_ns, &dummy_in, nullptr, &dummy_out, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Node-centric EBE row product.
+//
+// MV0303 'X=AY' computes per element W1 = XA12*Y(2)+XA13*Y(3),
+// W2 = XA23*Y(3)+XA21*Y(1), W3 = XA31*Y(1)+XA32*Y(2) (mv0303.f:123-130) and
+// ASSVEC adds W(:,IDP) into X(IKLE(:,IDP)) for IDP=1,2,3 in element order
+// (assvec.f:88-93).  For node i that is the left-to-right sum
+//   diag_i + sum over (IDP,IELEM) with IKLE(IELEM,IDP)=i of W_IDP(IELEM)
+// in (IDP, IELEM) order.  The gather index lists, per node, the packed pairs
+// (IELEM<<2 | IDP-1) in exactly that order, so each thread reproduces the
+// scatter's additions for its node without atomics.
+//
+// Column of XM holding XA(k,l) (0-based local points): symmetric storage
+// keeps one column per edge (k+l-1); 'Q' storage keeps M12,M13,M23 in
+// columns 0..2 and M21,M31,M32 in 3..5 (om1111.f:43-50).
+// ---------------------------------------------------------------------------
+template <bool SYM>
+__device__ __forceinline__ int xm_col(int k, int l) {
+  return SYM ? (k + l - 1) : (k < l ? (k + l - 1) : (k + l + 2));
+}
+
+template <typename T, bool SYM, bool TRANS, class V>
+__device__ __forceinline__ T row_sum(T acc, int i, const int *__restrict__ ptr,
+                                     const int *__restrict__ ek, const int *__restrict__ ik,
+                                     const T *__restrict__ xm, int ne, V vec) {
+  const int j0 = __ldg(ptr + i), j1 = __ldg(ptr + i + 1);
+  for (int j = j0; j < j1; ++j) {
+    const int p = __ldg(ek + j);
+    const int e = p >> 2, k = p & 3;
+    const int a = (k == 2) ? 0 : k + 1;  // (k+1) mod 3
+    const int b = (k == 0) ? 2 : k - 1;  // (k+2) mod 3
+    const int va = __ldg(ik + (size_t)a * ne + e);
+    const int vb = __ldg(ik + (size_t)b * ne + e);
+    const int ca = TRANS ? xm_col<SYM>(a, k) : xm_col<SYM>(k, a);
+    const int cb = TRANS ? xm_col<SYM>(b, k) : xm_col<SYM>(k, b);
+    const T xa = __ldg(xm + (size_t)ca * ne + e);
+    const T xb = __ldg(xm + (size_t)cb * ne + e);
+    const T w = add(mul(xa, vec(va)), mul(xb, vec(vb)));
+    acc = add(acc, w);
+  }
+  return acc;
+}
+
+// Difference form of the same product for the binary32 inner operator:
+// each W term is XA(k,a) (y_a - y_i) + XA(k,b) (y_b - y_i); the diagonal part
+// is s_i y_i with s_i the row sum (see k_rowsum).
+template <typename T, class V>
+__device__ __forceinline__ T row_sum_diff(T acc, T yi, int i, const int *__restrict__ ptr,
+                                          const int *__restrict__ ek, const int *__restrict__ ik,
+                                          const T *__restrict__ xm, int ne, V vec) {
+  const int j0 = __ldg(ptr + i), j1 = __ldg(ptr + i + 1);
+  for (int j = j0; j < j1; ++j) {
+    const int p = __ldg(ek + j);
+    const int e = p >> 2, k = p & 3;
+    const int a = (k == 2) ? 0 : k + 1;
+    const int b = (k == 0) ? 2 : k - 1;
+    const int va = __ldg(ik + (size_t)a * ne + e);
+    const int vb = __ldg(ik + (size_t)b * ne + e);
+    const T xa = __ldg(xm + (size_t)(k + a - 1) * ne + e);
+    const T xb = __ldg(xm + (size_t)(k + b - 1) * ne + e);
+    const T w = add(mul(xa, sub(vec(va), yi)), mul(xb, sub(vec(vb), yi)));
+    acc = add(acc, w);
+  }
+  return acc;
+}
+
+template <int TD, typename T>
+__device__ __forceinline__ T diag_term(T yi, const T *__restrict__ da, int i) {
+  if (TD == DIA_Q) return mul(yi, da[i]);  // OV 'X=YZ' (mv0303.f:150)
+  if (TD == DIA_I) return yi;              // OV 'X=Y'  (mv0303.f:157)
+  return T(0);                             // OV 'X=C' with 0 (mv0303.f:159)
+}
+
+__device__ __forceinline__ long long blk_lo(int b, int n, int nb) {
+  return (long long)b * n / nb;
+}
+
+}  // namespace bief

@@ -1,0 +1,472 @@
+// bief_kernels.cuh -- sm_100a kernels of the BIEF EBE P1 CG path.
+//
+//  k_matvec      MATVEC 'X=..AY' / 'X=..TAY' (matvec.f:316-380 ->
+//                mv0303.f:117-630 + assvec.f:88-93), node-centric gather.
+//  k_precd1_*    PRECD1 change of variables (precd1.f:88-158, om1111.f:559-600).
+//  k_cg64        GRACJG (gracjg.F:169-420) as ONE persistent cooperative
+//                kernel: two grid reductions per iteration, fused vector
+//                updates, convergence tested on the device.
+//  k_mixed       binary32 inner CG + binary64 refinement, one persistent kernel.
+//  k_wave_*      on-device MT01AA + MT02AA + ASSVEC diagonal assembly.
+//  k_coef_grad   per-element adjoint gradient -lambda_e^T K_e x_e.
+#pragma once
+
+#include "bief_device.cuh"
+
+namespace bief {
+
+constexpr int CG_THREADS = 256;
+
+// ---------------------------------------------------------------------------
+// MATVEC
+// ---------------------------------------------------------------------------
+enum : int { OP_AY = 0, OP_XPAY, OP_MAY, OP_XMAY, OP_XPCAY, OP_CAY };
+
+template <int TD, bool SYM, bool TRANS>
+__global__ void __launch_bounds__(256) k_matvec(int npoin, int nelem, const int *__restrict__ ptr,
+                                                const int *__restrict__ ek, const int *__restrict__ ik,
+                                                const double *__restrict__ xm,
+                                                const double *__restrict__ da,
+                                                const double *__restrict__ y, double *x, int opc,
+                                                double c) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    double acc = diag_term<TD>(y[i], da, i);
+    acc = row_sum<double, SYM, TRANS>(acc, i, ptr, ek, ik, xm, nelem,
+                                      [&](int j) { return __ldg(y + j); });
+    // OS combination of MESH%T into X (matvec.f:369-380, :329-340)
+    double r;
+    switch (opc) {
+      case OP_AY: r = acc; break;
+      case OP_XPAY: r = add(x[i], acc); break;
+      case OP_MAY: r = -acc; break;
+      case OP_XMAY: r = sub(x[i], acc); break;
+      case OP_XPCAY: r = add(x[i], mul(c, acc)); break;
+      default: r = mul(c, acc); break;
+    }
+    x[i] = r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// PRECD1 change of variables, DIADON=.FALSE., PREXSM=.TRUE.
+// Node part: D = A%D; [|D|]; D = SQRT(D); X = X*D; D = 1/D guarded
+// (ovd.f:92-102: |D| > 1e-10 ? 1/D : 1.0); diagonal of D.A.D
+// (om1111.f:561-570: 'Q' -> DM*D*D, 'I' -> D*D); B = B*D.
+// ---------------------------------------------------------------------------
+__global__ void k_precd1_nodes(int npoin, int precon, int td_in, const double *__restrict__ dm,
+                               double *x, const double *b_in, double *b_out, double *dsc,
+                               double *dms) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    double d = dm[i];
+    if (precon == 5) d = fabs(d);
+    d = __dsqrt_rn(d);
+    x[i] = mul(x[i], d);
+    d = (fabs(d) > 1.0e-10) ? __ddiv_rn(1.0, d) : 1.0;
+    dsc[i] = d;
+    if (td_in == DIA_Q) {
+      dms[i] = mul(mul(dm[i], d), d);
+    } else if (td_in == DIA_I) {
+      dms[i] = mul(d, d);
+    } else {
+      dms[i] = dm[i];
+    }
+    b_out[i] = mul(b_in[i], d);
+  }
+}
+
+// Off-diagonal part of OM1111 'M=DMD' (om1111.f:589-600):
+// XM(e,1)*D(i2)*D(i1), XM(e,2)*D(i3)*D(i1), XM(e,3)*D(i3)*D(i2) (and the
+// same for columns 4..6 of 'Q' storage).  Optionally also writes the
+// binary32 copy used by the mixed-precision solver.
+__global__ void k_precd1_elems(int nelem, int ndiag, const int *__restrict__ ik,
+                               const double *__restrict__ dsc, const double *__restrict__ xm,
+                               double *xms, float *xm32) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
+    const double d1 = dsc[ik[e]], d2 = dsc[ik[(size_t)nelem + e]],
+                 d3 = dsc[ik[2 * (size_t)nelem + e]];
+    for (int c = 0; c < ndiag; ++c) {
+      const int cc = c % 3;
+      const double da = cc == 0 ? d2 : d3;
+      const double db = cc == 2 ? d2 : d1;
+      const double v = mul(mul(xm[(size_t)c * nelem + e], da), db);
+      xms[(size_t)c * nelem + e] = v;
+      if (xm32 && c < 3) xm32[(size_t)c * nelem + e] = (float)v;
+    }
+  }
+}
+
+// Row sums of the symmetric scaled operator in binary64, in ASSVEC order
+// (diagonal first, then XA(k,a)+XA(k,b) per W term), rounded to binary32:
+// the diagonal of the difference-form binary32 inner operator.
+template <int TD>
+__global__ void k_rowsum(int npoin, int nelem, const int *__restrict__ ptr,
+                         const int *__restrict__ ek, const int *__restrict__ ik,
+                         const double *__restrict__ xm, const double *__restrict__ da,
+                         float *s32) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    double s = TD == DIA_Q ? da[i] : (TD == DIA_I ? 1.0 : 0.0);
+    for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
+      const int p = ek[j], e = p >> 2, k = p & 3;
+      const int a = (k == 2) ? 0 : k + 1;
+      const int b = (k == 0) ? 2 : k - 1;
+      s = add(s, add(xm[(size_t)(k + a - 1) * nelem + e], xm[(size_t)(k + b - 1) * nelem + e]));
+    }
+    s32[i] = (float)s;
+  }
+}
+
+__global__ void k_to_f32(int n, const double *__restrict__ a, float *b) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+// ---------------------------------------------------------------------------
+// GRACJG as a persistent kernel.
+// ---------------------------------------------------------------------------
+struct CgP {
+  int npoin, nelem, nitmax;
+  double eps;
+  const int *ptr, *ek, *ik;
+  const double *xm, *da;  // working (scaled) matrix
+  const double *dsc;      // change of variables to undo (nullptr: none)
+  double *x;
+  const double *b;
+  double *r, *d0, *d1, *ad;
+  double *part;
+  Ctl *ctl;
+  long long timeout_ns;
+};
+
+template <int TD, bool SYM>
+__global__ void __launch_bounds__(CG_THREADS) k_cg64(CgP P) {
+  const int T = blockDim.x, t = threadIdx.x;
+  const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
+  const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
+  double *x = P.x, *r = P.r, *ad = P.ad;
+  const double *b = P.b, *da = P.da;
+  const bool lead = (blockIdx.x == 0 && t == 0);
+  double s, red;
+
+  auto finish = [&](int status, int m, double rmrm, double xl, int relat) {
+    if (P.dsc)  // solve.f:637-641: X = X*D
+      for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
+    if (lead) {
+      P.ctl->status = status;
+      P.ctl->nit = m;
+      P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
+      P.ctl->relat = relat;
+    }
+  };
+
+  // XL = P_DOTS(B,B) (gracjg.F:189)
+  s = 0.0;
+  for (int i = lo + t; i < hi; i += T) s = add(s, mul(b[i], b[i]));
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+  double xl = red;
+  if (__dsqrt_rn(xl) < 1.0e-15) {  // gracjg.F:194-202: X = 0
+    for (int i = lo + t; i < hi; i += T) x[i] = 0.0;
+    finish(ST_OK, 0, 0.0, 1.0, 0);
+    return;
+  }
+  int relat = 1;
+  if (xl < 1.0) { xl = 1.0; relat = 0; }  // gracjg.F:204-209
+  const double tol = mul(xl, mul(P.eps, P.eps));
+
+  // R = A X - B (gracjg.F:213-216)
+  s = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    double acc = diag_term<TD>(x[i], da, i);
+    acc = row_sum<double, SYM, false>(acc, i, P.ptr, P.ek, P.ik, P.xm, P.nelem,
+                                      [&](int j) { return x[j]; });
+    const double ri = sub(acc, b[i]);
+    r[i] = ri;
+    s = add(s, mul(ri, ri));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+  double rmrm = red, rmgm = rmrm;
+  if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
+  if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }
+
+  // D = G (= R), AD = A D, DAD, RO (gracjg.F:248-261)
+  double *cur = P.d0, *nxt = P.d1;
+  s = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    const double di = r[i];
+    cur[i] = di;
+    double acc = diag_term<TD>(di, da, i);
+    acc = row_sum<double, SYM, false>(acc, i, P.ptr, P.ek, P.ik, P.xm, P.nelem,
+                                      [&](int j) { return r[j]; });
+    ad[i] = acc;
+    s = add(s, mul(di, acc));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+  double dad = red;
+  if (!(dad > 0.0)) { finish(isnan(dad) ? ST_NAN : ST_BREAKDOWN, 0, rmrm, xl, relat); return; }
+  double ro = __ddiv_rn(rmgm, dad);
+
+  for (int m = 1;; ++m) {
+    // X = X - RO*D (gracjg.F:268 / :387) fused with R = R - RO*AD (:290)
+    // and RMRM = P_DOTS(R,R) (:295)
+    const double nro = -ro;
+    s = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      x[i] = add(x[i], mul(nro, cur[i]));
+      const double ri = add(r[i], mul(nro, ad[i]));
+      r[i] = ri;
+      s = add(s, mul(ri, ri));
+    }
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+    const double rm1gm1 = rmgm;
+    rmrm = red;
+    rmgm = rmrm;
+    if (isnan(rmrm)) { finish(ST_NAN, m, rmrm, xl, relat); return; }
+    if (rmrm <= tol) { finish(ST_OK, m, rmrm, xl, relat); return; }  // :303
+    const double beta = __ddiv_rn(rmgm, rm1gm1);                       // :357
+
+    // D = R + BETA*D (:361) computed where it is needed, AD = A D (:376),
+    // DAD = P_DOTS(D,AD) (:382).  Every thread that needs D at node j
+    // recomputes R(j)+BETA*D(j) from the previous direction, which gives
+    // the same bits as the owner's value; the owner also stores it.
+    s = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      const double di = add(r[i], mul(beta, cur[i]));
+      nxt[i] = di;
+      double acc = diag_term<TD>(di, da, i);
+      acc = row_sum<double, SYM, false>(acc, i, P.ptr, P.ek, P.ik, P.xm, P.nelem,
+                                        [&](int j) { return add(r[j], mul(beta, cur[j])); });
+      ad[i] = acc;
+      s = add(s, mul(di, acc));
+    }
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+    dad = red;
+    if (!(dad > 0.0)) { finish(isnan(dad) ? ST_NAN : ST_BREAKDOWN, m, rmrm, xl, relat); return; }
+    ro = __ddiv_rn(rmgm, dad);  // :383 (RMDM = RMGM)
+    double *tmp = cur; cur = nxt; nxt = tmp;
+
+    if (m >= P.nitmax) {  // :406 -- last X update, then stop unconverged
+      const double nr = -ro;
+      for (int i = lo + t; i < hi; i += T) x[i] = add(x[i], mul(nr, cur[i]));
+      finish(m, m, rmrm, xl, relat);
+      return;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision, one launch: a binary32 CG on the binary32 copy of the
+// scaled EBE operator (binary32 vectors, products and dot accumulation)
+// whose correction z is folded into the binary64 solution whenever the
+// recursive binary32 residual has dropped by inner_tol against the last
+// true residual (or looks converged).  Each such update recomputes the true
+// residual b - A x in binary64 with the binary64 operator, tests it against
+// outer_tol and restarts the binary32 residual from it while keeping the
+// search direction (beta from the recursive residual).
+// ---------------------------------------------------------------------------
+struct MixP {
+  int npoin, nelem, max_outer, max_inner;
+  double outer_tol, inner_tol;
+  const int *ptr, *ek, *ik;
+  const double *xm, *da;  // scaled binary64 operator
+  const float *xm32, *s32;  // binary32 off-diagonals, binary32 row sums
+  const double *dsc;
+  double *x;
+  const double *b;
+  float *z, *ri, *p0, *p1, *q;
+  double *part;
+  Ctl *ctl;
+  long long timeout_ns;
+};
+
+template <int TD>
+__global__ void __launch_bounds__(CG_THREADS) k_mixed(MixP P) {
+  const int T = blockDim.x, t = threadIdx.x;
+  const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
+  const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
+  double *x = P.x;
+  const double *b = P.b;
+  float *z = P.z, *ri = P.ri, *q = P.q;
+  const bool lead = (blockIdx.x == 0 && t == 0);
+  double s, red;
+  float sf;
+  int inner = 0, outer = 0;
+
+  auto finish = [&](int status, double rr, double xl) {
+    if (P.dsc)
+      for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
+    if (lead) {
+      P.ctl->status = status;
+      P.ctl->nit = inner;
+      P.ctl->outer = outer;
+      P.ctl->relres = __dsqrt_rn(__ddiv_rn(rr, xl));
+    }
+  };
+
+  s = 0.0;
+  for (int i = lo + t; i < hi; i += T) s = add(s, mul(b[i], b[i]));
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+  double xl = red;
+  if (__dsqrt_rn(xl) < 1.0e-15) {
+    for (int i = lo + t; i < hi; i += T) x[i] = 0.0;
+    finish(ST_OK, 0.0, 1.0);
+    return;
+  }
+  if (xl < 1.0) xl = 1.0;
+  const double otol = mul(xl, mul(P.outer_tol, P.outer_tol));
+  const float itol2 = (float)mul(P.inner_tol, P.inner_tol);
+
+  // true residual r = b - A x (binary64), r32 = (float)r; returns false on
+  // a barrier timeout.  rr and rho receive ||r||^2 and ||r32||^2.
+  double rr;
+  float rho;
+  auto true_residual = [&]() -> bool {
+    double sd = 0.0;
+    float s32 = 0.0f;
+    for (int i = lo + t; i < hi; i += T) {
+      double acc = diag_term<TD>(x[i], P.da, i);
+      acc = row_sum<double, true, false>(acc, i, P.ptr, P.ek, P.ik, P.xm, P.nelem,
+                                         [&](int j) { return x[j]; });
+      const double rv = sub(b[i], acc);
+      sd = add(sd, mul(rv, rv));
+      const float r32 = (float)rv;
+      ri[i] = r32;
+      s32 = add(s32, mul(r32, r32));
+    }
+    return grid_reduce<1, 1>(P.ctl, P.part, P.timeout_ns, &sd, &s32, &rr, &rho);
+  };
+
+  if (!true_residual()) return;
+  if (isnan(rr)) { finish(ST_NAN, rr, xl); return; }
+  if (rr <= otol) { finish(ST_OK, rr, xl); return; }
+  float rmax = rho, beta = 0.0f;
+  for (int i = lo + t; i < hi; i += T) z[i] = 0.0f;
+  float *cur = P.p0, *nxt = P.p1;
+  bool first = true;
+  for (;;) {
+    // p = r + beta p, evaluated where needed; q = A32 p; p.q
+    sf = 0.0f;
+    for (int i = lo + t; i < hi; i += T) {
+      const float pi = first ? ri[i] : add(ri[i], mul(beta, cur[i]));
+      nxt[i] = pi;
+      float acc = mul(pi, P.s32[i]);
+      if (first)
+        acc = row_sum_diff<float>(acc, pi, i, P.ptr, P.ek, P.ik, P.xm32, P.nelem,
+                                  [&](int k) { return ri[k]; });
+      else
+        acc = row_sum_diff<float>(acc, pi, i, P.ptr, P.ek, P.ik, P.xm32, P.nelem,
+                                  [&](int k) { return add(ri[k], mul(beta, cur[k])); });
+      q[i] = acc;
+      sf = add(sf, mul(pi, acc));
+    }
+    float pq;
+    if (!grid_reduce<0, 1>(P.ctl, P.part, P.timeout_ns, nullptr, &sf, nullptr, &pq)) return;
+    if (!(pq > 0.0f)) { finish(isnan(pq) ? ST_NAN : ST_BREAKDOWN, rr, xl); return; }
+    const float alpha = __fdiv_rn(rho, pq);
+    sf = 0.0f;
+    for (int i = lo + t; i < hi; i += T) {
+      z[i] = add(z[i], mul(alpha, nxt[i]));
+      const float rv = sub(ri[i], mul(alpha, q[i]));
+      ri[i] = rv;
+      sf = add(sf, mul(rv, rv));
+    }
+    float rho_new;
+    if (!grid_reduce<0, 1>(P.ctl, P.part, P.timeout_ns, nullptr, &sf, nullptr, &rho_new)) return;
+    const float rho_rec = rho_new, rho_old = rho;
+    ++inner;
+    { float *tmp = cur; cur = nxt; nxt = tmp; }
+    const bool last = inner >= P.max_inner;
+    if (last || rho_new <= mul(itol2, rmax) || (double)rho_new <= otol) {
+      // reliable update: x += z in binary64, then the true residual
+      for (int i = lo + t; i < hi; i += T) {
+        x[i] = add(x[i], (double)z[i]);
+        z[i] = 0.0f;
+      }
+      if (!grid_sync(P.ctl, P.part, P.timeout_ns)) return;
+      if (!true_residual()) return;
+      ++outer;
+      if (isnan(rr)) { finish(ST_NAN, rr, xl); return; }
+      if (rr <= otol) { finish(ST_OK, rr, xl); return; }
+      if (last || outer >= P.max_outer) { finish(inner, rr, xl); return; }
+      rho_new = rho;
+      rmax = rho;
+    }
+    beta = __fdiv_rn(rho_rec, rho_old);
+    rho = rho_new;
+    first = false;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Wave-equation operator assembly (mt01aa.f, mt02aa.f:106-149, ASSVEC
+// diagonals, OM 'M=M+N').  Element pass writes XM and the element diagonal
+// terms; node pass sums the diagonals in ASSVEC order.
+// ew layout: [0] mass diagonal (same for the three points), [1..3] diffusion
+// diagonal of points 1..3.
+// ---------------------------------------------------------------------------
+__global__ void k_wave_elems(int nelem, const int *__restrict__ ik, const double *__restrict__ xc,
+                             const double *__restrict__ yc, const double *__restrict__ coef,
+                             double *xm, double *ew, int *err) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
+    const int i1 = ik[e], i2 = ik[(size_t)nelem + e], i3 = ik[2 * (size_t)nelem + e];
+    const double x1 = xc[i1], y1 = yc[i1];
+    const double X2 = sub(xc[i2], x1), X3 = sub(xc[i3], x1);  // inbief.f:385-391
+    const double Y2 = sub(yc[i2], y1), Y3 = sub(yc[i3], y1);
+    const double surf = mul(0.5, sub(mul(X2, Y3), mul(X3, Y2)));  // surv11.f:63
+    if (sub(mul(X2, Y3), mul(Y2, X3)) < 1.0e-20) atomicExch(err, 1);  // geoelt.f:82
+    // MT01AA, XMUL = 1
+    const double det = mul(surf, __ddiv_rn(1.0, 12.0));
+    // MT02AA, P0 isotropic, XMUL = 1, U = coef
+    const double s2d = __ddiv_rn(mul(1.0, 0.25), surf);
+    const double visc1 = mul(coef[e], s2d);
+    const double bpe = mul(visc1, add(mul(Y3, Y3), mul(X3, X3)));
+    const double cpf = mul(visc1, add(mul(Y2, Y3), mul(X2, X3)));
+    const double apd = mul(visc1, add(mul(Y2, Y2), mul(X2, X2)));
+    // OM 'M=M+N': XM(mass) + XM(diffusion)
+    xm[e] = add(det, sub(cpf, bpe));
+    xm[(size_t)nelem + e] = add(det, sub(cpf, apd));
+    xm[2 * (size_t)nelem + e] = add(det, -cpf);
+    ew[e] = add(det, det);
+    ew[(size_t)nelem + e] = sub(add(apd, bpe), mul(2.0, cpf));
+    ew[2 * (size_t)nelem + e] = bpe;
+    ew[3 * (size_t)nelem + e] = apd;
+  }
+}
+
+__global__ void k_wave_nodes(int npoin, const int *__restrict__ ptr, const int *__restrict__ ek,
+                             int nelem, const double *__restrict__ ew, double *dm) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    double sm = 0.0, sd = 0.0;
+    for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
+      const int p = ek[j], e = p >> 2, k = p & 3;
+      sm = add(sm, ew[e]);
+      sd = add(sd, ew[(size_t)(1 + k) * nelem + e]);
+    }
+    dm[i] = add(sm, sd);
+  }
+}
+
+// Per-element gradient g_e = -lambda_e^T K_e x_e with K_e the unit-
+// coefficient MT02AA element matrix (rows sum to zero, so
+// lambda^T K x = -sum_{k<l} K_kl (lambda_k - lambda_l)(x_k - x_l)).
+__global__ void k_coef_grad(int nelem, const int *__restrict__ ik, const double *__restrict__ xc,
+                            const double *__restrict__ yc, const double *__restrict__ lam,
+                            const double *__restrict__ xs, double *grad) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
+    const int i1 = ik[e], i2 = ik[(size_t)nelem + e], i3 = ik[2 * (size_t)nelem + e];
+    const double x1 = xc[i1], y1 = yc[i1];
+    const double X2 = xc[i2] - x1, X3 = xc[i3] - x1;
+    const double Y2 = yc[i2] - y1, Y3 = yc[i3] - y1;
+    const double surf = 0.5 * (X2 * Y3 - X3 * Y2);
+    const double s2d = 0.25 / surf;
+    const double bpe = s2d * (Y3 * Y3 + X3 * X3);
+    const double cpf = s2d * (Y2 * Y3 + X2 * X3);
+    const double apd = s2d * (Y2 * Y2 + X2 * X2);
+    const double k12 = cpf - bpe, k13 = cpf - apd, k23 = -cpf;
+    const double l1 = lam[i1], l2 = lam[i2], l3 = lam[i3];
+    const double u1 = xs[i1], u2 = xs[i2], u3 = xs[i3];
+    const double lkx = -(k12 * (l1 - l2) * (u1 - u2) + k13 * (l1 - l3) * (u1 - u3) +
+                         k23 * (l2 - l3) * (u2 - u3));
+    grad[e] = -lkx;
+  }
+}
+
+}  // namespace bief

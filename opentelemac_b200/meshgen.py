@@ -1,0 +1,131 @@
+"""Synthetic P1 triangle meshes and wave-equation coefficients.
+
+These generate the inputs the solver is measured on: an n x n node grid on
+the unit square, each quad split along one diagonal, interior nodes
+jittered, and a per-element depth field h_e.  The wave-equation operator is
+A = M + dt*g*h_e*K_e (mass matrix plus depth-weighted stiffness), assembled
+by the library's on-device assembly (bief_assemble_wave_dev).
+
+Node numbering is row-major (node (i, j) -> j*n + i, i along x); elements
+are numbered quad by quad, two triangles per quad, both counter-clockwise.
+Connectivity is returned 0-based with shape (nelem, 3); the Fortran-order
+1-based IKLE(NELMAX,3) the C ABI takes is `ikle_fortran(ikle0)`.
+"""
+import numpy as np
+
+DT = 1.0
+GRAV = 9.81
+
+
+def square_mesh(n, seed=12345, jitter=0.2):
+    """n x n nodes on [0,1]^2; interior nodes moved by U(-jitter, jitter)*dx
+    in x and y (one seeded generator, x then y draws).  Returns
+    (x, y, ikle0) with ikle0 int32 (nelem, 3)."""
+    if n < 2:
+        raise ValueError("n >= 2 required")
+    dx = 1.0 / (n - 1)
+    ii, jj = np.meshgrid(np.arange(n), np.arange(n), indexing="xy")
+    x = (ii * dx).astype(np.float64).ravel()
+    y = (jj * dx).astype(np.float64).ravel()
+    interior = ((ii > 0) & (ii < n - 1) & (jj > 0) & (jj < n - 1)).ravel()
+    rng = np.random.default_rng(seed)
+    k = int(interior.sum())
+    if k and jitter:
+        jx = rng.uniform(-jitter, jitter, size=k) * dx
+        jy = rng.uniform(-jitter, jitter, size=k) * dx
+        x[interior] += jx
+        y[interior] += jy
+    qi, qj = np.meshgrid(np.arange(n - 1), np.arange(n - 1), indexing="xy")
+    a = (qj * n + qi).ravel()           # (i, j)
+    b = a + 1                           # (i+1, j)
+    c = a + n + 1                       # (i+1, j+1)
+    d = a + n                           # (i, j+1)
+    t1 = np.stack([a, b, c], axis=1)
+    t2 = np.stack([a, c, d], axis=1)
+    ikle0 = np.empty((2 * a.size, 3), dtype=np.int32)
+    ikle0[0::2] = t1
+    ikle0[1::2] = t2
+    return x, y, ikle0
+
+
+def centroids(x, y, ikle0):
+    return x[ikle0].mean(axis=1), y[ikle0].mean(axis=1)
+
+
+def depth_smooth(x, y, ikle0):
+    """h_e = 5 + 4 sin(2 pi x_c) cos(2 pi y_c) at the element centroid."""
+    xc, yc = centroids(x, y, ikle0)
+    return 5.0 + 4.0 * np.sin(2.0 * np.pi * xc) * np.cos(2.0 * np.pi * yc)
+
+
+def element_neighbours(ikle0):
+    """Edge neighbours of each element, -1 where none: (nelem, 3)."""
+    ne = ikle0.shape[0]
+    edges = np.concatenate([ikle0[:, [0, 1]], ikle0[:, [1, 2]], ikle0[:, [2, 0]]])
+    edges.sort(axis=1)
+    owner = np.tile(np.arange(ne), 3)
+    key = edges[:, 0].astype(np.int64) * (int(ikle0.max()) + 1) + edges[:, 1]
+    order = np.argsort(key, kind="stable")
+    ks = key[order]
+    nb = -np.ones((ne, 3), dtype=np.int64)
+    slot = np.repeat(np.arange(3), ne)
+    same = ks[1:] == ks[:-1]
+    i0, i1 = order[:-1][same], order[1:][same]
+    nb[owner[i0], slot[i0]] = owner[i1]
+    nb[owner[i1], slot[i1]] = owner[i0]
+    return nb
+
+
+def depth_loguniform(ikle0, seed=4242, lo=0.5, hi=500.0, passes=3):
+    """h_e log-uniform in [lo, hi] (seeded), then `passes` rounds of
+    arithmetic averaging of each element with its edge neighbours."""
+    rng = np.random.default_rng(seed)
+    h = np.exp(rng.uniform(np.log(lo), np.log(hi), size=ikle0.shape[0]))
+    nb = element_neighbours(ikle0)
+    valid = nb >= 0
+    cnt = 1.0 + valid.sum(axis=1)
+    for _ in range(passes):
+        s = h.copy()
+        for k in range(3):
+            m = valid[:, k]
+            s[m] += h[nb[m, k]]
+        h = s / cnt
+    return h
+
+
+def wave_coef(h, dt=DT, g=GRAV):
+    """Per-element diffusion coefficient dt*g*h_e of A = M + dt*g*h_e*K_e."""
+    return (dt * g) * np.asarray(h, dtype=np.float64)
+
+
+def random_solution(npoin, seed=777):
+    return np.random.default_rng(seed).uniform(-1.0, 1.0, size=npoin)
+
+
+def ikle_fortran(ikle0, nelmax=None):
+    """0-based (nelem, 3) -> Fortran IKLE(NELMAX,3): column-major, 1-based,
+    as a flat int32 array of length 3*NELMAX."""
+    ne = ikle0.shape[0]
+    nelmax = ne if nelmax is None else nelmax
+    out = np.zeros((3, nelmax), dtype=np.int32)
+    out[:, :ne] = ikle0.T + 1
+    return out.ravel()
+
+
+def shuffled(x, y, ikle0, seed=99):
+    """The same mesh with nodes and elements renumbered at random (and each
+    element's vertices rotated), to exercise unstructured numbering."""
+    rng = np.random.default_rng(seed)
+    n = x.size
+    perm = rng.permutation(n)          # new index -> old node
+    inv = np.empty(n, dtype=np.int64)
+    inv[perm] = np.arange(n)
+    eperm = rng.permutation(ikle0.shape[0])
+    ik = inv[ikle0[eperm]]
+    rot = rng.integers(0, 3, size=ik.shape[0])
+    ik = np.stack([ik[np.arange(ik.shape[0]), (rot + s) % 3] for s in range(3)], axis=1)
+    return x[perm], y[perm], ik.astype(np.int32), perm, eperm
+
+
+def mesh_size_for_npoin(npoin):
+    return max(2, int(round(np.sqrt(npoin))))

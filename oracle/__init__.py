@@ -1,0 +1,167 @@
+"""CPU oracle for the BIEF EBE P1 CG path -- TEST INFRASTRUCTURE ONLY.
+
+A plain-C restatement (bief_oracle.c) of the reference Fortran routines
+SOLVE/PRECD1/GRACJG/MATVEC/MV0303/ASSVEC/DOT and of the element matrices
+MT01AA/MT02AA, loaded with ctypes.  Only the tests, the smoke check and the
+benchmark's CPU-baseline leg use it; the product library never does.
+
+Parity unpinned: the reference cannot be compiled here (Fortran, no
+compiler) and ships no solver-level golden vectors; the restatement is
+cross-checked against dense numpy / scipy computations instead.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libbief_oracle.so")
+
+DOT_SEQUENTIAL = 0
+DOT_BLOCKED = 1
+
+_lib = None
+
+
+def build(force=False):
+    src = os.path.join(HERE, "bief_oracle.c")
+    if force or not os.path.exists(LIB) or os.path.getmtime(src) > os.path.getmtime(LIB):
+        subprocess.run(["make", "-s", "-B" if force else "-s", "-C", HERE], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        P = ctypes.POINTER
+        d, i, c = ctypes.c_double, ctypes.c_int, ctypes.c_char
+        pd, pi = P(d), P(i)
+        L.orc_wave_matrix.argtypes = [i, i, pd, pd, pi, pi, pi, pd, pd, pd]
+        L.orc_wave_matrix_parts.argtypes = [i, i, pd, pd, pi, pi, pi, pd]
+        L.orc_matvec.argtypes = [ctypes.c_char_p, i, i, pi, pi, pi, pd, pd, c, pd, i, c, pd,
+                                 d, pd, pd]
+        L.orc_dot.argtypes = [i, pd, pd]
+        L.orc_dot.restype = d
+        L.orc_dot_blocked.argtypes = [i, pd, pd, i, i]
+        L.orc_dot_blocked.restype = d
+        L.orc_precd1.argtypes = [i, i, pi, pi, pi, i, pd, pd, P(c), pd, i, c, pd, pd]
+        L.orc_solve.argtypes = [i, i, pi, pi, pi, pd, pd, pd, P(c), pd, i, c, i, i, i, d, i, i,
+                                i, pi, pd, pi]
+        L.orc_solve_mixed.argtypes = [i, i, pi, pi, pi, pd, pd, pd, c, pd, c, i, d, d, i, i, i,
+                                      i, pi, pi, pd]
+        _lib = L
+    return _lib
+
+
+def _pd(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _pi(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _cols(ikle0):
+    """0-based IKLE (nelem, 3) -> three contiguous int32 columns."""
+    ik = np.ascontiguousarray(np.asarray(ikle0, dtype=np.int32).T)
+    return ik, ik[0], ik[1], ik[2]
+
+
+def wave_matrix(x, y, ikle0, coef):
+    """A = M + coef_e K_e as PROPAG builds AM1 (mass MT01AA + P0 diffusion
+    MT02AA, diagonals by ASSVEC).  Returns dm (npoin,), xm (3, nelem)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    coef = np.ascontiguousarray(coef, dtype=np.float64)
+    ik, a, b, c = _cols(ikle0)
+    n, ne = x.size, ik.shape[1]
+    dm = np.empty(n)
+    xm = np.empty((3, ne))
+    st = lib().orc_wave_matrix(n, ne, _pd(x), _pd(y), _pi(a), _pi(b), _pi(c), _pd(coef),
+                               _pd(dm), _pd(xm))
+    if st:
+        raise ValueError("orc_wave_matrix status %d" % st)
+    return dm, xm
+
+
+def unit_stiffness(x, y, ikle0):
+    """Off-diagonal terms (3, nelem) of the unit-coefficient MT02AA matrix."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    ik, a, b, c = _cols(ikle0)
+    kxm = np.empty((3, ik.shape[1]))
+    st = lib().orc_wave_matrix_parts(x.size, ik.shape[1], _pd(x), _pd(y), _pi(a), _pi(b),
+                                     _pi(c), _pd(kxm))
+    if st:
+        raise ValueError("orc_wave_matrix_parts status %d" % st)
+    return kxm
+
+
+def matvec(op, ikle0, dm, typdia, xm, typext, y, c=0.0, x=None):
+    """MATVEC(OP,X,A,Y,C): returns the new X (a copy)."""
+    ik, a, b, cc = _cols(ikle0)
+    n, ne = np.asarray(y).size, ik.shape[1]
+    xm = np.ascontiguousarray(xm, dtype=np.float64).reshape(-1, ne)
+    out = np.zeros(n) if x is None else np.array(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    t = np.empty(n)
+    w = np.empty(3 * ne + 1)
+    st = lib().orc_matvec(op.encode(), n, ne, _pi(a), _pi(b), _pi(cc), _pd(out), _pd(dm),
+                          typdia.encode(), _pd(xm), ne, typext.encode(), _pd(y), c, _pd(t), _pd(w))
+    if st:
+        raise ValueError("orc_matvec status %d" % st)
+    return out
+
+
+def dot(x, y, mode=DOT_SEQUENTIAL, nblocks=1, nthreads=256):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    if mode == DOT_BLOCKED:
+        return lib().orc_dot_blocked(x.size, _pd(x), _pd(y), nblocks, nthreads)
+    return lib().orc_dot(x.size, _pd(x), _pd(y))
+
+
+def solve(ikle0, dm, typdia, xm, typext, b, x0=None, precon=2, nitmax=100000, eps=1e-8,
+          slv=1, dot_mode=DOT_SEQUENTIAL, nblocks=1, nthreads=256):
+    """SOLVE(X,A,B) with SLV=1.  Works on copies; returns a dict with x, the
+    mutated b/dm/xm/typdia (as the reference leaves them), status, nit,
+    relres, relat."""
+    ik, a, bb, c = _cols(ikle0)
+    n, ne = np.asarray(b).size, ik.shape[1]
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    b = np.array(b, dtype=np.float64)
+    dm = np.array(dm, dtype=np.float64)
+    xm = np.array(xm, dtype=np.float64).reshape(-1, ne).copy()
+    td = ctypes.c_char(typdia.encode())
+    nit, relat = ctypes.c_int(0), ctypes.c_int(0)
+    relres = ctypes.c_double(0.0)
+    st = lib().orc_solve(n, ne, _pi(a), _pi(bb), _pi(c), _pd(x), _pd(b), _pd(dm),
+                         ctypes.byref(td), _pd(xm), ne, typext.encode(), slv, precon, nitmax,
+                         eps, dot_mode, nblocks, nthreads, ctypes.byref(nit),
+                         ctypes.byref(relres), ctypes.byref(relat))
+    return dict(x=x, b=b, dm=dm, xm=xm, typdia=td.value.decode(), status=st, nit=nit.value,
+                relres=relres.value, relat=relat.value)
+
+
+def solve_mixed(ikle0, dm, typdia, xm, b, x0=None, precon=2, inner_tol=1e-4, outer_tol=1e-8,
+                max_outer=50, max_inner=100000, nblocks=1, nthreads=256):
+    """Mixed-precision solve (binary32 inner CG, binary64 refinement) in the
+    device kernels' exact operation order."""
+    ik, a, bb, c = _cols(ikle0)
+    n, ne = np.asarray(b).size, ik.shape[1]
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    xm = np.ascontiguousarray(xm, dtype=np.float64).reshape(3, ne)
+    outer, inner = ctypes.c_int(0), ctypes.c_int(0)
+    relres = ctypes.c_double(0.0)
+    st = lib().orc_solve_mixed(n, ne, _pi(a), _pi(bb), _pi(c), _pd(x), _pd(b), _pd(dm),
+                               typdia.encode(), _pd(xm), b"S", precon, inner_tol, outer_tol,
+                               max_outer, max_inner, nblocks, nthreads, ctypes.byref(outer),
+                               ctypes.byref(inner), ctypes.byref(relres))
+    return dict(x=x, status=st, outer=outer.value, inner=inner.value, relres=relres.value)

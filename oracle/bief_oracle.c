@@ -1,0 +1,722 @@
+/*
+ * bief_oracle.c -- CPU restatement of BIEF's EBE P1 CG path.  TEST ORACLE
+ * ONLY (see bief_oracle.h): loaded by the tests, the smoke check and the
+ * benchmark's CPU-baseline leg, never by the product library.
+ *
+ * Parity unpinned: the Fortran reference cannot be compiled here and ships
+ * no solver-level golden vectors; see tests/test_oracle.py for the
+ * independent dense/scipy cross-checks that stand in for a pin.
+ *
+ * Every routine names the reference lines it restates (paths relative to
+ * the TELEMAC-MASCARET source tree).  Loop orders and operand orders are
+ * kept as in the Fortran so that the binary64 results are the same bits an
+ * x86-64 build of the reference produces (no FMA contraction).
+ */
+#include "bief_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------ */
+/* mesh geometry                                                        */
+/* ------------------------------------------------------------------ */
+
+/* inbief.f:369-391 -- XEL/YEL relative to the element's first node
+ * (OV_2 'X=X-Y   '), surv11.f:56-64 -- SURFAC = 0.5*(X2*Y3-X3*Y2),
+ * geoelt.f:73-84 -- a determinant below 1e-20 is a fatal mesh error. */
+int orc_geometry(int nelem, const double *x, const double *y,
+                 const int *ik0, const int *ik1, const int *ik2,
+                 double *xel2, double *xel3, double *yel2, double *yel3,
+                 double *surfac)
+{
+    for (int e = 0; e < nelem; ++e) {
+        double x1 = x[ik0[e]], y1 = y[ik0[e]];
+        double X2 = x[ik1[e]] - x1;
+        double X3 = x[ik2[e]] - x1;
+        double Y2 = y[ik1[e]] - y1;
+        double Y3 = y[ik2[e]] - y1;
+        xel2[e] = X2; xel3[e] = X3; yel2[e] = Y2; yel3[e] = Y3;
+        surfac[e] = 0.5 * (X2 * Y3 - X3 * Y2);
+        double det = X2 * Y3 - Y2 * X3; /* geoelt.f:80 T12*T23-T22*T13 */
+        if (det < 1.0e-20) return ORC_ERR_BAD_MESH;
+    }
+    return ORC_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* element matrices                                                     */
+/* ------------------------------------------------------------------ */
+
+/* mt01aa.f:82-103 -- P1 mass matrix: off-diagonals S/12*XMUL, diagonal
+ * twice that (DET + DET). */
+void orc_mt01aa(int nelem, double xmul, const double *surfac,
+                double *a11, double *a12, double *a13,
+                double *a22, double *a23, double *a33)
+{
+    double sur12 = xmul / 12.0;
+    for (int e = 0; e < nelem; ++e) {
+        double det = surfac[e] * sur12;
+        a12[e] = det; a13[e] = det; a23[e] = det;
+        a11[e] = det + det; a22[e] = det + det; a33[e] = det + det;
+    }
+}
+
+/* mt02aa.f:106-149 -- P1 diffusion matrix with a P0 (per-element)
+ * isotropic coefficient U (IELMNU=10, ISO=1). */
+void orc_mt02aa_p0(int nelem, double xmul, const double *u,
+                   const double *xel2, const double *xel3,
+                   const double *yel2, const double *yel3,
+                   const double *surfac,
+                   double *a11, double *a12, double *a13,
+                   double *a22, double *a23, double *a33)
+{
+    for (int e = 0; e < nelem; ++e) {
+        double X2 = xel2[e], X3 = xel3[e], Y2 = yel2[e], Y3 = yel3[e];
+        double s2d = xmul * 0.25 / surfac[e];
+        double visc1 = u[e] * s2d;
+        double bpe = visc1 * (Y3 * Y3 + X3 * X3);
+        double cpf = visc1 * (Y2 * Y3 + X2 * X3);
+        double apd = visc1 * (Y2 * Y2 + X2 * X2);
+        a11[e] = apd + bpe - 2.0 * cpf;
+        a22[e] = bpe;
+        a33[e] = apd;
+        a12[e] = cpf - bpe;
+        a13[e] = cpf - apd;
+        a23[e] = -cpf;
+    }
+}
+
+/* assvec.f:80-93 + assve1.f:101 (MODASS=1, LV=1, no mask): X(IKLE(E,IDP))
+ * += W(E,IDP), local point IDP outer, element inner. */
+void orc_assvec(double *x, int npoin, int nelem,
+                const int *ik0, const int *ik1, const int *ik2,
+                const double *w1, const double *w2, const double *w3,
+                int init)
+{
+    if (init) for (int i = 0; i < npoin; ++i) x[i] = 0.0;
+    const int *ik[3] = {ik0, ik1, ik2};
+    const double *w[3] = {w1, w2, w3};
+    for (int idp = 0; idp < 3; ++idp)
+        for (int e = 0; e < nelem; ++e)
+            x[ik[idp][e]] = x[ik[idp][e]] + w[idp][e];
+}
+
+/* The wave-equation operator A = M + coef_e * K_e built the way PROPAG
+ * builds AM1: MATRIX('M=N', mass) then MATRIX('M=M+N', diffusion)
+ * (propag.F:661-677,1407).  Each MATRIX call assembles its own diagonal
+ * with ASSVEC (matrix.f:218-227) and OM1111 'M=M+N' adds diagonals and
+ * off-diagonals with OV 'X=X+Y' (om1111.f:299-312).  The mass term uses
+ * XMUL=1; the diffusion term uses XMUL=1 and U(e)=coef[e].
+ * Output: dm[npoin], xm[3*nelem] (columns M12, M13, M23). */
+int orc_wave_matrix(int npoin, int nelem, const double *x, const double *y,
+                    const int *ik0, const int *ik1, const int *ik2,
+                    const double *coef, double *dm, double *xm)
+{
+    double *g = (double *)malloc(sizeof(double) * 5 * (size_t)nelem);
+    double *a = (double *)malloc(sizeof(double) * 6 * (size_t)nelem);
+    double *dn = (double *)malloc(sizeof(double) * (size_t)npoin);
+    if (!g || !a || !dn) { free(g); free(a); free(dn); return ORC_ERR_ARGS; }
+    double *xel2 = g, *xel3 = g + nelem, *yel2 = g + 2 * (size_t)nelem,
+           *yel3 = g + 3 * (size_t)nelem, *surf = g + 4 * (size_t)nelem;
+    int st = orc_geometry(nelem, x, y, ik0, ik1, ik2, xel2, xel3, yel2, yel3,
+                          surf);
+    if (st) { free(g); free(a); free(dn); return st; }
+    double *a11 = a, *a12 = a + nelem, *a13 = a + 2 * (size_t)nelem,
+           *a22 = a + 3 * (size_t)nelem, *a23 = a + 4 * (size_t)nelem,
+           *a33 = a + 5 * (size_t)nelem;
+    /* mass: M=N */
+    orc_mt01aa(nelem, 1.0, surf, a11, a12, a13, a22, a23, a33);
+    orc_assvec(dm, npoin, nelem, ik0, ik1, ik2, a11, a22, a33, 1);
+    for (int e = 0; e < nelem; ++e) {
+        xm[e] = a12[e];
+        xm[nelem + e] = a13[e];
+        xm[2 * (size_t)nelem + e] = a23[e];
+    }
+    /* diffusion: M=M+N */
+    orc_mt02aa_p0(nelem, 1.0, coef, xel2, xel3, yel2, yel3, surf,
+                  a11, a12, a13, a22, a23, a33);
+    orc_assvec(dn, npoin, nelem, ik0, ik1, ik2, a11, a22, a33, 1);
+    for (int i = 0; i < npoin; ++i) dm[i] = dm[i] + dn[i];
+    for (int e = 0; e < nelem; ++e) {
+        xm[e] = xm[e] + a12[e];
+        xm[nelem + e] = xm[nelem + e] + a13[e];
+        xm[2 * (size_t)nelem + e] = xm[2 * (size_t)nelem + e] + a23[e];
+    }
+    free(g); free(a); free(dn);
+    return ORC_OK;
+}
+
+/* Off-diagonal terms of the unit-coefficient diffusion matrix K_e
+ * (mt02aa.f:106-149 with XMUL=1, U=1): kxm[3*nelem] = K12, K13, K23.
+ * Used by the adjoint gradient checks. */
+int orc_wave_matrix_parts(int npoin, int nelem, const double *x, const double *y,
+                          const int *ik0, const int *ik1, const int *ik2,
+                          double *kxm)
+{
+    (void)npoin;
+    double *g = (double *)malloc(sizeof(double) * 5 * (size_t)nelem);
+    double *a = (double *)malloc(sizeof(double) * 4 * (size_t)nelem);
+    double *one = (double *)malloc(sizeof(double) * (size_t)nelem);
+    if (!g || !a || !one) { free(g); free(a); free(one); return ORC_ERR_ARGS; }
+    for (int e = 0; e < nelem; ++e) one[e] = 1.0;
+    double *xel2 = g, *xel3 = g + nelem, *yel2 = g + 2 * (size_t)nelem,
+           *yel3 = g + 3 * (size_t)nelem, *surf = g + 4 * (size_t)nelem;
+    int st = orc_geometry(nelem, x, y, ik0, ik1, ik2, xel2, xel3, yel2, yel3,
+                          surf);
+    if (st == ORC_OK)
+        orc_mt02aa_p0(nelem, 1.0, one, xel2, xel3, yel2, yel3, surf,
+                      a, kxm, kxm + nelem, a + nelem, kxm + 2 * (size_t)nelem,
+                      a + 2 * (size_t)nelem);
+    free(g); free(a); free(one);
+    return st;
+}
+
+/* ------------------------------------------------------------------ */
+/* matrix-vector product                                                */
+/* ------------------------------------------------------------------ */
+
+/* MATVEC 'X=...AY' for an EBE P1-P1 matrix: MATVCT selects MV0303 with
+ * the AAS/AAQ column maps (matvct.f:152-170,255-306), MV0303 'X=AY' or
+ * 'X=TAY' fills W1..W3 and the diagonal part (mv0303.f:117-165,405-456),
+ * ASSVEC adds W into MESH%T (matvct.f:550-560), and MATVEC combines T into
+ * X with OS (matvec.f:316-380).  t[npoin] and w[3*nelem] are work arrays
+ * (MESH%T and MESH%W). */
+int orc_matvec(const char *op, int npoin, int nelem,
+               const int *ik0, const int *ik1, const int *ik2,
+               double *x, const double *da, char typdia,
+               const double *xm, int ld, char typext,
+               const double *y, double c, double *t, double *w)
+{
+    int trans = (strstr(op, "TAY") != NULL);
+    const double *xa12, *xa13, *xa23, *xa21, *xa31, *xa32;
+    if (typext == 'S') {
+        xa12 = xm; xa13 = xm + ld; xa23 = xm + 2 * (size_t)ld;
+        xa21 = xa12; xa31 = xa13; xa32 = xa23;
+    } else if (typext == 'Q') {
+        xa12 = xm; xa13 = xm + ld; xa23 = xm + 2 * (size_t)ld;
+        xa21 = xm + 3 * (size_t)ld; xa31 = xm + 4 * (size_t)ld;
+        xa32 = xm + 5 * (size_t)ld;
+    } else if (typext == '0') {
+        xa12 = xa13 = xa23 = xa21 = xa31 = xa32 = NULL;
+    } else {
+        return ORC_ERR_ARGS;
+    }
+    double *w1 = w, *w2 = w + nelem, *w3 = w + 2 * (size_t)nelem;
+    if (xa12 == NULL) {
+        for (int e = 0; e < nelem; ++e) w1[e] = w2[e] = w3[e] = 0.0;
+    } else if (!trans) {
+        for (int e = 0; e < nelem; ++e) {
+            w1[e] = xa12[e] * y[ik1[e]] + xa13[e] * y[ik2[e]];
+            w2[e] = xa23[e] * y[ik2[e]] + xa21[e] * y[ik0[e]];
+            w3[e] = xa31[e] * y[ik0[e]] + xa32[e] * y[ik1[e]];
+        }
+    } else {
+        for (int e = 0; e < nelem; ++e) {
+            w1[e] = xa21[e] * y[ik1[e]] + xa31[e] * y[ik2[e]];
+            w2[e] = xa12[e] * y[ik0[e]] + xa32[e] * y[ik2[e]];
+            w3[e] = xa13[e] * y[ik0[e]] + xa23[e] * y[ik1[e]];
+        }
+    }
+    if (typdia == 'Q') {
+        for (int i = 0; i < npoin; ++i) t[i] = y[i] * da[i];
+    } else if (typdia == 'I') {
+        for (int i = 0; i < npoin; ++i) t[i] = y[i];
+    } else if (typdia == '0') {
+        for (int i = 0; i < npoin; ++i) t[i] = 0.0;
+    } else {
+        return ORC_ERR_ARGS;
+    }
+    orc_assvec(t, npoin, nelem, ik0, ik1, ik2, w1, w2, w3, 0);
+
+    const char *tail = op + 2; /* matvec.f compares OP(3:8) */
+    if (!trans) {
+        if (!strncmp(tail, "AY", 2) && (tail[2] == ' ' || tail[2] == 0)) {
+            for (int i = 0; i < npoin; ++i) x[i] = t[i];
+        } else if (!strncmp(tail, "X+AY", 4)) {
+            for (int i = 0; i < npoin; ++i) x[i] = x[i] + t[i];
+        } else if (!strncmp(tail, "-AY", 3)) {
+            for (int i = 0; i < npoin; ++i) x[i] = -t[i];
+        } else if (!strncmp(tail, "X-AY", 4)) {
+            for (int i = 0; i < npoin; ++i) x[i] = x[i] - t[i];
+        } else if (!strncmp(tail, "X+CAY", 5)) {
+            for (int i = 0; i < npoin; ++i) x[i] = x[i] + c * t[i];
+        } else if (!strncmp(tail, "CAY", 3)) {
+            for (int i = 0; i < npoin; ++i) x[i] = c * t[i];
+        } else {
+            return ORC_ERR_ARGS;
+        }
+    } else {
+        if (!strncmp(tail, "TAY", 3)) {
+            for (int i = 0; i < npoin; ++i) x[i] = t[i];
+        } else if (!strncmp(tail, "-TAY", 4)) {
+            for (int i = 0; i < npoin; ++i) x[i] = -t[i];
+        } else if (!strncmp(tail, "X+TAY", 5)) {
+            for (int i = 0; i < npoin; ++i) x[i] = x[i] + t[i];
+        } else if (!strncmp(tail, "X-TAY", 5)) {
+            for (int i = 0; i < npoin; ++i) x[i] = x[i] - t[i];
+        } else if (!strncmp(tail, "X+CTAY", 6)) {
+            for (int i = 0; i < npoin; ++i) x[i] = x[i] + c * t[i];
+        } else {
+            return ORC_ERR_ARGS;
+        }
+    }
+    return ORC_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* dot products                                                         */
+/* ------------------------------------------------------------------ */
+
+/* dot.f:50-54 -- sequential left-to-right sum (P_DOTS with NCSIZE<=1,
+ * p_dots.f:146-149). */
+double orc_dot(int n, const double *x, const double *y)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s = s + x[i] * y[i];
+    return s;
+}
+
+/* The device kernels' fixed summation tree for a block of `nt` thread
+ * partials: a xor-butterfly inside each 32-lane warp (offsets 16..1),
+ * then the warp totals (zero-padded to 32) through one more butterfly. */
+static double tree64(const double *v, int nt)
+{
+    double lanes[32], wsum[32];
+    int nw = nt / 32;
+    for (int w = 0; w < 32; ++w) wsum[w] = 0.0;
+    for (int w = 0; w < nw; ++w) {
+        for (int l = 0; l < 32; ++l) lanes[l] = v[w * 32 + l];
+        for (int o = 16; o >= 1; o >>= 1) {
+            double nxt[32];
+            for (int l = 0; l < 32; ++l) nxt[l] = lanes[l] + lanes[l ^ o];
+            memcpy(lanes, nxt, sizeof(lanes));
+        }
+        wsum[w] = lanes[0];
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        double nxt[32];
+        for (int l = 0; l < 32; ++l) nxt[l] = wsum[l] + wsum[l ^ o];
+        memcpy(wsum, nxt, sizeof(wsum));
+    }
+    return wsum[0];
+}
+
+static float tree32(const float *v, int nt)
+{
+    float lanes[32], wsum[32];
+    int nw = nt / 32;
+    for (int w = 0; w < 32; ++w) wsum[w] = 0.0f;
+    for (int w = 0; w < nw; ++w) {
+        for (int l = 0; l < 32; ++l) lanes[l] = v[w * 32 + l];
+        for (int o = 16; o >= 1; o >>= 1) {
+            float nxt[32];
+            for (int l = 0; l < 32; ++l) nxt[l] = lanes[l] + lanes[l ^ o];
+            memcpy(lanes, nxt, sizeof(lanes));
+        }
+        wsum[w] = lanes[0];
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        float nxt[32];
+        for (int l = 0; l < 32; ++l) nxt[l] = wsum[l] + wsum[l ^ o];
+        memcpy(wsum, nxt, sizeof(wsum));
+    }
+    return wsum[0];
+}
+
+static long long blk_lo(int b, int n, int nb) { return (long long)b * n / nb; }
+
+/* The device kernels' dot order: block b owns nodes
+ * [b*n/nb, (b+1)*n/nb); thread t sums nodes lo+t, lo+t+nt, ... left to
+ * right; the block's nt partials go through tree64; the nb block partials
+ * are summed the same way (thread t: partials t, t+nt, ...; then tree64). */
+double orc_dot_blocked(int n, const double *x, const double *y,
+                       int nb, int nt)
+{
+    double *part = (double *)malloc(sizeof(double) * (size_t)nb);
+    double *v = (double *)malloc(sizeof(double) * (size_t)nt);
+    for (int b = 0; b < nb; ++b) {
+        long long lo = blk_lo(b, n, nb), hi = blk_lo(b + 1, n, nb);
+        for (int t = 0; t < nt; ++t) {
+            double s = 0.0;
+            for (long long i = lo + t; i < hi; i += nt) s = s + x[i] * y[i];
+            v[t] = s;
+        }
+        part[b] = tree64(v, nt);
+    }
+    for (int t = 0; t < nt; ++t) {
+        double s = 0.0;
+        for (int b = t; b < nb; b += nt) s = s + part[b];
+        v[t] = s;
+    }
+    double r = tree64(v, nt);
+    free(part); free(v);
+    return r;
+}
+
+static float dot_blocked32(int n, const float *x, const float *y, int nb, int nt)
+{
+    float *part = (float *)malloc(sizeof(float) * (size_t)nb);
+    float *v = (float *)malloc(sizeof(float) * (size_t)nt);
+    for (int b = 0; b < nb; ++b) {
+        long long lo = blk_lo(b, n, nb), hi = blk_lo(b + 1, n, nb);
+        for (int t = 0; t < nt; ++t) {
+            float s = 0.0f;
+            for (long long i = lo + t; i < hi; i += nt) s = s + x[i] * y[i];
+            v[t] = s;
+        }
+        part[b] = tree32(v, nt);
+    }
+    for (int t = 0; t < nt; ++t) {
+        float s = 0.0f;
+        for (int b = t; b < nb; b += nt) s = s + part[b];
+        v[t] = s;
+    }
+    float r = tree32(v, nt);
+    free(part); free(v);
+    return r;
+}
+
+static double pdots(int mode, int n, const double *x, const double *y,
+                    int nb, int nt)
+{
+    return mode == ORC_DOT_BLOCKED ? orc_dot_blocked(n, x, y, nb, nt)
+                                   : orc_dot(n, x, y);
+}
+
+/* ------------------------------------------------------------------ */
+/* diagonal preconditioning                                             */
+/* ------------------------------------------------------------------ */
+
+/* precd1.f:88-158 with DIADON=.FALSE., PREXSM=.TRUE., NCSIZE<=1:
+ *   D = A%D; [PRECON=5: D=|D|]; D = SQRT(D); X = X*D;
+ *   D = 1/D guarded (ovd.f:92-102, IOPT=2: |D|>1e-10 ? 1/D : 1.0);
+ *   A = D*A*D (om.f:249-255 -> om1111.f:559-600);
+ *   PRECON divisible by 2 or 3: TYPDIA = 'I' (precd1.f:137-142);
+ *   B = B*D.
+ * d[npoin] receives D (the reference's TBB(IT1)). */
+int orc_precd1(int npoin, int nelem, const int *ik0, const int *ik1,
+               const int *ik2, int precon, double *x, double *dm,
+               char *typdia, double *xm, int ld, char typext, double *b,
+               double *d)
+{
+    for (int i = 0; i < npoin; ++i) d[i] = dm[i];
+    if (precon == 5)
+        for (int i = 0; i < npoin; ++i) d[i] = fabs(d[i]);
+    for (int i = 0; i < npoin; ++i) d[i] = sqrt(d[i]);
+    for (int i = 0; i < npoin; ++i) x[i] = x[i] * d[i];
+    for (int i = 0; i < npoin; ++i)
+        d[i] = (fabs(d[i]) > 1.0e-10) ? 1.0 / d[i] : 1.0;
+    /* OM1111 'M=DMD': diagonal part */
+    if (*typdia == 'Q') {
+        for (int i = 0; i < npoin; ++i) dm[i] = dm[i] * d[i];
+        for (int i = 0; i < npoin; ++i) dm[i] = dm[i] * d[i];
+    } else if (*typdia == 'I') {
+        for (int i = 0; i < npoin; ++i) dm[i] = d[i] * d[i];
+        *typdia = 'Q';
+    } else if (*typdia != '0') {
+        return ORC_ERR_ARGS;
+    }
+    /* OM1111 'M=DMD': off-diagonal part (om1111.f:589-600) */
+    if (typext == 'S' || typext == 'Q') {
+        double *x1 = xm, *x2 = xm + ld, *x3 = xm + 2 * (size_t)ld;
+        for (int e = 0; e < nelem; ++e) {
+            x1[e] = x1[e] * d[ik1[e]] * d[ik0[e]];
+            x2[e] = x2[e] * d[ik2[e]] * d[ik0[e]];
+            x3[e] = x3[e] * d[ik2[e]] * d[ik1[e]];
+        }
+        if (typext == 'Q') {
+            double *x4 = xm + 3 * (size_t)ld, *x5 = xm + 4 * (size_t)ld,
+                   *x6 = xm + 5 * (size_t)ld;
+            for (int e = 0; e < nelem; ++e) {
+                x4[e] = x4[e] * d[ik1[e]] * d[ik0[e]];
+                x5[e] = x5[e] * d[ik2[e]] * d[ik0[e]];
+                x6[e] = x6[e] * d[ik2[e]] * d[ik1[e]];
+            }
+        }
+    }
+    if (precon % 2 == 0 || precon % 3 == 0) *typdia = 'I';
+    for (int i = 0; i < npoin; ++i) b[i] = b[i] * d[i];
+    return ORC_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* conjugate gradient                                                   */
+/* ------------------------------------------------------------------ */
+
+/* gracjg.F:169-437 without preconditioning matrices (PRECON 1/2/3/5 fold
+ * into the change of variables done by PRECD1, so G aliases R).
+ * Convention R = A X - B; stop when RMRM <= XL*EPS**2 or M = NITMAX.
+ * Returns ORC_OK, or the iteration count (>0) when NITMAX was reached
+ * without convergence, or a negative error. */
+int orc_gracjg(int npoin, int nelem, const int *ik0, const int *ik1,
+               const int *ik2, double *x, const double *da, char typdia,
+               const double *xm, int ld, char typext, const double *b,
+               int nitmax, double eps, int dot_mode, int nb, int nt,
+               int *nit_out, double *relres_out, int *relat_out)
+{
+    size_t n = (size_t)npoin;
+    double *r = (double *)malloc(sizeof(double) * n);
+    double *dd = (double *)malloc(sizeof(double) * n);
+    double *ad = (double *)malloc(sizeof(double) * n);
+    double *t = (double *)malloc(sizeof(double) * n);
+    double *w = (double *)malloc(sizeof(double) * 3 * (size_t)nelem + 1);
+    int m = 0, st = ORC_OK, relat;
+    double xl, rmrm, rmgm, rmdm, rm1gm1, dad, ro, beta;
+    if (!r || !dd || !ad || !t || !w) { st = ORC_ERR_ARGS; goto done; }
+
+    xl = pdots(dot_mode, npoin, b, b, nb, nt);            /* :189 */
+    if (sqrt(xl) < 1.0e-15) {                             /* :194-202 */
+        for (size_t i = 0; i < n; ++i) x[i] = 0.0;
+        rmrm = 0.0; xl = 1.0; relat = 0;
+        goto fin;
+    }
+    if (xl < 1.0) { xl = 1.0; relat = 0; } else { relat = 1; }  /* :204-209 */
+
+    st = orc_matvec("X=AY    ", npoin, nelem, ik0, ik1, ik2, r, da, typdia,
+                    xm, ld, typext, x, 0.0, t, w);        /* :213 */
+    if (st) goto done;
+    for (size_t i = 0; i < n; ++i) r[i] = r[i] - b[i];    /* :215 */
+    rmrm = pdots(dot_mode, npoin, r, r, nb, nt);          /* :216 */
+    rmgm = rmrm;
+    if (rmrm < eps * eps * xl) goto fin;                  /* :219 */
+
+    for (size_t i = 0; i < n; ++i) dd[i] = r[i];          /* :248 */
+    st = orc_matvec("X=AY    ", npoin, nelem, ik0, ik1, ik2, ad, da, typdia,
+                    xm, ld, typext, dd, 0.0, t, w);       /* :254 */
+    if (st) goto done;
+    dad = pdots(dot_mode, npoin, dd, ad, nb, nt);         /* :260 */
+    ro = rmgm / dad;                                      /* :261 */
+    for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * dd[i];   /* :268 */
+
+    for (;;) {
+        m = m + 1;                                        /* :284 */
+        for (size_t i = 0; i < n; ++i) r[i] = r[i] + (-ro) * ad[i];  /* :290 */
+        rm1gm1 = rmgm;
+        rmrm = pdots(dot_mode, npoin, r, r, nb, nt);      /* :295 */
+        rmdm = rmrm;
+        rmgm = rmrm;
+        if (rmrm <= xl * (eps * eps)) goto fin;           /* :303,324 */
+        beta = rmgm / rm1gm1;                             /* :357 */
+        for (size_t i = 0; i < n; ++i) dd[i] = r[i] + beta * dd[i];  /* :361 */
+        st = orc_matvec("X=AY    ", npoin, nelem, ik0, ik1, ik2, ad, da,
+                        typdia, xm, ld, typext, dd, 0.0, t, w);   /* :376 */
+        if (st) goto done;
+        dad = pdots(dot_mode, npoin, dd, ad, nb, nt);     /* :382 */
+        ro = rmdm / dad;                                  /* :383 */
+        for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * dd[i];  /* :387 */
+        if (m >= nitmax) { st = m; goto fin; }            /* :406 */
+    }
+fin:
+    if (nit_out) *nit_out = m;
+    if (relres_out) *relres_out = sqrt(rmrm / xl);
+    if (relat_out) *relat_out = relat;
+done:
+    free(r); free(dd); free(ad); free(t); free(w);
+    return st;
+}
+
+/* solve.f:387-649 for SLV=1 (GRACJG) on a single (non-block) matrix:
+ * PRECON 0 -> 1; diagonal change of variables when PRECON is divisible by
+ * 2, 3 or 5 (solve.f:484-498); CG; X = X*D to undo the change of variables
+ * (solve.f:637-641).  Inputs x, b, dm, typdia, xm are modified in place
+ * exactly as the reference modifies them. */
+int orc_solve(int npoin, int nelem, const int *ik0, const int *ik1,
+              const int *ik2, double *x, double *b, double *dm,
+              char *typdia, double *xm, int ld, char typext, int slv,
+              int precon, int nitmax, double eps, int dot_mode,
+              int nb, int nt, int *nit_out, double *relres_out,
+              int *relat_out)
+{
+    if (slv != 1) return ORC_ERR_UNSUPPORTED;
+    if (precon == 0) precon = 1;
+    if (precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 ||
+        precon % 17 == 0)
+        return ORC_ERR_UNSUPPORTED;
+    int diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
+    double *d = NULL;
+    if (diag) {
+        d = (double *)malloc(sizeof(double) * (size_t)npoin);
+        int st = orc_precd1(npoin, nelem, ik0, ik1, ik2, precon, x, dm, typdia,
+                            xm, ld, typext, b, d);
+        if (st) { free(d); return st; }
+    }
+    int st = orc_gracjg(npoin, nelem, ik0, ik1, ik2, x, dm, *typdia, xm, ld,
+                        typext, b, nitmax, eps, dot_mode, nb, nt, nit_out,
+                        relres_out, relat_out);
+    if (diag) {
+        for (int i = 0; i < npoin; ++i) x[i] = x[i] * d[i];
+        free(d);
+    }
+    return st;
+}
+
+/* ------------------------------------------------------------------ */
+/* mixed precision (no reference counterpart)                           */
+/* ------------------------------------------------------------------ */
+
+/* binary32 EBE product q = A32 p in difference form:
+ *   q_i = s_i p_i + sum over the W terms of node i of
+ *         XA(k,a) (p_a - p_i) + XA(k,b) (p_b - p_i)
+ * with s_i the binary64 row sum (diagonal + every off-diagonal term of row
+ * i, in ASSVEC order) rounded once to binary32.  Rounding the coefficients
+ * then leaves constant vectors exact, so the small mass-dominated
+ * eigenvalues of the wave operator survive the binary32 copy.  Per-node
+ * summation order as ASSVEC (diagonal term first, then local point 1, 2, 3
+ * contributions in element order). */
+static void mv32_sym(int npoin, int nelem, const int *ik0, const int *ik1,
+                     const int *ik2, const float *s32, const float *xm,
+                     const float *p, float *q, float *w)
+{
+    const float *m12 = xm, *m13 = xm + nelem, *m23 = xm + 2 * (size_t)nelem;
+    float *w1 = w, *w2 = w + nelem, *w3 = w + 2 * (size_t)nelem;
+    for (int e = 0; e < nelem; ++e) {
+        float p1 = p[ik0[e]], p2 = p[ik1[e]], p3 = p[ik2[e]];
+        w1[e] = m12[e] * (p2 - p1) + m13[e] * (p3 - p1);
+        w2[e] = m23[e] * (p3 - p2) + m12[e] * (p1 - p2);
+        w3[e] = m13[e] * (p1 - p3) + m23[e] * (p2 - p3);
+    }
+    for (int i = 0; i < npoin; ++i) q[i] = p[i] * s32[i];
+    for (int e = 0; e < nelem; ++e) q[ik0[e]] = q[ik0[e]] + w1[e];
+    for (int e = 0; e < nelem; ++e) q[ik1[e]] = q[ik1[e]] + w2[e];
+    for (int e = 0; e < nelem; ++e) q[ik2[e]] = q[ik2[e]] + w3[e];
+}
+
+/* binary64 row sums of a symmetric EBE operator, in ASSVEC order:
+ * s_i = diag_i + sum over the W terms of node i of (XA(k,a) + XA(k,b)). */
+static void rowsum64_sym(int npoin, int nelem, const int *ik0, const int *ik1,
+                         const int *ik2, const double *da, char typdia,
+                         const double *xm, double *s, double *w)
+{
+    const double *m12 = xm, *m13 = xm + nelem, *m23 = xm + 2 * (size_t)nelem;
+    double *w1 = w, *w2 = w + nelem, *w3 = w + 2 * (size_t)nelem;
+    for (int e = 0; e < nelem; ++e) {
+        w1[e] = m12[e] + m13[e];
+        w2[e] = m23[e] + m12[e];
+        w3[e] = m13[e] + m23[e];
+    }
+    for (int i = 0; i < npoin; ++i)
+        s[i] = typdia == 'Q' ? da[i] : (typdia == 'I' ? 1.0 : 0.0);
+    for (int e = 0; e < nelem; ++e) s[ik0[e]] = s[ik0[e]] + w1[e];
+    for (int e = 0; e < nelem; ++e) s[ik1[e]] = s[ik1[e]] + w2[e];
+    for (int e = 0; e < nelem; ++e) s[ik2[e]] = s[ik2[e]] + w3[e];
+}
+
+/* Mixed-precision solve (the device kernel's exact operation order):
+ * PRECD1 scaling in binary64 on copies; binary32 copy of the scaled EBE
+ * operator; one binary32 CG (binary32 vectors, matvec and dots) whose
+ * correction z is folded into the binary64 solution ("reliable update")
+ * whenever its recursive residual has dropped by inner_tol relative to the
+ * last true residual, or looks converged.  Each update recomputes the true
+ * residual r = b - A x in binary64, tests it against outer_tol (relative to
+ * ||b||, absolute when ||b||^2 < 1, as GRACJG), and restarts the binary32
+ * residual from it while keeping the search direction (beta from the
+ * recursive residual).  Symmetric storage only; inputs other than x are not
+ * modified.  Returns 0 when converged, the inner iteration count when
+ * max_inner or max_outer ran out, or a negative error. */
+int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
+                    const int *ik2, double *x, const double *b,
+                    const double *dm_in, char typdia_in, const double *xm_in,
+                    char typext, int precon, double inner_tol,
+                    double outer_tol, int max_outer, int max_inner,
+                    int nb, int nt, int *outer_out, int *inner_total_out,
+                    double *relres_out)
+{
+    if (typext != 'S') return ORC_ERR_UNSUPPORTED;
+    size_t n = (size_t)npoin, ne = (size_t)nelem;
+    double *dm = (double *)malloc(sizeof(double) * n);
+    double *xm = (double *)malloc(sizeof(double) * 3 * ne);
+    double *bs = (double *)malloc(sizeof(double) * n);
+    double *d = (double *)malloc(sizeof(double) * n);
+    double *r = (double *)malloc(sizeof(double) * n);
+    double *t = (double *)malloc(sizeof(double) * n);
+    double *w = (double *)malloc(sizeof(double) * 3 * ne + 1);
+    float *xm32 = (float *)malloc(sizeof(float) * 3 * ne);
+    float *dm32 = (float *)malloc(sizeof(float) * n);
+    float *z = (float *)malloc(sizeof(float) * n);
+    float *ri = (float *)malloc(sizeof(float) * n);
+    float *p = (float *)malloc(sizeof(float) * n);
+    float *q = (float *)malloc(sizeof(float) * n);
+    float *w32 = (float *)malloc(sizeof(float) * 3 * ne + 1);
+    int st = ORC_OK, outer = 0, inner = 0, diag = 0;
+    double xl = 0.0, rr = 0.0, otol = 0.0;
+    float rho = 0.0f, rmax = 0.0f, itol2 = 0.0f;
+    char typdia = typdia_in;
+    if (!dm || !xm || !bs || !d || !r || !t || !w || !xm32 || !dm32 || !z ||
+        !ri || !p || !q || !w32) { st = ORC_ERR_ARGS; goto done; }
+    memcpy(dm, dm_in, sizeof(double) * n);
+    memcpy(xm, xm_in, sizeof(double) * 3 * ne);
+    memcpy(bs, b, sizeof(double) * n);
+    if (precon == 0) precon = 1;
+    diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
+    if (diag) {
+        st = orc_precd1(npoin, nelem, ik0, ik1, ik2, precon, x, dm, &typdia,
+                        xm, nelem, typext, bs, d);
+        if (st) goto done;
+    }
+    for (size_t k = 0; k < 3 * ne; ++k) xm32[k] = (float)xm[k];
+    rowsum64_sym(npoin, nelem, ik0, ik1, ik2, dm, typdia, xm, t, w);
+    for (size_t i = 0; i < n; ++i) dm32[i] = (float)t[i];
+
+    xl = orc_dot_blocked(npoin, bs, bs, nb, nt);
+    if (sqrt(xl) < 1.0e-15) {
+        for (size_t i = 0; i < n; ++i) x[i] = 0.0;
+        rr = 0.0; xl = 1.0;
+        goto fin;
+    }
+    if (xl < 1.0) xl = 1.0;
+    otol = xl * (outer_tol * outer_tol);
+    itol2 = (float)(inner_tol * inner_tol);
+
+    /* true residual r = b - A x (binary64), its binary32 copy, both norms */
+#define TRUE_RESIDUAL()                                                         \
+    do {                                                                        \
+        st = orc_matvec("X=AY    ", npoin, nelem, ik0, ik1, ik2, t, dm,          \
+                        typdia, xm, nelem, typext, x, 0.0, r, w);               \
+        if (st) goto done;                                                      \
+        for (size_t i = 0; i < n; ++i) { r[i] = bs[i] - t[i]; ri[i] = (float)r[i]; } \
+        rr = orc_dot_blocked(npoin, r, r, nb, nt);                              \
+        rho = dot_blocked32(npoin, ri, ri, nb, nt);                             \
+    } while (0)
+
+    TRUE_RESIDUAL();
+    if (isnan(rr)) { st = ORC_ERR_NAN; goto fin; }
+    if (rr <= otol) goto fin;
+    rmax = rho;
+    for (size_t i = 0; i < n; ++i) { z[i] = 0.0f; p[i] = ri[i]; }
+    for (;;) {
+        mv32_sym(npoin, nelem, ik0, ik1, ik2, dm32, xm32, p, q, w32);
+        float pq = dot_blocked32(npoin, p, q, nb, nt);
+        if (!(pq > 0.0f)) { st = isnan(pq) ? ORC_ERR_NAN : ORC_ERR_BREAKDOWN; goto fin; }
+        float alpha = rho / pq;
+        for (size_t i = 0; i < n; ++i) z[i] = z[i] + alpha * p[i];
+        for (size_t i = 0; i < n; ++i) ri[i] = ri[i] - alpha * q[i];
+        float rho_new = dot_blocked32(npoin, ri, ri, nb, nt);
+        float rho_rec = rho_new, rho_old = rho;
+        ++inner;
+        int last = inner >= max_inner;
+        if (last || rho_new <= itol2 * rmax || (double)rho_new <= otol) {
+            for (size_t i = 0; i < n; ++i) { x[i] = x[i] + (double)z[i]; z[i] = 0.0f; }
+            TRUE_RESIDUAL();
+            ++outer;
+            if (isnan(rr)) { st = ORC_ERR_NAN; goto fin; }
+            if (rr <= otol) goto fin;
+            if (last || outer >= max_outer) { st = inner; goto fin; }
+            rho_new = rho;
+            rmax = rho;
+        }
+        float beta = rho_rec / rho_old;
+        rho = rho_new;
+        for (size_t i = 0; i < n; ++i) p[i] = ri[i] + beta * p[i];
+    }
+#undef TRUE_RESIDUAL
+fin:
+    if (diag) for (size_t i = 0; i < n; ++i) x[i] = x[i] * d[i];
+    if (outer_out) *outer_out = outer;
+    if (inner_total_out) *inner_total_out = inner;
+    if (relres_out) *relres_out = sqrt(rr / xl);
+done:
+    free(dm); free(xm); free(bs); free(d); free(r); free(t); free(w);
+    free(xm32); free(dm32); free(z); free(ri); free(p); free(q); free(w32);
+    return st;
+}

@@ -1,0 +1,90 @@
+"""CPU-side checks of the C ABI library: it loads without a GPU, exports
+every function include/bief_b200.h declares, and rejects bad meshes before
+touching the device."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from opentelemac_b200 import _native, meshgen as mg
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    txt = open(os.path.join(ROOT, "include", "bief_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(bief_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_header():
+    names = header_functions()
+    assert len(names) >= 15
+    L = ctypes.CDLL(_native.LIB)
+    for n in names:
+        assert hasattr(L, n), n
+    assert sorted(_native.EXPORTS) == names
+
+
+def test_strerror():
+    L = _native.lib()
+    assert L.bief_strerror(0) == b"ok"
+    assert b"NITMAX" in L.bief_strerror(12)
+    for s in range(-9, 0):
+        assert L.bief_strerror(s) != b"unknown status"
+
+
+def test_bad_mesh_rejected_on_host():
+    """IKLE entries outside 1..NPOIN are caught before any device call."""
+    _, _, ik = mg.square_mesh(5)
+    fort = mg.ikle_fortran(ik)
+    fort[7] = 0
+    h = ctypes.c_void_p()
+    L = _native.lib()
+    st = L.bief_mesh_create(25, ik.shape[0], ik.shape[0], fort.ctypes.data_as(ctypes.c_void_p),
+                            0, ctypes.byref(h))
+    assert st == _native.BIEF_ERR_BAD_MESH and not h.value
+    fort[7] = 26
+    st = L.bief_mesh_create(25, ik.shape[0], ik.shape[0], fort.ctypes.data_as(ctypes.c_void_p),
+                            0, ctypes.byref(h))
+    assert st == _native.BIEF_ERR_BAD_MESH
+    st = L.bief_mesh_create(0, ik.shape[0], ik.shape[0], fort.ctypes.data_as(ctypes.c_void_p),
+                            0, ctypes.byref(h))
+    assert st == _native.BIEF_ERR_ARGS
+    st = L.bief_mesh_create(25, ik.shape[0], ik.shape[0] - 1,
+                            fort.ctypes.data_as(ctypes.c_void_p), 0, ctypes.byref(h))
+    assert st == _native.BIEF_ERR_ARGS
+
+
+def test_null_handle_calls():
+    L = _native.lib()
+    assert L.bief_destroy(None) == _native.BIEF_ERR_ARGS
+    assert L.bief_launch_info(None, None, None) == _native.BIEF_ERR_ARGS
+    assert L.bief_kernel_launches(None) == -1
+
+
+def test_meshgen_shapes_and_orientation():
+    x, y, ik = mg.square_mesh(11)
+    assert x.size == 121 and ik.shape == (200, 3)
+    X, Y = x[ik], y[ik]
+    area = 0.5 * ((X[:, 1] - X[:, 0]) * (Y[:, 2] - Y[:, 0]) - (X[:, 2] - X[:, 0]) * (Y[:, 1] - Y[:, 0]))
+    assert (area > 0).all()
+    np.testing.assert_allclose(area.sum(), 1.0, rtol=1e-12)
+    xs, ys, iks, perm, eperm = mg.shuffled(x, y, ik)
+    X, Y = xs[iks], ys[iks]
+    area2 = 0.5 * ((X[:, 1] - X[:, 0]) * (Y[:, 2] - Y[:, 0]) - (X[:, 2] - X[:, 0]) * (Y[:, 1] - Y[:, 0]))
+    np.testing.assert_allclose(np.sort(area2), np.sort(area))
+    f = mg.ikle_fortran(ik, nelmax=210)
+    assert f.size == 630 and f.min() == 0 and f.max() == 121
+
+
+def test_depth_fields():
+    x, y, ik = mg.square_mesh(41)
+    h = mg.depth_smooth(x, y, ik)
+    assert 1.0 <= h.min() and h.max() <= 9.0
+    h2 = mg.depth_loguniform(ik)
+    assert 0.5 <= h2.min() and h2.max() <= 500.0
+    nb = mg.element_neighbours(ik)
+    assert ((nb >= 0).sum(axis=1) >= 1).all()
