@@ -19,7 +19,10 @@
  *     TYPEXT='S' (columns M12,M13,M23) or 6 for TYPEXT='Q' (then M21,M31,
  *     M32), following om1111.f:43-50.  DM is A%D%R(NPOIN).
  *   - TYPDIA is 'Q' (any diagonal), 'I' (identity) or '0' (zero).
- *   - Host pointers unless the function name ends in _dev.
+ *   - Host pointers unless the function name ends in _dev.  The _dev
+ *     functions take a cudaStream_t (as void*) and run in stream order on
+ *     it; NULL is CUDA's default stream.  The host-pointer functions use the
+ *     handle's own stream and return after the results are on the host.
  *   - Every function returns an int status: 0 = success; > 0 = the solve
  *     stopped at NITMAX without converging (the value is the iteration
  *     count); < 0 = an error (see BIEF_ERR_*).  The reference aborts with
@@ -93,7 +96,7 @@ int bief_get_matrix(bief_handle *h, double *dm, double *xm, char *typdia);
  * B.  relres_out receives SQRT(RMRM/XL) as printed by GRACJG. */
 int bief_solve(bief_handle *h, double *x, double *b, bief_slvcfg *cfg,
                int flags, double *relres_out);
-/* Same with device pointers, on `stream` (cudaStream_t, NULL = handle's). */
+/* Same with device pointers, on `stream`. */
 int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg,
                    int flags, double *relres_out, void *stream);
 

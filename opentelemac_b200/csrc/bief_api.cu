@@ -395,7 +395,7 @@ int bief_get_matrix_dev(bief_handle *h, double *dm, double *xm, void *stream) {
   if (!h || !dm || !xm) return BIEF_ERR_ARGS;
   if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
   DevGuard g(h->dev);
-  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  cudaStream_t st = (cudaStream_t)stream;
   const size_t n = (size_t)h->npoin, ne = (size_t)h->nelem;
   CK(cudaMemcpyAsync(dm, h->d_dm, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpyAsync(xm, h->d_xm, sizeof(double) * 3 * ne, cudaMemcpyDeviceToDevice, st));
@@ -409,7 +409,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   if (st) return st;
   if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
   DevGuard g(h->dev);
-  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  cudaStream_t s = (cudaStream_t)stream;
   const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
   const bool sym = h->typext != 'Q';
   int td = typdia_code(h->typdia);
@@ -494,7 +494,7 @@ int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b, int precon,
   if (precon < 0 || precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 || precon % 17 == 0)
     return BIEF_ERR_UNSUPPORTED;
   DevGuard g(h->dev);
-  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  cudaStream_t s = (cudaStream_t)stream;
   const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
   int td = typdia_code(h->typdia), st;
   const double *xm = h->d_xm, *da = h->d_dm, *bw = b;
@@ -585,7 +585,7 @@ int bief_matvec_dev(bief_handle *h, const char *op, double *x, const double *y, 
   if (st) return st;
   if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
   DevGuard g(h->dev);
-  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  cudaStream_t s = (cudaStream_t)stream;
   const int td = typdia_code(h->typdia);
   const bool sym = h->typext != 'Q';
   const size_t nb = sizeof(double) * h->npoin;
@@ -628,7 +628,7 @@ int bief_assemble_wave_dev(bief_handle *h, const double *xc, const double *yc,
   int st = ensure_matrix_buffers(h);
   if (st) return st;
   if (!h->d_ew && (st = dalloc(&h->d_ew, 4 * (size_t)h->nelem))) return st;
-  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  cudaStream_t s = (cudaStream_t)stream;
   CK(cudaMemsetAsync(h->d_err, 0, sizeof(int), s));
   k_wave_elems<<<grid_for(h->nelem, h->nsm), 256, 0, s>>>(h->nelem, h->d_ik, xc, yc, coef,
                                                           h->d_xm, h->d_ew, h->d_err);
@@ -650,7 +650,7 @@ int bief_wave_coef_grad_dev(bief_handle *h, const double *xc, const double *yc,
                             const double *lambda, const double *x, double *grad, void *stream) {
   if (!h || !xc || !yc || !lambda || !x || !grad) return BIEF_ERR_ARGS;
   DevGuard g(h->dev);
-  cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+  cudaStream_t s = (cudaStream_t)stream;
   k_coef_grad<<<grid_for(h->nelem, h->nsm), 256, 0, s>>>(h->nelem, h->d_ik, xc, yc, lambda, x,
                                                          grad);
   h->launches++;

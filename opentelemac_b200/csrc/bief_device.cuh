@@ -184,47 +184,60 @@ __device__ __forceinline__ int xm_col(int k, int l) {
   return SYM ? (k + l - 1) : (k < l ? (k + l - 1) : (k + l + 2));
 }
 
-template <typename T, bool SYM, bool TRANS, class V>
-__device__ __forceinline__ T row_sum(T acc, int i, const int *__restrict__ ptr,
-                                     const int *__restrict__ ek, const int *__restrict__ ik,
-                                     const T *__restrict__ xm, int ne, V vec) {
-  const int j0 = __ldg(ptr + i), j1 = __ldg(ptr + i + 1);
-  for (int j = j0; j < j1; ++j) {
-    const int p = __ldg(ek + j);
-    const int e = p >> 2, k = p & 3;
-    const int a = (k == 2) ? 0 : k + 1;  // (k+1) mod 3
-    const int b = (k == 0) ? 2 : k - 1;  // (k+2) mod 3
-    const int va = __ldg(ik + (size_t)a * ne + e);
-    const int vb = __ldg(ik + (size_t)b * ne + e);
-    const int ca = TRANS ? xm_col<SYM>(a, k) : xm_col<SYM>(k, a);
-    const int cb = TRANS ? xm_col<SYM>(b, k) : xm_col<SYM>(k, b);
-    const T xa = __ldg(xm + (size_t)ca * ne + e);
-    const T xb = __ldg(xm + (size_t)cb * ne + e);
-    const T w = add(mul(xa, vec(va)), mul(xb, vec(vb)));
-    acc = add(acc, w);
+// Product W of one gather entry p = (IELEM<<2 | k): the two off-diagonal
+// terms of row k of element IELEM times the vector at the element's two
+// other points.  DIFF selects the difference form used by the binary32
+// inner operator: XA(k,a) (y_a - y_k) + XA(k,b) (y_b - y_k).
+template <typename T, bool SYM, bool TRANS, bool DIFF, class V>
+__device__ __forceinline__ T entry_product(int p, const int *__restrict__ ik,
+                                           const T *__restrict__ xm, int ne, V vec) {
+  const int e = p >> 2, k = p & 3;
+  const int a = (k == 2) ? 0 : k + 1;  // (k+1) mod 3
+  const int b = (k == 0) ? 2 : k - 1;  // (k+2) mod 3
+  const int va = __ldg(ik + (size_t)a * ne + e);
+  const int vb = __ldg(ik + (size_t)b * ne + e);
+  const int ca = TRANS ? xm_col<SYM>(a, k) : xm_col<SYM>(k, a);
+  const int cb = TRANS ? xm_col<SYM>(b, k) : xm_col<SYM>(k, b);
+  const T xa = __ldg(xm + (size_t)ca * ne + e);
+  const T xb = __ldg(xm + (size_t)cb * ne + e);
+  if (DIFF) {
+    const T yk = vec(__ldg(ik + (size_t)k * ne + e));
+    return add(mul(xa, sub(vec(va), yk)), mul(xb, sub(vec(vb), yk)));
   }
-  return acc;
+  return add(mul(xa, vec(va)), mul(xb, vec(vb)));
 }
 
-// Difference form of the same product for the binary32 inner operator:
-// each W term is XA(k,a) (y_a - y_i) + XA(k,b) (y_b - y_i); the diagonal part
-// is s_i y_i with s_i the row sum (see k_rowsum).
-template <typename T, class V>
-__device__ __forceinline__ T row_sum_diff(T acc, T yi, int i, const int *__restrict__ ptr,
-                                          const int *__restrict__ ek, const int *__restrict__ ik,
-                                          const T *__restrict__ xm, int ne, V vec) {
-  const int j0 = __ldg(ptr + i), j1 = __ldg(ptr + i + 1);
-  for (int j = j0; j < j1; ++j) {
-    const int p = __ldg(ek + j);
-    const int e = p >> 2, k = p & 3;
-    const int a = (k == 2) ? 0 : k + 1;
-    const int b = (k == 0) ? 2 : k - 1;
-    const int va = __ldg(ik + (size_t)a * ne + e);
-    const int vb = __ldg(ik + (size_t)b * ne + e);
-    const T xa = __ldg(xm + (size_t)(k + a - 1) * ne + e);
-    const T xb = __ldg(xm + (size_t)(k + b - 1) * ne + e);
-    const T w = add(mul(xa, sub(vec(va), yi)), mul(xb, sub(vec(vb), yi)));
-    acc = add(acc, w);
+// Shared-memory capacity of one gather tile, in entries per thread.
+constexpr int TILE_ENTRIES_PER_THREAD = 8;
+
+// Gather product for a tile of nn <= blockDim.x consecutive nodes starting
+// at n0; thread t owns node n0+t.  All threads of the block call it.
+// The entries of the tile are contiguous in the gather index: every thread
+// computes entry products (strided, so index loads are coalesced and many
+// loads are in flight) into smW, then each owner adds its node's products
+// to acc in index order -- the same left-to-right sum ASSVEC performs.
+// Tiles with more entries than `cap` are processed in chunks, in order.
+template <typename T, bool SYM, bool TRANS, bool DIFF, class V>
+__device__ __forceinline__ T tile_gather(int n0, int nn, T acc, const int *__restrict__ ptr,
+                                         const int *__restrict__ ek, const int *__restrict__ ik,
+                                         const T *__restrict__ xm, int ne, V vec, T *smW,
+                                         int cap) {
+  const int t = threadIdx.x;
+  const int j0 = __ldg(ptr + n0), j1 = __ldg(ptr + n0 + nn);
+  int my0 = 0, my1 = 0;
+  if (t < nn) {
+    my0 = __ldg(ptr + n0 + t);
+    my1 = __ldg(ptr + n0 + t + 1);
+  }
+  for (int c0 = j0; c0 < j1; c0 += cap) {
+    const int c1 = min(c0 + cap, j1);
+#pragma unroll 4
+    for (int j = c0 + t; j < c1; j += blockDim.x)
+      smW[j - c0] = entry_product<T, SYM, TRANS, DIFF>(__ldg(ek + j), ik, xm, ne, vec);
+    __syncthreads();
+    const int lo = max(my0, c0), hi = min(my1, c1);
+    for (int j = lo; j < hi; ++j) acc = add(acc, smW[j - c0]);
+    __syncthreads();
   }
   return acc;
 }

@@ -29,21 +29,27 @@ __global__ void __launch_bounds__(256) k_matvec(int npoin, int nelem, const int 
                                                 const double *__restrict__ da,
                                                 const double *__restrict__ y, double *x, int opc,
                                                 double c) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
-    double acc = diag_term<TD>(y[i], da, i);
-    acc = row_sum<double, SYM, TRANS>(acc, i, ptr, ek, ik, xm, nelem,
-                                      [&](int j) { return __ldg(y + j); });
-    // OS combination of MESH%T into X (matvec.f:369-380, :329-340)
-    double r;
-    switch (opc) {
-      case OP_AY: r = acc; break;
-      case OP_XPAY: r = add(x[i], acc); break;
-      case OP_MAY: r = -acc; break;
-      case OP_XMAY: r = sub(x[i], acc); break;
-      case OP_XPCAY: r = add(x[i], mul(c, acc)); break;
-      default: r = mul(c, acc); break;
+  __shared__ double smW[256 * TILE_ENTRIES_PER_THREAD];
+  const int T = blockDim.x, t = threadIdx.x;
+  for (int n0 = blockIdx.x * T; n0 < npoin; n0 += gridDim.x * T) {
+    const int nn = min(T, npoin - n0), i = n0 + t;
+    double acc = t < nn ? diag_term<TD>(__ldg(y + i), da, i) : 0.0;
+    acc = tile_gather<double, SYM, TRANS, false>(n0, nn, acc, ptr, ek, ik, xm, nelem,
+                                                 [&](int j) { return __ldg(y + j); }, smW,
+                                                 T * TILE_ENTRIES_PER_THREAD);
+    if (t < nn) {
+      // OS combination of MESH%T into X (matvec.f:369-380, :329-340)
+      double r;
+      switch (opc) {
+        case OP_AY: r = acc; break;
+        case OP_XPAY: r = add(x[i], acc); break;
+        case OP_MAY: r = -acc; break;
+        case OP_XMAY: r = sub(x[i], acc); break;
+        case OP_XPCAY: r = add(x[i], mul(c, acc)); break;
+        default: r = mul(c, acc); break;
+      }
+      x[i] = r;
     }
-    x[i] = r;
   }
 }
 
@@ -138,7 +144,9 @@ struct CgP {
 };
 
 template <int TD, bool SYM>
-__global__ void __launch_bounds__(CG_THREADS) k_cg64(CgP P) {
+__global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
+  __shared__ double smW[CG_THREADS * TILE_ENTRIES_PER_THREAD];
+  constexpr int CAP = CG_THREADS * TILE_ENTRIES_PER_THREAD;
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -174,13 +182,16 @@ __global__ void __launch_bounds__(CG_THREADS) k_cg64(CgP P) {
 
   // R = A X - B (gracjg.F:213-216)
   s = 0.0;
-  for (int i = lo + t; i < hi; i += T) {
-    double acc = diag_term<TD>(x[i], da, i);
-    acc = row_sum<double, SYM, false>(acc, i, P.ptr, P.ek, P.ik, P.xm, P.nelem,
-                                      [&](int j) { return x[j]; });
-    const double ri = sub(acc, b[i]);
-    r[i] = ri;
-    s = add(s, mul(ri, ri));
+  for (int n0 = lo; n0 < hi; n0 += T) {
+    const int nn = min(T, hi - n0), i = n0 + t;
+    double acc = t < nn ? diag_term<TD>(x[i], da, i) : 0.0;
+    acc = tile_gather<double, SYM, false, false>(n0, nn, acc, P.ptr, P.ek, P.ik, P.xm, P.nelem,
+                                                 [&](int j) { return x[j]; }, smW, CAP);
+    if (t < nn) {
+      const double ri = sub(acc, b[i]);
+      r[i] = ri;
+      s = add(s, mul(ri, ri));
+    }
   }
   if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
   double rmrm = red, rmgm = rmrm;
@@ -190,14 +201,20 @@ __global__ void __launch_bounds__(CG_THREADS) k_cg64(CgP P) {
   // D = G (= R), AD = A D, DAD, RO (gracjg.F:248-261)
   double *cur = P.d0, *nxt = P.d1;
   s = 0.0;
-  for (int i = lo + t; i < hi; i += T) {
-    const double di = r[i];
-    cur[i] = di;
-    double acc = diag_term<TD>(di, da, i);
-    acc = row_sum<double, SYM, false>(acc, i, P.ptr, P.ek, P.ik, P.xm, P.nelem,
-                                      [&](int j) { return r[j]; });
-    ad[i] = acc;
-    s = add(s, mul(di, acc));
+  for (int n0 = lo; n0 < hi; n0 += T) {
+    const int nn = min(T, hi - n0), i = n0 + t;
+    double di = 0.0, acc = 0.0;
+    if (t < nn) {
+      di = r[i];
+      cur[i] = di;
+      acc = diag_term<TD>(di, da, i);
+    }
+    acc = tile_gather<double, SYM, false, false>(n0, nn, acc, P.ptr, P.ek, P.ik, P.xm, P.nelem,
+                                                 [&](int j) { return r[j]; }, smW, CAP);
+    if (t < nn) {
+      ad[i] = acc;
+      s = add(s, mul(di, acc));
+    }
   }
   if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
   double dad = red;
@@ -228,14 +245,21 @@ __global__ void __launch_bounds__(CG_THREADS) k_cg64(CgP P) {
     // recomputes R(j)+BETA*D(j) from the previous direction, which gives
     // the same bits as the owner's value; the owner also stores it.
     s = 0.0;
-    for (int i = lo + t; i < hi; i += T) {
-      const double di = add(r[i], mul(beta, cur[i]));
-      nxt[i] = di;
-      double acc = diag_term<TD>(di, da, i);
-      acc = row_sum<double, SYM, false>(acc, i, P.ptr, P.ek, P.ik, P.xm, P.nelem,
-                                        [&](int j) { return add(r[j], mul(beta, cur[j])); });
-      ad[i] = acc;
-      s = add(s, mul(di, acc));
+    for (int n0 = lo; n0 < hi; n0 += T) {
+      const int nn = min(T, hi - n0), i = n0 + t;
+      double di = 0.0, acc = 0.0;
+      if (t < nn) {
+        di = add(r[i], mul(beta, cur[i]));
+        nxt[i] = di;
+        acc = diag_term<TD>(di, da, i);
+      }
+      acc = tile_gather<double, SYM, false, false>(
+          n0, nn, acc, P.ptr, P.ek, P.ik, P.xm, P.nelem,
+          [&](int j) { return add(r[j], mul(beta, cur[j])); }, smW, CAP);
+      if (t < nn) {
+        ad[i] = acc;
+        s = add(s, mul(di, acc));
+      }
     }
     if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
     dad = red;
@@ -278,7 +302,10 @@ struct MixP {
 };
 
 template <int TD>
-__global__ void __launch_bounds__(CG_THREADS) k_mixed(MixP P) {
+__global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
+  __shared__ double smW[CG_THREADS * TILE_ENTRIES_PER_THREAD];
+  float *smW32 = reinterpret_cast<float *>(smW);
+  constexpr int CAP = CG_THREADS * TILE_ENTRIES_PER_THREAD;
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -321,15 +348,19 @@ __global__ void __launch_bounds__(CG_THREADS) k_mixed(MixP P) {
   auto true_residual = [&]() -> bool {
     double sd = 0.0;
     float s32 = 0.0f;
-    for (int i = lo + t; i < hi; i += T) {
-      double acc = diag_term<TD>(x[i], P.da, i);
-      acc = row_sum<double, true, false>(acc, i, P.ptr, P.ek, P.ik, P.xm, P.nelem,
-                                         [&](int j) { return x[j]; });
-      const double rv = sub(b[i], acc);
-      sd = add(sd, mul(rv, rv));
-      const float r32 = (float)rv;
-      ri[i] = r32;
-      s32 = add(s32, mul(r32, r32));
+    for (int n0 = lo; n0 < hi; n0 += T) {
+      const int nn = min(T, hi - n0), i = n0 + t;
+      double acc = t < nn ? diag_term<TD>(x[i], P.da, i) : 0.0;
+      acc = tile_gather<double, true, false, false>(n0, nn, acc, P.ptr, P.ek, P.ik, P.xm,
+                                                    P.nelem, [&](int j) { return x[j]; }, smW,
+                                                    CAP);
+      if (t < nn) {
+        const double rv = sub(b[i], acc);
+        sd = add(sd, mul(rv, rv));
+        const float r32 = (float)rv;
+        ri[i] = r32;
+        s32 = add(s32, mul(r32, r32));
+      }
     }
     return grid_reduce<1, 1>(P.ctl, P.part, P.timeout_ns, &sd, &s32, &rr, &rho);
   };
@@ -344,18 +375,26 @@ __global__ void __launch_bounds__(CG_THREADS) k_mixed(MixP P) {
   for (;;) {
     // p = r + beta p, evaluated where needed; q = A32 p; p.q
     sf = 0.0f;
-    for (int i = lo + t; i < hi; i += T) {
-      const float pi = first ? ri[i] : add(ri[i], mul(beta, cur[i]));
-      nxt[i] = pi;
-      float acc = mul(pi, P.s32[i]);
+    for (int n0 = lo; n0 < hi; n0 += T) {
+      const int nn = min(T, hi - n0), i = n0 + t;
+      float pi = 0.0f, acc = 0.0f;
+      if (t < nn) {
+        pi = first ? ri[i] : add(ri[i], mul(beta, cur[i]));
+        nxt[i] = pi;
+        acc = mul(pi, P.s32[i]);
+      }
       if (first)
-        acc = row_sum_diff<float>(acc, pi, i, P.ptr, P.ek, P.ik, P.xm32, P.nelem,
-                                  [&](int k) { return ri[k]; });
+        acc = tile_gather<float, true, false, true>(n0, nn, acc, P.ptr, P.ek, P.ik, P.xm32,
+                                                    P.nelem, [&](int k) { return ri[k]; }, smW32,
+                                                    2 * CAP);
       else
-        acc = row_sum_diff<float>(acc, pi, i, P.ptr, P.ek, P.ik, P.xm32, P.nelem,
-                                  [&](int k) { return add(ri[k], mul(beta, cur[k])); });
-      q[i] = acc;
-      sf = add(sf, mul(pi, acc));
+        acc = tile_gather<float, true, false, true>(
+            n0, nn, acc, P.ptr, P.ek, P.ik, P.xm32, P.nelem,
+            [&](int k) { return add(ri[k], mul(beta, cur[k])); }, smW32, 2 * CAP);
+      if (t < nn) {
+        q[i] = acc;
+        sf = add(sf, mul(pi, acc));
+      }
     }
     float pq;
     if (!grid_reduce<0, 1>(P.ctl, P.part, P.timeout_ns, nullptr, &sf, nullptr, &pq)) return;

@@ -124,7 +124,7 @@ def test_solve_golden_21(oracle_mod):
     for nit in (1, 10):
         gi = _gpu_solve(p, eps=1e-30, nitmax=nit)
         assert gi["status"] == nit
-        np.testing.assert_array_equal(gi["x"], gd[f"x_nit{nit}"])
+        np.testing.assert_array_equal(gi["x"], gd[f"x_nit{nit}_blocked"])
 
 
 def test_mutate_inputs(oracle_mod):
