@@ -30,7 +30,14 @@ struct bief_handle {
   int has_matrix = 0;
   // working (scaled) matrix and change of variables
   double *d_dms = nullptr, *d_xms = nullptr, *d_dsc = nullptr;
-  float *d_xm32 = nullptr, *d_dm32 = nullptr;
+  // gather-ready layouts (32-node slices): records and binary32 segments
+  int *d_meta = nullptr, *d_rec_off = nullptr, *d_seg_off = nullptr, *d_seg_col = nullptr;
+  int2 *d_rec_idx = nullptr;
+  uchar2 *d_rec_slot = nullptr;
+  double2 *d_rec_c = nullptr;
+  float *d_seg_c = nullptr, *d_s32 = nullptr;
+  long long nrec = 0, nseg = 0;
+  int max_nnb = 0;
   // vectors
   double *d_x = nullptr, *d_b = nullptr, *d_bs = nullptr, *d_r = nullptr, *d_d0 = nullptr,
          *d_d1 = nullptr, *d_ad = nullptr, *d_t = nullptr;
@@ -122,15 +129,10 @@ void dispatch_mv(bief_handle *h, int td, bool sym, bool tr, const double *xm, co
 #undef MV_CASE
 }
 
-void *cg_kernel(int td, bool sym) {
-  if (sym) {
-    if (td == DIA_Q) return (void *)k_cg64<DIA_Q, true>;
-    if (td == DIA_I) return (void *)k_cg64<DIA_I, true>;
-    return (void *)k_cg64<DIA_0, true>;
-  }
-  if (td == DIA_Q) return (void *)k_cg64<DIA_Q, false>;
-  if (td == DIA_I) return (void *)k_cg64<DIA_I, false>;
-  return (void *)k_cg64<DIA_0, false>;
+void *cg_kernel(int td) {
+  if (td == DIA_Q) return (void *)k_cg64<DIA_Q>;
+  if (td == DIA_I) return (void *)k_cg64<DIA_I>;
+  return (void *)k_cg64<DIA_0>;
 }
 
 void *mixed_kernel(int td) {
@@ -143,8 +145,7 @@ void *mixed_kernel(int td) {
 // reduced for small meshes so that each thread has at least two nodes.
 int persistent_grid(int npoin, int nsm, int *out) {
   int best = 1 << 30;
-  void *ks[] = {cg_kernel(DIA_Q, true), cg_kernel(DIA_I, true), cg_kernel(DIA_0, true),
-                cg_kernel(DIA_Q, false), cg_kernel(DIA_I, false), cg_kernel(DIA_0, false),
+  void *ks[] = {cg_kernel(DIA_Q), cg_kernel(DIA_I), cg_kernel(DIA_0),
                 mixed_kernel(DIA_Q), mixed_kernel(DIA_I), mixed_kernel(DIA_0)};
   for (void *k : ks) {
     int bps = 0;
@@ -170,7 +171,6 @@ int ensure_matrix_buffers(bief_handle *h) {
   int st;
   if ((st = dalloc(&h->d_xm, 6 * ne))) return st;
   if ((st = dalloc(&h->d_xms, 6 * ne))) return st;
-  if ((st = dalloc(&h->d_xm32, 3 * ne))) return st;
   return BIEF_OK;
 }
 
@@ -194,7 +194,7 @@ int launch_coop(bief_handle *h, void *k, void *arg, cudaStream_t st) {
 // PRECD1 (precd1.f:88-158) into the working matrix; x scaled in place,
 // b_out = D*b_in.  Returns the working TYPDIA.
 int do_precd1(bief_handle *h, int precon, double *x, const double *b_in, double *b_out,
-              bool want32, int *td_work, cudaStream_t st) {
+              int *td_work, cudaStream_t st) {
   const int n = h->npoin;
   const int td_in = typdia_code(h->typdia);
   k_precd1_nodes<<<grid_for(n, h->nsm), 256, 0, st>>>(n, precon, td_in, h->d_dm, x, b_in, b_out,
@@ -202,8 +202,8 @@ int do_precd1(bief_handle *h, int precon, double *x, const double *b_in, double 
   h->launches++;
   const int ndiag = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
   if (ndiag) {
-    k_precd1_elems<<<grid_for(h->nelem, h->nsm), 256, 0, st>>>(
-        h->nelem, ndiag, h->d_ik, h->d_dsc, h->d_xm, h->d_xms, want32 ? h->d_xm32 : nullptr);
+    k_precd1_elems<<<grid_for(h->nelem, h->nsm), 256, 0, st>>>(h->nelem, ndiag, h->d_ik,
+                                                                h->d_dsc, h->d_xm, h->d_xms);
     h->launches++;
   }
   // TYPDIA after OM 'M=DMD' is 'Q' (unless '0'); PRECON divisible by 2
@@ -213,6 +213,33 @@ int do_precd1(bief_handle *h, int precon, double *x, const double *b_in, double 
   *td_work = td;
   CK(cudaGetLastError());
   return BIEF_OK;
+}
+
+// Records of the working operator xm (binary64 gather-ready layout).
+int build_records(bief_handle *h, const double *xm, cudaStream_t st) {
+  const int g = grid_for(h->npoin, h->nsm);
+  if (h->typext == 'Q')
+    k_build_rec<false><<<g, 256, 0, st>>>(h->npoin, h->nelem, h->d_ptr, h->d_ek, xm, h->d_rec_off,
+                                         h->d_rec_c);
+  else
+    k_build_rec<true><<<g, 256, 0, st>>>(h->npoin, h->nelem, h->d_ptr, h->d_ek, xm, h->d_rec_off,
+                                        h->d_rec_c);
+  h->launches++;
+  CK(cudaGetLastError());
+  return BIEF_OK;
+}
+
+Sell sell_of(const bief_handle *h) {
+  Sell S;
+  S.meta = h->d_meta;
+  S.rec_off = h->d_rec_off;
+  S.rec_idx = h->d_rec_idx;
+  S.rec_c = h->d_rec_c;
+  S.seg_off = h->d_seg_off;
+  S.seg_col = h->d_seg_col;
+  S.seg_c = h->d_seg_c;
+  S.s32 = h->d_s32;
+  return S;
 }
 
 int check_cfg(const bief_slvcfg *cfg, int *precon) {
@@ -273,12 +300,76 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
       ek[pos[v]++] = (e << 2) | k;
     }
 
+  // Sliced layouts (32-node slices).  Records: one per gather entry, with
+  // its two neighbour nodes.  Segments: the distinct neighbours of each
+  // node in order of first appearance among its entries; each record also
+  // gets the slots of its two neighbours for the binary32 assembly.
+  const int nsl = (npoin + 31) / 32;
+  std::vector<int> rec_off(nsl + 1, 0), seg_off(nsl + 1, 0), meta(npoin, 0), nnb(npoin, 0);
+  std::vector<int> nb_list;  // per node, consecutive
+  std::vector<int> nb_ptr(npoin + 1, 0);
+  std::vector<unsigned char> slot_a(3 * (size_t)nelem), slot_b(3 * (size_t)nelem);
+  int max_nnb = 0;
+  nb_list.reserve(7 * (size_t)npoin);
+  for (int i = 0; i < npoin; ++i) {
+    const size_t base = nb_list.size();
+    for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
+      const int e = ek[j] >> 2, k = ek[j] & 3;
+      const int va = ik[(size_t)((k + 1) % 3) * nelem + e];
+      const int vb = ik[(size_t)((k + 2) % 3) * nelem + e];
+      int sl[2];
+      const int v2[2] = {va, vb};
+      for (int q = 0; q < 2; ++q) {
+        size_t t = base;
+        while (t < nb_list.size() && nb_list[t] != v2[q]) ++t;
+        if (t == nb_list.size()) nb_list.push_back(v2[q]);
+        sl[q] = (int)(t - base);
+      }
+      slot_a[j] = (unsigned char)std::min(sl[0], 255);
+      slot_b[j] = (unsigned char)std::min(sl[1], 255);
+    }
+    nnb[i] = (int)(nb_list.size() - base);
+    nb_ptr[i + 1] = (int)nb_list.size();
+    max_nnb = std::max(max_nnb, nnb[i]);
+    const int d = ptr[i + 1] - ptr[i];
+    if (d > 0xffff || nnb[i] > 0x7fff) return BIEF_ERR_SIZE;
+    meta[i] = d | (nnb[i] << 16);
+  }
+  for (int sgi = 0; sgi < nsl; ++sgi) {
+    int wr = 0, ws = 0;
+    for (int i = 32 * sgi; i < std::min(npoin, 32 * sgi + 32); ++i) {
+      wr = std::max(wr, ptr[i + 1] - ptr[i]);
+      ws = std::max(ws, nnb[i]);
+    }
+    const long long r = (long long)rec_off[sgi] + 32LL * wr, q = (long long)seg_off[sgi] + 32LL * ws;
+    if (r > 0x7fffffffLL || q > 0x7fffffffLL) return BIEF_ERR_SIZE;
+    rec_off[sgi + 1] = (int)r;
+    seg_off[sgi + 1] = (int)q;
+  }
+  const size_t nrec = (size_t)rec_off[nsl], nseg = (size_t)seg_off[nsl];
+  std::vector<int2> rec_idx(nrec, make_int2(0, 0));
+  std::vector<uchar2> rec_slot(nrec, make_uchar2(0, 0));
+  std::vector<int> seg_col(nseg, 0);
+  for (int i = 0; i < npoin; ++i) {
+    const int rb = rec_off[i >> 5] + (i & 31), sb = seg_off[i >> 5] + (i & 31);
+    for (int m = 0; m < ptr[i + 1] - ptr[i]; ++m) {
+      const int j = ptr[i] + m, e = ek[j] >> 2, k = ek[j] & 3;
+      rec_idx[rb + 32 * m] = make_int2(ik[(size_t)((k + 1) % 3) * nelem + e],
+                                       ik[(size_t)((k + 2) % 3) * nelem + e]);
+      rec_slot[rb + 32 * m] = make_uchar2(slot_a[j], slot_b[j]);
+    }
+    for (int q = 0; q < nnb[i]; ++q) seg_col[sb + 32 * q] = nb_list[nb_ptr[i] + q];
+  }
+
   bief_handle *h = new (std::nothrow) bief_handle;
   if (!h) return BIEF_ERR_ARGS;
   h->dev = device;
   h->npoin = npoin;
   h->nelem = nelem;
   h->nelmax = nelmax;
+  h->nrec = (long long)nrec;
+  h->nseg = (long long)nseg;
+  h->max_nnb = max_nnb;
   int st = BIEF_OK;
   {
     DevGuard g(device);
@@ -295,12 +386,16 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
     if ((st = dalloc(&h->d_ptr, n + 1)) || (st = dalloc(&h->d_ek, 3 * ne)) ||
         (st = dalloc(&h->d_ik, 3 * ne)) || (st = dalloc(&h->d_dm, n)) ||
         (st = dalloc(&h->d_dms, n)) || (st = dalloc(&h->d_dsc, n)) ||
-        (st = dalloc(&h->d_dm32, n)) || (st = dalloc(&h->d_x, n)) || (st = dalloc(&h->d_b, n)) ||
+        (st = dalloc(&h->d_s32, n)) || (st = dalloc(&h->d_x, n)) || (st = dalloc(&h->d_b, n)) ||
         (st = dalloc(&h->d_bs, n)) || (st = dalloc(&h->d_r, n)) || (st = dalloc(&h->d_d0, n)) ||
         (st = dalloc(&h->d_d1, n)) || (st = dalloc(&h->d_ad, n)) || (st = dalloc(&h->d_t, n)) ||
         (st = dalloc(&h->d_z, n)) || (st = dalloc(&h->d_ri, n)) || (st = dalloc(&h->d_p0, n)) ||
         (st = dalloc(&h->d_p1, n)) || (st = dalloc(&h->d_q, n)) || (st = dalloc(&h->d_err, 1)) ||
-        (st = dalloc(&h->d_ctl, 1)))
+        (st = dalloc(&h->d_ctl, 1)) || (st = dalloc(&h->d_meta, n)) ||
+        (st = dalloc(&h->d_rec_off, (size_t)nsl + 1)) || (st = dalloc(&h->d_seg_off, (size_t)nsl + 1)) ||
+        (st = dalloc(&h->d_rec_idx, nrec)) || (st = dalloc(&h->d_rec_slot, nrec)) ||
+        (st = dalloc(&h->d_rec_c, nrec)) || (st = dalloc(&h->d_seg_col, nseg)) ||
+        (st = dalloc(&h->d_seg_c, nseg)))
       return fail(st);
     if ((st = persistent_grid(npoin, h->nsm, &h->G))) return fail(st);
     if ((st = dalloc(&h->d_part, 2 * (size_t)h->G + 2))) return fail(st);
@@ -312,6 +407,20 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
                              h->stream)) != cudaSuccess ||
         (e = cudaMemcpyAsync(h->d_ik, ik.data(), sizeof(int) * 3 * ne, cudaMemcpyHostToDevice,
                              h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_meta, meta.data(), sizeof(int) * n, cudaMemcpyHostToDevice,
+                             h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_rec_off, rec_off.data(), sizeof(int) * (nsl + 1),
+                             cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_seg_off, seg_off.data(), sizeof(int) * (nsl + 1),
+                             cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_rec_idx, rec_idx.data(), sizeof(int2) * nrec,
+                             cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_rec_slot, rec_slot.data(), sizeof(uchar2) * nrec,
+                             cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(h->d_seg_col, seg_col.data(), sizeof(int) * nseg,
+                             cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->d_seg_c, 0, sizeof(float) * nseg, h->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(h->d_rec_c, 0, sizeof(double2) * nrec, h->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(h->stream)) != cudaSuccess)
       return fail(cuda_fail(e, "mesh upload", __LINE__));
   }
@@ -324,9 +433,10 @@ int bief_destroy(bief_handle *h) {
   DevGuard g(h->dev);
   if (h->stream) cudaStreamSynchronize(h->stream);
   void *bufs[] = {h->d_ptr, h->d_ek, h->d_ik, h->d_dm, h->d_xm, h->d_dms, h->d_xms, h->d_dsc,
-                  h->d_xm32, h->d_dm32, h->d_x, h->d_b, h->d_bs, h->d_r, h->d_d0, h->d_d1,
+                  h->d_s32, h->d_x, h->d_b, h->d_bs, h->d_r, h->d_d0, h->d_d1,
                   h->d_ad, h->d_t, h->d_z, h->d_ri, h->d_p0, h->d_p1, h->d_q, h->d_part,
-                  h->d_ew, h->d_ctl, h->d_err};
+                  h->d_ew, h->d_ctl, h->d_err, h->d_meta, h->d_rec_off, h->d_seg_off,
+                  h->d_rec_idx, h->d_rec_slot, h->d_rec_c, h->d_seg_col, h->d_seg_c};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -411,25 +521,25 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   DevGuard g(h->dev);
   cudaStream_t s = (cudaStream_t)stream;
   const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
-  const bool sym = h->typext != 'Q';
   int td = typdia_code(h->typdia);
   const double *xm = h->d_xm, *da = h->d_dm;
   const double *bw = b;
   if (diag) {
-    if ((st = do_precd1(h, precon, x, b, h->d_bs, false, &td, s))) return st;
+    if ((st = do_precd1(h, precon, x, b, h->d_bs, &td, s))) return st;
     xm = h->d_xms;
     da = h->d_dms;
     bw = h->d_bs;
   }
+  if (h->typext == '0') {  // no off-diagonal terms: zero records
+    CK(cudaMemsetAsync(h->d_xms, 0, sizeof(double) * 3 * h->nelem, s));
+    xm = h->d_xms;
+  }
+  if ((st = build_records(h, xm, s))) return st;
   CgP P;
   P.npoin = h->npoin;
-  P.nelem = h->nelem;
   P.nitmax = cfg->nitmax;
   P.eps = cfg->eps;
-  P.ptr = h->d_ptr;
-  P.ek = h->d_ek;
-  P.ik = h->d_ik;
-  P.xm = xm;
+  P.S = sell_of(h);
   P.da = da;
   P.dsc = diag ? h->d_dsc : nullptr;
   P.x = x;
@@ -443,7 +553,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   P.timeout_ns = h->timeout_ns;
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
   CK(cudaEventRecord(h->ev[0], s));
-  if ((st = launch_coop(h, cg_kernel(td, sym), &P, s))) return st;
+  if ((st = launch_coop(h, cg_kernel(td), &P, s))) return st;
   CK(cudaEventRecord(h->ev[1], s));
   CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -493,48 +603,42 @@ int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b, int precon,
   if (precon == 0) precon = 1;
   if (precon < 0 || precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 || precon % 17 == 0)
     return BIEF_ERR_UNSUPPORTED;
+  if (h->max_nnb > MAX_NEIGHBOURS) return BIEF_ERR_SIZE;
   DevGuard g(h->dev);
   cudaStream_t s = (cudaStream_t)stream;
   const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
   int td = typdia_code(h->typdia), st;
   const double *xm = h->d_xm, *da = h->d_dm, *bw = b;
   if (diag) {
-    if ((st = do_precd1(h, precon, x, b, h->d_bs, true, &td, s))) return st;
+    if ((st = do_precd1(h, precon, x, b, h->d_bs, &td, s))) return st;
     xm = h->d_xms;
     da = h->d_dms;
     bw = h->d_bs;
-  } else {
-    k_to_f32<<<grid_for(3 * h->nelem, h->nsm), 256, 0, s>>>(3 * h->nelem, h->d_xm, h->d_xm32);
-    h->launches++;
   }
-  // binary32 row sums of the scaled operator (difference-form diagonal)
-  {
+  if ((st = build_records(h, xm, s))) return st;
+  {  // binary32 edge-assembled copy of the working operator
     const int gn = grid_for(h->npoin, h->nsm);
+#define SEG_ARGS                                                                              \
+  h->npoin, h->nelem, h->d_ptr, h->d_ek, xm, da, h->d_meta, h->d_rec_off, h->d_rec_slot, \
+      h->d_seg_off, h->d_seg_c, h->d_s32
     if (td == DIA_Q)
-      k_rowsum<DIA_Q><<<gn, 256, 0, s>>>(h->npoin, h->nelem, h->d_ptr, h->d_ek, h->d_ik, xm, da,
-                                         h->d_dm32);
+      k_build_seg32<DIA_Q><<<gn, 256, 0, s>>>(SEG_ARGS);
     else if (td == DIA_I)
-      k_rowsum<DIA_I><<<gn, 256, 0, s>>>(h->npoin, h->nelem, h->d_ptr, h->d_ek, h->d_ik, xm, da,
-                                         h->d_dm32);
+      k_build_seg32<DIA_I><<<gn, 256, 0, s>>>(SEG_ARGS);
     else
-      k_rowsum<DIA_0><<<gn, 256, 0, s>>>(h->npoin, h->nelem, h->d_ptr, h->d_ek, h->d_ik, xm, da,
-                                         h->d_dm32);
+      k_build_seg32<DIA_0><<<gn, 256, 0, s>>>(SEG_ARGS);
+#undef SEG_ARGS
     h->launches++;
+    CK(cudaGetLastError());
   }
   MixP P;
   P.npoin = h->npoin;
-  P.nelem = h->nelem;
   P.max_outer = max_outer;
   P.max_inner = max_inner;
   P.outer_tol = outer_tol;
   P.inner_tol = inner_tol;
-  P.ptr = h->d_ptr;
-  P.ek = h->d_ek;
-  P.ik = h->d_ik;
-  P.xm = xm;
+  P.S = sell_of(h);
   P.da = da;
-  P.xm32 = h->d_xm32;
-  P.s32 = h->d_dm32;
   P.dsc = diag ? h->d_dsc : nullptr;
   P.x = x;
   P.b = bw;

@@ -207,37 +207,67 @@ __device__ __forceinline__ T entry_product(int p, const int *__restrict__ ik,
   return add(mul(xa, vec(va)), mul(xb, vec(vb)));
 }
 
-// Shared-memory capacity of one gather tile, in entries per thread.
-constexpr int TILE_ENTRIES_PER_THREAD = 8;
+// EBE row product of node i straight from the element arrays: the node's
+// gather entries in ASSVEC order, each W term added left to right.
+template <typename T, bool SYM, bool TRANS, class V>
+__device__ __forceinline__ T ebe_row(int i, T acc, const int *__restrict__ ptr,
+                                     const int *__restrict__ ek, const int *__restrict__ ik,
+                                     const T *__restrict__ xm, int ne, V vec) {
+  const int j0 = __ldg(ptr + i), j1 = __ldg(ptr + i + 1);
+#pragma unroll 2
+  for (int j = j0; j < j1; ++j)
+    acc = add(acc, entry_product<T, SYM, TRANS, false>(__ldg(ek + j), ik, xm, ne, vec));
+  return acc;
+}
 
-// Gather product for a tile of nn <= blockDim.x consecutive nodes starting
-// at n0; thread t owns node n0+t.  All threads of the block call it.
-// The entries of the tile are contiguous in the gather index: every thread
-// computes entry products (strided, so index loads are coalesced and many
-// loads are in flight) into smW, then each owner adds its node's products
-// to acc in index order -- the same left-to-right sum ASSVEC performs.
-// Tiles with more entries than `cap` are processed in chunks, in order.
-template <typename T, bool SYM, bool TRANS, bool DIFF, class V>
-__device__ __forceinline__ T tile_gather(int n0, int nn, T acc, const int *__restrict__ ptr,
-                                         const int *__restrict__ ek, const int *__restrict__ ik,
-                                         const T *__restrict__ xm, int ne, V vec, T *smW,
-                                         int cap) {
-  const int t = threadIdx.x;
-  const int j0 = __ldg(ptr + n0), j1 = __ldg(ptr + n0 + nn);
-  int my0 = 0, my1 = 0;
-  if (t < nn) {
-    my0 = __ldg(ptr + n0 + t);
-    my1 = __ldg(ptr + n0 + t + 1);
+// ---------------------------------------------------------------------------
+// Gather-ready layouts, 32-node slices (sliced ELL): entry m of node i is
+// stored at off[i/32] + 32*m + i%32, so the 32 lanes of a warp that own the
+// 32 nodes of a slice read consecutive words.
+//
+// Records (binary64 GRACJG): per gather entry of node i, in ASSVEC order,
+// the two coefficients (XA(k,a), XA(k,b)) and the two node numbers (a, b).
+// The row product is then exactly the EBE W sum of ebe_row, read as a
+// coalesced stream plus two node gathers per entry.
+//
+// Segments (binary32 inner operator): per distinct neighbour j of node i,
+// in order of first appearance among the entries, the binary32 assembled
+// coefficient c_ij; product in difference form s_i y_i + sum c_ij (y_j-y_i).
+// ---------------------------------------------------------------------------
+struct Sell {
+  const int *meta;        // per node: gather entries | neighbours << 16
+  const int *rec_off;     // per slice: first record
+  const int2 *rec_idx;    // per record: (a, b)
+  const double2 *rec_c;   // per record: (XA(k,a), XA(k,b)) of the operator
+  const int *seg_off;     // per slice: first segment slot
+  const int *seg_col;     // per slot: neighbour
+  const float *seg_c;     // per slot: binary32 coefficient
+  const float *s32;       // per node: binary32 row sum
+};
+
+template <class V>
+__device__ __forceinline__ double rec_row(int i, double acc, const Sell &S, V vec) {
+  const int deg = __ldg(S.meta + i) & 0xffff;
+  const int base = __ldg(S.rec_off + (i >> 5)) + (i & 31);
+#pragma unroll 2
+  for (int m = 0; m < deg; ++m) {
+    const double2 c = __ldg(S.rec_c + base + 32 * m);
+    const int2 v = __ldg(S.rec_idx + base + 32 * m);
+    acc = add(acc, add(mul(c.x, vec(v.x)), mul(c.y, vec(v.y))));
   }
-  for (int c0 = j0; c0 < j1; c0 += cap) {
-    const int c1 = min(c0 + cap, j1);
-#pragma unroll 4
-    for (int j = c0 + t; j < c1; j += blockDim.x)
-      smW[j - c0] = entry_product<T, SYM, TRANS, DIFF>(__ldg(ek + j), ik, xm, ne, vec);
-    __syncthreads();
-    const int lo = max(my0, c0), hi = min(my1, c1);
-    for (int j = lo; j < hi; ++j) acc = add(acc, smW[j - c0]);
-    __syncthreads();
+  return acc;
+}
+
+template <class V>
+__device__ __forceinline__ float seg_row(int i, float yi, const Sell &S, V vec) {
+  const int nnb = __ldg(S.meta + i) >> 16;
+  const int base = __ldg(S.seg_off + (i >> 5)) + (i & 31);
+  float acc = mul(yi, __ldg(S.s32 + i));
+#pragma unroll 2
+  for (int m = 0; m < nnb; ++m) {
+    const int j = __ldg(S.seg_col + base + 32 * m);
+    const float c = __ldg(S.seg_c + base + 32 * m);
+    acc = add(acc, mul(c, sub(vec(j), yi)));
   }
   return acc;
 }
@@ -249,8 +279,10 @@ __device__ __forceinline__ T diag_term(T yi, const T *__restrict__ da, int i) {
   return T(0);                             // OV 'X=C' with 0 (mv0303.f:159)
 }
 
+// Node range of block b of a persistent kernel: [blk_lo(b), blk_lo(b+1)),
+// rounded down to multiples of 32 so that warps coincide with slices.
 __device__ __forceinline__ long long blk_lo(int b, int n, int nb) {
-  return (long long)b * n / nb;
+  return b >= nb ? (long long)n : (((long long)b * n / nb) & ~31LL);
 }
 
 }  // namespace bief

@@ -1,14 +1,17 @@
 // bief_kernels.cuh -- sm_100a kernels of the BIEF EBE P1 CG path.
 //
-//  k_matvec      MATVEC 'X=..AY' / 'X=..TAY' (matvec.f:316-380 ->
-//                mv0303.f:117-630 + assvec.f:88-93), node-centric gather.
-//  k_precd1_*    PRECD1 change of variables (precd1.f:88-158, om1111.f:559-600).
-//  k_cg64        GRACJG (gracjg.F:169-420) as ONE persistent cooperative
-//                kernel: two grid reductions per iteration, fused vector
-//                updates, convergence tested on the device.
-//  k_mixed       binary32 inner CG + binary64 refinement, one persistent kernel.
-//  k_wave_*      on-device MT01AA + MT02AA + ASSVEC diagonal assembly.
-//  k_coef_grad   per-element adjoint gradient -lambda_e^T K_e x_e.
+//  k_matvec       MATVEC 'X=..AY' / 'X=..TAY' (matvec.f:316-380 ->
+//                 mv0303.f:117-630 + assvec.f:88-93), node-centric gather
+//                 straight from the EBE arrays.
+//  k_precd1_*     PRECD1 change of variables (precd1.f:88-158, om1111.f:559-600).
+//  k_build_rec    binary64 gather-ready records of the scaled operator.
+//  k_build_seg32  binary32 edge-assembled copy of the scaled operator.
+//  k_cg64         GRACJG (gracjg.F:169-420) as ONE persistent cooperative
+//                 kernel: two grid reductions per iteration, fused vector
+//                 updates, convergence tested on the device.
+//  k_mixed        binary32 CG with binary64 reliable updates, one launch.
+//  k_wave_*       on-device MT01AA + MT02AA + ASSVEC diagonal assembly.
+//  k_coef_grad    per-element adjoint gradient -lambda_e^T K_e x_e.
 #pragma once
 
 #include "bief_device.cuh"
@@ -29,27 +32,21 @@ __global__ void __launch_bounds__(256) k_matvec(int npoin, int nelem, const int 
                                                 const double *__restrict__ da,
                                                 const double *__restrict__ y, double *x, int opc,
                                                 double c) {
-  __shared__ double smW[256 * TILE_ENTRIES_PER_THREAD];
-  const int T = blockDim.x, t = threadIdx.x;
-  for (int n0 = blockIdx.x * T; n0 < npoin; n0 += gridDim.x * T) {
-    const int nn = min(T, npoin - n0), i = n0 + t;
-    double acc = t < nn ? diag_term<TD>(__ldg(y + i), da, i) : 0.0;
-    acc = tile_gather<double, SYM, TRANS, false>(n0, nn, acc, ptr, ek, ik, xm, nelem,
-                                                 [&](int j) { return __ldg(y + j); }, smW,
-                                                 T * TILE_ENTRIES_PER_THREAD);
-    if (t < nn) {
-      // OS combination of MESH%T into X (matvec.f:369-380, :329-340)
-      double r;
-      switch (opc) {
-        case OP_AY: r = acc; break;
-        case OP_XPAY: r = add(x[i], acc); break;
-        case OP_MAY: r = -acc; break;
-        case OP_XMAY: r = sub(x[i], acc); break;
-        case OP_XPCAY: r = add(x[i], mul(c, acc)); break;
-        default: r = mul(c, acc); break;
-      }
-      x[i] = r;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    double acc = diag_term<TD>(__ldg(y + i), da, i);
+    acc = ebe_row<double, SYM, TRANS>(i, acc, ptr, ek, ik, xm, nelem,
+                                      [&](int j) { return __ldg(y + j); });
+    // OS combination of MESH%T into X (matvec.f:369-380, :329-340)
+    double r;
+    switch (opc) {
+      case OP_AY: r = acc; break;
+      case OP_XPAY: r = add(x[i], acc); break;
+      case OP_MAY: r = -acc; break;
+      case OP_XMAY: r = sub(x[i], acc); break;
+      case OP_XPCAY: r = add(x[i], mul(c, acc)); break;
+      default: r = mul(c, acc); break;
     }
+    x[i] = r;
   }
 }
 
@@ -82,11 +79,10 @@ __global__ void k_precd1_nodes(int npoin, int precon, int td_in, const double *_
 
 // Off-diagonal part of OM1111 'M=DMD' (om1111.f:589-600):
 // XM(e,1)*D(i2)*D(i1), XM(e,2)*D(i3)*D(i1), XM(e,3)*D(i3)*D(i2) (and the
-// same for columns 4..6 of 'Q' storage).  Optionally also writes the
-// binary32 copy used by the mixed-precision solver.
+// same for columns 4..6 of 'Q' storage).
 __global__ void k_precd1_elems(int nelem, int ndiag, const int *__restrict__ ik,
                                const double *__restrict__ dsc, const double *__restrict__ xm,
-                               double *xms, float *xm32) {
+                               double *xms) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
     const double d1 = dsc[ik[e]], d2 = dsc[ik[(size_t)nelem + e]],
                  d3 = dsc[ik[2 * (size_t)nelem + e]];
@@ -94,46 +90,71 @@ __global__ void k_precd1_elems(int nelem, int ndiag, const int *__restrict__ ik,
       const int cc = c % 3;
       const double da = cc == 0 ? d2 : d3;
       const double db = cc == 2 ? d2 : d1;
-      const double v = mul(mul(xm[(size_t)c * nelem + e], da), db);
-      xms[(size_t)c * nelem + e] = v;
-      if (xm32 && c < 3) xm32[(size_t)c * nelem + e] = (float)v;
+      xms[(size_t)c * nelem + e] = mul(mul(xm[(size_t)c * nelem + e], da), db);
     }
   }
 }
 
-// Row sums of the symmetric scaled operator in binary64, in ASSVEC order
-// (diagonal first, then XA(k,a)+XA(k,b) per W term), rounded to binary32:
-// the diagonal of the difference-form binary32 inner operator.
-template <int TD>
-__global__ void k_rowsum(int npoin, int nelem, const int *__restrict__ ptr,
-                         const int *__restrict__ ek, const int *__restrict__ ik,
-                         const double *__restrict__ xm, const double *__restrict__ da,
-                         float *s32) {
+// ---------------------------------------------------------------------------
+// Gather-ready layouts of the working operator (see Sell in bief_device.cuh)
+// ---------------------------------------------------------------------------
+template <bool SYM>
+__global__ void k_build_rec(int npoin, int nelem, const int *__restrict__ ptr,
+                            const int *__restrict__ ek, const double *__restrict__ xm,
+                            const int *__restrict__ rec_off, double2 *rec_c) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
-    double s = TD == DIA_Q ? da[i] : (TD == DIA_I ? 1.0 : 0.0);
-    for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
-      const int p = ek[j], e = p >> 2, k = p & 3;
-      const int a = (k == 2) ? 0 : k + 1;
-      const int b = (k == 0) ? 2 : k - 1;
-      s = add(s, add(xm[(size_t)(k + a - 1) * nelem + e], xm[(size_t)(k + b - 1) * nelem + e]));
+    const int j0 = ptr[i], deg = ptr[i + 1] - j0;
+    const int base = rec_off[i >> 5] + (i & 31);
+    for (int m = 0; m < deg; ++m) {
+      const int p = ek[j0 + m], e = p >> 2, k = p & 3;
+      const int a = (k == 2) ? 0 : k + 1, b = (k == 0) ? 2 : k - 1;
+      rec_c[base + 32 * m] = make_double2(xm[(size_t)xm_col<SYM>(k, a) * nelem + e],
+                                          xm[(size_t)xm_col<SYM>(k, b) * nelem + e]);
     }
+  }
+}
+
+// Binary32 edge-assembled operator: per node, slot coefficients and the row
+// sum accumulated in binary64 in gather order, rounded once (symmetric
+// storage).  rec_slot holds, per record, the slots of its two neighbours.
+constexpr int MAX_NEIGHBOURS = 64;
+
+template <int TD>
+__global__ void k_build_seg32(int npoin, int nelem, const int *__restrict__ ptr,
+                              const int *__restrict__ ek, const double *__restrict__ xm,
+                              const double *__restrict__ da, const int *__restrict__ meta,
+                              const int *__restrict__ rec_off,
+                              const uchar2 *__restrict__ rec_slot,
+                              const int *__restrict__ seg_off, float *seg_c, float *s32) {
+  double c64[MAX_NEIGHBOURS];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    const int j0 = ptr[i], deg = ptr[i + 1] - j0, nnb = meta[i] >> 16;
+    const int rb = rec_off[i >> 5] + (i & 31), sb = seg_off[i >> 5] + (i & 31);
+    for (int q = 0; q < nnb; ++q) c64[q] = 0.0;
+    double s = TD == DIA_Q ? da[i] : (TD == DIA_I ? 1.0 : 0.0);
+    for (int m = 0; m < deg; ++m) {
+      const int p = ek[j0 + m], e = p >> 2, k = p & 3;
+      const int a = (k == 2) ? 0 : k + 1, b = (k == 0) ? 2 : k - 1;
+      const double xa = xm[(size_t)(k + a - 1) * nelem + e];
+      const double xb = xm[(size_t)(k + b - 1) * nelem + e];
+      const uchar2 sl = rec_slot[rb + 32 * m];
+      c64[sl.x] = add(c64[sl.x], xa);
+      c64[sl.y] = add(c64[sl.y], xb);
+      s = add(s, add(xa, xb));
+    }
+    for (int q = 0; q < nnb; ++q) seg_c[sb + 32 * q] = (float)c64[q];
     s32[i] = (float)s;
   }
-}
-
-__global__ void k_to_f32(int n, const double *__restrict__ a, float *b) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    b[i] = (float)a[i];
 }
 
 // ---------------------------------------------------------------------------
 // GRACJG as a persistent kernel.
 // ---------------------------------------------------------------------------
 struct CgP {
-  int npoin, nelem, nitmax;
+  int npoin, nitmax;
   double eps;
-  const int *ptr, *ek, *ik;
-  const double *xm, *da;  // working (scaled) matrix
+  Sell S;                 // records of the working (scaled) operator
+  const double *da;       // working diagonal
   const double *dsc;      // change of variables to undo (nullptr: none)
   double *x;
   const double *b;
@@ -143,10 +164,8 @@ struct CgP {
   long long timeout_ns;
 };
 
-template <int TD, bool SYM>
+template <int TD>
 __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
-  __shared__ double smW[CG_THREADS * TILE_ENTRIES_PER_THREAD];
-  constexpr int CAP = CG_THREADS * TILE_ENTRIES_PER_THREAD;
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -182,16 +201,12 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
 
   // R = A X - B (gracjg.F:213-216)
   s = 0.0;
-  for (int n0 = lo; n0 < hi; n0 += T) {
-    const int nn = min(T, hi - n0), i = n0 + t;
-    double acc = t < nn ? diag_term<TD>(x[i], da, i) : 0.0;
-    acc = tile_gather<double, SYM, false, false>(n0, nn, acc, P.ptr, P.ek, P.ik, P.xm, P.nelem,
-                                                 [&](int j) { return x[j]; }, smW, CAP);
-    if (t < nn) {
-      const double ri = sub(acc, b[i]);
-      r[i] = ri;
-      s = add(s, mul(ri, ri));
-    }
+  for (int i = lo + t; i < hi; i += T) {
+    double acc = diag_term<TD>(x[i], da, i);
+    acc = rec_row(i, acc, P.S, [&](int j) { return x[j]; });
+    const double ri = sub(acc, b[i]);
+    r[i] = ri;
+    s = add(s, mul(ri, ri));
   }
   if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
   double rmrm = red, rmgm = rmrm;
@@ -201,20 +216,13 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
   // D = G (= R), AD = A D, DAD, RO (gracjg.F:248-261)
   double *cur = P.d0, *nxt = P.d1;
   s = 0.0;
-  for (int n0 = lo; n0 < hi; n0 += T) {
-    const int nn = min(T, hi - n0), i = n0 + t;
-    double di = 0.0, acc = 0.0;
-    if (t < nn) {
-      di = r[i];
-      cur[i] = di;
-      acc = diag_term<TD>(di, da, i);
-    }
-    acc = tile_gather<double, SYM, false, false>(n0, nn, acc, P.ptr, P.ek, P.ik, P.xm, P.nelem,
-                                                 [&](int j) { return r[j]; }, smW, CAP);
-    if (t < nn) {
-      ad[i] = acc;
-      s = add(s, mul(di, acc));
-    }
+  for (int i = lo + t; i < hi; i += T) {
+    const double di = r[i];
+    cur[i] = di;
+    double acc = diag_term<TD>(di, da, i);
+    acc = rec_row(i, acc, P.S, [&](int j) { return r[j]; });
+    ad[i] = acc;
+    s = add(s, mul(di, acc));
   }
   if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
   double dad = red;
@@ -245,21 +253,13 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
     // recomputes R(j)+BETA*D(j) from the previous direction, which gives
     // the same bits as the owner's value; the owner also stores it.
     s = 0.0;
-    for (int n0 = lo; n0 < hi; n0 += T) {
-      const int nn = min(T, hi - n0), i = n0 + t;
-      double di = 0.0, acc = 0.0;
-      if (t < nn) {
-        di = add(r[i], mul(beta, cur[i]));
-        nxt[i] = di;
-        acc = diag_term<TD>(di, da, i);
-      }
-      acc = tile_gather<double, SYM, false, false>(
-          n0, nn, acc, P.ptr, P.ek, P.ik, P.xm, P.nelem,
-          [&](int j) { return add(r[j], mul(beta, cur[j])); }, smW, CAP);
-      if (t < nn) {
-        ad[i] = acc;
-        s = add(s, mul(di, acc));
-      }
+    for (int i = lo + t; i < hi; i += T) {
+      const double di = add(r[i], mul(beta, cur[i]));
+      nxt[i] = di;
+      double acc = diag_term<TD>(di, da, i);
+      acc = rec_row(i, acc, P.S, [&](int j) { return add(r[j], mul(beta, cur[j])); });
+      ad[i] = acc;
+      s = add(s, mul(di, acc));
     }
     if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
     dad = red;
@@ -277,21 +277,21 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
 }
 
 // ---------------------------------------------------------------------------
-// Mixed precision, one launch: a binary32 CG on the binary32 copy of the
-// scaled EBE operator (binary32 vectors, products and dot accumulation)
-// whose correction z is folded into the binary64 solution whenever the
-// recursive binary32 residual has dropped by inner_tol against the last
-// true residual (or looks converged).  Each such update recomputes the true
-// residual b - A x in binary64 with the binary64 operator, tests it against
-// outer_tol and restarts the binary32 residual from it while keeping the
-// search direction (beta from the recursive residual).
+// Mixed precision, one launch: a binary32 CG on the binary32 edge-assembled
+// copy of the scaled operator (binary32 vectors, products and dot
+// accumulation) whose correction z is folded into the binary64 solution
+// whenever the recursive binary32 residual has dropped by inner_tol against
+// the last true residual (or looks converged).  Each such update
+// recomputes the true residual b - A x in binary64 with the binary64
+// operator, tests it against outer_tol and restarts the binary32 residual
+// from it while keeping the search direction (beta from the recursive
+// residual).
 // ---------------------------------------------------------------------------
 struct MixP {
-  int npoin, nelem, max_outer, max_inner;
+  int npoin, max_outer, max_inner;
   double outer_tol, inner_tol;
-  const int *ptr, *ek, *ik;
-  const double *xm, *da;  // scaled binary64 operator
-  const float *xm32, *s32;  // binary32 off-diagonals, binary32 row sums
+  Sell S;                 // binary64 records + binary32 segments
+  const double *da;
   const double *dsc;
   double *x;
   const double *b;
@@ -303,9 +303,6 @@ struct MixP {
 
 template <int TD>
 __global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
-  __shared__ double smW[CG_THREADS * TILE_ENTRIES_PER_THREAD];
-  float *smW32 = reinterpret_cast<float *>(smW);
-  constexpr int CAP = CG_THREADS * TILE_ENTRIES_PER_THREAD;
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -341,26 +338,21 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
   const double otol = mul(xl, mul(P.outer_tol, P.outer_tol));
   const float itol2 = (float)mul(P.inner_tol, P.inner_tol);
 
-  // true residual r = b - A x (binary64), r32 = (float)r; returns false on
-  // a barrier timeout.  rr and rho receive ||r||^2 and ||r32||^2.
+  // true residual r = b - A x (binary64), r32 = (float)r; rr and rho receive
+  // ||r||^2 and ||r32||^2; false on a barrier timeout.
   double rr;
   float rho;
   auto true_residual = [&]() -> bool {
     double sd = 0.0;
     float s32 = 0.0f;
-    for (int n0 = lo; n0 < hi; n0 += T) {
-      const int nn = min(T, hi - n0), i = n0 + t;
-      double acc = t < nn ? diag_term<TD>(x[i], P.da, i) : 0.0;
-      acc = tile_gather<double, true, false, false>(n0, nn, acc, P.ptr, P.ek, P.ik, P.xm,
-                                                    P.nelem, [&](int j) { return x[j]; }, smW,
-                                                    CAP);
-      if (t < nn) {
-        const double rv = sub(b[i], acc);
-        sd = add(sd, mul(rv, rv));
-        const float r32 = (float)rv;
-        ri[i] = r32;
-        s32 = add(s32, mul(r32, r32));
-      }
+    for (int i = lo + t; i < hi; i += T) {
+      double acc = diag_term<TD>(x[i], P.da, i);
+      acc = rec_row(i, acc, P.S, [&](int j) { return x[j]; });
+      const double rv = sub(b[i], acc);
+      sd = add(sd, mul(rv, rv));
+      const float r32 = (float)rv;
+      ri[i] = r32;
+      s32 = add(s32, mul(r32, r32));
     }
     return grid_reduce<1, 1>(P.ctl, P.part, P.timeout_ns, &sd, &s32, &rr, &rho);
   };
@@ -375,26 +367,18 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
   for (;;) {
     // p = r + beta p, evaluated where needed; q = A32 p; p.q
     sf = 0.0f;
-    for (int n0 = lo; n0 < hi; n0 += T) {
-      const int nn = min(T, hi - n0), i = n0 + t;
-      float pi = 0.0f, acc = 0.0f;
-      if (t < nn) {
-        pi = first ? ri[i] : add(ri[i], mul(beta, cur[i]));
-        nxt[i] = pi;
-        acc = mul(pi, P.s32[i]);
+    for (int i = lo + t; i < hi; i += T) {
+      float pi, acc;
+      if (first) {
+        pi = ri[i];
+        acc = seg_row(i, pi, P.S, [&](int k) { return ri[k]; });
+      } else {
+        pi = add(ri[i], mul(beta, cur[i]));
+        acc = seg_row(i, pi, P.S, [&](int k) { return add(ri[k], mul(beta, cur[k])); });
       }
-      if (first)
-        acc = tile_gather<float, true, false, true>(n0, nn, acc, P.ptr, P.ek, P.ik, P.xm32,
-                                                    P.nelem, [&](int k) { return ri[k]; }, smW32,
-                                                    2 * CAP);
-      else
-        acc = tile_gather<float, true, false, true>(
-            n0, nn, acc, P.ptr, P.ek, P.ik, P.xm32, P.nelem,
-            [&](int k) { return add(ri[k], mul(beta, cur[k])); }, smW32, 2 * CAP);
-      if (t < nn) {
-        q[i] = acc;
-        sf = add(sf, mul(pi, acc));
-      }
+      nxt[i] = pi;
+      q[i] = acc;
+      sf = add(sf, mul(pi, acc));
     }
     float pq;
     if (!grid_reduce<0, 1>(P.ctl, P.part, P.timeout_ns, nullptr, &sf, nullptr, &pq)) return;

@@ -324,7 +324,13 @@ static float tree32(const float *v, int nt)
     return wsum[0];
 }
 
-static long long blk_lo(int b, int n, int nb) { return (long long)b * n / nb; }
+/* Node range of block b: [blk_lo(b), blk_lo(b+1)), starts rounded down to
+ * a multiple of 32 so that every warp's nodes lie in one 32-node slice. */
+static long long blk_lo(int b, int n, int nb)
+{
+    if (b >= nb) return n;
+    return ((long long)b * n / nb) & ~31LL;
+}
 
 /* The device kernels' dot order: block b owns nodes
  * [b*n/nb, (b+1)*n/nb); thread t sums nodes lo+t, lo+t+nt, ... left to
@@ -555,51 +561,103 @@ int orc_solve(int npoin, int nelem, const int *ik0, const int *ik1,
 /* mixed precision (no reference counterpart)                           */
 /* ------------------------------------------------------------------ */
 
-/* binary32 EBE product q = A32 p in difference form:
- *   q_i = s_i p_i + sum over the W terms of node i of
- *         XA(k,a) (p_a - p_i) + XA(k,b) (p_b - p_i)
- * with s_i the binary64 row sum (diagonal + every off-diagonal term of row
- * i, in ASSVEC order) rounded once to binary32.  Rounding the coefficients
- * then leaves constant vectors exact, so the small mass-dominated
- * eigenvalues of the wave operator survive the binary32 copy.  Per-node
- * summation order as ASSVEC (diagonal term first, then local point 1, 2, 3
- * contributions in element order). */
-static void mv32_sym(int npoin, int nelem, const int *ik0, const int *ik1,
-                     const int *ik2, const float *s32, const float *xm,
-                     const float *p, float *q, float *w)
+/* Node -> (element, local point) gather lists in ASSVEC order (local point
+ * outer, element inner), the order in which ASSVEC adds into each node. */
+static int build_gather(int npoin, int nelem, const int *ik0, const int *ik1,
+                        const int *ik2, int **ptr_out, int **ek_out)
 {
-    const float *m12 = xm, *m13 = xm + nelem, *m23 = xm + 2 * (size_t)nelem;
-    float *w1 = w, *w2 = w + nelem, *w3 = w + 2 * (size_t)nelem;
-    for (int e = 0; e < nelem; ++e) {
-        float p1 = p[ik0[e]], p2 = p[ik1[e]], p3 = p[ik2[e]];
-        w1[e] = m12[e] * (p2 - p1) + m13[e] * (p3 - p1);
-        w2[e] = m23[e] * (p3 - p2) + m12[e] * (p1 - p2);
-        w3[e] = m13[e] * (p1 - p3) + m23[e] * (p2 - p3);
-    }
-    for (int i = 0; i < npoin; ++i) q[i] = p[i] * s32[i];
-    for (int e = 0; e < nelem; ++e) q[ik0[e]] = q[ik0[e]] + w1[e];
-    for (int e = 0; e < nelem; ++e) q[ik1[e]] = q[ik1[e]] + w2[e];
-    for (int e = 0; e < nelem; ++e) q[ik2[e]] = q[ik2[e]] + w3[e];
+    int *ptr = (int *)calloc((size_t)npoin + 1, sizeof(int));
+    int *ek = (int *)malloc(sizeof(int) * 3 * (size_t)nelem);
+    int *pos = (int *)malloc(sizeof(int) * (size_t)npoin);
+    if (!ptr || !ek || !pos) { free(ptr); free(ek); free(pos); return ORC_ERR_ARGS; }
+    const int *ik[3] = {ik0, ik1, ik2};
+    for (int k = 0; k < 3; ++k)
+        for (int e = 0; e < nelem; ++e) ptr[ik[k][e] + 1]++;
+    for (int i = 0; i < npoin; ++i) ptr[i + 1] += ptr[i];
+    for (int i = 0; i < npoin; ++i) pos[i] = ptr[i];
+    for (int k = 0; k < 3; ++k)
+        for (int e = 0; e < nelem; ++e) ek[pos[ik[k][e]]++] = (e << 2) | k;
+    free(pos);
+    *ptr_out = ptr;
+    *ek_out = ek;
+    return ORC_OK;
 }
 
-/* binary64 row sums of a symmetric EBE operator, in ASSVEC order:
- * s_i = diag_i + sum over the W terms of node i of (XA(k,a) + XA(k,b)). */
-static void rowsum64_sym(int npoin, int nelem, const int *ik0, const int *ik1,
-                         const int *ik2, const double *da, char typdia,
-                         const double *xm, double *s, double *w)
+/* Binary32 edge (segment) form of a symmetric EBE operator, built the way
+ * the device builds it: for node i, scan its gather entries in ASSVEC
+ * order; each entry (element e, local point k) contributes XA(k,a) to the
+ * neighbour a = IKLE(e,(k+1) mod 3) and XA(k,b) to b = IKLE(e,(k+2) mod 3)
+ * (the per-edge assembly ASSEX3 performs for segment storage).  Neighbours
+ * get slots in order of first appearance; slot coefficients and the row sum
+ * s_i = diag_i + sum of (XA(k,a) + XA(k,b)) are accumulated in binary64 in
+ * scan order and rounded once to binary32. */
+typedef struct {
+    int npoin;
+    int *nptr;    /* npoin+1: slot range of each node */
+    int *col;     /* neighbour of each slot */
+    float *val;   /* binary32 coefficient of each slot */
+    float *s32;   /* binary32 row sums */
+} seg32;
+
+static void seg32_free(seg32 *g)
 {
-    const double *m12 = xm, *m13 = xm + nelem, *m23 = xm + 2 * (size_t)nelem;
-    double *w1 = w, *w2 = w + nelem, *w3 = w + 2 * (size_t)nelem;
-    for (int e = 0; e < nelem; ++e) {
-        w1[e] = m12[e] + m13[e];
-        w2[e] = m23[e] + m12[e];
-        w3[e] = m13[e] + m23[e];
+    free(g->nptr); free(g->col); free(g->val); free(g->s32);
+}
+
+static int seg32_build(int npoin, int nelem, const int *ik0, const int *ik1,
+                       const int *ik2, const int *ptr, const int *ek,
+                       const double *da, char typdia, const double *xm,
+                       seg32 *g)
+{
+    const int *ik[3] = {ik0, ik1, ik2};
+    const double *m[3] = {xm, xm + nelem, xm + 2 * (size_t)nelem};
+    size_t cap = 2 * (size_t)ptr[npoin] + 1;
+    g->npoin = npoin;
+    g->nptr = (int *)malloc(sizeof(int) * ((size_t)npoin + 1));
+    g->col = (int *)malloc(sizeof(int) * cap);
+    g->val = (float *)malloc(sizeof(float) * cap);
+    g->s32 = (float *)malloc(sizeof(float) * (size_t)npoin);
+    double *c64 = (double *)malloc(sizeof(double) * cap);
+    if (!g->nptr || !g->col || !g->val || !g->s32 || !c64) { free(c64); return ORC_ERR_ARGS; }
+    size_t top = 0;
+    for (int i = 0; i < npoin; ++i) {
+        size_t base = top;
+        g->nptr[i] = (int)base;
+        double srow = typdia == 'Q' ? da[i] : (typdia == 'I' ? 1.0 : 0.0);
+        for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
+            int e = ek[j] >> 2, k = ek[j] & 3;
+            int a = (k + 1) % 3, b = (k + 2) % 3;
+            int v[2] = {ik[a][e], ik[b][e]};
+            double x[2] = {m[k + a - 1][e], m[k + b - 1][e]};
+            for (int q = 0; q < 2; ++q) {
+                size_t sl = base;
+                while (sl < top && g->col[sl] != v[q]) ++sl;
+                if (sl == top) { g->col[top] = v[q]; c64[top] = 0.0; ++top; }
+                c64[sl] = c64[sl] + x[q];
+            }
+            srow = srow + (x[0] + x[1]);
+        }
+        for (size_t sl = base; sl < top; ++sl) g->val[sl] = (float)c64[sl];
+        g->s32[i] = (float)srow;
     }
-    for (int i = 0; i < npoin; ++i)
-        s[i] = typdia == 'Q' ? da[i] : (typdia == 'I' ? 1.0 : 0.0);
-    for (int e = 0; e < nelem; ++e) s[ik0[e]] = s[ik0[e]] + w1[e];
-    for (int e = 0; e < nelem; ++e) s[ik1[e]] = s[ik1[e]] + w2[e];
-    for (int e = 0; e < nelem; ++e) s[ik2[e]] = s[ik2[e]] + w3[e];
+    g->nptr[npoin] = (int)top;
+    free(c64);
+    return ORC_OK;
+}
+
+/* q = A32 p in difference form: q_i = s_i p_i + sum over slots of
+ * c (p_j - p_i), slots in order.  Rounding the coefficients then leaves
+ * constant vectors exact, so the small mass-dominated eigenvalues of the
+ * wave operator survive the binary32 copy. */
+static void seg32_mv(const seg32 *g, const float *p, float *q)
+{
+    for (int i = 0; i < g->npoin; ++i) {
+        float pi = p[i];
+        float acc = pi * g->s32[i];
+        for (int sl = g->nptr[i]; sl < g->nptr[i + 1]; ++sl)
+            acc = acc + g->val[sl] * (p[g->col[sl]] - pi);
+        q[i] = acc;
+    }
 }
 
 /* Mixed-precision solve (the device kernel's exact operation order):
@@ -631,19 +689,19 @@ int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
     double *r = (double *)malloc(sizeof(double) * n);
     double *t = (double *)malloc(sizeof(double) * n);
     double *w = (double *)malloc(sizeof(double) * 3 * ne + 1);
-    float *xm32 = (float *)malloc(sizeof(float) * 3 * ne);
-    float *dm32 = (float *)malloc(sizeof(float) * n);
     float *z = (float *)malloc(sizeof(float) * n);
     float *ri = (float *)malloc(sizeof(float) * n);
     float *p = (float *)malloc(sizeof(float) * n);
     float *q = (float *)malloc(sizeof(float) * n);
-    float *w32 = (float *)malloc(sizeof(float) * 3 * ne + 1);
+    int *gptr = NULL, *gek = NULL;
+    seg32 g = {0, NULL, NULL, NULL, NULL};
     int st = ORC_OK, outer = 0, inner = 0, diag = 0;
     double xl = 0.0, rr = 0.0, otol = 0.0;
     float rho = 0.0f, rmax = 0.0f, itol2 = 0.0f;
     char typdia = typdia_in;
-    if (!dm || !xm || !bs || !d || !r || !t || !w || !xm32 || !dm32 || !z ||
-        !ri || !p || !q || !w32) { st = ORC_ERR_ARGS; goto done; }
+    if (!dm || !xm || !bs || !d || !r || !t || !w || !z || !ri || !p || !q) {
+        st = ORC_ERR_ARGS; goto done;
+    }
     memcpy(dm, dm_in, sizeof(double) * n);
     memcpy(xm, xm_in, sizeof(double) * 3 * ne);
     memcpy(bs, b, sizeof(double) * n);
@@ -654,9 +712,9 @@ int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
                         xm, nelem, typext, bs, d);
         if (st) goto done;
     }
-    for (size_t k = 0; k < 3 * ne; ++k) xm32[k] = (float)xm[k];
-    rowsum64_sym(npoin, nelem, ik0, ik1, ik2, dm, typdia, xm, t, w);
-    for (size_t i = 0; i < n; ++i) dm32[i] = (float)t[i];
+    if ((st = build_gather(npoin, nelem, ik0, ik1, ik2, &gptr, &gek))) goto done;
+    if ((st = seg32_build(npoin, nelem, ik0, ik1, ik2, gptr, gek, dm, typdia, xm, &g)))
+        goto done;
 
     xl = orc_dot_blocked(npoin, bs, bs, nb, nt);
     if (sqrt(xl) < 1.0e-15) {
@@ -685,7 +743,7 @@ int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
     rmax = rho;
     for (size_t i = 0; i < n; ++i) { z[i] = 0.0f; p[i] = ri[i]; }
     for (;;) {
-        mv32_sym(npoin, nelem, ik0, ik1, ik2, dm32, xm32, p, q, w32);
+        seg32_mv(&g, p, q);
         float pq = dot_blocked32(npoin, p, q, nb, nt);
         if (!(pq > 0.0f)) { st = isnan(pq) ? ORC_ERR_NAN : ORC_ERR_BREAKDOWN; goto fin; }
         float alpha = rho / pq;
@@ -717,6 +775,7 @@ fin:
     if (relres_out) *relres_out = sqrt(rr / xl);
 done:
     free(dm); free(xm); free(bs); free(d); free(r); free(t); free(w);
-    free(xm32); free(dm32); free(z); free(ri); free(p); free(q); free(w32);
+    free(z); free(ri); free(p); free(q); free(gptr); free(gek);
+    seg32_free(&g);
     return st;
 }
