@@ -30,20 +30,22 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False):
+def build(force=False, verbose=False, defines=(), out=None):
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [
         os.path.join(ROOT, "include", "bief_b200.h"), __file__]
-    if not force and not _stale(LIB, deps):
-        return LIB
+    target = out or LIB
+    if not force and not _stale(target, deps):
+        return target
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-I", os.path.join(ROOT, "include"), "-o", LIB, *srcs]
+           "-I", os.path.join(ROOT, "include"), *[f"-D{d}" for d in defines], "-o", target,
+           *srcs]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
-    return LIB
+    return target
 
 
 if __name__ == "__main__":

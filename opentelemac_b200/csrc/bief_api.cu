@@ -398,7 +398,7 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
         (st = dalloc(&h->d_seg_c, nseg)))
       return fail(st);
     if ((st = persistent_grid(npoin, h->nsm, &h->G))) return fail(st);
-    if ((st = dalloc(&h->d_part, 2 * (size_t)h->G + 2))) return fail(st);
+    if ((st = dalloc(&h->d_part, 4 * (size_t)h->G + 4))) return fail(st);
     if ((e = cudaMallocHost((void **)&h->h_ctl, sizeof(Ctl))) != cudaSuccess)
       return fail(cuda_fail(e, "cudaMallocHost", __LINE__));
     if ((e = cudaMemcpyAsync(h->d_ptr, ptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice,

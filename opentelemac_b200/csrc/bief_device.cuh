@@ -66,34 +66,36 @@ __device__ __forceinline__ unsigned long long global_ns() {
 
 // Control block of one persistent solve (device memory, zeroed per launch).
 struct Ctl {
-  unsigned int count;  // barrier arrivals
-  unsigned int gen;    // barrier generation
-  int status;          // final status (written by block 0) or error
-  int nit;             // iterations (CG) / total inner iterations (mixed)
-  int relat;           // 1: relative test, 0: absolute (||B||^2 < 1)
-  int outer;           // mixed: outer refinement steps
-  int pad0, pad1;
-  double red[4];       // reduction results published by the last block
-  double relres;       // SQRT(RMRM/XL) at exit
+  unsigned long long arrivals;  // grid-barrier arrivals, never reset in a launch
+  int status;                   // final status (written by block 0) or error
+  int nit;                      // iterations (CG) / total inner iterations (mixed)
+  int relat;                    // 1: relative test, 0: absolute (||B||^2 < 1)
+  int outer;                    // mixed: outer refinement steps
+  double relres;                // SQRT(RMRM/XL) at exit
 };
 
 // Grid-wide reduction + barrier.  Each block reduces its thread partials
-// with block_tree (ND binary64 values, NF binary32 values), thread 0 stores
-// them and arrives on the counter; the last block to arrive sums the block
-// partials in block order (thread t: partials t, t+T, ...; then block_tree),
-// publishes the totals and advances the generation; the other blocks wait
-// for the generation with a bounded spin (globaltimer), after which they
-// record ST_TIMEOUT and return false instead of hanging.
+// with block_tree (ND binary64 values, NF binary32 values); thread 0 stores
+// them in this barrier's half of `part` (two halves used alternately, so a
+// block that runs ahead never overwrites partials another block may still
+// read) and arrives on a monotonic counter.  The k-th barrier of a launch
+// is complete when the counter reaches k*G.  Every block then sums the G
+// block partials in block order (thread t: partials t, t+T, ...; then
+// block_tree), so all blocks obtain the same bits without a second round
+// trip.  The wait is bounded (globaltimer): on timeout the block records
+// ST_TIMEOUT and returns false instead of hanging.
+// `nbar` counts this block's barriers (uniform across the block).
 template <int ND, int NF>
-__device__ __noinline__ bool grid_reduce(Ctl *ctl, double *part, long long timeout_ns,
-                                         const double *vd, const float *vf,
-                                         double *od, float *of) {
+__device__ __noinline__ bool grid_reduce(Ctl *ctl, double *part, long long timeout_ns, int &nbar,
+                                         const double *vd, const float *vf, double *od,
+                                         float *of) {
   __shared__ double smd[32];
   __shared__ float smf[32];
-  __shared__ int s_last, s_err;
-  __shared__ unsigned s_gen;
+  __shared__ int s_err;
   constexpr int NV = ND + NF;
   const int G = gridDim.x, T = blockDim.x, t = threadIdx.x;
+  const unsigned long long k = (unsigned long long)(++nbar);
+  double *buf = part + (size_t)(k & 1) * (size_t)G * NV;
   double bd[ND > 0 ? ND : 1];
   float bf[NF > 0 ? NF : 1];
 #pragma unroll
@@ -102,65 +104,60 @@ __device__ __noinline__ bool grid_reduce(Ctl *ctl, double *part, long long timeo
   for (int q = 0; q < NF; ++q) bf[q] = block_tree(vf[q], smf);
   if (t == 0) {
 #pragma unroll
-    for (int q = 0; q < ND; ++q) part[(size_t)blockIdx.x * NV + q] = bd[q];
+    for (int q = 0; q < ND; ++q) buf[(size_t)blockIdx.x * NV + q] = bd[q];
 #pragma unroll
-    for (int q = 0; q < NF; ++q) part[(size_t)blockIdx.x * NV + ND + q] = (double)bf[q];
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(ctl->gen), cnt(ctl->count);
-    unsigned g0 = gen.load(cuda::memory_order_relaxed);
-    unsigned a = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
-    s_last = (a == (unsigned)(G - 1));
-    s_gen = g0;
-    s_err = 0;
-  }
-  __syncthreads();
-  if (s_last) {
-#pragma unroll
-    for (int q = 0; q < ND; ++q) {
-      double acc = 0.0;
-      for (int k = t; k < G; k += T) acc = add(acc, __ldcg(part + (size_t)k * NV + q));
-      double tot = block_tree(acc, smd);
-      if (t == 0) ctl->red[q] = tot;
-    }
-#pragma unroll
-    for (int q = 0; q < NF; ++q) {
-      float acc = 0.0f;
-      for (int k = t; k < G; k += T) acc = add(acc, (float)__ldcg(part + (size_t)k * NV + ND + q));
-      float tot = block_tree(acc, smf);
-      if (t == 0) ctl->red[ND + q] = (double)tot;
-    }
-    if (t == 0) {
-      cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(ctl->gen), cnt(ctl->count);
-      cnt.store(0u, cuda::memory_order_relaxed);
-      gen.fetch_add(1u, cuda::memory_order_release);
-    }
-  } else if (t == 0) {
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(ctl->gen);
+    for (int q = 0; q < NF; ++q) buf[(size_t)blockIdx.x * NV + ND + q] = (double)bf[q];
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> cnt(ctl->arrivals);
+    cnt.fetch_add(1ull, cuda::memory_order_release);
+    const unsigned long long target = k * (unsigned long long)G;
     const unsigned long long t0 = global_ns();
-    unsigned ns = 32;
-    while (gen.load(cuda::memory_order_acquire) == s_gen) {
+    s_err = 0;
+    while (cnt.load(cuda::memory_order_acquire) < target) {
       if ((long long)(global_ns() - t0) > timeout_ns) {
         s_err = 1;
         atomicExch(&ctl->status, (int)ST_TIMEOUT);
         break;
       }
-      __nanosleep(ns);
-      if (ns < 256) ns <<= 1;
+      __nanosleep(20);
     }
   }
   __syncthreads();
   if (s_err) return false;
 #pragma unroll
-  for (int q = 0; q < ND; ++q) od[q] = __ldcg(&ctl->red[q]);
+  for (int q = 0; q < ND; ++q) {
+    double acc = 0.0;
+    for (int b = t; b < G; b += T) acc = add(acc, __ldcg(buf + (size_t)b * NV + q));
+    od[q] = block_tree(acc, smd);
+  }
 #pragma unroll
-  for (int q = 0; q < NF; ++q) of[q] = (float)__ldcg(&ctl->red[ND + q]);
-  if (__ldcg(&ctl->status) == (int)ST_TIMEOUT) return false;
+  for (int q = 0; q < NF; ++q) {
+    float acc = 0.0f;
+    for (int b = t; b < G; b += T) acc = add(acc, (float)__ldcg(buf + (size_t)b * NV + ND + q));
+    of[q] = block_tree(acc, smf);
+  }
+  // block_tree leaves the total in warp 0; broadcast it to the block
+  __shared__ double bcd[ND > 0 ? ND : 1];
+  __shared__ float bcf[NF > 0 ? NF : 1];
+  if (t == 0) {
+#pragma unroll
+    for (int q = 0; q < ND; ++q) bcd[q] = od[q];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) bcf[q] = of[q];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < ND; ++q) od[q] = bcd[q];
+#pragma unroll
+  for (int q = 0; q < NF; ++q) of[q] = bcf[q];
+  __syncthreads();
   return true;
 }
 
 // Plain grid barrier (no values) built on grid_reduce.
-__device__ __forceinline__ bool grid_sync(Ctl *ctl, double *part, long long timeout_ns) {
+__device__ __forceinline__ bool grid_sync(Ctl *ctl, double *part, long long timeout_ns,
+                                          int &nbar) {
   double dummy_in = 0.0, dummy_out;
-  return grid_reduce<1, 0>(ctl, part, timeout_ns, &dummy_in, nullptr, &dummy_out, nullptr);
+  return grid_reduce<1, 0>(ctl, part, timeout_ns, nbar, &dummy_in, nullptr, &dummy_out, nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -256,6 +253,55 @@ __device__ __forceinline__ double rec_row(int i, double acc, const Sell &S, V ve
     acc = add(acc, add(mul(c.x, vec(v.x)), mul(c.y, vec(v.y))));
   }
   return acc;
+}
+
+// Two rows at once (nodes i0 and, if has1, i1): independent load chains
+// interleaved so that twice as many loads are in flight per thread.  Each
+// row's additions keep their own order, so the bits equal rec_row's.
+template <class V>
+__device__ __forceinline__ void rec_row2(int i0, int i1, bool has1, double &a0, double &a1,
+                                         const Sell &S, V vec) {
+  const int d0 = __ldg(S.meta + i0) & 0xffff;
+  const int d1 = has1 ? (__ldg(S.meta + i1) & 0xffff) : 0;
+  const int b0 = __ldg(S.rec_off + (i0 >> 5)) + (i0 & 31);
+  const int b1 = has1 ? __ldg(S.rec_off + (i1 >> 5)) + (i1 & 31) : 0;
+  const int dm = max(d0, d1);
+  for (int m = 0; m < dm; ++m) {
+    if (m < d0) {
+      const double2 c = __ldg(S.rec_c + b0 + 32 * m);
+      const int2 v = __ldg(S.rec_idx + b0 + 32 * m);
+      a0 = add(a0, add(mul(c.x, vec(v.x)), mul(c.y, vec(v.y))));
+    }
+    if (m < d1) {
+      const double2 c = __ldg(S.rec_c + b1 + 32 * m);
+      const int2 v = __ldg(S.rec_idx + b1 + 32 * m);
+      a1 = add(a1, add(mul(c.x, vec(v.x)), mul(c.y, vec(v.y))));
+    }
+  }
+}
+
+template <class V>
+__device__ __forceinline__ void seg_row2(int i0, int i1, bool has1, float y0, float y1,
+                                         float &a0, float &a1, const Sell &S, V vec) {
+  const int n0 = __ldg(S.meta + i0) >> 16;
+  const int n1 = has1 ? (__ldg(S.meta + i1) >> 16) : 0;
+  const int b0 = __ldg(S.seg_off + (i0 >> 5)) + (i0 & 31);
+  const int b1 = has1 ? __ldg(S.seg_off + (i1 >> 5)) + (i1 & 31) : 0;
+  a0 = mul(y0, __ldg(S.s32 + i0));
+  a1 = has1 ? mul(y1, __ldg(S.s32 + i1)) : 0.0f;
+  const int nm = max(n0, n1);
+  for (int m = 0; m < nm; ++m) {
+    if (m < n0) {
+      const int j = __ldg(S.seg_col + b0 + 32 * m);
+      const float c = __ldg(S.seg_c + b0 + 32 * m);
+      a0 = add(a0, mul(c, sub(vec(j), y0)));
+    }
+    if (m < n1) {
+      const int j = __ldg(S.seg_col + b1 + 32 * m);
+      const float c = __ldg(S.seg_c + b1 + 32 * m);
+      a1 = add(a1, mul(c, sub(vec(j), y1)));
+    }
+  }
 }
 
 template <class V>

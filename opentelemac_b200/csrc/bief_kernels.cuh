@@ -18,7 +18,17 @@
 
 namespace bief {
 
-constexpr int CG_THREADS = 256;
+// Shape of the persistent solver kernels: threads per block (one or more
+// blocks per SM) and rows interleaved per thread in the gather phases.
+#ifndef BIEF_CG_THREADS
+#define BIEF_CG_THREADS 1024
+#endif
+#ifndef BIEF_ROW_ILP
+#define BIEF_ROW_ILP 1
+#endif
+constexpr int CG_THREADS = BIEF_CG_THREADS;
+constexpr int CG_MIN_BLOCKS = 1024 / BIEF_CG_THREADS;
+constexpr int ROW_ILP = BIEF_ROW_ILP;
 
 // ---------------------------------------------------------------------------
 // MATVEC
@@ -165,7 +175,7 @@ struct CgP {
 };
 
 template <int TD>
-__global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
+__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -173,6 +183,7 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
   const double *b = P.b, *da = P.da;
   const bool lead = (blockIdx.x == 0 && t == 0);
   double s, red;
+  int nbar = 0;
 
   auto finish = [&](int status, int m, double rmrm, double xl, int relat) {
     if (P.dsc)  // solve.f:637-641: X = X*D
@@ -188,7 +199,7 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
   // XL = P_DOTS(B,B) (gracjg.F:189)
   s = 0.0;
   for (int i = lo + t; i < hi; i += T) s = add(s, mul(b[i], b[i]));
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
   double xl = red;
   if (__dsqrt_rn(xl) < 1.0e-15) {  // gracjg.F:194-202: X = 0
     for (int i = lo + t; i < hi; i += T) x[i] = 0.0;
@@ -201,14 +212,21 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
 
   // R = A X - B (gracjg.F:213-216)
   s = 0.0;
-  for (int i = lo + t; i < hi; i += T) {
-    double acc = diag_term<TD>(x[i], da, i);
-    acc = rec_row(i, acc, P.S, [&](int j) { return x[j]; });
-    const double ri = sub(acc, b[i]);
-    r[i] = ri;
-    s = add(s, mul(ri, ri));
+  for (int i = lo + t; i < hi; i += ROW_ILP * T) {
+    const int i1 = i + T;
+    const bool h1 = ROW_ILP == 2 && i1 < hi;
+    double a0 = diag_term<TD>(x[i], da, i), a1 = h1 ? diag_term<TD>(x[i1], da, i1) : 0.0;
+    rec_row2(i, i1, h1, a0, a1, P.S, [&](int j) { return x[j]; });
+    const double r0 = sub(a0, b[i]);
+    r[i] = r0;
+    s = add(s, mul(r0, r0));
+    if (h1) {
+      const double r1 = sub(a1, b[i1]);
+      r[i1] = r1;
+      s = add(s, mul(r1, r1));
+    }
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
   double rmrm = red, rmgm = rmrm;
   if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
   if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }
@@ -216,15 +234,22 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
   // D = G (= R), AD = A D, DAD, RO (gracjg.F:248-261)
   double *cur = P.d0, *nxt = P.d1;
   s = 0.0;
-  for (int i = lo + t; i < hi; i += T) {
-    const double di = r[i];
-    cur[i] = di;
-    double acc = diag_term<TD>(di, da, i);
-    acc = rec_row(i, acc, P.S, [&](int j) { return r[j]; });
-    ad[i] = acc;
-    s = add(s, mul(di, acc));
+  for (int i = lo + t; i < hi; i += ROW_ILP * T) {
+    const int i1 = i + T;
+    const bool h1 = ROW_ILP == 2 && i1 < hi;
+    const double d0 = r[i], d1 = h1 ? r[i1] : 0.0;
+    cur[i] = d0;
+    if (h1) cur[i1] = d1;
+    double a0 = diag_term<TD>(d0, da, i), a1 = h1 ? diag_term<TD>(d1, da, i1) : 0.0;
+    rec_row2(i, i1, h1, a0, a1, P.S, [&](int j) { return r[j]; });
+    ad[i] = a0;
+    s = add(s, mul(d0, a0));
+    if (h1) {
+      ad[i1] = a1;
+      s = add(s, mul(d1, a1));
+    }
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
   double dad = red;
   if (!(dad > 0.0)) { finish(isnan(dad) ? ST_NAN : ST_BREAKDOWN, 0, rmrm, xl, relat); return; }
   double ro = __ddiv_rn(rmgm, dad);
@@ -240,7 +265,7 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
       r[i] = ri;
       s = add(s, mul(ri, ri));
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
     const double rm1gm1 = rmgm;
     rmrm = red;
     rmgm = rmrm;
@@ -253,15 +278,23 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_cg64(CgP P) {
     // recomputes R(j)+BETA*D(j) from the previous direction, which gives
     // the same bits as the owner's value; the owner also stores it.
     s = 0.0;
-    for (int i = lo + t; i < hi; i += T) {
-      const double di = add(r[i], mul(beta, cur[i]));
-      nxt[i] = di;
-      double acc = diag_term<TD>(di, da, i);
-      acc = rec_row(i, acc, P.S, [&](int j) { return add(r[j], mul(beta, cur[j])); });
-      ad[i] = acc;
-      s = add(s, mul(di, acc));
+    for (int i = lo + t; i < hi; i += ROW_ILP * T) {
+      const int i1 = i + T;
+      const bool h1 = ROW_ILP == 2 && i1 < hi;
+      const double d0 = add(r[i], mul(beta, cur[i]));
+      const double d1 = h1 ? add(r[i1], mul(beta, cur[i1])) : 0.0;
+      nxt[i] = d0;
+      if (h1) nxt[i1] = d1;
+      double a0 = diag_term<TD>(d0, da, i), a1 = h1 ? diag_term<TD>(d1, da, i1) : 0.0;
+      rec_row2(i, i1, h1, a0, a1, P.S, [&](int j) { return add(r[j], mul(beta, cur[j])); });
+      ad[i] = a0;
+      s = add(s, mul(d0, a0));
+      if (h1) {
+        ad[i1] = a1;
+        s = add(s, mul(d1, a1));
+      }
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
     dad = red;
     if (!(dad > 0.0)) { finish(isnan(dad) ? ST_NAN : ST_BREAKDOWN, m, rmrm, xl, relat); return; }
     ro = __ddiv_rn(rmgm, dad);  // :383 (RMDM = RMGM)
@@ -302,7 +335,7 @@ struct MixP {
 };
 
 template <int TD>
-__global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
+__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_mixed(MixP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -312,7 +345,7 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
   const bool lead = (blockIdx.x == 0 && t == 0);
   double s, red;
   float sf;
-  int inner = 0, outer = 0;
+  int inner = 0, outer = 0, nbar = 0;
 
   auto finish = [&](int status, double rr, double xl) {
     if (P.dsc)
@@ -327,7 +360,7 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
 
   s = 0.0;
   for (int i = lo + t; i < hi; i += T) s = add(s, mul(b[i], b[i]));
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, &s, nullptr, &red, nullptr)) return;
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
   double xl = red;
   if (__dsqrt_rn(xl) < 1.0e-15) {
     for (int i = lo + t; i < hi; i += T) x[i] = 0.0;
@@ -345,16 +378,25 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
   auto true_residual = [&]() -> bool {
     double sd = 0.0;
     float s32 = 0.0f;
-    for (int i = lo + t; i < hi; i += T) {
-      double acc = diag_term<TD>(x[i], P.da, i);
-      acc = rec_row(i, acc, P.S, [&](int j) { return x[j]; });
-      const double rv = sub(b[i], acc);
-      sd = add(sd, mul(rv, rv));
-      const float r32 = (float)rv;
-      ri[i] = r32;
-      s32 = add(s32, mul(r32, r32));
+    for (int i = lo + t; i < hi; i += ROW_ILP * T) {
+      const int i1 = i + T;
+      const bool h1 = ROW_ILP == 2 && i1 < hi;
+      double a0 = diag_term<TD>(x[i], P.da, i), a1 = h1 ? diag_term<TD>(x[i1], P.da, i1) : 0.0;
+      rec_row2(i, i1, h1, a0, a1, P.S, [&](int j) { return x[j]; });
+      const double r0 = sub(b[i], a0);
+      sd = add(sd, mul(r0, r0));
+      const float q0 = (float)r0;
+      ri[i] = q0;
+      s32 = add(s32, mul(q0, q0));
+      if (h1) {
+        const double r1 = sub(b[i1], a1);
+        sd = add(sd, mul(r1, r1));
+        const float q1 = (float)r1;
+        ri[i1] = q1;
+        s32 = add(s32, mul(q1, q1));
+      }
     }
-    return grid_reduce<1, 1>(P.ctl, P.part, P.timeout_ns, &sd, &s32, &rr, &rho);
+    return grid_reduce<1, 1>(P.ctl, P.part, P.timeout_ns, nbar, &sd, &s32, &rr, &rho);
   };
 
   if (!true_residual()) return;
@@ -367,21 +409,31 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
   for (;;) {
     // p = r + beta p, evaluated where needed; q = A32 p; p.q
     sf = 0.0f;
-    for (int i = lo + t; i < hi; i += T) {
-      float pi, acc;
+    for (int i = lo + t; i < hi; i += ROW_ILP * T) {
+      const int i1 = i + T;
+      const bool h1 = ROW_ILP == 2 && i1 < hi;
+      float p0, p1 = 0.0f, a0, a1;
       if (first) {
-        pi = ri[i];
-        acc = seg_row(i, pi, P.S, [&](int k) { return ri[k]; });
+        p0 = ri[i];
+        if (h1) p1 = ri[i1];
+        seg_row2(i, i1, h1, p0, p1, a0, a1, P.S, [&](int k) { return ri[k]; });
       } else {
-        pi = add(ri[i], mul(beta, cur[i]));
-        acc = seg_row(i, pi, P.S, [&](int k) { return add(ri[k], mul(beta, cur[k])); });
+        p0 = add(ri[i], mul(beta, cur[i]));
+        if (h1) p1 = add(ri[i1], mul(beta, cur[i1]));
+        seg_row2(i, i1, h1, p0, p1, a0, a1, P.S,
+                 [&](int k) { return add(ri[k], mul(beta, cur[k])); });
       }
-      nxt[i] = pi;
-      q[i] = acc;
-      sf = add(sf, mul(pi, acc));
+      nxt[i] = p0;
+      q[i] = a0;
+      sf = add(sf, mul(p0, a0));
+      if (h1) {
+        nxt[i1] = p1;
+        q[i1] = a1;
+        sf = add(sf, mul(p1, a1));
+      }
     }
     float pq;
-    if (!grid_reduce<0, 1>(P.ctl, P.part, P.timeout_ns, nullptr, &sf, nullptr, &pq)) return;
+    if (!grid_reduce<0, 1>(P.ctl, P.part, P.timeout_ns, nbar, nullptr, &sf, nullptr, &pq)) return;
     if (!(pq > 0.0f)) { finish(isnan(pq) ? ST_NAN : ST_BREAKDOWN, rr, xl); return; }
     const float alpha = __fdiv_rn(rho, pq);
     sf = 0.0f;
@@ -392,7 +444,7 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
       sf = add(sf, mul(rv, rv));
     }
     float rho_new;
-    if (!grid_reduce<0, 1>(P.ctl, P.part, P.timeout_ns, nullptr, &sf, nullptr, &rho_new)) return;
+    if (!grid_reduce<0, 1>(P.ctl, P.part, P.timeout_ns, nbar, nullptr, &sf, nullptr, &rho_new)) return;
     const float rho_rec = rho_new, rho_old = rho;
     ++inner;
     { float *tmp = cur; cur = nxt; nxt = tmp; }
@@ -403,7 +455,7 @@ __global__ void __launch_bounds__(CG_THREADS, 4) k_mixed(MixP P) {
         x[i] = add(x[i], (double)z[i]);
         z[i] = 0.0f;
       }
-      if (!grid_sync(P.ctl, P.part, P.timeout_ns)) return;
+      if (!grid_sync(P.ctl, P.part, P.timeout_ns, nbar)) return;
       if (!true_residual()) return;
       ++outer;
       if (isnan(rr)) { finish(ST_NAN, rr, xl); return; }

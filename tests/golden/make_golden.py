@@ -47,15 +47,15 @@ def main():
     for nit in (1, 10):
         r = oracle.solve(ik, dm, "Q", xm, "S", b, precon=2, nitmax=nit, eps=1e-30)
         out[f"x_nit{nit}"] = r["x"]
-        # the device's dot order for a mesh this size: 1 block of 256 threads
+        # the device's dot order for a mesh this size: 1 block of 1024 threads
         r = oracle.solve(ik, dm, "Q", xm, "S", b, precon=2, nitmax=nit, eps=1e-30,
-                         dot_mode=oracle.DOT_BLOCKED, nblocks=1, nthreads=256)
+                         dot_mode=oracle.DOT_BLOCKED, nblocks=1, nthreads=1024)
         out[f"x_nit{nit}_blocked"] = r["x"]
     r = oracle.solve(ik, dm, "Q", xm, "S", b, precon=2, nitmax=100000, eps=1e-8)
     out.update(x_final=r["x"], nit_final=r["nit"], relres_final=r["relres"],
                b_scaled=r["b"], xm_scaled=r["xm"], dm_scaled=r["dm"])
     rb = oracle.solve(ik, dm, "Q", xm, "S", b, precon=2, nitmax=100000, eps=1e-8,
-                      dot_mode=oracle.DOT_BLOCKED, nblocks=1, nthreads=256)
+                      dot_mode=oracle.DOT_BLOCKED, nblocks=1, nthreads=1024)
     out.update(x_final_blocked=rb["x"], nit_final_blocked=rb["nit"])
     for op in ("X=AY    ", "X=TAY   "):
         out["mv_" + op.strip().replace("=", "")] = oracle.matvec(op, ik, dm, "Q", xm, "S", xt)

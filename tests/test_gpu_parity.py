@@ -118,7 +118,7 @@ def test_solve_golden_21(oracle_mod):
     gd = np.load(os.path.join(GOLDEN, "golden_21.npz"))
     p = dict(x=gd["x"], ik=gd["ikle0"], dm=gd["dm"], xm=gd["xm"], b=gd["b"])
     g = _gpu_solve(p)
-    assert g["mesh"].launch_info() == (1, 256)
+    assert g["mesh"].launch_info() == (1, 1024)
     np.testing.assert_array_equal(g["x"], gd["x_final_blocked"])
     assert g["nit"] == int(gd["nit_final_blocked"])
     for nit in (1, 10):
