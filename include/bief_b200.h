@@ -151,6 +151,26 @@ long long bief_kernel_launches(bief_handle *h);
 
 const char *bief_strerror(int status);
 
+/* SOLVE (SLV=1, diagonal preconditioning) for callers that cannot allocate
+ * device memory, e.g. a host code whose device arrays are owned by an
+ * OpenACC/OpenMP data region or a pool allocator, or that must not call
+ * cudaMalloc/cudaFree (and their implicit synchronisation) inside its time
+ * loop.  No counterpart in the reference: it is the same GRACJG as
+ * bief_solve_dev, but takes no handle and allocates nothing.  All arrays
+ * are the caller's device arrays: IKLE(NELMAX,3) 1-based, DM(NPOIN),
+ * XM(NELMAX,NDIAG), X, B.  As the reference SOLVE does, it leaves
+ * B = D.B, DM and XM = the scaled D.A.D (TYPDIA 'I' for PRECON 2/3).
+ * Everything else (gather index, work vectors, reduction partials) lives
+ * in one fixed ~6.6 MB device array inside the library: at most 65,536
+ * nodes and 131,072 elements (NELMAX), else BIEF_ERR_SIZE.  Calls share
+ * that array, so calls that overlap on the GPU race; the first call on a
+ * device looks up the array's address and should come before any stream
+ * capture.  TYPEXT 'S' or 'Q'. */
+int bief_solve_noalloc(int npoin, int nelem, int nelmax, const int *ikle,
+                       double *dm, double *xm, char typdia, char typext,
+                       double *x, double *b, bief_slvcfg *cfg,
+                       double *relres_out, int device, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,7 +29,7 @@ EXPORTS = [
     "bief_get_matrix", "bief_get_matrix_dev", "bief_solve", "bief_solve_dev",
     "bief_solve_mixed", "bief_solve_mixed_dev", "bief_matvec", "bief_matvec_dev",
     "bief_assemble_wave_dev", "bief_wave_coef_grad_dev", "bief_launch_info",
-    "bief_last_timing", "bief_kernel_launches", "bief_strerror",
+    "bief_last_timing", "bief_kernel_launches", "bief_strerror", "bief_solve_noalloc",
 ]
 
 
@@ -82,6 +82,7 @@ def lib():
                                   ctypes.POINTER(ctypes.c_float)], i),
             "bief_kernel_launches": ([vp], ctypes.c_longlong),
             "bief_strerror": ([i], ctypes.c_char_p),
+            "bief_solve_noalloc": ([i, i, i, vp, vp, vp, c, c, vp, vp, pcfg, pd, i, vp], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

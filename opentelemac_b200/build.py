@@ -13,7 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libbief_b200.so")
 
-SOURCES = ["bief_api.cu"]
+SOURCES = ["bief_api.cu", "bief_noalloc.cu"]
 HEADERS = ["bief_device.cuh", "bief_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

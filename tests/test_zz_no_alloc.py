@@ -1,0 +1,99 @@
+"""bief_solve_noalloc, the SOLVE entry point for callers that cannot
+allocate device memory -- for example a Fortran model whose device arrays
+belong to an OpenACC/OpenMP data region or to a pool allocator, or a code
+that must not call cudaMalloc/cudaFree (with their implicit device
+synchronisation) inside its time loop.  It takes the caller's device arrays
+and a fixed scratch array compiled into the library, and must give exactly
+what the handle-based bief_solve_dev gives, call after call.
+
+This file is collected last on purpose: the test runs after every other
+test in a normal run, and also passes alone in a fresh process."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from opentelemac_b200 import _native, bief, meshgen as mg
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(n, seed):
+    import torch
+    x, y, ik = mg.square_mesh(n, seed=seed)
+    coef = mg.wave_coef(mg.depth_loguniform(ik, seed=seed) if seed % 2 else
+                        mg.depth_smooth(x, y, ik))
+    mesh = bief.Mesh(ik, x.size)
+    A = bief.Matrix(mesh)
+    t = lambda a: torch.tensor(a, device="cuda", dtype=torch.float64)
+    A.assemble_wave(t(x), t(y), t(coef))
+    dm, xm, _ = A.get()
+    b = np.random.default_rng(seed).uniform(-1, 1, x.size)
+    return ik, mesh, A, dm, xm, b
+
+
+def _cfg(eps=1e-10):
+    return bief.SlvCfg(slv=1, nitmax=100000, precon=2, krylov=0, eps=eps, zero=0.0)
+
+
+def _noalloc(ik, dm, xm, b, cfg):
+    import torch
+    n, ne = dm.size, ik.shape[0]
+    d_ikle = torch.tensor(mg.ikle_fortran(ik), device="cuda")
+    d_dm = torch.tensor(dm, device="cuda")
+    d_xm = torch.tensor(np.ascontiguousarray(xm), device="cuda")
+    d_x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    d_b = torch.tensor(b, device="cuda")
+    relres = ctypes.c_double()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    st = _native.lib().bief_solve_noalloc(
+        n, ne, ne, ctypes.c_void_p(d_ikle.data_ptr()), ctypes.c_void_p(d_dm.data_ptr()),
+        ctypes.c_void_p(d_xm.data_ptr()), b"Q", b"S", ctypes.c_void_p(d_x.data_ptr()),
+        ctypes.c_void_p(d_b.data_ptr()), ctypes.byref(cfg), ctypes.byref(relres), 0, stream)
+    torch.cuda.synchronize()
+    return st, d_x.cpu().numpy(), d_b.cpu().numpy(), d_dm.cpu().numpy(), d_xm.cpu().numpy(), \
+        relres.value
+
+
+def test_noalloc_matches_handle_solve_twice():
+    for n, seed in ((101, 4), (181, 7)):          # two calls in a row, two meshes
+        ik, mesh, A, dm, xm, b = _problem(n, seed)
+        ref_cfg = _cfg()
+        x_ref, b_ref = np.zeros(dm.size), b.copy()
+        st_ref, nit_ref, rel_ref = bief.solve(x_ref, A, b_ref, ref_cfg, mutate=True)
+        dm_ref, xm_ref, td = A.get()
+        cfg = _cfg()
+        st, x, b_out, dm_out, xm_out, rel = _noalloc(ik, dm, xm, b, cfg)
+        assert st == st_ref == 0 and cfg.ok == 1
+        assert cfg.nit == nit_ref and rel == rel_ref
+        np.testing.assert_array_equal(x, x_ref)
+        # the reference SOLVE's side effects: B = D.B, A = D.A.D
+        np.testing.assert_array_equal(b_out, b_ref)
+        np.testing.assert_array_equal(dm_out, dm_ref)
+        np.testing.assert_array_equal(xm_out, xm_ref)
+        mesh.close()
+
+
+def test_noalloc_rejects_oversize_and_bad_mesh():
+    import torch
+    L = _native.lib()
+    dummy = torch.zeros(16, dtype=torch.float64, device="cuda")
+    p = ctypes.c_void_p(dummy.data_ptr())
+    cfg = _cfg()
+    st = L.bief_solve_noalloc(65537, 10, 10, p, p, p, b"Q", b"S", p, p, ctypes.byref(cfg), None,
+                              0, None)
+    assert st == _native.BIEF_ERR_SIZE
+    st = L.bief_solve_noalloc(100, 131073, 131073, p, p, p, b"Q", b"S", p, p, ctypes.byref(cfg),
+                              None, 0, None)
+    assert st == _native.BIEF_ERR_SIZE
+    _, _, ik = mg.square_mesh(11)
+    fort = mg.ikle_fortran(ik)
+    fort[5] = 500                                     # node number outside 1..NPOIN
+    d_ikle = torch.tensor(fort, device="cuda")
+    d = torch.zeros(121, dtype=torch.float64, device="cuda") + 1.0
+    dx = torch.zeros(3 * ik.shape[0], dtype=torch.float64, device="cuda")
+    st = L.bief_solve_noalloc(121, ik.shape[0], ik.shape[0], ctypes.c_void_p(d_ikle.data_ptr()),
+                              ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(dx.data_ptr()), b"Q",
+                              b"S", ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(d.data_ptr()),
+                              ctypes.byref(cfg), None, 0, None)
+    assert st == _native.BIEF_ERR_BAD_MESH
