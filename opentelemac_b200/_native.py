@@ -30,6 +30,7 @@ EXPORTS = [
     "bief_solve_mixed", "bief_solve_mixed_dev", "bief_matvec", "bief_matvec_dev",
     "bief_assemble_wave_dev", "bief_wave_coef_grad_dev", "bief_launch_info",
     "bief_last_timing", "bief_kernel_launches", "bief_strerror", "bief_solve_noalloc",
+    "bief_batch_solve_mixed_dev",
 ]
 
 
@@ -83,6 +84,8 @@ def lib():
             "bief_kernel_launches": ([vp], ctypes.c_longlong),
             "bief_strerror": ([i], ctypes.c_char_p),
             "bief_solve_noalloc": ([i, i, i, vp, vp, vp, c, c, vp, vp, pcfg, pd, i, vp], i),
+            "bief_batch_solve_mixed_dev": ([vp, i, vp, vp, vp, vp, i, d, d, i, i, i, vp, vp, vp,
+                                            vp, vp], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

@@ -1,0 +1,110 @@
+"""Batched solve of many independent P1 meshes in one persistent launch.
+
+The meshes become the diagonal blocks of one block-diagonal mesh (each
+instance's nodes start on a multiple of 32); `bief_batch_solve_mixed_dev`
+runs the mixed-precision algorithm on every instance at once with its own
+scalars and convergence mask.  The work tile (1024 x nodes-per-thread nodes)
+is chosen by a small autotuner that times a few inner iterations of each
+candidate on the actual batch.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native, bief
+
+
+class BatchSolver:
+    def __init__(self, meshes, device=0):
+        """meshes: list of (npoin, ikle0) with ikle0 (nelem, 3) 0-based."""
+        import torch
+        self.device = torch.device("cuda", device)
+        self.ninst = len(meshes)
+        if not 1 <= self.ninst <= 512:
+            raise ValueError("1..512 instances")
+        offs, n_list, e_off, ik_all = [], [], [], []
+        off, eo = 0, 0
+        for npoin, ik in meshes:
+            offs.append(off)
+            n_list.append(int(npoin))
+            e_off.append(eo)
+            ik_all.append(np.asarray(ik, dtype=np.int64) + off)
+            eo += ik.shape[0]
+            off += (int(npoin) + 31) // 32 * 32
+        self.node_off = np.array(offs, dtype=np.int32)
+        self.npoin = np.array(n_list, dtype=np.int32)
+        self.elem_off = np.array(e_off + [eo], dtype=np.int64)
+        self.total_nodes = off
+        self.mesh = bief.Mesh(np.concatenate(ik_all).astype(np.int32), off, device=device)
+        self.A = bief.Matrix(self.mesh)
+        self.tuned_npt = None
+        self.last = None
+
+    # -- layout helpers
+    def gather(self, vecs, fill=0.0):
+        """Per-instance vectors -> one device vector over the whole mesh."""
+        import torch
+        out = torch.full((self.total_nodes,), fill, dtype=torch.float64, device=self.device)
+        for k, v in enumerate(vecs):
+            o, n = int(self.node_off[k]), int(self.npoin[k])
+            out[o:o + n] = torch.as_tensor(v, dtype=torch.float64, device=self.device)
+        return out
+
+    def scatter(self, x):
+        return [x[int(o):int(o) + int(n)] for o, n in zip(self.node_off, self.npoin)]
+
+    def assemble_wave(self, xs, ys, coefs):
+        """A_k = M_k + coef_e K_e for every instance (coordinates and per-
+        element coefficients per instance)."""
+        import torch
+        xc, yc = self.gather(xs), self.gather(ys)
+        coef = torch.cat([torch.as_tensor(c, dtype=torch.float64, device=self.device)
+                          for c in coefs])
+        self.A.assemble_wave(xc, yc, coef.contiguous())
+
+    # -- solve
+    def solve_mixed(self, x, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, max_outer=1000,
+                    max_inner=1000000, nodes_per_thread=None):
+        """x (in/out), b: device vectors over the whole mesh.  Returns a dict
+        of per-instance status, inner/outer counts, relres and kernel ms."""
+        import torch
+        if nodes_per_thread is None:
+            nodes_per_thread = self.autotune(b, precon, inner_tol, outer_tol)
+        ni = self.ninst
+        st = np.zeros(ni, dtype=np.int32)
+        outer = np.zeros(ni, dtype=np.int32)
+        inner = np.zeros(ni, dtype=np.int32)
+        relres = np.zeros(ni, dtype=np.float64)
+        vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        s = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        rc = _native.lib().bief_batch_solve_mixed_dev(
+            self.mesh.handle, ni, vp(self.node_off), vp(self.npoin),
+            ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(b.data_ptr()), precon, inner_tol,
+            outer_tol, max_outer, max_inner, nodes_per_thread, vp(st), vp(outer), vp(inner),
+            vp(relres), s)
+        if rc < 0:
+            raise bief.BiefError(rc, "batched solve")
+        self.last = dict(status=st, outer=outer, inner=inner, relres=relres,
+                         kernel_ms=self.mesh.last_timing()[0], nodes_per_thread=nodes_per_thread)
+        return self.last
+
+    def autotune(self, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, candidates=(1, 2, 4),
+                 probe_inner=30):
+        """Pick nodes-per-thread by timing `probe_inner` inner iterations of
+        every instance with each candidate (kernel time per inner
+        iteration, summed over instances)."""
+        import torch
+        if self.tuned_npt is not None:
+            return self.tuned_npt
+        best, best_t = None, None
+        for npt in candidates:
+            x = torch.zeros_like(b)
+            r = self.solve_mixed(x, b, precon, inner_tol, outer_tol, 1000, probe_inner, npt)
+            per = r["kernel_ms"] / max(int(r["inner"].max()), 1)
+            if best_t is None or per < best_t:
+                best, best_t = npt, per
+        self.tuned_npt = best
+        return best
+
+    def close(self):
+        self.mesh.close()

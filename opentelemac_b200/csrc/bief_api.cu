@@ -14,7 +14,7 @@
 #include <vector>
 
 #include "../../include/bief_b200.h"
-#include "bief_kernels.cuh"
+#include "bief_batch.cuh"
 
 using namespace bief;
 
@@ -45,6 +45,11 @@ struct bief_handle {
   double *d_part = nullptr, *d_ew = nullptr;
   Ctl *d_ctl = nullptr, *h_ctl = nullptr;
   int *d_err = nullptr;
+  // batched solve: per-instance metadata, outputs and tile partials
+  int *d_binst = nullptr;      // 3*BATCH_MAX_INST+1 ints (off, n, t0) + outputs
+  double *d_brel = nullptr;
+  double *d_bpart = nullptr;
+  long long bpart_cap = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   float solve_ms = 0.f, matvec_ms = 0.f;
   long long launches = 0;
@@ -436,7 +441,8 @@ int bief_destroy(bief_handle *h) {
                   h->d_s32, h->d_x, h->d_b, h->d_bs, h->d_r, h->d_d0, h->d_d1,
                   h->d_ad, h->d_t, h->d_z, h->d_ri, h->d_p0, h->d_p1, h->d_q, h->d_part,
                   h->d_ew, h->d_ctl, h->d_err, h->d_meta, h->d_rec_off, h->d_seg_off,
-                  h->d_rec_idx, h->d_rec_slot, h->d_rec_c, h->d_seg_col, h->d_seg_c};
+                  h->d_rec_idx, h->d_rec_slot, h->d_rec_c, h->d_seg_col, h->d_seg_c,
+                  h->d_binst, h->d_brel, h->d_bpart};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -759,6 +765,142 @@ int bief_wave_coef_grad_dev(bief_handle *h, const double *xc, const double *yc,
                                                          grad);
   h->launches++;
   CK(cudaGetLastError());
+  return BIEF_OK;
+}
+
+int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
+                               const int *npoin_inst, double *x, const double *b, int precon,
+                               double inner_tol, double outer_tol, int max_outer, int max_inner,
+                               int nodes_per_thread, int *status, int *outer_out,
+                               int *inner_out, double *relres_out, void *stream) {
+  if (!h || !node_off || !npoin_inst || !x || !b || !status || !outer_out || !inner_out ||
+      !relres_out || max_inner < 1 || max_outer < 0)
+    return BIEF_ERR_ARGS;
+  if (ninst < 1 || ninst > BATCH_MAX_INST) return BIEF_ERR_SIZE;
+  if (nodes_per_thread != 1 && nodes_per_thread != 2 && nodes_per_thread != 4 &&
+      nodes_per_thread != 8)
+    return BIEF_ERR_ARGS;
+  if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
+  if (h->typext != 'S') return BIEF_ERR_UNSUPPORTED;
+  if (h->max_nnb > MAX_NEIGHBOURS) return BIEF_ERR_SIZE;
+  if (precon == 0) precon = 1;
+  if (precon < 0 || precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 || precon % 17 == 0)
+    return BIEF_ERR_UNSUPPORTED;
+  // instance ranges: ascending, disjoint, 32-aligned starts, inside the mesh
+  const int C = CG_THREADS * nodes_per_thread;
+  std::vector<int> meta(3 * BATCH_MAX_INST + 1, 0);
+  int t0 = 0;
+  for (int i = 0; i < ninst; ++i) {
+    if (node_off[i] < 0 || node_off[i] % 32 != 0 || npoin_inst[i] < 1 ||
+        (long long)node_off[i] + npoin_inst[i] > h->npoin ||
+        (i > 0 && node_off[i] < node_off[i - 1] + npoin_inst[i - 1]))
+      return BIEF_ERR_ARGS;
+    meta[i] = node_off[i];
+    meta[BATCH_MAX_INST + i] = npoin_inst[i];
+    meta[2 * BATCH_MAX_INST + i] = t0;
+    t0 += (npoin_inst[i] + C - 1) / C;
+  }
+  meta[2 * BATCH_MAX_INST + ninst] = t0;
+  const int ntiles = t0;
+  DevGuard g(h->dev);
+  cudaStream_t s = (cudaStream_t)stream;
+  int st;
+  if (!h->d_binst && ((st = dalloc(&h->d_binst, 7 * (size_t)BATCH_MAX_INST + 1)) ||
+                      (st = dalloc(&h->d_brel, (size_t)BATCH_MAX_INST))))
+    return st;
+  if (h->bpart_cap < 4LL * ntiles) {
+    if (h->d_bpart) CK(cudaFree(h->d_bpart));
+    h->d_bpart = nullptr;
+    if ((st = dalloc(&h->d_bpart, 4 * (size_t)ntiles))) return st;
+    h->bpart_cap = 4LL * ntiles;
+  }
+  int *d_off = h->d_binst, *d_cnt = h->d_binst + BATCH_MAX_INST,
+      *d_t0 = h->d_binst + 2 * BATCH_MAX_INST, *d_st = h->d_binst + 3 * BATCH_MAX_INST + 1,
+      *d_in = d_st + BATCH_MAX_INST, *d_out = d_in + BATCH_MAX_INST;
+  CK(cudaMemcpyAsync(h->d_binst, meta.data(), sizeof(int) * (3 * BATCH_MAX_INST + 1),
+                     cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(h->d_err, 0, sizeof(int), s));
+  k_check_blockdiag<<<grid_for(h->nelem, h->nsm), 256, 0, s>>>(h->nelem, h->d_ik, ninst, d_off,
+                                                               d_cnt, h->d_err);
+  h->launches++;
+  int err = 0;
+  CK(cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (err) return BIEF_ERR_ARGS;
+
+  const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
+  int td = typdia_code(h->typdia);
+  const double *xm = h->d_xm, *da = h->d_dm, *bw = b;
+  if (diag) {
+    if ((st = do_precd1(h, precon, x, b, h->d_bs, &td, s))) return st;
+    xm = h->d_xms;
+    da = h->d_dms;
+    bw = h->d_bs;
+  }
+  if ((st = build_records(h, xm, s))) return st;
+  {
+    const int gn = grid_for(h->npoin, h->nsm);
+#define SEG_ARGS                                                                              \
+  h->npoin, h->nelem, h->d_ptr, h->d_ek, xm, da, h->d_meta, h->d_rec_off, h->d_rec_slot, \
+      h->d_seg_off, h->d_seg_c, h->d_s32
+    if (td == DIA_Q)
+      k_build_seg32<DIA_Q><<<gn, 256, 0, s>>>(SEG_ARGS);
+    else if (td == DIA_I)
+      k_build_seg32<DIA_I><<<gn, 256, 0, s>>>(SEG_ARGS);
+    else
+      k_build_seg32<DIA_0><<<gn, 256, 0, s>>>(SEG_ARGS);
+#undef SEG_ARGS
+    h->launches++;
+    CK(cudaGetLastError());
+  }
+  void *k = td == DIA_Q ? (void *)k_batch<DIA_Q>
+            : td == DIA_I ? (void *)k_batch<DIA_I> : (void *)k_batch<DIA_0>;
+  int bps = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, CG_THREADS, 0));
+  if (bps < 1) return BIEF_ERR_CUDA;
+  const int G = std::max(1, std::min(bps * h->nsm, ntiles));
+  BatchP P;
+  P.ninst = ninst;
+  P.npt = nodes_per_thread;
+  P.max_outer = max_outer;
+  P.max_inner = max_inner;
+  P.outer_tol = outer_tol;
+  P.inner_tol = inner_tol;
+  P.inst_off = d_off;
+  P.inst_n = d_cnt;
+  P.inst_t0 = d_t0;
+  P.S = sell_of(h);
+  P.da = da;
+  P.dsc = diag ? h->d_dsc : nullptr;
+  P.x = x;
+  P.b = bw;
+  P.z = h->d_z;
+  P.ri = h->d_ri;
+  P.p0 = h->d_p0;
+  P.p1 = h->d_p1;
+  P.q = h->d_q;
+  P.part = h->d_bpart;
+  P.ntiles = ntiles;
+  P.ctl = h->d_ctl;
+  P.st_out = d_st;
+  P.inner_out = d_in;
+  P.outer_out = d_out;
+  P.relres_out = h->d_brel;
+  P.timeout_ns = h->timeout_ns;
+  CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
+  CK(cudaEventRecord(h->ev[0], s));
+  void *args[] = {&P};
+  CK(cudaLaunchCooperativeKernel(k, dim3(G), dim3(CG_THREADS), args, 0, s));
+  h->launches++;
+  CK(cudaEventRecord(h->ev[1], s));
+  CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(status, d_st, sizeof(int) * ninst, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(inner_out, d_in, sizeof(int) * ninst, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(outer_out, d_out, sizeof(int) * ninst, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(relres_out, h->d_brel, sizeof(double) * ninst, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaEventElapsedTime(&h->solve_ms, h->ev[0], h->ev[1]));
+  if (h->h_ctl->status == ST_TIMEOUT) return BIEF_ERR_DEVICE_TIMEOUT;
   return BIEF_OK;
 }
 

@@ -153,6 +153,32 @@ __device__ __noinline__ bool grid_reduce(Ctl *ctl, double *part, long long timeo
   return true;
 }
 
+// Grid barrier without values: all blocks' preceding writes are visible to
+// every block after it returns true.  Same monotonic counter and bounded
+// wait as grid_reduce (the two may be mixed in one launch).
+static __device__ __noinline__ bool grid_barrier(Ctl *ctl, long long timeout_ns, int &nbar) {
+  __shared__ int s_err;
+  const unsigned long long k = (unsigned long long)(++nbar);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> cnt(ctl->arrivals);
+    cnt.fetch_add(1ull, cuda::memory_order_release);
+    const unsigned long long target = k * (unsigned long long)gridDim.x;
+    const unsigned long long t0 = global_ns();
+    s_err = 0;
+    while (cnt.load(cuda::memory_order_acquire) < target) {
+      if ((long long)(global_ns() - t0) > timeout_ns) {
+        s_err = 1;
+        atomicExch(&ctl->status, (int)ST_TIMEOUT);
+        break;
+      }
+      __nanosleep(20);
+    }
+  }
+  __syncthreads();
+  return !s_err;
+}
+
 // Plain grid barrier (no values) built on grid_reduce.
 __device__ __forceinline__ bool grid_sync(Ctl *ctl, double *part, long long timeout_ns,
                                           int &nbar) {

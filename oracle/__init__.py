@@ -165,3 +165,37 @@ def solve_mixed(ikle0, dm, typdia, xm, b, x0=None, precon=2, inner_tol=1e-4, out
                                max_outer, max_inner, nblocks, nthreads, ctypes.byref(outer),
                                ctypes.byref(inner), ctypes.byref(relres))
     return dict(x=x, status=st, outer=outer.value, inner=inner.value, relres=relres.value)
+
+
+def dot_batch(x, y, nthreads=1024, npt=1):
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    L = lib()
+    L.orc_dot_batch.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int]
+    L.orc_dot_batch.restype = ctypes.c_double
+    return L.orc_dot_batch(x.size, _pd(x), _pd(y), nthreads, npt)
+
+
+def solve_mixed_batch(ikle0, dm, typdia, xm, b, x0=None, precon=2, inner_tol=1e-4,
+                      outer_tol=1e-8, max_outer=1000, max_inner=1000000, nthreads=1024, npt=1):
+    """One instance of the batched mixed-precision solver, in the batched
+    kernel's dot order (tiles of nthreads*npt nodes, warp sum of tiles)."""
+    ik, a, bb, c = _cols(ikle0)
+    n, ne = np.asarray(b).size, ik.shape[1]
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    xm = np.ascontiguousarray(xm, dtype=np.float64).reshape(3, ne)
+    L = lib()
+    P = ctypes.POINTER
+    d, i, ch = ctypes.c_double, ctypes.c_int, ctypes.c_char
+    L.orc_solve_mixed_batch.argtypes = [i, i, P(i), P(i), P(i), P(d), P(d), P(d), ch, P(d), ch,
+                                        i, d, d, i, i, i, i, P(i), P(i), P(d)]
+    outer, inner = ctypes.c_int(0), ctypes.c_int(0)
+    relres = ctypes.c_double(0.0)
+    st = L.orc_solve_mixed_batch(n, ne, _pi(a), _pi(bb), _pi(c), _pd(x), _pd(b), _pd(dm),
+                                 typdia.encode(), _pd(xm), b"S", precon, inner_tol, outer_tol,
+                                 max_outer, max_inner, nthreads, npt, ctypes.byref(outer),
+                                 ctypes.byref(inner), ctypes.byref(relres))
+    return dict(x=x, status=st, outer=outer.value, inner=inner.value, relres=relres.value)

@@ -383,6 +383,102 @@ static float dot_blocked32(int n, const float *x, const float *y, int nb, int nt
     return r;
 }
 
+/* The batched solver's dot order for one instance of n nodes: tiles of
+ * C = nt*npt consecutive nodes; in a tile, thread t sums nodes t, t+nt, ...
+ * (npt of them) left to right and the nt thread sums go through tree64;
+ * the instance total is a 32-lane warp sum: lane l adds tile partials l,
+ * l+32, ... left to right, then a xor-butterfly (offsets 16..1). */
+static double warp_tree64(double *lanes)
+{
+    for (int o = 16; o >= 1; o >>= 1) {
+        double nxt[32];
+        for (int l = 0; l < 32; ++l) nxt[l] = lanes[l] + lanes[l ^ o];
+        memcpy(lanes, nxt, sizeof(nxt));
+    }
+    return lanes[0];
+}
+
+static float warp_tree32(float *lanes)
+{
+    for (int o = 16; o >= 1; o >>= 1) {
+        float nxt[32];
+        for (int l = 0; l < 32; ++l) nxt[l] = lanes[l] + lanes[l ^ o];
+        memcpy(lanes, nxt, sizeof(nxt));
+    }
+    return lanes[0];
+}
+
+double orc_dot_batch(int n, const double *x, const double *y, int nt, int npt)
+{
+    const int C = nt * npt, ntile = (n + C - 1) / C;
+    double *part = (double *)malloc(sizeof(double) * (size_t)(ntile + 1));
+    double *v = (double *)malloc(sizeof(double) * (size_t)nt);
+    for (int k = 0; k < ntile; ++k) {
+        for (int t = 0; t < nt; ++t) {
+            double s = 0.0;
+            for (int j = 0; j < npt; ++j) {
+                long long i = (long long)k * C + t + (long long)j * nt;
+                if (i < n) s = s + x[i] * y[i];
+            }
+            v[t] = s;
+        }
+        part[k] = tree64(v, nt);
+    }
+    double lanes[32];
+    for (int l = 0; l < 32; ++l) {
+        double s = 0.0;
+        for (int k = l; k < ntile; k += 32) s = s + part[k];
+        lanes[l] = s;
+    }
+    double r = warp_tree64(lanes);
+    free(part); free(v);
+    return r;
+}
+
+static float dot_batch32(int n, const float *x, const float *y, int nt, int npt)
+{
+    const int C = nt * npt, ntile = (n + C - 1) / C;
+    float *part = (float *)malloc(sizeof(float) * (size_t)(ntile + 1));
+    float *v = (float *)malloc(sizeof(float) * (size_t)nt);
+    for (int k = 0; k < ntile; ++k) {
+        for (int t = 0; t < nt; ++t) {
+            float s = 0.0f;
+            for (int j = 0; j < npt; ++j) {
+                long long i = (long long)k * C + t + (long long)j * nt;
+                if (i < n) s = s + x[i] * y[i];
+            }
+            v[t] = s;
+        }
+        part[k] = tree32(v, nt);
+    }
+    float lanes[32];
+    for (int l = 0; l < 32; ++l) {
+        float s = 0.0f;
+        for (int k = l; k < ntile; k += 32) s = s + part[k];
+        lanes[l] = s;
+    }
+    float r = warp_tree32(lanes);
+    free(part); free(v);
+    return r;
+}
+
+/* Dot-product order used by the mixed-precision solvers: the persistent
+ * single-mesh kernel's blocked order (nb blocks of nt threads) or the
+ * batched kernel's tiled order (nt threads, npt nodes per thread). */
+typedef struct { int batch; int nb; int nt; int npt; } dotspec;
+
+static double dot64s(const dotspec *ds, int n, const double *x, const double *y)
+{
+    return ds->batch ? orc_dot_batch(n, x, y, ds->nt, ds->npt)
+                     : orc_dot_blocked(n, x, y, ds->nb, ds->nt);
+}
+
+static float dot32s(const dotspec *ds, int n, const float *x, const float *y)
+{
+    return ds->batch ? dot_batch32(n, x, y, ds->nt, ds->npt)
+                     : dot_blocked32(n, x, y, ds->nb, ds->nt);
+}
+
 static double pdots(int mode, int n, const double *x, const double *y,
                     int nb, int nt)
 {
@@ -672,13 +768,13 @@ static void seg32_mv(const seg32 *g, const float *p, float *q)
  * recursive residual).  Symmetric storage only; inputs other than x are not
  * modified.  Returns 0 when converged, the inner iteration count when
  * max_inner or max_outer ran out, or a negative error. */
-int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
-                    const int *ik2, double *x, const double *b,
-                    const double *dm_in, char typdia_in, const double *xm_in,
-                    char typext, int precon, double inner_tol,
-                    double outer_tol, int max_outer, int max_inner,
-                    int nb, int nt, int *outer_out, int *inner_total_out,
-                    double *relres_out)
+static int mixed_impl(int npoin, int nelem, const int *ik0, const int *ik1,
+                      const int *ik2, double *x, const double *b,
+                      const double *dm_in, char typdia_in, const double *xm_in,
+                      char typext, int precon, double inner_tol,
+                      double outer_tol, int max_outer, int max_inner,
+                      const dotspec *ds, int *outer_out, int *inner_total_out,
+                      double *relres_out)
 {
     if (typext != 'S') return ORC_ERR_UNSUPPORTED;
     size_t n = (size_t)npoin, ne = (size_t)nelem;
@@ -716,7 +812,7 @@ int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
     if ((st = seg32_build(npoin, nelem, ik0, ik1, ik2, gptr, gek, dm, typdia, xm, &g)))
         goto done;
 
-    xl = orc_dot_blocked(npoin, bs, bs, nb, nt);
+    xl = dot64s(ds, npoin, bs, bs);
     if (sqrt(xl) < 1.0e-15) {
         for (size_t i = 0; i < n; ++i) x[i] = 0.0;
         rr = 0.0; xl = 1.0;
@@ -733,8 +829,8 @@ int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
                         typdia, xm, nelem, typext, x, 0.0, r, w);               \
         if (st) goto done;                                                      \
         for (size_t i = 0; i < n; ++i) { r[i] = bs[i] - t[i]; ri[i] = (float)r[i]; } \
-        rr = orc_dot_blocked(npoin, r, r, nb, nt);                              \
-        rho = dot_blocked32(npoin, ri, ri, nb, nt);                             \
+        rr = dot64s(ds, npoin, r, r);                                          \
+        rho = dot32s(ds, npoin, ri, ri);                                       \
     } while (0)
 
     TRUE_RESIDUAL();
@@ -744,12 +840,12 @@ int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
     for (size_t i = 0; i < n; ++i) { z[i] = 0.0f; p[i] = ri[i]; }
     for (;;) {
         seg32_mv(&g, p, q);
-        float pq = dot_blocked32(npoin, p, q, nb, nt);
+        float pq = dot32s(ds, npoin, p, q);
         if (!(pq > 0.0f)) { st = isnan(pq) ? ORC_ERR_NAN : ORC_ERR_BREAKDOWN; goto fin; }
         float alpha = rho / pq;
         for (size_t i = 0; i < n; ++i) z[i] = z[i] + alpha * p[i];
         for (size_t i = 0; i < n; ++i) ri[i] = ri[i] - alpha * q[i];
-        float rho_new = dot_blocked32(npoin, ri, ri, nb, nt);
+        float rho_new = dot32s(ds, npoin, ri, ri);
         float rho_rec = rho_new, rho_old = rho;
         ++inner;
         int last = inner >= max_inner;
@@ -778,4 +874,34 @@ done:
     free(z); free(ri); free(p); free(q); free(gptr); free(gek);
     seg32_free(&g);
     return st;
+}
+
+int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
+                    const int *ik2, double *x, const double *b,
+                    const double *dm_in, char typdia_in, const double *xm_in,
+                    char typext, int precon, double inner_tol,
+                    double outer_tol, int max_outer, int max_inner,
+                    int nb, int nt, int *outer_out, int *inner_total_out,
+                    double *relres_out)
+{
+    dotspec ds = {0, nb, nt, 1};
+    return mixed_impl(npoin, nelem, ik0, ik1, ik2, x, b, dm_in, typdia_in, xm_in,
+                      typext, precon, inner_tol, outer_tol, max_outer, max_inner,
+                      &ds, outer_out, inner_total_out, relres_out);
+}
+
+/* One instance of the batched solver: the same algorithm with the batched
+ * kernel's dot order (nt threads per tile, npt nodes per thread). */
+int orc_solve_mixed_batch(int npoin, int nelem, const int *ik0, const int *ik1,
+                          const int *ik2, double *x, const double *b,
+                          const double *dm_in, char typdia_in, const double *xm_in,
+                          char typext, int precon, double inner_tol,
+                          double outer_tol, int max_outer, int max_inner,
+                          int nt, int npt, int *outer_out, int *inner_total_out,
+                          double *relres_out)
+{
+    dotspec ds = {1, 0, nt, npt};
+    return mixed_impl(npoin, nelem, ik0, ik1, ik2, x, b, dm_in, typdia_in, xm_in,
+                      typext, precon, inner_tol, outer_tol, max_outer, max_inner,
+                      &ds, outer_out, inner_total_out, relres_out);
 }

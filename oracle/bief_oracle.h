@@ -106,6 +106,16 @@ int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
                     int nblocks, int nthreads, int *outer_out,
                     int *inner_total_out, double *relres_out);
 
+double orc_dot_batch(int n, const double *x, const double *y, int nt, int npt);
+
+int orc_solve_mixed_batch(int npoin, int nelem, const int *ik0, const int *ik1,
+                          const int *ik2, double *x, const double *b,
+                          const double *dm_in, char typdia_in, const double *xm_in,
+                          char typext, int precon, double inner_tol,
+                          double outer_tol, int max_outer, int max_inner,
+                          int nt, int npt, int *outer_out, int *inner_total_out,
+                          double *relres_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -223,3 +223,13 @@ def test_golden_101(oracle_mod, cfg0_problem):
     r = oracle_mod.solve(p["ik"], p["dm"], "Q", p["xm"], "S", p["b"], eps=1e-8)
     np.testing.assert_array_equal(r["x"], g["x_final"])
     assert r["nit"] == int(g["nit_final"])
+
+
+def test_batch_dot_order(oracle_mod, rng):
+    v = rng.uniform(-1, 1, 70001)
+    w = rng.uniform(-1, 1, 70001)
+    exact = float(np.dot(v.astype(np.longdouble), w.astype(np.longdouble)))
+    for npt in (1, 2, 4):
+        assert abs(oracle_mod.dot_batch(v, w, 1024, npt) - exact) < 1e-11
+    ints = np.arange(1, 3001, dtype=np.float64)
+    assert oracle_mod.dot_batch(ints, np.ones_like(ints), 1024, 1) == 3000 * 3001 / 2
