@@ -199,3 +199,23 @@ def solve_mixed_batch(ikle0, dm, typdia, xm, b, x0=None, precon=2, inner_tol=1e-
                                  max_outer, max_inner, nthreads, npt, ctypes.byref(outer),
                                  ctypes.byref(inner), ctypes.byref(relres))
     return dict(x=x, status=st, outer=outer.value, inner=inner.value, relres=relres.value)
+
+
+def solve_omp(ikle0, dm, xm, b, x0=None, nitmax=1000000, eps=1e-8, nthreads=None):
+    """Binary64 SOLVE (PRECON 2, symmetric) on `nthreads` host threads."""
+    ik, a, bb, c = _cols(ikle0)
+    n, ne = np.asarray(b).size, ik.shape[1]
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    xm = np.ascontiguousarray(xm, dtype=np.float64).reshape(3, ne)
+    L = lib()
+    P = ctypes.POINTER
+    d, i = ctypes.c_double, ctypes.c_int
+    L.orc_solve_omp.argtypes = [i, i, P(i), P(i), P(i), P(d), P(d), P(d), P(d), i, d, i, P(i),
+                                P(d)]
+    nit, relres = ctypes.c_int(0), ctypes.c_double(0.0)
+    st = L.orc_solve_omp(n, ne, _pi(a), _pi(bb), _pi(c), _pd(x), _pd(b), _pd(dm), _pd(xm),
+                         nitmax, eps, nthreads or (os.cpu_count() or 1), ctypes.byref(nit),
+                         ctypes.byref(relres))
+    return dict(x=x, status=st, nit=nit.value, relres=relres.value)

@@ -17,6 +17,9 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 /* ------------------------------------------------------------------ */
 /* mesh geometry                                                        */
@@ -904,4 +907,147 @@ int orc_solve_mixed_batch(int npoin, int nelem, const int *ik0, const int *ik1,
     return mixed_impl(npoin, nelem, ik0, ik1, ik2, x, b, dm_in, typdia_in, xm_in,
                       typext, precon, inner_tol, outer_tol, max_outer, max_inner,
                       &ds, outer_out, inner_total_out, relres_out);
+}
+
+
+/* ------------------------------------------------------------------ */
+/* multi-threaded port (CPU baseline on all host cores)                 */
+/* ------------------------------------------------------------------ */
+
+/* The binary64 SOLVE/GRACJG algorithm of orc_solve on `nthreads` OpenMP
+ * threads, standing in for the reference run with one MPI rank per core:
+ * the matvec gathers each node's ASSVEC contributions in ASSVEC order (same
+ * bits as the sequential scatter), vector updates are node-parallel, and
+ * dot products sum per-thread partials of static node chunks in thread
+ * order.  Symmetric storage, PRECON 2. */
+static void mv_gather(int npoin, const int *ptr, const int *ek, const int *ik0,
+                      const int *ik1, const int *ik2, const double *xm,
+                      int nelem, char typdia, const double *da,
+                      const double *y, double *out)
+{
+    const int *ik[3] = {ik0, ik1, ik2};
+    const double *m[3] = {xm, xm + nelem, xm + 2 * (size_t)nelem};
+    #pragma omp for schedule(static)
+    for (int i = 0; i < npoin; ++i) {
+        double acc = typdia == 'Q' ? y[i] * da[i] : (typdia == 'I' ? y[i] : 0.0);
+        for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
+            int e = ek[j] >> 2, k = ek[j] & 3, a = (k + 1) % 3, b = (k + 2) % 3;
+            acc = acc + (m[k + a - 1][e] * y[ik[a][e]] + m[k + b - 1][e] * y[ik[b][e]]);
+        }
+        out[i] = acc;
+    }
+}
+
+static double dot_omp(int n, const double *x, const double *y, double *part)
+{
+    int nt = 1, t = 0;
+#ifdef _OPENMP
+    nt = omp_get_num_threads();
+    t = omp_get_thread_num();
+#endif
+    double s = 0.0;
+    #pragma omp for schedule(static)
+    for (int i = 0; i < n; ++i) s = s + x[i] * y[i];
+    part[t] = s;
+    #pragma omp barrier
+    double r = 0.0;
+    for (int k = 0; k < nt; ++k) r = r + part[k];
+    #pragma omp barrier
+    return r;
+}
+
+int orc_solve_omp(int npoin, int nelem, const int *ik0, const int *ik1,
+                  const int *ik2, double *x, const double *b_in,
+                  const double *dm_in, const double *xm_in, int nitmax,
+                  double eps, int nthreads, int *nit_out, double *relres_out)
+{
+    size_t n = (size_t)npoin, ne = (size_t)nelem;
+    int *ptr = NULL, *ek = NULL;
+    if (build_gather(npoin, nelem, ik0, ik1, ik2, &ptr, &ek)) return ORC_ERR_ARGS;
+    double *xm = (double *)malloc(sizeof(double) * 3 * ne);
+    double *b = (double *)malloc(sizeof(double) * n);
+    double *d = (double *)malloc(sizeof(double) * n);
+    double *r = (double *)malloc(sizeof(double) * n);
+    double *dd = (double *)malloc(sizeof(double) * n);
+    double *ad = (double *)malloc(sizeof(double) * n);
+    double part[1024];
+    int st = ORC_OK, m_out = 0;
+    double rel_out = 0.0;
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 1024) nthreads = 1024;
+#ifdef _OPENMP
+    omp_set_num_threads(nthreads);
+#endif
+    #pragma omp parallel
+    {
+        /* PRECD1 (PRECON 2) */
+        #pragma omp for schedule(static)
+        for (int i = 0; i < npoin; ++i) {
+            double di = sqrt(dm_in[i]);
+            x[i] = x[i] * di;
+            di = (fabs(di) > 1.0e-10) ? 1.0 / di : 1.0;
+            d[i] = di;
+            b[i] = b_in[i] * di;
+        }
+        #pragma omp for schedule(static)
+        for (int e = 0; e < nelem; ++e) {
+            xm[e] = xm_in[e] * d[ik1[e]] * d[ik0[e]];
+            xm[ne + e] = xm_in[ne + e] * d[ik2[e]] * d[ik0[e]];
+            xm[2 * ne + e] = xm_in[2 * ne + e] * d[ik2[e]] * d[ik1[e]];
+        }
+        double xl = dot_omp(npoin, b, b, part), rmrm, rmgm, rm1gm1, dad, ro, beta;
+        int m = 0, relat = 1;
+        if (sqrt(xl) < 1.0e-15) {
+            #pragma omp for schedule(static)
+            for (int i = 0; i < npoin; ++i) x[i] = 0.0;
+            rmrm = 0.0; xl = 1.0;
+            goto fin;
+        }
+        if (xl < 1.0) { xl = 1.0; relat = 0; }
+        (void)relat;
+        mv_gather(npoin, ptr, ek, ik0, ik1, ik2, xm, nelem, 'I', NULL, x, r);
+        #pragma omp for schedule(static)
+        for (int i = 0; i < npoin; ++i) r[i] = r[i] - b[i];
+        rmrm = dot_omp(npoin, r, r, part);
+        rmgm = rmrm;
+        if (rmrm < eps * eps * xl) goto fin;
+        #pragma omp for schedule(static)
+        for (int i = 0; i < npoin; ++i) dd[i] = r[i];
+        mv_gather(npoin, ptr, ek, ik0, ik1, ik2, xm, nelem, 'I', NULL, dd, ad);
+        dad = dot_omp(npoin, dd, ad, part);
+        ro = rmgm / dad;
+        #pragma omp for schedule(static)
+        for (int i = 0; i < npoin; ++i) x[i] = x[i] + (-ro) * dd[i];
+        for (;;) {
+            m = m + 1;
+            #pragma omp for schedule(static)
+            for (int i = 0; i < npoin; ++i) r[i] = r[i] + (-ro) * ad[i];
+            rm1gm1 = rmgm;
+            rmrm = dot_omp(npoin, r, r, part);
+            rmgm = rmrm;
+            if (rmrm <= xl * (eps * eps)) break;
+            beta = rmgm / rm1gm1;
+            #pragma omp for schedule(static)
+            for (int i = 0; i < npoin; ++i) dd[i] = r[i] + beta * dd[i];
+            mv_gather(npoin, ptr, ek, ik0, ik1, ik2, xm, nelem, 'I', NULL, dd, ad);
+            dad = dot_omp(npoin, dd, ad, part);
+            ro = rmgm / dad;
+            #pragma omp for schedule(static)
+            for (int i = 0; i < npoin; ++i) x[i] = x[i] + (-ro) * dd[i];
+            if (m >= nitmax) break;
+        }
+    fin:
+        #pragma omp for schedule(static)
+        for (int i = 0; i < npoin; ++i) x[i] = x[i] * d[i];
+        #pragma omp single
+        {
+            m_out = m;
+            rel_out = sqrt(rmrm / xl);
+            st = (m >= nitmax && !(rmrm <= xl * (eps * eps))) ? m : ORC_OK;
+        }
+    }
+    if (nit_out) *nit_out = m_out;
+    if (relres_out) *relres_out = rel_out;
+    free(ptr); free(ek); free(xm); free(b); free(d); free(r); free(dd); free(ad);
+    return st;
 }

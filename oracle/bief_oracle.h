@@ -116,6 +116,11 @@ int orc_solve_mixed_batch(int npoin, int nelem, const int *ik0, const int *ik1,
                           int nt, int npt, int *outer_out, int *inner_total_out,
                           double *relres_out);
 
+int orc_solve_omp(int npoin, int nelem, const int *ik0, const int *ik1,
+                  const int *ik2, double *x, const double *b_in,
+                  const double *dm_in, const double *xm_in, int nitmax,
+                  double eps, int nthreads, int *nit_out, double *relres_out);
+
 #ifdef __cplusplus
 }
 #endif
