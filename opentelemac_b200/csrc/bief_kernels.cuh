@@ -26,8 +26,11 @@ namespace bief {
 #ifndef BIEF_ROW_ILP
 #define BIEF_ROW_ILP 1
 #endif
+#ifndef BIEF_CG_MIN_BLOCKS
+#define BIEF_CG_MIN_BLOCKS (1024 / BIEF_CG_THREADS)
+#endif
 constexpr int CG_THREADS = BIEF_CG_THREADS;
-constexpr int CG_MIN_BLOCKS = 1024 / BIEF_CG_THREADS;
+constexpr int CG_MIN_BLOCKS = BIEF_CG_MIN_BLOCKS;
 constexpr int ROW_ILP = BIEF_ROW_ILP;
 
 // ---------------------------------------------------------------------------
