@@ -40,13 +40,23 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=1001, help="nodes per side of the mesh")
     ap.add_argument("--eps", type=float, default=1e-8)
+    ap.add_argument("--depth", default="smooth", choices=["smooth", "loguniform"],
+                    help="smooth: h = 5 + 4 sin(2 pi x) cos(2 pi y); loguniform: h log-uniform "
+                         "in [0.5, 500] m, 3 passes of neighbour averaging")
+    ap.add_argument("--inner-tol", type=float, default=None,
+                    help="refinement threshold of the mixed solve: the binary32 residual is "
+                         "refreshed from a binary64 one after dropping by this factor "
+                         "(default 0.1 for wave1m, 1e-4 for batch256)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="wave1m", choices=["wave1m", "batch256"],
                     help="wave1m: the 1M-node solve (default); batch256: 256 independent "
                          "meshes of 2,000-200,000 nodes in one persistent launch per rank")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.inner_tol is None:
+        args.inner_tol = 1e-4 if args.workload == "batch256" else 0.1
+    return args
 
 
 def algorithmic_bytes(npoin, nelem):
@@ -119,12 +129,17 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def build_problem(n, device):
+def depth_field(depth, x, y, ik):
+    from opentelemac_b200 import meshgen as mg
+    return mg.depth_loguniform(ik) if depth == "loguniform" else mg.depth_smooth(x, y, ik)
+
+
+def build_problem(n, device, depth="smooth"):
     """Mesh, operator (assembled on the device), manufactured solution."""
     import torch
     from opentelemac_b200 import bief, meshgen as mg
     x, y, ik = mg.square_mesh(n)
-    coef = mg.wave_coef(mg.depth_smooth(x, y, ik))
+    coef = mg.wave_coef(depth_field(depth, x, y, ik))
     npoin = x.size
     mesh = bief.Mesh(ik, npoin, device=device)
     A = bief.Matrix(mesh)
@@ -137,14 +152,14 @@ def build_problem(n, device):
                 nelem=ik.shape[0])
 
 
-def cpu_baseline(n, eps, nit_full, seconds, ik=None):
+def cpu_baseline(n, eps, nit_full, seconds, depth="smooth"):
     """The oracle's reference-order binary64 SOLVE on one host core, timed on
     a bounded number of CG iterations and extrapolated to a full solve."""
     import oracle
     from opentelemac_b200 import meshgen as mg
     oracle.build()
     x, y, ik = mg.square_mesh(n)
-    coef = mg.wave_coef(mg.depth_smooth(x, y, ik))
+    coef = mg.wave_coef(depth_field(depth, x, y, ik))
     dm, xm = oracle.wave_matrix(x, y, ik, coef)
     b = oracle.matvec("X=AY    ", ik, dm, "Q", xm, "S", mg.random_solution(x.size))
     args = (ik, dm, "Q", xm, "S", b)
@@ -211,7 +226,7 @@ def run_reference(args, ws, rank):
     oracle.build()
     nthreads = os.cpu_count() or 1
     x, y, ik = mg.square_mesh(args.n)
-    coef = mg.wave_coef(mg.depth_smooth(x, y, ik))
+    coef = mg.wave_coef(depth_field(args.depth, x, y, ik))
     dm, xm = oracle.wave_matrix(x, y, ik, coef)
     b = oracle.matvec("X=AY    ", ik, dm, "Q", xm, "S", mg.random_solution(x.size))
     full = oracle.solve_omp(ik, dm, xm, b, eps=args.eps, nthreads=nthreads)
@@ -273,16 +288,18 @@ def run_batch(args, ws, rank, local):
     bs.assemble_wave(xs, ys, coefs)
     b = bs.gather(bvs)
     x = torch.zeros_like(b)
-    npt = bs.autotune(b, inner_tol=1e-4, outer_tol=args.eps)
+    npt = bs.autotune(b, inner_tol=args.inner_tol, outer_tol=args.eps)
     flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    clean = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     times, kern = [], []
     for s in range(args.warmup + args.steps):
-        flush.fill_(float(s))
+        flush.fill_(float(s))   # 1 GiB written, then 256 MB read: L2 flushed, lines clean
+        clean.sum()
         x.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        r = bs.solve_mixed(x, b, inner_tol=1e-4, outer_tol=args.eps, nodes_per_thread=npt)
+        r = bs.solve_mixed(x, b, inner_tol=args.inner_tol, outer_tol=args.eps, nodes_per_thread=npt)
         e1.record()
         e1.synchronize()
         if s >= args.warmup:
@@ -330,19 +347,27 @@ def main():
     from opentelemac_b200 import bief
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    P = build_problem(args.n, local)
+    P = build_problem(args.n, local, args.depth)
     A, b, mesh = P["A"], P["b"], P["mesh"]
     npoin, nelem = P["npoin"], P["nelem"]
     by = algorithmic_bytes(npoin, nelem)
-    # 1 GiB written before every timed kernel: flushes the 126 MB L2 and keeps
-    # the GPU busy while the host enqueues the next timed launch
+    # Before every timed kernel 1 GiB is written (flushes the 126 MB L2 and
+    # keeps the GPU busy while the host enqueues the timed launch), then 256 MB
+    # are read, so that the L2 holds clean lines and the timed kernel does not
+    # pay for writing back the flush's dirty ones.
     flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    clean = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def flush_l2(s):
+        flush.fill_(float(s))
+        clean.sum()
+
     x = torch.zeros_like(b)
     cfg = bief.SlvCfg(slv=1, nitmax=1000000, precon=2, krylov=0, eps=args.eps, zero=0.0)
 
     def run_mixed():
         x.zero_()
-        return bief.solve_mixed(x, A, b, precon=2, inner_tol=1e-4, outer_tol=args.eps)
+        return bief.solve_mixed(x, A, b, precon=2, inner_tol=args.inner_tol, outer_tol=args.eps)
 
     def run_fp64():
         x.zero_()
@@ -353,7 +378,7 @@ def main():
         the library's kernel time of the solver launch."""
         out, kern, res = [], [], None
         for s in range(warmup + steps):
-            flush.fill_(float(s))
+            flush_l2(s)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
@@ -375,9 +400,9 @@ def main():
     # standalone EBE matvec bandwidth (binary64, full diagonal)
     y = P["xt"]
     out = torch.zeros_like(y)
-    mv_ms = []
+    mv_ms, mv_lib = [], []
     for s in range(args.warmup + 20):
-        flush.fill_(float(s))
+        flush_l2(s)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -386,7 +411,9 @@ def main():
         e1.synchronize()
         if s >= args.warmup:
             mv_ms.append(e0.elapsed_time(e1))
-    mv_t = statistics.median(mv_ms)
+            mv_lib.append(mesh.last_timing()[1])   # events around the launch itself
+    mv_t = statistics.median(mv_lib)
+    mv_t_call = statistics.median(mv_ms)
 
     # headline: mixed precision, timed steps, clocks sampled meanwhile
     barrier(ws)
@@ -416,7 +443,7 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         A.set(dm_p, xm_p, "Q", "S")
-        bief.solve_mixed(x_p, A, b_p, precon=2, inner_tol=1e-4, outer_tol=args.eps)
+        bief.solve_mixed(x_p, A, b_p, precon=2, inner_tol=args.inner_tol, outer_tol=args.eps)
         t1 = time.perf_counter()
         if s >= args.warmup:
             e2e.append((t1 - t0) * 1e3)
@@ -424,7 +451,7 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.n, args.eps, nit64, args.cpu_seconds)
+        cpu = cpu_baseline(args.n, args.eps, nit64, args.cpu_seconds, args.depth)
 
     peaks = {}
     try:
@@ -453,8 +480,9 @@ def main():
             "dtype": "f32 inner / f64 refinement", "data": "synthetic",
             "config": {"workload": f"wave-equation SOLVE (CG, diagonal precon, relres "
                                    f"{args.eps:g}) on the {args.n}x{args.n}-node P1 mesh",
-                       "npoin": npoin, "nelem": nelem, "parallelism": f"replicas x{ws}",
-                       "l2": "1 GiB buffer written before every timed step"},
+                       "npoin": npoin, "nelem": nelem, "depth": args.depth,
+                       "inner_tol": args.inner_tol, "parallelism": f"replicas x{ws}",
+                       "l2": "1 GiB written then 256 MB read before every timed step"},
             "time_to_solution_ms": {"mixed": step_ms, "fp64": f64_step_ms,
                                     "mixed_kernel": kern_ms, "fp64_kernel": f64_kern_ms},
             "speedup_mixed_vs_fp64": f64_step_ms / step_ms,
@@ -463,6 +491,9 @@ def main():
             "error": {"mixed_vs_fp64": mixed_vs_f64, "mixed_vs_xtrue": mixed_x_err,
                       "fp64_vs_xtrue": f64_x_err},
             "matvec": {"op": "X=AY binary64 TYPDIA=Q", "kernel": "k_matvec", "ms": mv_t,
+                       "ms_call": mv_t_call,
+                       "timing": "ms: library events around the launch; ms_call: torch events "
+                                 "around the Python call",
                        "gbs": mv_gbs, "frac": mv_gbs / hbm, "bytes": by["mv64"],
                        "traffic": traffic.get("k_matvec_bytes_per_launch")},
             "fp64_cg": {"kernel": "k_cg64", "gbs": f64_bytes / (f64_kern_ms * 1e-3) / 1e9,

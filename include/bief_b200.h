@@ -101,10 +101,14 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg,
                    int flags, double *relres_out, void *stream);
 
 /* Mixed precision (no reference counterpart): binary32 copy of the scaled
- * operator and binary32 inner CG (stopped at inner_tol relative),
- * binary64 residual and update in an outer refinement loop stopped at
- * outer_tol (relative to ||D.B||, absolute when that is < 1).  B is not
- * modified.  outer_out/inner_out: outer steps and total inner iterations. */
+ * operator and one binary32 CG whose correction is folded into the binary64
+ * solution (a refinement step: x += z, r = b - A x in binary64, binary32
+ * residual restarted from r, search direction kept) each time its residual
+ * has dropped by the factor inner_tol since the last refinement (0.1 keeps
+ * the iteration count of binary64 CG; smaller values refine less often).
+ * Stops when the binary64 residual reaches outer_tol (relative to ||D.B||,
+ * absolute when that is < 1).  B is not modified.  outer_out/inner_out:
+ * refinement steps and total inner iterations. */
 int bief_solve_mixed(bief_handle *h, double *x, const double *b,
                      int precon, double inner_tol, double outer_tol,
                      int max_outer, int max_inner, int *outer_out,
@@ -161,8 +165,10 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
 /* Shape of the device dot-product tree: number of blocks and threads per
  * block of the persistent solver kernel. */
 int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads);
-/* Kernel time (ms, CUDA events on the handle's stream) of the last solve
- * kernel and of the last matvec kernel. */
+/* Kernel time (ms, CUDA events recorded around the launch on the stream
+ * the call used) of the last solve kernel and of the last matvec kernel.  For
+ * bief_matvec_dev, which returns before its kernel ends, the matvec time is
+ * that of the last call whose kernel had completed when this is called. */
 int bief_last_timing(bief_handle *h, float *solve_ms, float *matvec_ms);
 /* Number of device kernels the library launched since the handle was made. */
 long long bief_kernel_launches(bief_handle *h);

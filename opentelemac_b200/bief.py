@@ -175,9 +175,10 @@ def solve(x, A, b, cfg, infogr=False, mutate=False):
     return st, cfg.nit, relres.value
 
 
-def solve_mixed(x, A, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, max_outer=1000,
+def solve_mixed(x, A, b, precon=2, inner_tol=0.1, outer_tol=1e-8, max_outer=1000,
                 max_inner=1000000):
-    """Mixed-precision solve (binary32 inner CG, binary64 refinement).
+    """Mixed-precision solve (binary32 inner CG, binary64 refinement each
+    time the binary32 residual has dropped by inner_tol).
     Returns (status, outer_steps, inner_iterations, relres)."""
     L = _native.lib()
     o, i = ctypes.c_int(), ctypes.c_int()

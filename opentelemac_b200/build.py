@@ -14,7 +14,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libbief_b200.so")
 
 SOURCES = ["bief_api.cu", "bief_noalloc.cu"]
-HEADERS = ["bief_device.cuh", "bief_kernels.cuh"]
+HEADERS = ["bief_device.cuh", "bief_kernels.cuh", "bief_batch.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

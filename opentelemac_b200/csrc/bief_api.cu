@@ -52,6 +52,7 @@ struct bief_handle {
   long long bpart_cap = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   float solve_ms = 0.f, matvec_ms = 0.f;
+  int mv_pending = 0;
   long long launches = 0;
   long long timeout_ns = 2000000000LL;
 };
@@ -714,6 +715,7 @@ int bief_matvec_dev(bief_handle *h, const char *op, double *x, const double *y, 
   h->launches++;
   CK(cudaGetLastError());
   CK(cudaEventRecord(h->ev[3], s));
+  h->mv_pending = 1;
   return BIEF_OK;
 }
 
@@ -728,6 +730,7 @@ int bief_matvec(bief_handle *h, const char *op, double *x, const double *y, doub
   CK(cudaMemcpyAsync(x, h->d_x, nb, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   CK(cudaEventElapsedTime(&h->matvec_ms, h->ev[2], h->ev[3]));
+  h->mv_pending = 0;
   return BIEF_OK;
 }
 
@@ -913,6 +916,15 @@ int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads) {
 
 int bief_last_timing(bief_handle *h, float *solve_ms, float *matvec_ms) {
   if (!h) return BIEF_ERR_ARGS;
+  if (h->mv_pending) {
+    // bief_matvec_dev returns before its kernel ends: read its events once
+    // the stream has passed them
+    DevGuard g(h->dev);
+    if (cudaEventQuery(h->ev[3]) == cudaSuccess) {
+      CK(cudaEventElapsedTime(&h->matvec_ms, h->ev[2], h->ev[3]));
+      h->mv_pending = 0;
+    }
+  }
   if (solve_ms) *solve_ms = h->solve_ms;
   if (matvec_ms) *matvec_ms = h->matvec_ms;
   return BIEF_OK;

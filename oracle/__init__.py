@@ -148,7 +148,7 @@ def solve(ikle0, dm, typdia, xm, typext, b, x0=None, precon=2, nitmax=100000, ep
                 relres=relres.value, relat=relat.value)
 
 
-def solve_mixed(ikle0, dm, typdia, xm, b, x0=None, precon=2, inner_tol=1e-4, outer_tol=1e-8,
+def solve_mixed(ikle0, dm, typdia, xm, b, x0=None, precon=2, inner_tol=0.1, outer_tol=1e-8,
                 max_outer=50, max_inner=100000, nblocks=1, nthreads=256):
     """Mixed-precision solve (binary32 inner CG, binary64 refinement) in the
     device kernels' exact operation order."""
@@ -177,7 +177,7 @@ def dot_batch(x, y, nthreads=1024, npt=1):
     return L.orc_dot_batch(x.size, _pd(x), _pd(y), nthreads, npt)
 
 
-def solve_mixed_batch(ikle0, dm, typdia, xm, b, x0=None, precon=2, inner_tol=1e-4,
+def solve_mixed_batch(ikle0, dm, typdia, xm, b, x0=None, precon=2, inner_tol=0.1,
                       outer_tol=1e-8, max_outer=1000, max_inner=1000000, nthreads=1024, npt=1):
     """One instance of the batched mixed-precision solver, in the batched
     kernel's dot order (tiles of nthreads*npt nodes, warp sum of tiles)."""
