@@ -40,6 +40,9 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=1001, help="nodes per side of the mesh")
     ap.add_argument("--eps", type=float, default=1e-8)
+    ap.add_argument("--storage", default="ebe", choices=["ebe", "seg"],
+                    help="matrix storage: ebe (element by element, STO=1) or seg (edge "
+                         "segments, STO=3, built from the EBE matrix by ASSEX3)")
     ap.add_argument("--depth", default="smooth", choices=["smooth", "loguniform"],
                     help="smooth: h = 5 + 4 sin(2 pi x) cos(2 pi y); loguniform: h log-uniform "
                          "in [0.5, 500] m, 3 passes of neighbour averaging")
@@ -59,8 +62,11 @@ def parse():
     return args
 
 
-def algorithmic_bytes(npoin, nelem):
+def algorithmic_bytes(npoin, nelem, nseg=None):
     """Algorithmic bytes (each input read once, each output written once)."""
+    if nseg is not None:   # segment storage: XA 8 B + GLOSEG 2x4 B per segment
+        return dict(mv64=16 * nseg + 24 * npoin, it64=16 * nseg + 88 * npoin,
+                    it32=12 * nseg + 48 * npoin, upd=16 * nseg + 48 * npoin)
     return dict(
         # EBE matvec 'X=AY' with a full diagonal, binary64: XM 3x8 + IKLE 3x4
         # per element; DM, Y in, X out per node
@@ -134,7 +140,7 @@ def depth_field(depth, x, y, ik):
     return mg.depth_loguniform(ik) if depth == "loguniform" else mg.depth_smooth(x, y, ik)
 
 
-def build_problem(n, device, depth="smooth"):
+def build_problem(n, device, depth="smooth", storage="ebe"):
     """Mesh, operator (assembled on the device), manufactured solution."""
     import torch
     from opentelemac_b200 import bief, meshgen as mg
@@ -145,11 +151,17 @@ def build_problem(n, device, depth="smooth"):
     A = bief.Matrix(mesh)
     t = lambda a: torch.tensor(a, device=f"cuda:{device}", dtype=torch.float64)
     A.assemble_wave(t(x), t(y), t(coef))
+    nseg = None
+    if storage == "seg":
+        g1, g2, _, _ = mg.segments(ik, npoin)
+        mesh.set_segments(g1, g2)
+        A.to_segments()
+        nseg = int(g1.size)
     xt = t(mg.random_solution(npoin))
     b = torch.zeros_like(xt)
     bief.matvec("X=AY    ", b, A, xt)
     return dict(x=x, y=y, ik=ik, coef=coef, mesh=mesh, A=A, xt=xt, b=b, npoin=npoin,
-                nelem=ik.shape[0])
+                nelem=ik.shape[0], nseg=nseg)
 
 
 def cpu_baseline(n, eps, nit_full, seconds, depth="smooth"):
@@ -347,10 +359,10 @@ def main():
     from opentelemac_b200 import bief
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    P = build_problem(args.n, local, args.depth)
+    P = build_problem(args.n, local, args.depth, args.storage)
     A, b, mesh = P["A"], P["b"], P["mesh"]
     npoin, nelem = P["npoin"], P["nelem"]
-    by = algorithmic_bytes(npoin, nelem)
+    by = algorithmic_bytes(npoin, nelem, P["nseg"])
     # Before every timed kernel 1 GiB is written (flushes the 126 MB L2 and
     # keeps the GPU busy while the host enqueues the timed launch), then 256 MB
     # are read, so that the L2 holds clean lines and the timed kernel does not
@@ -442,7 +454,10 @@ def main():
         x_p[:] = 0.0
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        A.set(dm_p, xm_p, "Q", "S")
+        if args.storage == "seg":
+            A.set_seg(dm_p, xm_p, "Q", "S")
+        else:
+            A.set(dm_p, xm_p, "Q", "S")
         bief.solve_mixed(x_p, A, b_p, precon=2, inner_tol=args.inner_tol, outer_tol=args.eps)
         t1 = time.perf_counter()
         if s >= args.warmup:
@@ -463,7 +478,8 @@ def main():
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     traffic = {}
     try:
-        with open(os.path.join(ROOT, "profiles", f"traffic_{args.n}.json")) as fh:
+        with open(os.path.join(ROOT, "profiles",
+                               f"traffic_{args.n}_{args.storage}_{args.depth}.json")) as fh:
             traffic = json.load(fh)
     except Exception:
         pass
@@ -480,7 +496,9 @@ def main():
             "dtype": "f32 inner / f64 refinement", "data": "synthetic",
             "config": {"workload": f"wave-equation SOLVE (CG, diagonal precon, relres "
                                    f"{args.eps:g}) on the {args.n}x{args.n}-node P1 mesh",
-                       "npoin": npoin, "nelem": nelem, "depth": args.depth,
+                       "npoin": npoin, "nelem": nelem, "nseg": P["nseg"],
+                       "storage": "segments (STO=3)" if args.storage == "seg" else "EBE (STO=1)",
+                       "depth": args.depth,
                        "inner_tol": args.inner_tol, "parallelism": f"replicas x{ws}",
                        "l2": "1 GiB written then 256 MB read before every timed step"},
             "time_to_solution_ms": {"mixed": step_ms, "fp64": f64_step_ms,
@@ -490,7 +508,8 @@ def main():
             "relres": {"mixed": relres, "fp64": f64_res[2]},
             "error": {"mixed_vs_fp64": mixed_vs_f64, "mixed_vs_xtrue": mixed_x_err,
                       "fp64_vs_xtrue": f64_x_err},
-            "matvec": {"op": "X=AY binary64 TYPDIA=Q", "kernel": "k_matvec", "ms": mv_t,
+            "matvec": {"op": "X=AY binary64 TYPDIA=Q",
+                       "kernel": "k_mvseg" if args.storage == "seg" else "k_matvec", "ms": mv_t,
                        "ms_call": mv_t_call,
                        "timing": "ms: library events around the launch; ms_call: torch events "
                                  "around the Python call",
@@ -508,7 +527,7 @@ def main():
                          "note": "binary32 working set is L2-resident (96% L2 hits): traffic "
                                  "from HBM is far below the algorithmic bytes"},
             "e2e": {"value": ws * 1000.0 / e2e_ms, "unit": UNIT,
-                    "h2d_bytes_per_step": 8 * (npoin + 3 * nelem) + 16 * npoin,
+                    "h2d_bytes_per_step": 8 * (npoin + int(xm_h.size)) + 16 * npoin,
                     "d2h_bytes_per_step": 8 * npoin, "ms_per_step": e2e_ms},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),

@@ -133,8 +133,33 @@ int bief_matvec_dev(bief_handle *h, const char *op, double *x,
  * Stores the result as the handle's matrix (TYPDIA 'Q', TYPEXT 'S'). */
 int bief_assemble_wave_dev(bief_handle *h, const double *x, const double *y,
                            const double *coef, void *stream);
-/* Copy the stored matrix to device arrays dm[npoin], xm[3*nelem]. */
+/* Copy the stored matrix to device arrays dm[npoin] and xm: EBE storage
+ * xm[ndiag*nelem] (leading dimension NELEM), segment storage xa[ncol*nseg]. */
 int bief_get_matrix_dev(bief_handle *h, double *dm, double *xm, void *stream);
+
+/* ---- Segment (edge) storage, MATRIX STORAGE = 3 ------------------------
+ * The segment numbering of the mesh: MESH%GLOSEG(MAXSEG,2) as STOSEG builds
+ * it (stoseg.f:94-225), 1-based, column-major, nseg <= maxseg segments.
+ * Every element face must be exactly one segment (the element-to-segment
+ * map that ASSEX3 uses is derived from it).  Replaces an earlier numbering;
+ * a stored segment matrix is dropped with it.  Replaces no reference
+ * routine: the Fortran side passes its MESH%GLOSEG once per mesh. */
+int bief_set_segments(bief_handle *h, int nseg, int maxseg, const int *gloseg);
+/* Matrix in segment storage (STO=3): DA(NPOIN) and XA(NSEG) for TYPEXT
+ * 'S' or XA(NSEG,2) for 'Q' (column 1: the coefficient of row GLOSEG(,1),
+ * column 2: of row GLOSEG(,2)).  bief_matvec then follows MVSEG
+ * (mvseg.f:110-720, via matvct.f:665-689), bief_solve / bief_solve_mixed
+ * scale it with OMSEG 'M=DMD' (omseg.f:509-541) and iterate on it. */
+int bief_set_matrix_seg(bief_handle *h, const double *da, const double *xa,
+                        char typdia, char typext);
+int bief_set_matrix_seg_dev(bief_handle *h, const double *da,
+                            const double *xa, char typdia, char typext);
+/* ASSEX3 (assex3.f:150-160 -> as3_1111_s.f / as3_1111_q.f): the stored EBE
+ * matrix becomes segment storage (off-diagonal terms summed per segment in
+ * element order; the diagonal unchanged).  Needs bief_set_segments. */
+int bief_ebe_to_seg(bief_handle *h, void *stream);
+/* Storage of the stored matrix: 1 (EBE) or 3 (segments). */
+int bief_matrix_storage(bief_handle *h);
 
 /* Adjoint gradient of a loss through x = A(coef)^-1 b with
  * A = M + coef_e K_e: grad[e] = -lambda_e^T K_e x_e (K_e from MT02AA with

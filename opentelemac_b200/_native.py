@@ -30,7 +30,8 @@ EXPORTS = [
     "bief_solve_mixed", "bief_solve_mixed_dev", "bief_matvec", "bief_matvec_dev",
     "bief_assemble_wave_dev", "bief_wave_coef_grad_dev", "bief_launch_info",
     "bief_last_timing", "bief_kernel_launches", "bief_strerror", "bief_solve_noalloc",
-    "bief_batch_solve_mixed_dev",
+    "bief_batch_solve_mixed_dev", "bief_set_segments", "bief_set_matrix_seg",
+    "bief_set_matrix_seg_dev", "bief_ebe_to_seg", "bief_matrix_storage",
 ]
 
 
@@ -86,6 +87,11 @@ def lib():
             "bief_solve_noalloc": ([i, i, i, vp, vp, vp, c, c, vp, vp, pcfg, pd, i, vp], i),
             "bief_batch_solve_mixed_dev": ([vp, i, vp, vp, vp, vp, i, d, d, i, i, i, vp, vp, vp,
                                             vp, vp], i),
+            "bief_set_segments": ([vp, i, i, vp], i),
+            "bief_set_matrix_seg": ([vp, vp, vp, c, c], i),
+            "bief_set_matrix_seg_dev": ([vp, vp, vp, c, c], i),
+            "bief_ebe_to_seg": ([vp, vp], i),
+            "bief_matrix_storage": ([vp], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

@@ -63,7 +63,7 @@ class BatchSolver:
         self.A.assemble_wave(xc, yc, coef.contiguous())
 
     # -- solve
-    def solve_mixed(self, x, b, precon=2, inner_tol=0.1, outer_tol=1e-8, max_outer=1000,
+    def solve_mixed(self, x, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, max_outer=1000,
                     max_inner=1000000, nodes_per_thread=None):
         """x (in/out), b: device vectors over the whole mesh.  Returns a dict
         of per-instance status, inner/outer counts, relres and kernel ms."""
@@ -88,7 +88,7 @@ class BatchSolver:
                          kernel_ms=self.mesh.last_timing()[0], nodes_per_thread=nodes_per_thread)
         return self.last
 
-    def autotune(self, b, precon=2, inner_tol=0.1, outer_tol=1e-8, candidates=(1, 2, 4),
+    def autotune(self, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, candidates=(1, 2, 4),
                  probe_inner=30):
         """Pick nodes-per-thread by timing `probe_inner` inner iterations of
         every instance with each candidate (kernel time per inner

@@ -90,6 +90,19 @@ class Mesh:
     def kernel_launches(self):
         return int(_native.lib().bief_kernel_launches(self._h))
 
+    def set_segments(self, g1, g2):
+        """Segment numbering (MESH%GLOSEG) from 0-based end points g1, g2
+        (see meshgen.segments for the STOSEG conventions).  Enables segment
+        storage (STO=3) matrices on this mesh."""
+        g1 = np.asarray(g1)
+        g2 = np.asarray(g2)
+        gl = np.ascontiguousarray(np.concatenate([g1, g2]).astype(np.int32) + 1)
+        self.nseg = int(g1.size)
+        _check(_native.lib().bief_set_segments(self._h, self.nseg, self.nseg,
+                                               gl.ctypes.data_as(ctypes.c_void_p)),
+               "bief_set_segments")
+        return self
+
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
             _native.lib().bief_destroy(self._h)
@@ -131,15 +144,44 @@ class Matrix:
         return self
 
     def get(self):
-        """Stored (dm, xm, typdia) as numpy arrays."""
-        nd = {"S": 3, "Q": 6, "0": 0}[self.typext]
+        """Stored (dm, xm, typdia) as numpy arrays: xm (ndiag, nelem) for EBE
+        storage, (ncol, nseg) for segment storage."""
+        seg = self.storage == 3
+        nd = ({"S": 1, "Q": 2, "0": 0} if seg else {"S": 3, "Q": 6, "0": 0})[self.typext]
         dm = np.empty(self.mesh.npoin)
-        xm = np.empty((max(nd, 1), self.mesh.nelem))
+        xm = np.empty((max(nd, 1), self.mesh.nseg if seg else self.mesh.nelem))
         td = ctypes.create_string_buffer(2)
         _check(_native.lib().bief_get_matrix(self.mesh.handle, _ptr(dm), _ptr(xm), td),
                "bief_get_matrix")
         self.typdia = td.value.decode()
         return dm, xm[:nd], self.typdia
+
+    def set_seg(self, da, xa, typdia="Q", typext="S"):
+        """Segment storage (STO=3): DA (npoin,) and XA (nseg,) for 'S' or
+        (2, nseg) for 'Q'; numpy arrays or torch CUDA tensors."""
+        L = _native.lib()
+        if _is_torch(da):
+            _check(L.bief_set_matrix_seg_dev(self.mesh.handle, _ptr(da), _ptr(xa),
+                                             typdia.encode(), typext.encode()),
+                   "bief_set_matrix_seg_dev")
+        else:
+            da = np.ascontiguousarray(da, dtype=np.float64)
+            xa = (np.ascontiguousarray(np.asarray(xa, dtype=np.float64).ravel())
+                  if typext != "0" else np.zeros(1))
+            _check(L.bief_set_matrix_seg(self.mesh.handle, _ptr(da), _ptr(xa), typdia.encode(),
+                                         typext.encode()), "bief_set_matrix_seg")
+        self.typdia, self.typext = typdia, typext
+        return self
+
+    def to_segments(self):
+        """ASSEX3: the stored EBE matrix becomes segment storage."""
+        _check(_native.lib().bief_ebe_to_seg(self.mesh.handle, None), "bief_ebe_to_seg")
+        return self
+
+    @property
+    def storage(self):
+        """1 (EBE) or 3 (segments)."""
+        return _check(_native.lib().bief_matrix_storage(self.mesh.handle), "bief_matrix_storage")
 
     def assemble_wave(self, xc, yc, coef):
         """A = M + coef_e K_e from device coordinates and coefficients

@@ -38,6 +38,15 @@ struct bief_handle {
   float *d_seg_c = nullptr, *d_s32 = nullptr;
   long long nrec = 0, nseg = 0;
   int max_nnb = 0;
+  // segment storage (STO=3): GLOSEG, per-node incident segments (sliced),
+  // faces of each segment, XA stored and scaled, per-slot coefficients
+  int sto = 1, has_segments = 0, nsg = 0;
+  long long nsg_slots = 0;
+  int *d_g1 = nullptr, *d_g2 = nullptr, *d_sg_meta = nullptr, *d_sg_off = nullptr,
+      *d_sg_sx = nullptr, *d_sg_col = nullptr;
+  int2 *d_segel = nullptr;
+  double *d_xa = nullptr, *d_xas = nullptr, *d_sg_c64 = nullptr;
+  float *d_sg_c32 = nullptr;
   // vectors
   double *d_x = nullptr, *d_b = nullptr, *d_bs = nullptr, *d_r = nullptr, *d_d0 = nullptr,
          *d_d1 = nullptr, *d_ad = nullptr, *d_t = nullptr;
@@ -135,24 +144,56 @@ void dispatch_mv(bief_handle *h, int td, bool sym, bool tr, const double *xm, co
 #undef MV_CASE
 }
 
-void *cg_kernel(int td) {
-  if (td == DIA_Q) return (void *)k_cg64<DIA_Q>;
-  if (td == DIA_I) return (void *)k_cg64<DIA_I>;
-  return (void *)k_cg64<DIA_0>;
+void *cg_kernel(int td, int sto) {
+  if (sto == 3) {
+    if (td == DIA_Q) return (void *)k_cg64<DIA_Q, 3>;
+    if (td == DIA_I) return (void *)k_cg64<DIA_I, 3>;
+    return (void *)k_cg64<DIA_0, 3>;
+  }
+  if (td == DIA_Q) return (void *)k_cg64<DIA_Q, 1>;
+  if (td == DIA_I) return (void *)k_cg64<DIA_I, 1>;
+  return (void *)k_cg64<DIA_0, 1>;
 }
 
-void *mixed_kernel(int td) {
-  if (td == DIA_Q) return (void *)k_mixed<DIA_Q>;
-  if (td == DIA_I) return (void *)k_mixed<DIA_I>;
-  return (void *)k_mixed<DIA_0>;
+void *mixed_kernel(int td, int sto) {
+  if (sto == 3) {
+    if (td == DIA_Q) return (void *)k_mixed<DIA_Q, 3>;
+    if (td == DIA_I) return (void *)k_mixed<DIA_I, 3>;
+    return (void *)k_mixed<DIA_0, 3>;
+  }
+  if (td == DIA_Q) return (void *)k_mixed<DIA_Q, 1>;
+  if (td == DIA_I) return (void *)k_mixed<DIA_I, 1>;
+  return (void *)k_mixed<DIA_0, 1>;
+}
+
+template <int TD, bool SYM, bool TR>
+void launch_mvseg(bief_handle *h, bool ext, const double *xa, const double *da, const double *y,
+                  double *x, int opc, double c, cudaStream_t st) {
+  k_mvseg<TD, SYM, TR><<<grid_for(h->npoin, h->nsm), 256, 0, st>>>(
+      h->npoin, h->nsg, ext, h->d_sg_meta, h->d_sg_off, h->d_sg_sx, h->d_sg_col, xa, da, y, x,
+      opc, c);
+}
+
+void dispatch_mvseg(bief_handle *h, int td, bool sym, bool tr, bool ext, const double *xa,
+                    const double *da, const double *y, double *x, int opc, double c,
+                    cudaStream_t st) {
+#define MVS_CASE(TD_, S_, T_) \
+  if (td == TD_ && sym == S_ && tr == T_) return launch_mvseg<TD_, S_, T_>(h, ext, xa, da, y, x, opc, c, st);
+  MVS_CASE(DIA_Q, true, false) MVS_CASE(DIA_I, true, false) MVS_CASE(DIA_0, true, false)
+  MVS_CASE(DIA_Q, false, false) MVS_CASE(DIA_I, false, false) MVS_CASE(DIA_0, false, false)
+  MVS_CASE(DIA_Q, true, true) MVS_CASE(DIA_I, true, true) MVS_CASE(DIA_0, true, true)
+  MVS_CASE(DIA_Q, false, true) MVS_CASE(DIA_I, false, true) MVS_CASE(DIA_0, false, true)
+#undef MVS_CASE
 }
 
 // Largest grid of the persistent kernels that is guaranteed co-resident,
 // reduced for small meshes so that each thread has at least two nodes.
 int persistent_grid(int npoin, int nsm, int *out) {
   int best = 1 << 30;
-  void *ks[] = {cg_kernel(DIA_Q), cg_kernel(DIA_I), cg_kernel(DIA_0),
-                mixed_kernel(DIA_Q), mixed_kernel(DIA_I), mixed_kernel(DIA_0)};
+  void *ks[] = {cg_kernel(DIA_Q, 1), cg_kernel(DIA_I, 1), cg_kernel(DIA_0, 1),
+                mixed_kernel(DIA_Q, 1), mixed_kernel(DIA_I, 1), mixed_kernel(DIA_0, 1),
+                cg_kernel(DIA_Q, 3), cg_kernel(DIA_I, 3), cg_kernel(DIA_0, 3),
+                mixed_kernel(DIA_Q, 3), mixed_kernel(DIA_I, 3), mixed_kernel(DIA_0, 3)};
   for (void *k : ks) {
     int bps = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, CG_THREADS, 0));
@@ -206,11 +247,20 @@ int do_precd1(bief_handle *h, int precon, double *x, const double *b_in, double 
   k_precd1_nodes<<<grid_for(n, h->nsm), 256, 0, st>>>(n, precon, td_in, h->d_dm, x, b_in, b_out,
                                                       h->d_dsc, h->d_dms);
   h->launches++;
-  const int ndiag = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
-  if (ndiag) {
-    k_precd1_elems<<<grid_for(h->nelem, h->nsm), 256, 0, st>>>(h->nelem, ndiag, h->d_ik,
-                                                                h->d_dsc, h->d_xm, h->d_xms);
-    h->launches++;
+  if (h->sto == 3) {
+    const int ncol = h->typext == 'Q' ? 2 : (h->typext == 'S' ? 1 : 0);
+    if (ncol) {
+      k_precd1_segs<<<grid_for(h->nsg, h->nsm), 256, 0, st>>>(h->nsg, ncol, h->d_g1, h->d_g2,
+                                                              h->d_dsc, h->d_xa, h->d_xas);
+      h->launches++;
+    }
+  } else {
+    const int ndiag = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
+    if (ndiag) {
+      k_precd1_elems<<<grid_for(h->nelem, h->nsm), 256, 0, st>>>(h->nelem, ndiag, h->d_ik,
+                                                                  h->d_dsc, h->d_xm, h->d_xms);
+      h->launches++;
+    }
   }
   // TYPDIA after OM 'M=DMD' is 'Q' (unless '0'); PRECON divisible by 2
   // or 3 then makes it the identity (precd1.f:137-142).
@@ -235,8 +285,35 @@ int build_records(bief_handle *h, const double *xm, cudaStream_t st) {
   return BIEF_OK;
 }
 
+// Per-slot binary64 coefficients of the working segment operator xa.
+int build_seg_coefs(bief_handle *h, const double *xa, cudaStream_t st) {
+  const int g = grid_for(h->npoin, h->nsm);
+  if (h->typext == 'Q')
+    k_build_sgc<false><<<g, 256, 0, st>>>(h->npoin, h->nsg, h->d_sg_meta, h->d_sg_off,
+                                         h->d_sg_sx, xa, h->d_sg_c64);
+  else
+    k_build_sgc<true><<<g, 256, 0, st>>>(h->npoin, h->nsg, h->d_sg_meta, h->d_sg_off,
+                                        h->d_sg_sx, xa, h->d_sg_c64);
+  h->launches++;
+  CK(cudaGetLastError());
+  return BIEF_OK;
+}
+
 Sell sell_of(const bief_handle *h) {
   Sell S;
+  S.sg_c = nullptr;
+  if (h->sto == 3) {  // segment slots stand in for records and binary32 slots
+    S.meta = h->d_sg_meta;
+    S.rec_off = h->d_sg_off;
+    S.rec_idx = nullptr;
+    S.rec_c = nullptr;
+    S.seg_off = h->d_sg_off;
+    S.seg_col = h->d_sg_col;
+    S.seg_c = h->d_sg_c32;
+    S.s32 = h->d_s32;
+    S.sg_c = h->d_sg_c64;
+    return S;
+  }
   S.meta = h->d_meta;
   S.rec_off = h->d_rec_off;
   S.rec_idx = h->d_rec_idx;
@@ -443,7 +520,9 @@ int bief_destroy(bief_handle *h) {
                   h->d_ad, h->d_t, h->d_z, h->d_ri, h->d_p0, h->d_p1, h->d_q, h->d_part,
                   h->d_ew, h->d_ctl, h->d_err, h->d_meta, h->d_rec_off, h->d_seg_off,
                   h->d_rec_idx, h->d_rec_slot, h->d_rec_c, h->d_seg_col, h->d_seg_c,
-                  h->d_binst, h->d_brel, h->d_bpart};
+                  h->d_binst, h->d_brel, h->d_bpart, h->d_g1, h->d_g2, h->d_sg_meta,
+                  h->d_sg_off, h->d_sg_sx, h->d_sg_col, h->d_segel, h->d_xa, h->d_xas,
+                  h->d_sg_c64, h->d_sg_c32};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -480,6 +559,7 @@ static int set_matrix_impl(bief_handle *h, const double *dm, const double *xm, c
   h->typdia = typdia == 'q' ? 'Q' : (typdia == 'i' ? 'I' : typdia);
   h->typext = typext;
   h->has_matrix = 1;
+  h->sto = 1;
   return BIEF_OK;
 }
 
@@ -498,11 +578,18 @@ int bief_get_matrix(bief_handle *h, double *dm, double *xm, char *typdia) {
   if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
   DevGuard g(h->dev);
   const size_t n = (size_t)h->npoin, ne = (size_t)h->nelem;
-  const int nd = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
   CK(cudaMemcpyAsync(dm, h->d_dm, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
-  if (nd && xm)
-    CK(cudaMemcpy2DAsync(xm, sizeof(double) * h->nelmax, h->d_xm, sizeof(double) * ne,
-                         sizeof(double) * ne, nd, cudaMemcpyDeviceToHost, h->stream));
+  if (h->sto == 3) {
+    const int nc = h->typext == 'Q' ? 2 : (h->typext == 'S' ? 1 : 0);
+    if (nc && xm)
+      CK(cudaMemcpyAsync(xm, h->d_xa, sizeof(double) * nc * h->nsg, cudaMemcpyDeviceToHost,
+                         h->stream));
+  } else {
+    const int nd = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
+    if (nd && xm)
+      CK(cudaMemcpy2DAsync(xm, sizeof(double) * h->nelmax, h->d_xm, sizeof(double) * ne,
+                           sizeof(double) * ne, nd, cudaMemcpyDeviceToHost, h->stream));
+  }
   CK(cudaStreamSynchronize(h->stream));
   if (typdia) *typdia = h->typdia;
   return BIEF_OK;
@@ -515,7 +602,16 @@ int bief_get_matrix_dev(bief_handle *h, double *dm, double *xm, void *stream) {
   cudaStream_t st = (cudaStream_t)stream;
   const size_t n = (size_t)h->npoin, ne = (size_t)h->nelem;
   CK(cudaMemcpyAsync(dm, h->d_dm, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  CK(cudaMemcpyAsync(xm, h->d_xm, sizeof(double) * 3 * ne, cudaMemcpyDeviceToDevice, st));
+  if (h->sto == 3) {
+    const int nc = h->typext == 'Q' ? 2 : (h->typext == 'S' ? 1 : 0);
+    if (nc)
+      CK(cudaMemcpyAsync(xm, h->d_xa, sizeof(double) * nc * h->nsg, cudaMemcpyDeviceToDevice,
+                         st));
+  } else {
+    const int nd = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
+    if (nd)
+      CK(cudaMemcpyAsync(xm, h->d_xm, sizeof(double) * nd * ne, cudaMemcpyDeviceToDevice, st));
+  }
   return BIEF_OK;
 }
 
@@ -529,19 +625,23 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   cudaStream_t s = (cudaStream_t)stream;
   const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
   int td = typdia_code(h->typdia);
-  const double *xm = h->d_xm, *da = h->d_dm;
+  const bool seg = h->sto == 3;
+  const double *xm = seg ? h->d_xa : h->d_xm, *da = h->d_dm;
   const double *bw = b;
   if (diag) {
     if ((st = do_precd1(h, precon, x, b, h->d_bs, &td, s))) return st;
-    xm = h->d_xms;
+    xm = seg ? h->d_xas : h->d_xms;
     da = h->d_dms;
     bw = h->d_bs;
   }
   if (h->typext == '0') {  // no off-diagonal terms: zero records
-    CK(cudaMemsetAsync(h->d_xms, 0, sizeof(double) * 3 * h->nelem, s));
-    xm = h->d_xms;
+    if (seg)
+      CK(cudaMemsetAsync(h->d_xas, 0, sizeof(double) * h->nsg, s));
+    else
+      CK(cudaMemsetAsync(h->d_xms, 0, sizeof(double) * 3 * h->nelem, s));
+    xm = seg ? h->d_xas : h->d_xms;
   }
-  if ((st = build_records(h, xm, s))) return st;
+  if ((st = seg ? build_seg_coefs(h, xm, s) : build_records(h, xm, s))) return st;
   CgP P;
   P.npoin = h->npoin;
   P.nitmax = cfg->nitmax;
@@ -560,7 +660,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   P.timeout_ns = h->timeout_ns;
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
   CK(cudaEventRecord(h->ev[0], s));
-  if ((st = launch_coop(h, cg_kernel(td), &P, s))) return st;
+  if ((st = launch_coop(h, cg_kernel(td, h->sto), &P, s))) return st;
   CK(cudaEventRecord(h->ev[1], s));
   CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -575,10 +675,17 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     // SOLVE leaves B = D.B and A = D.A.D with TYPDIA from PRECD1
     CK(cudaMemcpyAsync(b, h->d_bs, sizeof(double) * h->npoin, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(h->d_dm, h->d_dms, sizeof(double) * h->npoin, cudaMemcpyDeviceToDevice, s));
-    const int nd = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
-    if (nd)
-      CK(cudaMemcpyAsync(h->d_xm, h->d_xms, sizeof(double) * nd * h->nelem,
-                         cudaMemcpyDeviceToDevice, s));
+    if (seg) {
+      const int nc = h->typext == 'Q' ? 2 : (h->typext == 'S' ? 1 : 0);
+      if (nc)
+        CK(cudaMemcpyAsync(h->d_xa, h->d_xas, sizeof(double) * nc * h->nsg,
+                           cudaMemcpyDeviceToDevice, s));
+    } else {
+      const int nd = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
+      if (nd)
+        CK(cudaMemcpyAsync(h->d_xm, h->d_xms, sizeof(double) * nd * h->nelem,
+                           cudaMemcpyDeviceToDevice, s));
+    }
     CK(cudaStreamSynchronize(s));
     h->typdia = td == DIA_I ? 'I' : (td == DIA_0 ? '0' : 'Q');
   }
@@ -610,20 +717,36 @@ int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b, int precon,
   if (precon == 0) precon = 1;
   if (precon < 0 || precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 || precon % 17 == 0)
     return BIEF_ERR_UNSUPPORTED;
-  if (h->max_nnb > MAX_NEIGHBOURS) return BIEF_ERR_SIZE;
+  const bool seg = h->sto == 3;
+  if (!seg && h->max_nnb > MAX_NEIGHBOURS) return BIEF_ERR_SIZE;
   DevGuard g(h->dev);
   cudaStream_t s = (cudaStream_t)stream;
   const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
   int td = typdia_code(h->typdia), st;
-  const double *xm = h->d_xm, *da = h->d_dm, *bw = b;
+  const double *xm = seg ? h->d_xa : h->d_xm, *da = h->d_dm, *bw = b;
   if (diag) {
     if ((st = do_precd1(h, precon, x, b, h->d_bs, &td, s))) return st;
-    xm = h->d_xms;
+    xm = seg ? h->d_xas : h->d_xms;
     da = h->d_dms;
     bw = h->d_bs;
   }
-  if ((st = build_records(h, xm, s))) return st;
-  {  // binary32 edge-assembled copy of the working operator
+  if (seg) {
+    // binary64 slot coefficients, then their binary32 copy and row sums
+    if ((st = build_seg_coefs(h, xm, s))) return st;
+    const int gn = grid_for(h->npoin, h->nsm);
+#define SG_ARGS h->npoin, h->d_sg_meta, h->d_sg_off, h->d_sg_c64, da, h->d_sg_c32, h->d_s32
+    if (td == DIA_Q)
+      k_build_sg32<DIA_Q><<<gn, 256, 0, s>>>(SG_ARGS);
+    else if (td == DIA_I)
+      k_build_sg32<DIA_I><<<gn, 256, 0, s>>>(SG_ARGS);
+    else
+      k_build_sg32<DIA_0><<<gn, 256, 0, s>>>(SG_ARGS);
+#undef SG_ARGS
+    h->launches++;
+    CK(cudaGetLastError());
+  } else if ((st = build_records(h, xm, s))) {
+    return st;
+  } else {  // binary32 edge-assembled copy of the working operator
     const int gn = grid_for(h->npoin, h->nsm);
 #define SEG_ARGS                                                                              \
   h->npoin, h->nelem, h->d_ptr, h->d_ek, xm, da, h->d_meta, h->d_rec_off, h->d_rec_slot, \
@@ -659,7 +782,7 @@ int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b, int precon,
   P.timeout_ns = h->timeout_ns;
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
   CK(cudaEventRecord(h->ev[0], s));
-  if ((st = launch_coop(h, mixed_kernel(td), &P, s))) return st;
+  if ((st = launch_coop(h, mixed_kernel(td, h->sto), &P, s))) return st;
   CK(cudaEventRecord(h->ev[1], s));
   CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -704,14 +827,18 @@ int bief_matvec_dev(bief_handle *h, const char *op, double *x, const double *y, 
     CK(cudaMemcpyAsync(h->d_t, y, nb, cudaMemcpyDeviceToDevice, s));
     y = h->d_t;
   }
-  const double *xm = h->d_xm;
-  if (h->typext == '0') {
-    // no off-diagonal terms: reuse the symmetric kernel on a zero operator
-    CK(cudaMemsetAsync(h->d_xms, 0, sizeof(double) * 3 * h->nelem, s));
-    xm = h->d_xms;
-  }
   CK(cudaEventRecord(h->ev[2], s));
-  dispatch_mv(h, td, sym, trans, xm, h->d_dm, y, x, opc, c, s);
+  if (h->sto == 3) {  // MVSEG
+    dispatch_mvseg(h, td, sym, trans, h->typext != '0', h->d_xa, h->d_dm, y, x, opc, c, s);
+  } else {
+    const double *xm = h->d_xm;
+    if (h->typext == '0') {
+      // no off-diagonal terms: reuse the symmetric kernel on a zero operator
+      CK(cudaMemsetAsync(h->d_xms, 0, sizeof(double) * 3 * h->nelem, s));
+      xm = h->d_xms;
+    }
+    dispatch_mv(h, td, sym, trans, xm, h->d_dm, y, x, opc, c, s);
+  }
   h->launches++;
   CK(cudaGetLastError());
   CK(cudaEventRecord(h->ev[3], s));
@@ -756,6 +883,7 @@ int bief_assemble_wave_dev(bief_handle *h, const double *xc, const double *yc,
   h->typdia = 'Q';
   h->typext = 'S';
   h->has_matrix = 1;
+  h->sto = 1;
   return BIEF_OK;
 }
 
@@ -784,7 +912,7 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
       nodes_per_thread != 8)
     return BIEF_ERR_ARGS;
   if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
-  if (h->typext != 'S') return BIEF_ERR_UNSUPPORTED;
+  if (h->typext != 'S' || h->sto != 1) return BIEF_ERR_UNSUPPORTED;
   if (h->max_nnb > MAX_NEIGHBOURS) return BIEF_ERR_SIZE;
   if (precon == 0) precon = 1;
   if (precon < 0 || precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 || precon % 17 == 0)
@@ -912,6 +1040,176 @@ int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads) {
   if (nblocks) *nblocks = h->G;
   if (nthreads) *nthreads = h->T;
   return BIEF_OK;
+}
+
+int bief_set_segments(bief_handle *h, int nseg, int maxseg, const int *gloseg) {
+  if (!h || !gloseg || nseg <= 0 || maxseg < nseg) return BIEF_ERR_ARGS;
+  const int n = h->npoin, ne = h->nelem;
+  std::vector<int> g1(nseg), g2(nseg);
+  for (int s = 0; s < nseg; ++s) {
+    const int a = gloseg[s], b = gloseg[(size_t)maxseg + s];
+    if (a < 1 || a > n || b < 1 || b > n || a == b) return BIEF_ERR_BAD_MESH;
+    g1[s] = a - 1;
+    g2[s] = b - 1;
+  }
+  // Element faces -> segments (face f joins local points f and f+1 mod 3);
+  // per segment its faces in element order (at most two).
+  std::vector<long long> key(nseg);
+  std::vector<int> ord(nseg);
+  for (int s = 0; s < nseg; ++s) {
+    key[s] = (long long)std::min(g1[s], g2[s]) * n + std::max(g1[s], g2[s]);
+    ord[s] = s;
+  }
+  std::sort(ord.begin(), ord.end(), [&](int a, int b) { return key[a] < key[b]; });
+  for (int q = 1; q < nseg; ++q)
+    if (key[ord[q]] == key[ord[q - 1]]) return BIEF_ERR_BAD_MESH;  // duplicated edge
+  std::vector<long long> skey(nseg);
+  for (int q = 0; q < nseg; ++q) skey[q] = key[ord[q]];
+  std::vector<int2> segel(nseg, make_int2(-1, -1));
+  std::vector<int> ik(3 * (size_t)ne);
+  if (cudaMemcpy(ik.data(), h->d_ik, sizeof(int) * 3 * (size_t)ne, cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return BIEF_ERR_CUDA;
+  for (int e = 0; e < ne; ++e)
+    for (int f = 0; f < 3; ++f) {
+      const int a = ik[(size_t)f * ne + e], b = ik[(size_t)((f + 1) % 3) * ne + e];
+      const long long k = (long long)std::min(a, b) * n + std::max(a, b);
+      auto it = std::lower_bound(skey.begin(), skey.end(), k);
+      if (it == skey.end() || *it != k) return BIEF_ERR_BAD_MESH;  // face without segment
+      const int s = ord[it - skey.begin()];
+      if (segel[s].x < 0)
+        segel[s].x = (e << 2) | f;
+      else if (segel[s].y < 0)
+        segel[s].y = (e << 2) | f;
+      else
+        return BIEF_ERR_BAD_MESH;  // edge of more than two elements
+    }
+  // Per node, incident segments in ascending order (the order in which MVSEG
+  // adds into the node), in 32-node slices.
+  std::vector<int> deg(n, 0);
+  for (int s = 0; s < nseg; ++s) {
+    deg[g1[s]]++;
+    deg[g2[s]]++;
+  }
+  const int nsl = (n + 31) / 32;
+  std::vector<int> off(nsl + 1, 0), meta(n);
+  for (int sl = 0; sl < nsl; ++sl) {
+    int w = 0;
+    for (int i = 32 * sl; i < std::min(n, 32 * sl + 32); ++i) w = std::max(w, deg[i]);
+    const long long o = (long long)off[sl] + 32LL * w;
+    if (o > 0x7fffffffLL) return BIEF_ERR_SIZE;
+    off[sl + 1] = (int)o;
+  }
+  for (int i = 0; i < n; ++i) {
+    if (deg[i] > 0x7fff) return BIEF_ERR_SIZE;
+    meta[i] = deg[i] | (deg[i] << 16);
+  }
+  const size_t nslot = (size_t)off[nsl];
+  std::vector<int> sx(nslot, 0), col(nslot, 0), fill(n, 0);
+  for (int s = 0; s < nseg; ++s)
+    for (int side = 0; side < 2; ++side) {
+      const int i = side ? g2[s] : g1[s];
+      const size_t q = (size_t)off[i >> 5] + (i & 31) + 32 * (size_t)fill[i]++;
+      sx[q] = (s << 1) | side;
+      col[q] = side ? g1[s] : g2[s];
+    }
+  DevGuard g(h->dev);
+  void *old[] = {h->d_g1, h->d_g2, h->d_sg_meta, h->d_sg_off, h->d_sg_sx, h->d_sg_col,
+                 h->d_segel, h->d_xa, h->d_xas, h->d_sg_c64, h->d_sg_c32};
+  CK(cudaStreamSynchronize(h->stream));
+  for (void *p : old)
+    if (p) cudaFree(p);
+  h->d_g1 = h->d_g2 = h->d_sg_meta = h->d_sg_off = h->d_sg_sx = h->d_sg_col = nullptr;
+  h->d_segel = nullptr;
+  h->d_xa = h->d_xas = h->d_sg_c64 = nullptr;
+  h->d_sg_c32 = nullptr;
+  h->has_segments = 0;
+  if (h->sto == 3) h->has_matrix = 0;  // the stored segment matrix belonged to the old numbering
+  h->sto = 1;
+  int st;
+  if ((st = dalloc(&h->d_g1, nseg)) || (st = dalloc(&h->d_g2, nseg)) ||
+      (st = dalloc(&h->d_sg_meta, n)) || (st = dalloc(&h->d_sg_off, (size_t)nsl + 1)) ||
+      (st = dalloc(&h->d_sg_sx, nslot)) || (st = dalloc(&h->d_sg_col, nslot)) ||
+      (st = dalloc(&h->d_segel, nseg)) || (st = dalloc(&h->d_xa, 2 * (size_t)nseg)) ||
+      (st = dalloc(&h->d_xas, 2 * (size_t)nseg)) || (st = dalloc(&h->d_sg_c64, nslot)) ||
+      (st = dalloc(&h->d_sg_c32, nslot)))
+    return st;
+  CK(cudaMemcpyAsync(h->d_g1, g1.data(), sizeof(int) * nseg, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_g2, g2.data(), sizeof(int) * nseg, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->d_sg_meta, meta.data(), sizeof(int) * n, cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaMemcpyAsync(h->d_sg_off, off.data(), sizeof(int) * (nsl + 1), cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaMemcpyAsync(h->d_sg_sx, sx.data(), sizeof(int) * nslot, cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaMemcpyAsync(h->d_sg_col, col.data(), sizeof(int) * nslot, cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaMemcpyAsync(h->d_segel, segel.data(), sizeof(int2) * nseg, cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaMemsetAsync(h->d_sg_c64, 0, sizeof(double) * nslot, h->stream));
+  CK(cudaMemsetAsync(h->d_sg_c32, 0, sizeof(float) * nslot, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->nsg = nseg;
+  h->nsg_slots = (long long)nslot;
+  h->has_segments = 1;
+  return BIEF_OK;
+}
+
+static int set_matrix_seg_impl(bief_handle *h, const double *da, const double *xa, char typdia,
+                               char typext, bool dev) {
+  if (!h || !da) return BIEF_ERR_ARGS;
+  if (!h->has_segments) return BIEF_ERR_NO_MATRIX;
+  if (typdia_code(typdia) < 0) return BIEF_ERR_ARGS;
+  if (typext != 'S' && typext != 'Q' && typext != '0') return BIEF_ERR_ARGS;
+  if (typext != '0' && !xa) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  const size_t n = (size_t)h->npoin;
+  const int nc = typext == 'Q' ? 2 : (typext == 'S' ? 1 : 0);
+  const cudaMemcpyKind kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CK(cudaMemcpyAsync(h->d_dm, da, sizeof(double) * n, kind, h->stream));
+  if (nc) CK(cudaMemcpyAsync(h->d_xa, xa, sizeof(double) * nc * h->nsg, kind, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->typdia = typdia == 'q' ? 'Q' : (typdia == 'i' ? 'I' : typdia);
+  h->typext = typext;
+  h->has_matrix = 1;
+  h->sto = 3;
+  return BIEF_OK;
+}
+
+int bief_set_matrix_seg(bief_handle *h, const double *da, const double *xa, char typdia,
+                        char typext) {
+  return set_matrix_seg_impl(h, da, xa, typdia, typext, false);
+}
+
+int bief_set_matrix_seg_dev(bief_handle *h, const double *da, const double *xa, char typdia,
+                            char typext) {
+  return set_matrix_seg_impl(h, da, xa, typdia, typext, true);
+}
+
+int bief_ebe_to_seg(bief_handle *h, void *stream) {
+  if (!h) return BIEF_ERR_ARGS;
+  if (!h->has_matrix || !h->has_segments) return BIEF_ERR_NO_MATRIX;
+  if (h->sto == 3) return BIEF_OK;
+  DevGuard g(h->dev);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int gs = grid_for(h->nsg, h->nsm);
+  if (h->typext == 'S')
+    k_assex3<true><<<gs, 256, 0, s>>>(h->nsg, h->nelem, h->nelem, h->d_segel, h->d_g1, h->d_ik,
+                                      h->d_xm, h->d_xa);
+  else if (h->typext == 'Q')
+    k_assex3<false><<<gs, 256, 0, s>>>(h->nsg, h->nelem, h->nelem, h->d_segel, h->d_g1, h->d_ik,
+                                       h->d_xm, h->d_xa);
+  if (h->typext != '0') h->launches++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  h->sto = 3;
+  return BIEF_OK;
+}
+
+int bief_matrix_storage(bief_handle *h) {
+  if (!h) return BIEF_ERR_ARGS;
+  if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
+  return h->sto;
 }
 
 int bief_last_timing(bief_handle *h, float *solve_ms, float *matvec_ms) {

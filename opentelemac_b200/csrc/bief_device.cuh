@@ -266,6 +266,7 @@ struct Sell {
   const int *seg_col;     // per slot: neighbour
   const float *seg_c;     // per slot: binary32 coefficient
   const float *s32;       // per node: binary32 row sum
+  const double *sg_c;     // segment storage: per slot, binary64 XA1/XA2
 };
 
 template <class V>
@@ -304,6 +305,36 @@ __device__ __forceinline__ void rec_row2(int i0, int i1, bool has1, double &a0, 
       a1 = add(a1, add(mul(c.x, vec(v.x)), mul(c.y, vec(v.y))));
     }
   }
+}
+
+// Segment storage (STO=3, MVSEG order, mvseg.f:129-135): node i has one
+// slot per incident segment, in ascending segment order, holding XA1 (node
+// is GLOSEG1) or XA2 (GLOSEG2) and the other end, in the sliced layout of
+// the binary32 slots (meta, rec_off and seg_col then describe these
+// slots).  Row: acc + XA*Y(other) per slot, left to right.
+template <class V>
+__device__ __forceinline__ void sgr_row2(int i0, int i1, bool has1, double &a0, double &a1,
+                                         const Sell &S, V vec) {
+  const int d0 = __ldg(S.meta + i0) & 0xffff;
+  const int d1 = has1 ? (__ldg(S.meta + i1) & 0xffff) : 0;
+  const int b0 = __ldg(S.rec_off + (i0 >> 5)) + (i0 & 31);
+  const int b1 = has1 ? __ldg(S.rec_off + (i1 >> 5)) + (i1 & 31) : 0;
+  const int dm = max(d0, d1);
+  for (int m = 0; m < dm; ++m) {
+    if (m < d0) a0 = add(a0, mul(__ldg(S.sg_c + b0 + 32 * m), vec(__ldg(S.seg_col + b0 + 32 * m))));
+    if (m < d1) a1 = add(a1, mul(__ldg(S.sg_c + b1 + 32 * m), vec(__ldg(S.seg_col + b1 + 32 * m))));
+  }
+}
+
+// Binary64 off-diagonal row product of the working operator in either
+// storage: EBE records (STO=1) or segments (STO=3).
+template <int STO, class V>
+__device__ __forceinline__ void op_row2(int i0, int i1, bool has1, double &a0, double &a1,
+                                        const Sell &S, V vec) {
+  if constexpr (STO == 3)
+    sgr_row2(i0, i1, has1, a0, a1, S, vec);
+  else
+    rec_row2(i0, i1, has1, a0, a1, S, vec);
 }
 
 template <class V>

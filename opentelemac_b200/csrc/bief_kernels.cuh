@@ -64,6 +64,153 @@ __global__ void __launch_bounds__(256) k_matvec(int npoin, int nelem, const int 
 }
 
 // ---------------------------------------------------------------------------
+// Segment storage (STO=3).  Per node, one slot per incident segment in
+// ascending segment order (sliced layout: slot m of node i at
+// off[i/32] + 32m + i%32): sx = ISEG<<1 | side (side 0: node is GLOSEG1,
+// side 1: GLOSEG2), col = the other end.  XA is XA(NSEG) ('S') or
+// XA(NSEG,2) ('Q', second column from NSEG on).
+// ---------------------------------------------------------------------------
+
+// MVSEG (mvseg.f:110-720): X takes the diagonal term through OV
+// (ov.f:177-324: 'X=YZ', 'X=CYZ' = (C*Y)*Z, 'X=X+YZ', ...), then for each
+// incident segment in ascending order X = X +/- [C*]XA*Y(other), the
+// additions the reference's segment loop makes into this node, in its order.
+template <int TD, bool SYM, bool TRANS>
+__global__ void __launch_bounds__(256) k_mvseg(int npoin, int nseg, bool ext,
+                                               const int *__restrict__ meta,
+                                               const int *__restrict__ off,
+                                               const int *__restrict__ sx,
+                                               const int *__restrict__ col,
+                                               const double *__restrict__ xa,
+                                               const double *__restrict__ da,
+                                               const double *__restrict__ y, double *x, int opc,
+                                               double c) {
+  const bool neg = (opc == OP_MAY || opc == OP_XMAY);
+  const bool cm = (opc == OP_CAY || opc == OP_XPCAY);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    const double yi = __ldg(y + i);
+    double r;
+    if (TD == DIA_0) {
+      // 'X=C' with 0 for X=AY, X=CAY, X=-AY; nothing for the X=X+.. forms
+      r = (opc == OP_AY || opc == OP_CAY || opc == OP_MAY) ? 0.0 : x[i];
+    } else {
+      const double d = TD == DIA_Q ? mul(yi, __ldg(da + i)) : yi;
+      const double cd = TD == DIA_Q ? mul(mul(c, yi), __ldg(da + i)) : mul(c, yi);
+      switch (opc) {
+        case OP_AY: r = d; break;
+        case OP_CAY: r = cd; break;
+        case OP_MAY: r = -d; break;
+        case OP_XPAY: r = add(x[i], d); break;
+        case OP_XMAY: r = sub(x[i], d); break;
+        default: r = add(x[i], cd); break;
+      }
+    }
+    if (ext) {
+      const int deg = __ldg(meta + i) & 0xffff;
+      const int base = __ldg(off + (i >> 5)) + (i & 31);
+      for (int m = 0; m < deg; ++m) {
+        const int p = __ldg(sx + base + 32 * m);
+        const int j = __ldg(col + base + 32 * m);
+        const int q = SYM ? 0 : ((p & 1) ^ (TRANS ? 1 : 0));
+        double a = __ldg(xa + (size_t)q * nseg + (p >> 1));
+        if (cm) a = mul(c, a);
+        const double t = mul(a, __ldg(y + j));
+        r = neg ? sub(r, t) : add(r, t);
+      }
+    }
+    x[i] = r;
+  }
+}
+
+// OMSEG 'M=DMD' off-diagonal part (omseg.f:530-541):
+// XA(ISEG) * D(GLOSEG1) * D(GLOSEG2), for each stored column.
+__global__ void k_precd1_segs(int nseg, int ncol, const int *__restrict__ g1,
+                              const int *__restrict__ g2, const double *__restrict__ dsc,
+                              const double *__restrict__ xa, double *xas) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+    const double d1 = dsc[g1[s]], d2 = dsc[g2[s]];
+    for (int q = 0; q < ncol; ++q)
+      xas[(size_t)q * nseg + s] = mul(mul(xa[(size_t)q * nseg + s], d1), d2);
+  }
+}
+
+// Per slot, the binary64 coefficient of the working operator's 'X=AY' row:
+// XA1 for side 0, XA2 for side 1.
+template <bool SYM>
+__global__ void k_build_sgc(int npoin, int nseg, const int *__restrict__ meta,
+                            const int *__restrict__ off, const int *__restrict__ sx,
+                            const double *__restrict__ xa, double *sg_c) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    const int deg = meta[i] & 0xffff;
+    const int base = off[i >> 5] + (i & 31);
+    for (int m = 0; m < deg; ++m) {
+      const int p = sx[base + 32 * m];
+      sg_c[base + 32 * m] = xa[(size_t)(SYM ? 0 : (p & 1)) * nseg + (p >> 1)];
+    }
+  }
+}
+
+// Binary32 operator of a symmetric segment matrix for the mixed solver: the
+// slot coefficients rounded, and the row sum diag + XA of each slot added
+// in slot order in binary64, rounded once.
+template <int TD>
+__global__ void k_build_sg32(int npoin, const int *__restrict__ meta, const int *__restrict__ off,
+                             const double *__restrict__ sg_c, const double *__restrict__ da,
+                             float *seg_c, float *s32) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    const int deg = meta[i] & 0xffff;
+    const int base = off[i >> 5] + (i & 31);
+    double srow = TD == DIA_Q ? da[i] : (TD == DIA_I ? 1.0 : 0.0);
+    for (int m = 0; m < deg; ++m) {
+      const double cv = sg_c[base + 32 * m];
+      seg_c[base + 32 * m] = (float)cv;
+      srow = add(srow, cv);
+    }
+    s32[i] = (float)srow;
+  }
+}
+
+// ASSEX3 for P1 (assex3.f:150-160 -> as3_1111_s.f:71-79, as3_1111_q.f:85-98,
+// STOXMT=1): each segment sums, from zero and in element order, the EBE
+// terms of the (at most two) element faces that it is: face 1 (points 1-2)
+// XMT(,1) [Q: and XMT(,4)], face 2 (2-3) XMT(,3) [XMT(,6)], face 3 (3-1)
+// XMT(,2) [XMT(,5)].  For 'Q' the term of row IKLE(f) goes to column
+// ORISEG (1 when GLOSEG1 = IKLE(f)) and the other to column 3-ORISEG.
+// segel: per segment, its faces (e<<2 | f) in element order, -1 if none.
+template <bool SYM>
+__global__ void k_assex3(int nseg, int nelem, int ld, const int2 *__restrict__ segel,
+                         const int *__restrict__ g1, const int *__restrict__ ik,
+                         const double *__restrict__ xmt, double *xa) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+    const int2 fe = segel[s];
+    double a1 = 0.0, a2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int p = q == 0 ? fe.x : fe.y;
+      if (p < 0) continue;
+      const int e = p >> 2, f = p & 3;
+      if (SYM) {
+        const int cs = f == 0 ? 0 : (f == 1 ? 2 : 1);
+        a1 = add(a1, xmt[(size_t)cs * ld + e]);
+      } else {
+        const int ca = f == 0 ? 0 : (f == 1 ? 2 : 4);   // row IKLE(f)
+        const int cb = f == 0 ? 3 : (f == 1 ? 5 : 1);   // row IKLE(f+1)
+        const double va = xmt[(size_t)ca * ld + e], vb = xmt[(size_t)cb * ld + e];
+        if (ik[(size_t)f * nelem + e] == g1[s]) {
+          a1 = add(a1, va);
+          a2 = add(a2, vb);
+        } else {
+          a2 = add(a2, va);
+          a1 = add(a1, vb);
+        }
+      }
+    }
+    xa[s] = a1;
+    if (!SYM) xa[(size_t)nseg + s] = a2;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // PRECD1 change of variables, DIADON=.FALSE., PREXSM=.TRUE.
 // Node part: D = A%D; [|D|]; D = SQRT(D); X = X*D; D = 1/D guarded
 // (ovd.f:92-102: |D| > 1e-10 ? 1/D : 1.0); diagonal of D.A.D
@@ -177,7 +324,7 @@ struct CgP {
   long long timeout_ns;
 };
 
-template <int TD>
+template <int TD, int STO>
 __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
@@ -219,7 +366,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
     const int i1 = i + T;
     const bool h1 = ROW_ILP == 2 && i1 < hi;
     double a0 = diag_term<TD>(x[i], da, i), a1 = h1 ? diag_term<TD>(x[i1], da, i1) : 0.0;
-    rec_row2(i, i1, h1, a0, a1, P.S, [&](int j) { return x[j]; });
+    op_row2<STO>(i, i1, h1, a0, a1, P.S, [&](int j) { return x[j]; });
     const double r0 = sub(a0, b[i]);
     r[i] = r0;
     s = add(s, mul(r0, r0));
@@ -244,7 +391,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
     cur[i] = d0;
     if (h1) cur[i1] = d1;
     double a0 = diag_term<TD>(d0, da, i), a1 = h1 ? diag_term<TD>(d1, da, i1) : 0.0;
-    rec_row2(i, i1, h1, a0, a1, P.S, [&](int j) { return r[j]; });
+    op_row2<STO>(i, i1, h1, a0, a1, P.S, [&](int j) { return r[j]; });
     ad[i] = a0;
     s = add(s, mul(d0, a0));
     if (h1) {
@@ -289,7 +436,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
       nxt[i] = d0;
       if (h1) nxt[i1] = d1;
       double a0 = diag_term<TD>(d0, da, i), a1 = h1 ? diag_term<TD>(d1, da, i1) : 0.0;
-      rec_row2(i, i1, h1, a0, a1, P.S, [&](int j) { return add(r[j], mul(beta, cur[j])); });
+      op_row2<STO>(i, i1, h1, a0, a1, P.S, [&](int j) { return add(r[j], mul(beta, cur[j])); });
       ad[i] = a0;
       s = add(s, mul(d0, a0));
       if (h1) {
@@ -337,7 +484,7 @@ struct MixP {
   long long timeout_ns;
 };
 
-template <int TD>
+template <int TD, int STO>
 __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_mixed(MixP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
@@ -385,7 +532,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_mixed(MixP P) {
       const int i1 = i + T;
       const bool h1 = ROW_ILP == 2 && i1 < hi;
       double a0 = diag_term<TD>(x[i], P.da, i), a1 = h1 ? diag_term<TD>(x[i1], P.da, i1) : 0.0;
-      rec_row2(i, i1, h1, a0, a1, P.S, [&](int j) { return x[j]; });
+      op_row2<STO>(i, i1, h1, a0, a1, P.S, [&](int j) { return x[j]; });
       const double r0 = sub(b[i], a0);
       sd = add(sd, mul(r0, r0));
       const float q0 = (float)r0;

@@ -129,3 +129,65 @@ def shuffled(x, y, ikle0, seed=99):
 
 def mesh_size_for_npoin(npoin):
     return max(2, int(round(np.sqrt(npoin))))
+
+
+def boundary_faces(ikle0):
+    """Boundary faces in boundary order: (elements, faces), face f joining
+    local points f and f+1 mod 3.  Faces of counter-clockwise elements that
+    have no neighbour run the boundary counter-clockwise; each loop is walked
+    from its lowest-numbered node, loops in order of that node."""
+    nb = element_neighbours(ikle0)
+    be, bf = np.nonzero(nb < 0)
+    start = ikle0[be, bf]
+    end = ikle0[be, (bf + 1) % 3]
+    by_start = {int(a): q for q, a in enumerate(start)}
+    seen = np.zeros(be.size, dtype=bool)
+    order = []
+    for q0 in np.argsort(start, kind="stable"):
+        if seen[q0]:
+            continue
+        q = int(q0)
+        while not seen[q]:
+            seen[q] = True
+            order.append(q)
+            q = by_start.get(int(end[q]), q)
+    order = np.array(order, dtype=np.int64)
+    return be[order].astype(np.int32), bf[order].astype(np.int32)
+
+
+def segments(ikle0, npoin):
+    """Segment numbering of a P1 mesh with the conventions of BIEF's STOSEG
+    (stoseg.f:94-225): the boundary segments first, in boundary order
+    (boundary_faces), with GLOSEG = (first, second) point of the face; then
+    every other edge, numbered at its first face in (element, face) order,
+    with GLOSEG ordered by node number.  Returns g1, g2 (0-based GLOSEG
+    columns), eltseg and oriseg (3, nelem): the segment of each element face
+    and 1 where GLOSEG(.,1) is the face's first point, else 2."""
+    ik = np.asarray(ikle0, dtype=np.int64)
+    ne = ik.shape[0]
+    a = np.concatenate([ik[:, 0], ik[:, 1], ik[:, 2]])      # face-major: f*ne + e
+    b = np.concatenate([ik[:, 1], ik[:, 2], ik[:, 0]])
+    key = np.minimum(a, b) * int(npoin) + np.maximum(a, b)
+    be, bf = boundary_faces(ikle0)
+    bq = bf.astype(np.int64) * ne + be              # face index of each boundary segment
+    bkeys = key[bq]
+    # the other edges, numbered in order of their first face in scan order
+    # (element outer, face inner)
+    q = np.arange(3 * ne)
+    scan = (q % ne) * 3 + q // ne
+    other = ~np.isin(key, bkeys)
+    ok, so = key[other], scan[other]
+    idx = np.lexsort((so, ok))
+    ks = ok[idx]
+    head = np.r_[True, ks[1:] != ks[:-1]]
+    first_scan, first_key = so[idx][head], ks[head]
+    keys_sorted = first_key[np.argsort(first_scan, kind="stable")]
+    g1 = np.concatenate([a[bq], keys_sorted // int(npoin)])
+    g2 = np.concatenate([b[bq], keys_sorted % int(npoin)])
+    allkeys = np.concatenate([bkeys, keys_sorted])
+    order = np.argsort(allkeys, kind="stable")
+    seg = order[np.searchsorted(allkeys[order], key)]
+    eltseg = seg.reshape(3, ne)
+    oriseg = np.where(a == g1[seg], 1, 2).reshape(3, ne)
+    return (g1.astype(np.int32), g2.astype(np.int32), eltseg.astype(np.int32),
+            oriseg.astype(np.int32))

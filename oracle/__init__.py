@@ -219,3 +219,116 @@ def solve_omp(ikle0, dm, xm, b, x0=None, nitmax=1000000, eps=1e-8, nthreads=None
                          nitmax, eps, nthreads or (os.cpu_count() or 1), ctypes.byref(nit),
                          ctypes.byref(relres))
     return dict(x=x, status=st, nit=nit.value, relres=relres.value)
+
+
+# -- segment storage (STO=3) ------------------------------------------------
+
+def _seg_lib():
+    L = lib()
+    if not getattr(L, "_seg_ready", False):
+        P = ctypes.POINTER
+        d, i, c = ctypes.c_double, ctypes.c_int, ctypes.c_char
+        pd, pi = P(d), P(i)
+        L.orc_stoseg.argtypes = [i, i, pi, pi, pi, i, pi, pi, pi, pi, pi, pi, pi]
+        L.orc_assex3.argtypes = [i, pi, pi, c, pd, i, i, pd]
+        L.orc_mvseg.argtypes = [ctypes.c_char_p, i, i, pi, pi, pd, pd, c, pd, c, pd, d]
+        L.orc_solve_seg.argtypes = [i, i, pi, pi, pd, pd, pd, P(c), pd, c, i, i, i, d, i, i, i,
+                                    pi, pd, pi]
+        L.orc_solve_mixed_seg.argtypes = [i, i, pi, pi, pd, pd, pd, c, pd, c, i, d, d, i, i, i,
+                                          i, pi, pi, pd]
+        L._seg_ready = True
+    return L
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def stoseg(ikle0, npoin, nelbor, nulone):
+    """STOSEG numbering: boundary segments first (element nelbor[s], face
+    nulone[s], in that order), then the remaining element faces.  Returns
+    g1, g2 (0-based GLOSEG columns), eltseg and oriseg (3, nelem)."""
+    ik, a, b, c = _cols(ikle0)
+    ne = ik.shape[1]
+    nelbor, nulone = _i32(nelbor), _i32(nulone)
+    cap = 3 * ne + 1
+    g1, g2 = np.empty(cap, np.int32), np.empty(cap, np.int32)
+    es, ori = np.empty((3, ne), np.int32), np.empty((3, ne), np.int32)
+    nseg = ctypes.c_int(0)
+    st = _seg_lib().orc_stoseg(npoin, ne, _pi(a), _pi(b), _pi(c), nelbor.size, _pi(nelbor),
+                               _pi(nulone), _pi(g1), _pi(g2), _pi(es), _pi(ori),
+                               ctypes.byref(nseg))
+    if st:
+        raise ValueError("orc_stoseg status %d" % st)
+    n = nseg.value
+    return g1[:n].copy(), g2[:n].copy(), es, ori
+
+
+def assex3(eltseg, oriseg, typext, xmt, nseg):
+    """EBE off-diagonal terms (3|6, nelem) -> segment XA: (nseg,) for 'S',
+    (2, nseg) for 'Q'."""
+    es, ori = _i32(eltseg), _i32(oriseg)
+    ne = es.shape[1]
+    xmt = np.ascontiguousarray(xmt, dtype=np.float64).reshape(-1, ne)
+    xa = np.empty((1 if typext == "S" else 2) * nseg)
+    st = _seg_lib().orc_assex3(ne, _pi(es), _pi(ori), typext.encode(), _pd(xmt), ne, nseg,
+                               _pd(xa))
+    if st:
+        raise ValueError("orc_assex3 status %d" % st)
+    return xa if typext == "S" else xa.reshape(2, nseg)
+
+
+def mvseg(op, g1, g2, dm, typdia, xa, typext, y, c=0.0, x=None):
+    """MATVEC on segment storage (MVSEG): returns the new X (a copy)."""
+    g1, g2 = _i32(g1), _i32(g2)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    n = y.size
+    out = np.zeros(n) if x is None else np.array(x, dtype=np.float64)
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    xa = np.ascontiguousarray(xa, dtype=np.float64).ravel()
+    st = _seg_lib().orc_mvseg(op.encode(), n, g1.size, _pi(g1), _pi(g2), _pd(out), _pd(dm),
+                              typdia.encode(), _pd(xa), typext.encode(), _pd(y), c)
+    if st:
+        raise ValueError("orc_mvseg status %d" % st)
+    return out
+
+
+def solve_seg(g1, g2, dm, typdia, xa, typext, b, x0=None, precon=2, nitmax=100000, eps=1e-8,
+              slv=1, dot_mode=DOT_SEQUENTIAL, nblocks=1, nthreads=256):
+    """SOLVE(SLV=1) on a segment-storage matrix; same outputs as solve()
+    (with 'xa' for the mutated off-diagonal terms)."""
+    g1, g2 = _i32(g1), _i32(g2)
+    b = np.array(b, dtype=np.float64)
+    n = b.size
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    dm = np.array(dm, dtype=np.float64)
+    xa = np.array(xa, dtype=np.float64).ravel().copy()
+    td = ctypes.c_char(typdia.encode())
+    nit, relat = ctypes.c_int(0), ctypes.c_int(0)
+    relres = ctypes.c_double(0.0)
+    st = _seg_lib().orc_solve_seg(n, g1.size, _pi(g1), _pi(g2), _pd(x), _pd(b), _pd(dm),
+                                  ctypes.byref(td), _pd(xa), typext.encode(), slv, precon,
+                                  nitmax, eps, dot_mode, nblocks, nthreads, ctypes.byref(nit),
+                                  ctypes.byref(relres), ctypes.byref(relat))
+    return dict(x=x, b=b, dm=dm, xa=xa, typdia=td.value.decode(), status=st, nit=nit.value,
+                relres=relres.value, relat=relat.value)
+
+
+def solve_mixed_seg(g1, g2, dm, typdia, xa, b, x0=None, precon=2, inner_tol=0.1,
+                    outer_tol=1e-8, max_outer=1000, max_inner=1000000, nblocks=1, nthreads=256):
+    """Mixed-precision solve on a symmetric segment-storage matrix in the
+    device kernels' exact operation order."""
+    g1, g2 = _i32(g1), _i32(g2)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    n = b.size
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    xa = np.ascontiguousarray(xa, dtype=np.float64).ravel()
+    outer, inner = ctypes.c_int(0), ctypes.c_int(0)
+    relres = ctypes.c_double(0.0)
+    st = _seg_lib().orc_solve_mixed_seg(n, g1.size, _pi(g1), _pi(g2), _pd(x), _pd(b), _pd(dm),
+                                        typdia.encode(), _pd(xa), b"S", precon, inner_tol,
+                                        outer_tol, max_outer, max_inner, nblocks, nthreads,
+                                        ctypes.byref(outer), ctypes.byref(inner),
+                                        ctypes.byref(relres))
+    return dict(x=x, status=st, outer=outer.value, inner=inner.value, relres=relres.value)

@@ -267,6 +267,91 @@ int orc_matvec(const char *op, int npoin, int nelem,
     return ORC_OK;
 }
 
+/* mvseg.f:110-720 -- MATVEC on segment storage (STO=3, P1): X takes the
+ * diagonal contribution through OV (ov.f:177-324 formulas), then for
+ * ISEG = 1..NSEG, in that order,
+ *   X(GLOSEG1) = X(GLOSEG1) +/- [C*]XA1(ISEG)*Y(GLOSEG2)
+ *   X(GLOSEG2) = X(GLOSEG2) +/- [C*]XA2(ISEG)*Y(GLOSEG1)
+ * with XA1/XA2 swapped for the transposed operations.  xa holds XA(NSEG)
+ * for TYPEXT 'S' (XA1 = XA2) or XA(NSEG,2) for 'Q' (matvct.f:681-688).
+ * g1/g2 are the 0-based GLOSEG columns. */
+int orc_mvseg(const char *op, int npoin, int nseg, const int *g1, const int *g2,
+              double *x, const double *da, char typdia, const double *xa,
+              char typext, const double *y, double c)
+{
+    char o[9];
+    int n = 0;
+    for (; n < 8 && op[n]; ++n) o[n] = op[n];
+    while (n > 0 && o[n - 1] == ' ') --n;
+    o[n] = 0;
+    /* dk: diagonal form (0 X=D, 1 X=cD, 2 X=-D, 3 X=X+D, 4 X=X-D, 5 X=X+cD);
+     * neg: subtract the segment terms; cm: multiply XA by C; tr: transposed */
+    int dk, neg = 0, cm = 0, tr = 0;
+    if (!strcmp(o, "X=AY")) dk = 0;
+    else if (!strcmp(o, "X=CAY")) { dk = 1; cm = 1; }
+    else if (!strcmp(o, "X=-AY")) { dk = 2; neg = 1; }
+    else if (!strcmp(o, "X=X+AY")) dk = 3;
+    else if (!strcmp(o, "X=X-AY")) { dk = 4; neg = 1; }
+    else if (!strcmp(o, "X=X+CAY")) { dk = 5; cm = 1; }
+    else if (!strcmp(o, "X=TAY")) { dk = 0; tr = 1; }
+    else if (!strcmp(o, "X=-TAY")) { dk = 2; neg = 1; tr = 1; }
+    else if (!strcmp(o, "X=X+TAY")) { dk = 3; tr = 1; }
+    else if (!strcmp(o, "X=X-TAY")) { dk = 4; neg = 1; tr = 1; }
+    else if (!strcmp(o, "X=X+CTAY")) { dk = 5; cm = 1; tr = 1; }
+    else return ORC_ERR_ARGS;
+    if (typdia != 'Q' && typdia != 'I' && typdia != '0') return ORC_ERR_ARGS;
+    for (int i = 0; i < npoin; ++i) {
+        double d = typdia == 'Q' ? y[i] * da[i] : y[i];        /* OV 'X=YZ' / 'X=Y' */
+        double cd = typdia == 'Q' ? c * y[i] * da[i] : c * y[i]; /* 'X=CYZ' / 'X=CY' */
+        if (typdia == '0') {
+            if (dk <= 2) x[i] = 0.0;                            /* OV 'X=C' with 0 */
+            continue;                                           /* X+.. : no term */
+        }
+        switch (dk) {
+            case 0: x[i] = d; break;
+            case 1: x[i] = cd; break;
+            case 2: x[i] = -d; break;
+            case 3: x[i] = x[i] + d; break;
+            case 4: x[i] = x[i] - d; break;
+            default: x[i] = x[i] + cd; break;
+        }
+    }
+    if (typext == '0') return ORC_OK;
+    if (typext != 'S' && typext != 'Q') return ORC_ERR_ARGS;
+    const double *xa1 = xa, *xa2 = typext == 'Q' ? xa + nseg : xa;
+    if (tr) { const double *t = xa1; xa1 = xa2; xa2 = t; }
+    for (int s = 0; s < nseg; ++s) {
+        double a1 = cm ? c * xa1[s] : xa1[s], a2 = cm ? c * xa2[s] : xa2[s];
+        if (neg) {
+            x[g1[s]] = x[g1[s]] - a1 * y[g2[s]];
+            x[g2[s]] = x[g2[s]] - a2 * y[g1[s]];
+        } else {
+            x[g1[s]] = x[g1[s]] + a1 * y[g2[s]];
+            x[g2[s]] = x[g2[s]] + a2 * y[g1[s]];
+        }
+    }
+    return ORC_OK;
+}
+
+/* The operator of a solve: EBE (STO=1) or segment (STO=3) storage. */
+typedef struct {
+    int sto;
+    int nelem, ld;
+    const int *ik0, *ik1, *ik2;
+    int nseg;
+    const int *g1, *g2;
+} opmesh;
+
+static int op_matvec(const opmesh *M, const char *op, int npoin, double *x,
+                     const double *da, char typdia, const double *xm,
+                     char typext, const double *y, double c, double *t, double *w)
+{
+    if (M->sto == 3)
+        return orc_mvseg(op, npoin, M->nseg, M->g1, M->g2, x, da, typdia, xm, typext, y, c);
+    return orc_matvec(op, npoin, M->nelem, M->ik0, M->ik1, M->ik2, x, da, typdia, xm,
+                      M->ld, typext, y, c, t, w);
+}
+
 /* ------------------------------------------------------------------ */
 /* dot products                                                         */
 /* ------------------------------------------------------------------ */
@@ -500,11 +585,11 @@ static double pdots(int mode, int n, const double *x, const double *y,
  *   PRECON divisible by 2 or 3: TYPDIA = 'I' (precd1.f:137-142);
  *   B = B*D.
  * d[npoin] receives D (the reference's TBB(IT1)). */
-int orc_precd1(int npoin, int nelem, const int *ik0, const int *ik1,
-               const int *ik2, int precon, double *x, double *dm,
-               char *typdia, double *xm, int ld, char typext, double *b,
-               double *d)
+static int precd1_impl(const opmesh *M, int npoin, int precon, double *x, double *dm,
+                       char *typdia, double *xm, char typext, double *b, double *d)
 {
+    const int nelem = M->nelem, ld = M->ld;
+    const int *ik0 = M->ik0, *ik1 = M->ik1, *ik2 = M->ik2;
     for (int i = 0; i < npoin; ++i) d[i] = dm[i];
     if (precon == 5)
         for (int i = 0; i < npoin; ++i) d[i] = fabs(d[i]);
@@ -522,8 +607,17 @@ int orc_precd1(int npoin, int nelem, const int *ik0, const int *ik1,
     } else if (*typdia != '0') {
         return ORC_ERR_ARGS;
     }
-    /* OM1111 'M=DMD': off-diagonal part (om1111.f:589-600) */
-    if (typext == 'S' || typext == 'Q') {
+    if (M->sto == 3) {
+        /* OMSEG 'M=DMD': off-diagonal part (omseg.f:530-541) */
+        if (typext == 'S' || typext == 'Q') {
+            for (int s = 0; s < M->nseg; ++s)
+                xm[s] = xm[s] * d[M->g1[s]] * d[M->g2[s]];
+            if (typext == 'Q')
+                for (int s = 0; s < M->nseg; ++s)
+                    xm[M->nseg + s] = xm[M->nseg + s] * d[M->g1[s]] * d[M->g2[s]];
+        }
+    } else if (typext == 'S' || typext == 'Q') {
+        /* OM1111 'M=DMD': off-diagonal part (om1111.f:589-600) */
         double *x1 = xm, *x2 = xm + ld, *x3 = xm + 2 * (size_t)ld;
         for (int e = 0; e < nelem; ++e) {
             x1[e] = x1[e] * d[ik1[e]] * d[ik0[e]];
@@ -545,6 +639,15 @@ int orc_precd1(int npoin, int nelem, const int *ik0, const int *ik1,
     return ORC_OK;
 }
 
+int orc_precd1(int npoin, int nelem, const int *ik0, const int *ik1,
+               const int *ik2, int precon, double *x, double *dm,
+               char *typdia, double *xm, int ld, char typext, double *b,
+               double *d)
+{
+    opmesh M = {1, nelem, ld, ik0, ik1, ik2, 0, NULL, NULL};
+    return precd1_impl(&M, npoin, precon, x, dm, typdia, xm, typext, b, d);
+}
+
 /* ------------------------------------------------------------------ */
 /* conjugate gradient                                                   */
 /* ------------------------------------------------------------------ */
@@ -554,12 +657,12 @@ int orc_precd1(int npoin, int nelem, const int *ik0, const int *ik1,
  * Convention R = A X - B; stop when RMRM <= XL*EPS**2 or M = NITMAX.
  * Returns ORC_OK, or the iteration count (>0) when NITMAX was reached
  * without convergence, or a negative error. */
-int orc_gracjg(int npoin, int nelem, const int *ik0, const int *ik1,
-               const int *ik2, double *x, const double *da, char typdia,
-               const double *xm, int ld, char typext, const double *b,
-               int nitmax, double eps, int dot_mode, int nb, int nt,
-               int *nit_out, double *relres_out, int *relat_out)
+static int gracjg_impl(const opmesh *M, int npoin, double *x, const double *da,
+                       char typdia, const double *xm, char typext, const double *b,
+                       int nitmax, double eps, int dot_mode, int nb, int nt,
+                       int *nit_out, double *relres_out, int *relat_out)
 {
+    const int nelem = M->sto == 3 ? 0 : M->nelem;
     size_t n = (size_t)npoin;
     double *r = (double *)malloc(sizeof(double) * n);
     double *dd = (double *)malloc(sizeof(double) * n);
@@ -578,8 +681,7 @@ int orc_gracjg(int npoin, int nelem, const int *ik0, const int *ik1,
     }
     if (xl < 1.0) { xl = 1.0; relat = 0; } else { relat = 1; }  /* :204-209 */
 
-    st = orc_matvec("X=AY    ", npoin, nelem, ik0, ik1, ik2, r, da, typdia,
-                    xm, ld, typext, x, 0.0, t, w);        /* :213 */
+    st = op_matvec(M, "X=AY    ", npoin, r, da, typdia, xm, typext, x, 0.0, t, w);  /* :213 */
     if (st) goto done;
     for (size_t i = 0; i < n; ++i) r[i] = r[i] - b[i];    /* :215 */
     rmrm = pdots(dot_mode, npoin, r, r, nb, nt);          /* :216 */
@@ -587,8 +689,7 @@ int orc_gracjg(int npoin, int nelem, const int *ik0, const int *ik1,
     if (rmrm < eps * eps * xl) goto fin;                  /* :219 */
 
     for (size_t i = 0; i < n; ++i) dd[i] = r[i];          /* :248 */
-    st = orc_matvec("X=AY    ", npoin, nelem, ik0, ik1, ik2, ad, da, typdia,
-                    xm, ld, typext, dd, 0.0, t, w);       /* :254 */
+    st = op_matvec(M, "X=AY    ", npoin, ad, da, typdia, xm, typext, dd, 0.0, t, w); /* :254 */
     if (st) goto done;
     dad = pdots(dot_mode, npoin, dd, ad, nb, nt);         /* :260 */
     ro = rmgm / dad;                                      /* :261 */
@@ -604,8 +705,8 @@ int orc_gracjg(int npoin, int nelem, const int *ik0, const int *ik1,
         if (rmrm <= xl * (eps * eps)) goto fin;           /* :303,324 */
         beta = rmgm / rm1gm1;                             /* :357 */
         for (size_t i = 0; i < n; ++i) dd[i] = r[i] + beta * dd[i];  /* :361 */
-        st = orc_matvec("X=AY    ", npoin, nelem, ik0, ik1, ik2, ad, da,
-                        typdia, xm, ld, typext, dd, 0.0, t, w);   /* :376 */
+        st = op_matvec(M, "X=AY    ", npoin, ad, da, typdia, xm, typext, dd, 0.0, t,
+                       w);                                /* :376 */
         if (st) goto done;
         dad = pdots(dot_mode, npoin, dd, ad, nb, nt);     /* :382 */
         ro = rmdm / dad;                                  /* :383 */
@@ -621,17 +722,26 @@ done:
     return st;
 }
 
+int orc_gracjg(int npoin, int nelem, const int *ik0, const int *ik1,
+               const int *ik2, double *x, const double *da, char typdia,
+               const double *xm, int ld, char typext, const double *b,
+               int nitmax, double eps, int dot_mode, int nb, int nt,
+               int *nit_out, double *relres_out, int *relat_out)
+{
+    opmesh M = {1, nelem, ld, ik0, ik1, ik2, 0, NULL, NULL};
+    return gracjg_impl(&M, npoin, x, da, typdia, xm, typext, b, nitmax, eps, dot_mode, nb, nt,
+                       nit_out, relres_out, relat_out);
+}
+
 /* solve.f:387-649 for SLV=1 (GRACJG) on a single (non-block) matrix:
  * PRECON 0 -> 1; diagonal change of variables when PRECON is divisible by
  * 2, 3 or 5 (solve.f:484-498); CG; X = X*D to undo the change of variables
  * (solve.f:637-641).  Inputs x, b, dm, typdia, xm are modified in place
  * exactly as the reference modifies them. */
-int orc_solve(int npoin, int nelem, const int *ik0, const int *ik1,
-              const int *ik2, double *x, double *b, double *dm,
-              char *typdia, double *xm, int ld, char typext, int slv,
-              int precon, int nitmax, double eps, int dot_mode,
-              int nb, int nt, int *nit_out, double *relres_out,
-              int *relat_out)
+static int solve_impl(const opmesh *M, int npoin, double *x, double *b, double *dm,
+                      char *typdia, double *xm, char typext, int slv, int precon,
+                      int nitmax, double eps, int dot_mode, int nb, int nt, int *nit_out,
+                      double *relres_out, int *relat_out)
 {
     if (slv != 1) return ORC_ERR_UNSUPPORTED;
     if (precon == 0) precon = 1;
@@ -642,18 +752,40 @@ int orc_solve(int npoin, int nelem, const int *ik0, const int *ik1,
     double *d = NULL;
     if (diag) {
         d = (double *)malloc(sizeof(double) * (size_t)npoin);
-        int st = orc_precd1(npoin, nelem, ik0, ik1, ik2, precon, x, dm, typdia,
-                            xm, ld, typext, b, d);
+        int st = precd1_impl(M, npoin, precon, x, dm, typdia, xm, typext, b, d);
         if (st) { free(d); return st; }
     }
-    int st = orc_gracjg(npoin, nelem, ik0, ik1, ik2, x, dm, *typdia, xm, ld,
-                        typext, b, nitmax, eps, dot_mode, nb, nt, nit_out,
-                        relres_out, relat_out);
+    int st = gracjg_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode, nb,
+                         nt, nit_out, relres_out, relat_out);
     if (diag) {
         for (int i = 0; i < npoin; ++i) x[i] = x[i] * d[i];
         free(d);
     }
     return st;
+}
+
+int orc_solve(int npoin, int nelem, const int *ik0, const int *ik1,
+              const int *ik2, double *x, double *b, double *dm,
+              char *typdia, double *xm, int ld, char typext, int slv,
+              int precon, int nitmax, double eps, int dot_mode,
+              int nb, int nt, int *nit_out, double *relres_out,
+              int *relat_out)
+{
+    opmesh M = {1, nelem, ld, ik0, ik1, ik2, 0, NULL, NULL};
+    return solve_impl(&M, npoin, x, b, dm, typdia, xm, typext, slv, precon, nitmax, eps,
+                      dot_mode, nb, nt, nit_out, relres_out, relat_out);
+}
+
+/* SOLVE (SLV=1) on a segment-storage matrix (STO=3): the same algorithm with
+ * MVSEG products and OMSEG scaling. */
+int orc_solve_seg(int npoin, int nseg, const int *g1, const int *g2, double *x, double *b,
+                  double *dm, char *typdia, double *xa, char typext, int slv, int precon,
+                  int nitmax, double eps, int dot_mode, int nb, int nt, int *nit_out,
+                  double *relres_out, int *relat_out)
+{
+    opmesh M = {3, 0, 0, NULL, NULL, NULL, nseg, g1, g2};
+    return solve_impl(&M, npoin, x, b, dm, typdia, xa, typext, slv, precon, nitmax, eps,
+                      dot_mode, nb, nt, nit_out, relres_out, relat_out);
 }
 
 /* ------------------------------------------------------------------ */
@@ -744,6 +876,58 @@ static int seg32_build(int npoin, int nelem, const int *ik0, const int *ik1,
     return ORC_OK;
 }
 
+/* Node -> incident segment lists in ascending segment order (the order in
+ * which MVSEG adds into each node): entries (ISEG<<1 | side), side 0 when
+ * the node is GLOSEG1 (its term uses XA1 and Y(GLOSEG2)), 1 when GLOSEG2. */
+static int build_seg_gather(int npoin, int nseg, const int *g1, const int *g2,
+                            int **ptr_out, int **idx_out)
+{
+    int *ptr = (int *)calloc((size_t)npoin + 1, sizeof(int));
+    int *idx = (int *)malloc(sizeof(int) * 2 * (size_t)nseg + 1);
+    int *pos = (int *)malloc(sizeof(int) * (size_t)npoin + 1);
+    if (!ptr || !idx || !pos) { free(ptr); free(idx); free(pos); return ORC_ERR_ARGS; }
+    for (int sg = 0; sg < nseg; ++sg) { ptr[g1[sg] + 1]++; ptr[g2[sg] + 1]++; }
+    for (int i = 0; i < npoin; ++i) ptr[i + 1] += ptr[i];
+    for (int i = 0; i < npoin; ++i) pos[i] = ptr[i];
+    for (int sg = 0; sg < nseg; ++sg) {
+        idx[pos[g1[sg]]++] = sg << 1;
+        idx[pos[g2[sg]]++] = (sg << 1) | 1;
+    }
+    free(pos);
+    *ptr_out = ptr;
+    *idx_out = idx;
+    return ORC_OK;
+}
+
+/* Binary32 form of a symmetric segment operator: for node i one slot per
+ * incident segment, in ascending segment order, holding the neighbour and
+ * (float)XA(ISEG); the row sum s_i = diag_i + XA of each incident segment,
+ * added in that order in binary64, rounded once. */
+static int seg32_build_seg(int npoin, const int *g1, const int *g2, const int *ptr,
+                           const int *idx, const double *da, char typdia, const double *xa,
+                           seg32 *g)
+{
+    size_t cap = (size_t)ptr[npoin] + 1;
+    g->npoin = npoin;
+    g->nptr = (int *)malloc(sizeof(int) * ((size_t)npoin + 1));
+    g->col = (int *)malloc(sizeof(int) * cap);
+    g->val = (float *)malloc(sizeof(float) * cap);
+    g->s32 = (float *)malloc(sizeof(float) * (size_t)npoin);
+    if (!g->nptr || !g->col || !g->val || !g->s32) return ORC_ERR_ARGS;
+    for (int i = 0; i <= npoin; ++i) g->nptr[i] = ptr[i];
+    for (int i = 0; i < npoin; ++i) {
+        double srow = typdia == 'Q' ? da[i] : (typdia == 'I' ? 1.0 : 0.0);
+        for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
+            int sg = idx[j] >> 1, side = idx[j] & 1;
+            g->col[j] = side ? g1[sg] : g2[sg];
+            g->val[j] = (float)xa[sg];
+            srow = srow + xa[sg];
+        }
+        g->s32[i] = (float)srow;
+    }
+    return ORC_OK;
+}
+
 /* q = A32 p in difference form: q_i = s_i p_i + sum over slots of
  * c (p_j - p_i), slots in order.  Rounding the coefficients then leaves
  * constant vectors exact, so the small mass-dominated eigenvalues of the
@@ -771,8 +955,7 @@ static void seg32_mv(const seg32 *g, const float *p, float *q)
  * recursive residual).  Symmetric storage only; inputs other than x are not
  * modified.  Returns 0 when converged, the inner iteration count when
  * max_inner or max_outer ran out, or a negative error. */
-static int mixed_impl(int npoin, int nelem, const int *ik0, const int *ik1,
-                      const int *ik2, double *x, const double *b,
+static int mixed_impl(const opmesh *M, int npoin, double *x, const double *b,
                       const double *dm_in, char typdia_in, const double *xm_in,
                       char typext, int precon, double inner_tol,
                       double outer_tol, int max_outer, int max_inner,
@@ -780,9 +963,13 @@ static int mixed_impl(int npoin, int nelem, const int *ik0, const int *ik1,
                       double *relres_out)
 {
     if (typext != 'S') return ORC_ERR_UNSUPPORTED;
+    const int nelem = M->sto == 3 ? 0 : M->nelem;
+    const int *ik0 = M->ik0, *ik1 = M->ik1, *ik2 = M->ik2;
     size_t n = (size_t)npoin, ne = (size_t)nelem;
+    /* off-diagonal values: 3 per element (EBE) or 1 per segment */
+    const size_t nxm = M->sto == 3 ? (size_t)M->nseg : 3 * ne;
     double *dm = (double *)malloc(sizeof(double) * n);
-    double *xm = (double *)malloc(sizeof(double) * 3 * ne);
+    double *xm = (double *)malloc(sizeof(double) * nxm + 1);
     double *bs = (double *)malloc(sizeof(double) * n);
     double *d = (double *)malloc(sizeof(double) * n);
     double *r = (double *)malloc(sizeof(double) * n);
@@ -802,18 +989,23 @@ static int mixed_impl(int npoin, int nelem, const int *ik0, const int *ik1,
         st = ORC_ERR_ARGS; goto done;
     }
     memcpy(dm, dm_in, sizeof(double) * n);
-    memcpy(xm, xm_in, sizeof(double) * 3 * ne);
+    memcpy(xm, xm_in, sizeof(double) * nxm);
     memcpy(bs, b, sizeof(double) * n);
     if (precon == 0) precon = 1;
     diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
     if (diag) {
-        st = orc_precd1(npoin, nelem, ik0, ik1, ik2, precon, x, dm, &typdia,
-                        xm, nelem, typext, bs, d);
+        st = precd1_impl(M, npoin, precon, x, dm, &typdia, xm, typext, bs, d);
         if (st) goto done;
     }
-    if ((st = build_gather(npoin, nelem, ik0, ik1, ik2, &gptr, &gek))) goto done;
-    if ((st = seg32_build(npoin, nelem, ik0, ik1, ik2, gptr, gek, dm, typdia, xm, &g)))
-        goto done;
+    if (M->sto == 3) {
+        if ((st = build_seg_gather(npoin, M->nseg, M->g1, M->g2, &gptr, &gek))) goto done;
+        if ((st = seg32_build_seg(npoin, M->g1, M->g2, gptr, gek, dm, typdia, xm, &g)))
+            goto done;
+    } else {
+        if ((st = build_gather(npoin, nelem, ik0, ik1, ik2, &gptr, &gek))) goto done;
+        if ((st = seg32_build(npoin, nelem, ik0, ik1, ik2, gptr, gek, dm, typdia, xm, &g)))
+            goto done;
+    }
 
     xl = dot64s(ds, npoin, bs, bs);
     if (sqrt(xl) < 1.0e-15) {
@@ -828,8 +1020,8 @@ static int mixed_impl(int npoin, int nelem, const int *ik0, const int *ik1,
     /* true residual r = b - A x (binary64), its binary32 copy, both norms */
 #define TRUE_RESIDUAL()                                                         \
     do {                                                                        \
-        st = orc_matvec("X=AY    ", npoin, nelem, ik0, ik1, ik2, t, dm,          \
-                        typdia, xm, nelem, typext, x, 0.0, r, w);               \
+        st = op_matvec(M, "X=AY    ", npoin, t, dm, typdia, xm, typext, x, 0.0, \
+                       r, w);                                                   \
         if (st) goto done;                                                      \
         for (size_t i = 0; i < n; ++i) { r[i] = bs[i] - t[i]; ri[i] = (float)r[i]; } \
         rr = dot64s(ds, npoin, r, r);                                          \
@@ -888,9 +1080,26 @@ int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
                     double *relres_out)
 {
     dotspec ds = {0, nb, nt, 1};
-    return mixed_impl(npoin, nelem, ik0, ik1, ik2, x, b, dm_in, typdia_in, xm_in,
+    opmesh M = {1, nelem, nelem, ik0, ik1, ik2, 0, NULL, NULL};
+    return mixed_impl(&M, npoin, x, b, dm_in, typdia_in, xm_in,
                       typext, precon, inner_tol, outer_tol, max_outer, max_inner,
                       &ds, outer_out, inner_total_out, relres_out);
+}
+
+/* Mixed-precision solve on a segment-storage matrix (symmetric XA(NSEG)):
+ * the same algorithm with the binary32 operator taken from the segments and
+ * the binary64 residual from MVSEG. */
+int orc_solve_mixed_seg(int npoin, int nseg, const int *g1, const int *g2, double *x,
+                        const double *b, const double *dm_in, char typdia_in,
+                        const double *xa_in, char typext, int precon, double inner_tol,
+                        double outer_tol, int max_outer, int max_inner, int nb, int nt,
+                        int *outer_out, int *inner_total_out, double *relres_out)
+{
+    dotspec ds = {0, nb, nt, 1};
+    opmesh M = {3, 0, 0, NULL, NULL, NULL, nseg, g1, g2};
+    return mixed_impl(&M, npoin, x, b, dm_in, typdia_in, xa_in, typext, precon, inner_tol,
+                      outer_tol, max_outer, max_inner, &ds, outer_out, inner_total_out,
+                      relres_out);
 }
 
 /* One instance of the batched solver: the same algorithm with the batched
@@ -904,7 +1113,8 @@ int orc_solve_mixed_batch(int npoin, int nelem, const int *ik0, const int *ik1,
                           double *relres_out)
 {
     dotspec ds = {1, 0, nt, npt};
-    return mixed_impl(npoin, nelem, ik0, ik1, ik2, x, b, dm_in, typdia_in, xm_in,
+    opmesh M = {1, nelem, nelem, ik0, ik1, ik2, 0, NULL, NULL};
+    return mixed_impl(&M, npoin, x, b, dm_in, typdia_in, xm_in,
                       typext, precon, inner_tol, outer_tol, max_outer, max_inner,
                       &ds, outer_out, inner_total_out, relres_out);
 }
@@ -1050,4 +1260,131 @@ int orc_solve_omp(int npoin, int nelem, const int *ik0, const int *ik1,
     if (relres_out) *relres_out = rel_out;
     free(ptr); free(ek); free(xm); free(b); free(d); free(r); free(dd); free(ad);
     return st;
+}
+
+/* ------------------------------------------------------------------ */
+/* segment storage (STO=3)                                              */
+/* ------------------------------------------------------------------ */
+
+typedef struct { long long key; int ef; } edge_key;
+
+static int cmp_edge(const void *a, const void *b)
+{
+    const edge_key *x = (const edge_key *)a, *y = (const edge_key *)b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    return x->ef < y->ef ? -1 : (x->ef > y->ef);
+}
+
+/* stoseg.f:94-225 for P1 triangles with NCSIZE <= 1.  The NELEB boundary
+ * segments come first, in the given order: boundary segment IELEB is face
+ * nulone[IELEB] (0-based; face f joins local points f and f+1 mod 3) of
+ * element nelbor[IELEB], GLOSEG = (IKLE(f), IKLE(f+1)) and ORISEG = 1
+ * (:108-115).  Then every element face without a segment, elements in
+ * order, faces 1..3, opens the next segment with GLOSEG ordered by node
+ * number (:127-145) and gives it to the neighbour across that face
+ * (IFABOR, computed here from IKLE), which must run the edge the other way
+ * (:146-186).  eltseg/oriseg: 3 x nelem, face-major, 0-based segment
+ * numbers, ORISEG 1 or 2.  Returns the segment count in *nseg_out. */
+int orc_stoseg(int npoin, int nelem, const int *ik0, const int *ik1, const int *ik2,
+               int neleb, const int *nelbor, const int *nulone, int *g1, int *g2,
+               int *eltseg, int *oriseg, int *nseg_out)
+{
+    const int *ik[3] = {ik0, ik1, ik2};
+    const int next[3] = {1, 2, 0};
+    size_t nf = 3 * (size_t)nelem;
+    edge_key *keys = (edge_key *)malloc(sizeof(edge_key) * nf + 1);
+    int *ifabor = (int *)malloc(sizeof(int) * nf + 1);
+    if (!keys || !ifabor) { free(keys); free(ifabor); return ORC_ERR_ARGS; }
+    for (int f = 0; f < 3; ++f)
+        for (int e = 0; e < nelem; ++e) {
+            int a = ik[f][e], b = ik[next[f]][e];
+            int lo = a < b ? a : b, hi = a < b ? b : a;
+            keys[(size_t)f * nelem + e].key = (long long)lo * npoin + hi;
+            keys[(size_t)f * nelem + e].ef = f * nelem + e;
+            ifabor[(size_t)f * nelem + e] = -1;
+        }
+    qsort(keys, nf, sizeof(edge_key), cmp_edge);
+    for (size_t q = 0; q + 1 < nf; ++q)
+        if (keys[q].key == keys[q + 1].key) {
+            int ea = keys[q].ef % nelem, eb = keys[q + 1].ef % nelem;
+            ifabor[keys[q].ef] = eb;
+            ifabor[keys[q + 1].ef] = ea;
+            ++q;
+        }
+    free(keys);
+    for (size_t q = 0; q < nf; ++q) eltseg[q] = -1;
+    for (int s = 0; s < neleb; ++s) {                           /* :108-115 */
+        int e = nelbor[s], f = nulone[s];
+        g1[s] = ik[f][e];
+        g2[s] = ik[next[f]][e];
+        eltseg[(size_t)f * nelem + e] = s;
+        oriseg[(size_t)f * nelem + e] = 1;
+    }
+    int nse = neleb, st = ORC_OK;
+    for (int e1 = 0; e1 < nelem && st == ORC_OK; ++e1)          /* :119-205 */
+        for (int f = 0; f < 3; ++f) {
+            if (eltseg[(size_t)f * nelem + e1] >= 0) continue;
+            int i1 = ik[f][e1], i2 = ik[next[f]][e1];
+            if (i1 == i2) { st = ORC_ERR_BAD_MESH; break; }
+            int s = nse++;
+            eltseg[(size_t)f * nelem + e1] = s;
+            if (i1 < i2) { g1[s] = i1; g2[s] = i2; oriseg[(size_t)f * nelem + e1] = 1; }
+            else { g1[s] = i2; g2[s] = i1; oriseg[(size_t)f * nelem + e1] = 2; }
+            int e2 = ifabor[(size_t)f * nelem + e1];
+            if (e2 < 0) continue;
+            int found = 0;
+            for (int jf = 0; jf < 3; ++jf) {
+                int j1 = ik[jf][e2], j2 = ik[next[jf]][e2];
+                if (i1 == j2 && i2 == j1) {
+                    eltseg[(size_t)jf * nelem + e2] = s;
+                    oriseg[(size_t)jf * nelem + e2] = 3 - oriseg[(size_t)f * nelem + e1];
+                    found = 1;
+                    break;
+                } else if (i1 == j1 && i2 == j2) {
+                    break;                                      /* wrongly oriented */
+                }
+            }
+            if (!found) { st = ORC_ERR_BAD_MESH; break; }
+        }
+    free(ifabor);
+    *nseg_out = nse;
+    return st;
+}
+
+/* assex3.f:150-160 -> as3_1111_s.f:71-79 ('S') and as3_1111_q.f:85-98
+ * ('Q', STOXMT=1): EBE off-diagonal terms summed into segments, element by
+ * element, from zero.  Face 1 (points 1-2) takes XMT(,1) [and XMT(,4)],
+ * face 2 (2-3) XMT(,3) [and XMT(,6)], face 3 (3-1) XMT(,2) [XMT(,5)]; for
+ * 'Q' the term of row IKLE(f) goes to column ORISEG of XA(NSEG,2) and the
+ * other to column 3-ORISEG.  xmt: ld x (3|6) column-major. */
+int orc_assex3(int nelem, const int *eltseg, const int *oriseg, char typext,
+               const double *xmt, int ld, int nseg, double *xa)
+{
+    const double *m[6];
+    for (int c = 0; c < 6; ++c) m[c] = xmt + (size_t)c * ld;
+    const int *es1 = eltseg, *es2 = eltseg + nelem, *es3 = eltseg + 2 * (size_t)nelem;
+    if (typext == 'S') {
+        for (int s = 0; s < nseg; ++s) xa[s] = 0.0;
+        for (int e = 0; e < nelem; ++e) {
+            xa[es1[e]] = xa[es1[e]] + m[0][e];
+            xa[es2[e]] = xa[es2[e]] + m[2][e];
+            xa[es3[e]] = xa[es3[e]] + m[1][e];
+        }
+        return ORC_OK;
+    }
+    if (typext != 'Q') return ORC_ERR_ARGS;
+    const int *o1 = oriseg, *o2 = oriseg + nelem, *o3 = oriseg + 2 * (size_t)nelem;
+    double *x1 = xa, *x2 = xa + nseg;
+#define XA(s, o) (*((o) == 1 ? &x1[s] : &x2[s]))
+    for (int s = 0; s < nseg; ++s) { x1[s] = 0.0; x2[s] = 0.0; }
+    for (int e = 0; e < nelem; ++e) {
+        XA(es1[e], o1[e]) = XA(es1[e], o1[e]) + m[0][e];
+        XA(es2[e], o2[e]) = XA(es2[e], o2[e]) + m[2][e];
+        XA(es3[e], o3[e]) = XA(es3[e], o3[e]) + m[4][e];
+        XA(es1[e], 3 - o1[e]) = XA(es1[e], 3 - o1[e]) + m[3][e];
+        XA(es2[e], 3 - o2[e]) = XA(es2[e], 3 - o2[e]) + m[5][e];
+        XA(es3[e], 3 - o3[e]) = XA(es3[e], 3 - o3[e]) + m[1][e];
+    }
+#undef XA
+    return ORC_OK;
 }

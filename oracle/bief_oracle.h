@@ -121,6 +121,30 @@ int orc_solve_omp(int npoin, int nelem, const int *ik0, const int *ik1,
                   const double *dm_in, const double *xm_in, int nitmax,
                   double eps, int nthreads, int *nit_out, double *relres_out);
 
+/* segment storage (STO=3): 0-based GLOSEG columns g1/g2; ELTSEG/ORISEG as
+ * 3 x nelem face-major arrays */
+int orc_stoseg(int npoin, int nelem, const int *ik0, const int *ik1, const int *ik2,
+               int neleb, const int *nelbor, const int *nulone, int *g1, int *g2,
+               int *eltseg, int *oriseg, int *nseg_out);
+
+int orc_assex3(int nelem, const int *eltseg, const int *oriseg, char typext,
+               const double *xmt, int ld, int nseg, double *xa);
+
+int orc_mvseg(const char *op, int npoin, int nseg, const int *g1, const int *g2,
+              double *x, const double *da, char typdia, const double *xa,
+              char typext, const double *y, double c);
+
+int orc_solve_seg(int npoin, int nseg, const int *g1, const int *g2, double *x, double *b,
+                  double *dm, char *typdia, double *xa, char typext, int slv, int precon,
+                  int nitmax, double eps, int dot_mode, int nb, int nt, int *nit_out,
+                  double *relres_out, int *relat_out);
+
+int orc_solve_mixed_seg(int npoin, int nseg, const int *g1, const int *g2, double *x,
+                        const double *b, const double *dm_in, char typdia_in,
+                        const double *xa_in, char typext, int precon, double inner_tol,
+                        double outer_tol, int max_outer, int max_inner, int nb, int nt,
+                        int *outer_out, int *inner_total_out, double *relres_out);
+
 #ifdef __cplusplus
 }
 #endif
