@@ -191,3 +191,27 @@ def segments(ikle0, npoin):
     oriseg = np.where(a == g1[seg], 1, 2).reshape(3, ne)
     return (g1.astype(np.int32), g2.astype(np.int32), eltseg.astype(np.int32),
             oriseg.astype(np.int32))
+
+
+def delaunay_mesh(npts, seed=2027):
+    """Unstructured P1 mesh: the Delaunay triangulation of `npts` points
+    (the unit square's corners, points along its edges and uniform random
+    points inside), elements counter-clockwise.  Node valences and boundary
+    shapes vary as in real meshes."""
+    from scipy.spatial import Delaunay
+    rng = np.random.default_rng(seed)
+    nb = max(4, int(np.sqrt(npts)))
+    t = np.sort(rng.uniform(0, 1, (4, nb)), axis=1)
+    edge = np.concatenate([np.stack([t[0], np.zeros(nb)], 1), np.stack([np.ones(nb), t[1]], 1),
+                           np.stack([t[2], np.ones(nb)], 1), np.stack([np.zeros(nb), t[3]], 1)])
+    corners = np.array([[0.0, 0.0], [1.0, 0.0], [1.0, 1.0], [0.0, 1.0]])
+    inner = rng.uniform(0.02, 0.98, (max(npts - 4 - 4 * nb, 0), 2))
+    pts = np.concatenate([corners, edge, inner])
+    tri = Delaunay(pts).simplices.astype(np.int64)
+    p = pts[tri]
+    area2 = ((p[:, 1, 0] - p[:, 0, 0]) * (p[:, 2, 1] - p[:, 0, 1])
+             - (p[:, 2, 0] - p[:, 0, 0]) * (p[:, 1, 1] - p[:, 0, 1]))
+    cw = area2 < 0
+    tri[cw] = tri[cw][:, [0, 2, 1]]
+    keep = np.abs(area2) > 1e-12
+    return pts[:, 0].copy(), pts[:, 1].copy(), tri[keep].astype(np.int32)
