@@ -71,7 +71,7 @@ typedef struct bief_handle bief_handle;
 /* Solve flags */
 #define BIEF_SOLVE_MUTATE_INPUTS  1  /* leave B = D.B and the stored matrix
                                         = D.A.D (TYPDIA 'I'), as SOLVE does */
-#define BIEF_SOLVE_INFOGR         2  /* print the GRACJG iteration message  */
+#define BIEF_SOLVE_INFOGR         2  /* print the method's iteration message */
 
 /* Mesh: replaces the MESH%IKLE / NPOIN / NELEM / NELMAX part of BIEF_MESH
  * (bief_def.f:205-498).  Validates IKLE and builds the node->element
@@ -92,8 +92,10 @@ int bief_set_matrix_dev(bief_handle *h, const double *dm, const double *xm,
 /* Read back the stored matrix (e.g. after a mutating solve). */
 int bief_get_matrix(bief_handle *h, double *dm, double *xm, char *typdia);
 
-/* SOLVE(X,A,B,...) for SLV=1: host X (initial guess in, solution out) and
- * B.  relres_out receives SQRT(RMRM/XL) as printed by GRACJG. */
+/* SOLVE(X,A,B,...) for SLV=1 (GRACJG, gracjg.F) and SLV=3 (EQUNOR, CG on
+ * the normal equations, equnor.f): host X (initial guess in, solution out)
+ * and B.  relres_out receives SQRT(RMRM/XL) as the method prints it.  Other
+ * SLV values return BIEF_ERR_UNSUPPORTED. */
 int bief_solve(bief_handle *h, double *x, double *b, bief_slvcfg *cfg,
                int flags, double *relres_out);
 /* Same with device pointers, on `stream`. */

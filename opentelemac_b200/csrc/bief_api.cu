@@ -35,6 +35,8 @@ struct bief_handle {
   int2 *d_rec_idx = nullptr;
   uchar2 *d_rec_slot = nullptr;
   double2 *d_rec_c = nullptr;
+  double2 *d_rec_ct = nullptr;   // transposed-operator records (EQUNOR, 'Q' storage)
+  double *d_sg_ct = nullptr;     // transposed-operator segment slots
   float *d_seg_c = nullptr, *d_s32 = nullptr;
   long long nrec = 0, nseg = 0;
   int max_nnb = 0;
@@ -155,6 +157,17 @@ void *cg_kernel(int td, int sto) {
   return (void *)k_cg64<DIA_0, 1>;
 }
 
+void *equnor_kernel(int td, int sto) {
+  if (sto == 3) {
+    if (td == DIA_Q) return (void *)k_equnor<DIA_Q, 3>;
+    if (td == DIA_I) return (void *)k_equnor<DIA_I, 3>;
+    return (void *)k_equnor<DIA_0, 3>;
+  }
+  if (td == DIA_Q) return (void *)k_equnor<DIA_Q, 1>;
+  if (td == DIA_I) return (void *)k_equnor<DIA_I, 1>;
+  return (void *)k_equnor<DIA_0, 1>;
+}
+
 void *mixed_kernel(int td, int sto) {
   if (sto == 3) {
     if (td == DIA_Q) return (void *)k_mixed<DIA_Q, 3>;
@@ -193,7 +206,9 @@ int persistent_grid(int npoin, int nsm, int *out) {
   void *ks[] = {cg_kernel(DIA_Q, 1), cg_kernel(DIA_I, 1), cg_kernel(DIA_0, 1),
                 mixed_kernel(DIA_Q, 1), mixed_kernel(DIA_I, 1), mixed_kernel(DIA_0, 1),
                 cg_kernel(DIA_Q, 3), cg_kernel(DIA_I, 3), cg_kernel(DIA_0, 3),
-                mixed_kernel(DIA_Q, 3), mixed_kernel(DIA_I, 3), mixed_kernel(DIA_0, 3)};
+                mixed_kernel(DIA_Q, 3), mixed_kernel(DIA_I, 3), mixed_kernel(DIA_0, 3),
+                equnor_kernel(DIA_Q, 1), equnor_kernel(DIA_I, 1), equnor_kernel(DIA_0, 1),
+                equnor_kernel(DIA_Q, 3), equnor_kernel(DIA_I, 3), equnor_kernel(DIA_0, 3)};
   for (void *k : ks) {
     int bps = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, CG_THREADS, 0));
@@ -221,13 +236,13 @@ int ensure_matrix_buffers(bief_handle *h) {
   return BIEF_OK;
 }
 
-void print_gracjg(int status, int nit, double relres, int relat) {
-  // gracjg.F:426-435 formats 102/202 (converged), 104/204 (NITMAX)
+void print_gracjg(int status, int nit, double relres, int relat, const char *name = "GRACJG") {
+  // gracjg.F:426-435 / equnor.f:317-332 formats (converged, NITMAX)
   if (status > 0)
-    printf(" GRACJG (BIEF) : EXCEEDING MAXIMUM ITERATIONS:%8d %s PRECISION:%16.7G\n", nit,
+    printf(" %s (BIEF) : EXCEEDING MAXIMUM ITERATIONS:%8d %s PRECISION:%16.7G\n", name, nit,
            relat ? "RELATIVE" : "ABSOLUTE", relres);
   else
-    printf(" GRACJG (BIEF) : %8d ITERATIONS, %s PRECISION:%16.7G\n", nit,
+    printf(" %s (BIEF) : %8d ITERATIONS, %s PRECISION:%16.7G\n", name, nit,
            relat ? "RELATIVE" : "ABSOLUTE", relres);
 }
 
@@ -299,6 +314,10 @@ int build_seg_coefs(bief_handle *h, const double *xa, cudaStream_t st) {
   return BIEF_OK;
 }
 
+// Transposed-operator coefficients for EQUNOR ('Q' storage; symmetric
+// storage reuses the operator's own).  Returns the Sell of A^T.
+int build_transposed(bief_handle *h, const double *xm, cudaStream_t st, Sell *out);
+
 Sell sell_of(const bief_handle *h) {
   Sell S;
   S.sg_c = nullptr;
@@ -325,9 +344,33 @@ Sell sell_of(const bief_handle *h) {
   return S;
 }
 
+int build_transposed(bief_handle *h, const double *xm, cudaStream_t st, Sell *out) {
+  Sell S = sell_of(h);
+  if (h->typext != 'Q') {
+    *out = S;
+    return BIEF_OK;
+  }
+  const int g = grid_for(h->npoin, h->nsm);
+  if (h->sto == 3) {
+    if (!h->d_sg_ct && dalloc(&h->d_sg_ct, (size_t)h->nsg_slots)) return BIEF_ERR_CUDA;
+    k_build_sgc<false, true><<<g, 256, 0, st>>>(h->npoin, h->nsg, h->d_sg_meta, h->d_sg_off,
+                                               h->d_sg_sx, xm, h->d_sg_ct);
+    S.sg_c = h->d_sg_ct;
+  } else {
+    if (!h->d_rec_ct && dalloc(&h->d_rec_ct, (size_t)h->nrec)) return BIEF_ERR_CUDA;
+    k_build_rec<false, true><<<g, 256, 0, st>>>(h->npoin, h->nelem, h->d_ptr, h->d_ek, xm,
+                                               h->d_rec_off, h->d_rec_ct);
+    S.rec_c = h->d_rec_ct;
+  }
+  h->launches++;
+  CK(cudaGetLastError());
+  *out = S;
+  return BIEF_OK;
+}
+
 int check_cfg(const bief_slvcfg *cfg, int *precon) {
   if (!cfg) return BIEF_ERR_ARGS;
-  if (cfg->slv != 1) return BIEF_ERR_UNSUPPORTED;
+  if (cfg->slv != 1 && cfg->slv != 3) return BIEF_ERR_UNSUPPORTED;
   int p = cfg->precon == 0 ? 1 : cfg->precon;
   if (p <= 0) return BIEF_ERR_ARGS;
   if (p % 7 == 0 || p % 11 == 0 || p % 13 == 0 || p % 17 == 0) return BIEF_ERR_UNSUPPORTED;
@@ -522,7 +565,7 @@ int bief_destroy(bief_handle *h) {
                   h->d_rec_idx, h->d_rec_slot, h->d_rec_c, h->d_seg_col, h->d_seg_c,
                   h->d_binst, h->d_brel, h->d_bpart, h->d_g1, h->d_g2, h->d_sg_meta,
                   h->d_sg_off, h->d_sg_sx, h->d_sg_col, h->d_segel, h->d_xa, h->d_xas,
-                  h->d_sg_c64, h->d_sg_c32};
+                  h->d_sg_c64, h->d_sg_c32, h->d_rec_ct, h->d_sg_ct};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -642,25 +685,48 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     xm = seg ? h->d_xas : h->d_xms;
   }
   if ((st = seg ? build_seg_coefs(h, xm, s) : build_records(h, xm, s))) return st;
-  CgP P;
-  P.npoin = h->npoin;
-  P.nitmax = cfg->nitmax;
-  P.eps = cfg->eps;
-  P.S = sell_of(h);
-  P.da = da;
-  P.dsc = diag ? h->d_dsc : nullptr;
-  P.x = x;
-  P.b = bw;
-  P.r = h->d_r;
-  P.d0 = h->d_d0;
-  P.d1 = h->d_d1;
-  P.ad = h->d_ad;
-  P.part = h->d_part;
-  P.ctl = h->d_ctl;
-  P.timeout_ns = h->timeout_ns;
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
-  CK(cudaEventRecord(h->ev[0], s));
-  if ((st = launch_coop(h, cg_kernel(td, h->sto), &P, s))) return st;
+  if (cfg->slv == 3) {  // EQUNOR
+    EqP P;
+    P.npoin = h->npoin;
+    P.nitmax = cfg->nitmax;
+    P.eps = cfg->eps;
+    P.S = sell_of(h);
+    if ((st = build_transposed(h, xm, s, &P.St))) return st;
+    P.da = da;
+    P.dsc = diag ? h->d_dsc : nullptr;
+    P.x = x;
+    P.b = bw;
+    P.r = h->d_r;
+    P.d0 = h->d_d0;
+    P.d1 = h->d_d1;
+    P.ad = h->d_ad;
+    P.t = h->d_t;
+    P.part = h->d_part;
+    P.ctl = h->d_ctl;
+    P.timeout_ns = h->timeout_ns;
+    CK(cudaEventRecord(h->ev[0], s));
+    if ((st = launch_coop(h, equnor_kernel(td, h->sto), &P, s))) return st;
+  } else {
+    CgP P;
+    P.npoin = h->npoin;
+    P.nitmax = cfg->nitmax;
+    P.eps = cfg->eps;
+    P.S = sell_of(h);
+    P.da = da;
+    P.dsc = diag ? h->d_dsc : nullptr;
+    P.x = x;
+    P.b = bw;
+    P.r = h->d_r;
+    P.d0 = h->d_d0;
+    P.d1 = h->d_d1;
+    P.ad = h->d_ad;
+    P.part = h->d_part;
+    P.ctl = h->d_ctl;
+    P.timeout_ns = h->timeout_ns;
+    CK(cudaEventRecord(h->ev[0], s));
+    if ((st = launch_coop(h, cg_kernel(td, h->sto), &P, s))) return st;
+  }
   CK(cudaEventRecord(h->ev[1], s));
   CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -670,7 +736,8 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   cfg->nit = c.nit;
   cfg->ok = (st == BIEF_OK) ? 1 : 0;
   if (relres_out) *relres_out = c.relres;
-  if (st >= 0 && ((flags & BIEF_SOLVE_INFOGR) || st > 0)) print_gracjg(st, c.nit, c.relres, c.relat);
+  if (st >= 0 && ((flags & BIEF_SOLVE_INFOGR) || st > 0))
+    print_gracjg(st, c.nit, c.relres, c.relat, cfg->slv == 3 ? "EQUNOR" : "GRACJG");
   if (diag && (flags & BIEF_SOLVE_MUTATE_INPUTS) && st >= 0) {
     // SOLVE leaves B = D.B and A = D.A.D with TYPDIA from PRECD1
     CK(cudaMemcpyAsync(b, h->d_bs, sizeof(double) * h->npoin, cudaMemcpyDeviceToDevice, s));
@@ -1115,7 +1182,7 @@ int bief_set_segments(bief_handle *h, int nseg, int maxseg, const int *gloseg) {
     }
   DevGuard g(h->dev);
   void *old[] = {h->d_g1, h->d_g2, h->d_sg_meta, h->d_sg_off, h->d_sg_sx, h->d_sg_col,
-                 h->d_segel, h->d_xa, h->d_xas, h->d_sg_c64, h->d_sg_c32};
+                 h->d_segel, h->d_xa, h->d_xas, h->d_sg_c64, h->d_sg_c32, h->d_sg_ct};
   CK(cudaStreamSynchronize(h->stream));
   for (void *p : old)
     if (p) cudaFree(p);
@@ -1123,6 +1190,7 @@ int bief_set_segments(bief_handle *h, int nseg, int maxseg, const int *gloseg) {
   h->d_segel = nullptr;
   h->d_xa = h->d_xas = h->d_sg_c64 = nullptr;
   h->d_sg_c32 = nullptr;
+  h->d_sg_ct = nullptr;
   h->has_segments = 0;
   if (h->sto == 3) h->has_matrix = 0;  // the stored segment matrix belonged to the old numbering
   h->sto = 1;

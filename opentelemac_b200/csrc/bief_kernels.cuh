@@ -136,7 +136,7 @@ __global__ void k_precd1_segs(int nseg, int ncol, const int *__restrict__ g1,
 
 // Per slot, the binary64 coefficient of the working operator's 'X=AY' row:
 // XA1 for side 0, XA2 for side 1.
-template <bool SYM>
+template <bool SYM, bool TRANS = false>
 __global__ void k_build_sgc(int npoin, int nseg, const int *__restrict__ meta,
                             const int *__restrict__ off, const int *__restrict__ sx,
                             const double *__restrict__ xa, double *sg_c) {
@@ -145,7 +145,7 @@ __global__ void k_build_sgc(int npoin, int nseg, const int *__restrict__ meta,
     const int base = off[i >> 5] + (i & 31);
     for (int m = 0; m < deg; ++m) {
       const int p = sx[base + 32 * m];
-      sg_c[base + 32 * m] = xa[(size_t)(SYM ? 0 : (p & 1)) * nseg + (p >> 1)];
+      sg_c[base + 32 * m] = xa[(size_t)(SYM ? 0 : ((p & 1) ^ (TRANS ? 1 : 0))) * nseg + (p >> 1)];
     }
   }
 }
@@ -258,7 +258,9 @@ __global__ void k_precd1_elems(int nelem, int ndiag, const int *__restrict__ ik,
 // ---------------------------------------------------------------------------
 // Gather-ready layouts of the working operator (see Sell in bief_device.cuh)
 // ---------------------------------------------------------------------------
-template <bool SYM>
+// TRANS: the coefficients of the transposed operator, XA(a,k) and XA(b,k)
+// (mv0303.f 'X=TAY'), for the same two neighbours.
+template <bool SYM, bool TRANS = false>
 __global__ void k_build_rec(int npoin, int nelem, const int *__restrict__ ptr,
                             const int *__restrict__ ek, const double *__restrict__ xm,
                             const int *__restrict__ rec_off, double2 *rec_c) {
@@ -268,8 +270,9 @@ __global__ void k_build_rec(int npoin, int nelem, const int *__restrict__ ptr,
     for (int m = 0; m < deg; ++m) {
       const int p = ek[j0 + m], e = p >> 2, k = p & 3;
       const int a = (k == 2) ? 0 : k + 1, b = (k == 0) ? 2 : k - 1;
-      rec_c[base + 32 * m] = make_double2(xm[(size_t)xm_col<SYM>(k, a) * nelem + e],
-                                          xm[(size_t)xm_col<SYM>(k, b) * nelem + e]);
+      const int ca = TRANS ? xm_col<SYM>(a, k) : xm_col<SYM>(k, a);
+      const int cb = TRANS ? xm_col<SYM>(b, k) : xm_col<SYM>(k, b);
+      rec_c[base + 32 * m] = make_double2(xm[(size_t)ca * nelem + e], xm[(size_t)cb * nelem + e]);
     }
   }
 }
@@ -451,6 +454,152 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
     double *tmp = cur; cur = nxt; nxt = tmp;
 
     if (m >= P.nitmax) {  // :406 -- last X update, then stop unconverged
+      const double nr = -ro;
+      for (int i = lo + t; i < hi; i += T) x[i] = add(x[i], mul(nr, cur[i]));
+      finish(m, m, rmrm, xl, relat);
+      return;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// EQUNOR (equnor.f:106-311): CG on the normal equations A^T A x = A^T b,
+// without preconditioning matrices (G aliases R), as ONE persistent kernel
+// with three grid reductions per iteration.  P.S describes the working
+// operator A, P.St its transpose (same neighbours, transposed
+// coefficients); P.t holds A^T R.  As in k_cg64 the new direction
+// D = BETA*D + A^T R is recomputed wherever it is needed, with the owner's
+// bits.
+// ---------------------------------------------------------------------------
+struct EqP {
+  int npoin, nitmax;
+  double eps;
+  Sell S, St;
+  const double *da, *dsc;
+  double *x;
+  const double *b;
+  double *r, *d0, *d1, *ad, *t;
+  double *part;
+  Ctl *ctl;
+  long long timeout_ns;
+};
+
+template <int TD, int STO>
+__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_equnor(EqP P) {
+  const int T = blockDim.x, t = threadIdx.x;
+  const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
+  const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
+  double *x = P.x, *r = P.r, *ad = P.ad, *atr = P.t;
+  const double *b = P.b, *da = P.da;
+  const bool lead = (blockIdx.x == 0 && t == 0);
+  double s, red;
+  int nbar = 0;
+  const bool h1 = false;
+
+  auto finish = [&](int status, int m, double rmrm, double xl, int relat) {
+    if (P.dsc)  // solve.f:637-641: X = X*D
+      for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
+    if (lead) {
+      P.ctl->status = status;
+      P.ctl->nit = m;
+      P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
+      P.ctl->relat = relat;
+    }
+  };
+  double a1 = 0.0;
+
+  // XL = P_DOTS(B,B), absolute mode below 1 (equnor.f:108-114)
+  s = 0.0;
+  for (int i = lo + t; i < hi; i += T) s = add(s, mul(b[i], b[i]));
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  double xl = red;
+  int relat = 1;
+  if (xl < 1.0) { xl = 1.0; relat = 0; }
+  const double tol = mul(xl, mul(P.eps, P.eps));
+
+  // R = A X - B, RMRM (:118-123)
+  s = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    double a0 = diag_term<TD>(x[i], da, i);
+    op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
+    const double r0 = sub(a0, b[i]);
+    r[i] = r0;
+    s = add(s, mul(r0, r0));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  double rmrm = red;
+  if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
+  if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }  // :127
+
+  // D = A^T R, TGMTGM (:160-163)
+  double *cur = P.d0, *nxt = P.d1;
+  s = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    double a0 = diag_term<TD>(r[i], da, i);
+    op_row2<STO>(i, i, h1, a0, a1, P.St, [&](int j) { return r[j]; });
+    cur[i] = a0;
+    s = add(s, mul(a0, a0));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  double tg = red;
+  // AD = A D, ADAD, RO (:169-189)
+  s = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    double a0 = diag_term<TD>(cur[i], da, i);
+    op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return cur[j]; });
+    ad[i] = a0;
+    s = add(s, mul(a0, a0));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  double adad = red;
+  if (!(adad > 0.0)) { finish(isnan(adad) ? ST_NAN : ST_BREAKDOWN, 0, rmrm, xl, relat); return; }
+  double ro = __ddiv_rn(tg, adad);
+
+  for (int m = 1;; ++m) {
+    // X = X - RO D (:195 / :278), R = R - RO AD (:207), RMRM (:211)
+    const double nro = -ro;
+    s = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      x[i] = add(x[i], mul(nro, cur[i]));
+      const double ri = add(r[i], mul(nro, ad[i]));
+      r[i] = ri;
+      s = add(s, mul(ri, ri));
+    }
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+    rmrm = red;
+    if (isnan(rmrm)) { finish(ST_NAN, m, rmrm, xl, relat); return; }
+    if (rmrm <= tol) { finish(ST_OK, m, rmrm, xl, relat); return; }  // :215
+
+    // A^T R (:240), TGMTGM (:244)
+    s = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      double a0 = diag_term<TD>(r[i], da, i);
+      op_row2<STO>(i, i, h1, a0, a1, P.St, [&](int j) { return r[j]; });
+      atr[i] = a0;
+      s = add(s, mul(a0, a0));
+    }
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+    const double tg1 = tg;
+    tg = red;
+    const double beta = __ddiv_rn(tg, tg1);  // :245
+
+    // D = BETA D + A^T R (:247-250) where needed, AD = A D (:256), ADAD (:272)
+    s = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      const double di = add(mul(beta, cur[i]), atr[i]);
+      nxt[i] = di;
+      double a0 = diag_term<TD>(di, da, i);
+      op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return add(mul(beta, cur[j]), atr[j]); });
+      ad[i] = a0;
+      s = add(s, mul(a0, a0));
+    }
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+    adad = red;
+    if (!(adad > 0.0)) { finish(isnan(adad) ? ST_NAN : ST_BREAKDOWN, m, rmrm, xl, relat); return; }
+    ro = __ddiv_rn(tg, adad);  // :274
+    double *tmp = cur; cur = nxt; nxt = tmp;
+
+    if (m >= P.nitmax) {  // :280 -- last X update, then stop unconverged
       const double nr = -ro;
       for (int i = lo + t; i < hi; i += T) x[i] = add(x[i], mul(nr, cur[i]));
       finish(m, m, rmrm, xl, relat);

@@ -733,7 +733,74 @@ int orc_gracjg(int npoin, int nelem, const int *ik0, const int *ik1,
                        nit_out, relres_out, relat_out);
 }
 
-/* solve.f:387-649 for SLV=1 (GRACJG) on a single (non-block) matrix:
+/* equnor.f:106-311 (CG on the normal equations) without preconditioning
+ * matrices (PREC false, so G aliases R, solve.f:473-474):
+ *   XL = B.B (absolute mode below 1); R = A X - B; RMRM = R.R; stop if
+ *   RMRM < EPS**2 XL; D = A^T R; TGMTGM = D.D; AD = A D; RO = TGMTGM/AD.AD;
+ *   X = X - RO D; then per iteration R = R - RO AD; RMRM = R.R; stop if
+ *   RMRM <= XL EPS**2; AD = A^T R; BETA = AD.AD / previous TGMTGM;
+ *   D = BETA D, D = D + AD (two passes, 'X=CX' then 'X=X+Y'); AD = A D;
+ *   RO = TGMTGM / AD.AD; X = X - RO D; stop at NITMAX. */
+static int equnor_impl(const opmesh *M, int npoin, double *x, const double *da, char typdia,
+                       const double *xm, char typext, const double *b, int nitmax, double eps,
+                       int dot_mode, int nb, int nt, int *nit_out, double *relres_out,
+                       int *relat_out)
+{
+    const int nelem = M->sto == 3 ? 0 : M->nelem;
+    size_t n = (size_t)npoin;
+    double *r = (double *)malloc(sizeof(double) * n);
+    double *dd = (double *)malloc(sizeof(double) * n);
+    double *ad = (double *)malloc(sizeof(double) * n);
+    double *t = (double *)malloc(sizeof(double) * n);
+    double *w = (double *)malloc(sizeof(double) * 3 * (size_t)nelem + 1);
+    int m = 0, st = ORC_OK, relat;
+    double xl, rmrm, tgmtgm, tg1tg1, adad, ro, beta;
+    if (!r || !dd || !ad || !t || !w) { st = ORC_ERR_ARGS; goto done; }
+    xl = pdots(dot_mode, npoin, b, b, nb, nt);                    /* :108 */
+    if (xl < 1.0) { xl = 1.0; relat = 0; } else { relat = 1; }    /* :109-114 */
+    st = op_matvec(M, "X=AY    ", npoin, r, da, typdia, xm, typext, x, 0.0, t, w);  /* :118 */
+    if (st) goto done;
+    for (size_t i = 0; i < n; ++i) r[i] = r[i] - b[i];          /* :119 */
+    rmrm = pdots(dot_mode, npoin, r, r, nb, nt);                 /* :123 */
+    if (rmrm < eps * eps * xl) goto fin;                         /* :127 */
+    st = op_matvec(M, "X=TAY   ", npoin, dd, da, typdia, xm, typext, r, 0.0, t, w); /* :160 */
+    if (st) goto done;
+    tgmtgm = pdots(dot_mode, npoin, dd, dd, nb, nt);             /* :163 */
+    st = op_matvec(M, "X=AY    ", npoin, ad, da, typdia, xm, typext, dd, 0.0, t, w); /* :169 */
+    if (st) goto done;
+    adad = pdots(dot_mode, npoin, ad, ad, nb, nt);               /* :187 */
+    ro = tgmtgm / adad;                                          /* :189 */
+    for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * dd[i];  /* :195 */
+    for (;;) {
+        m = m + 1;                                               /* :201 */
+        for (size_t i = 0; i < n; ++i) r[i] = r[i] + (-ro) * ad[i];      /* :207 */
+        rmrm = pdots(dot_mode, npoin, r, r, nb, nt);             /* :211 */
+        if (rmrm <= xl * (eps * eps)) goto fin;                  /* :215 */
+        st = op_matvec(M, "X=TAY   ", npoin, ad, da, typdia, xm, typext, r, 0.0, t, w); /* :240 */
+        if (st) goto done;
+        tg1tg1 = tgmtgm;                                         /* :243 */
+        tgmtgm = pdots(dot_mode, npoin, ad, ad, nb, nt);         /* :244 */
+        beta = tgmtgm / tg1tg1;                                  /* :245 */
+        for (size_t i = 0; i < n; ++i) dd[i] = beta * dd[i];     /* :247 */
+        for (size_t i = 0; i < n; ++i) dd[i] = dd[i] + ad[i];    /* :250 */
+        st = op_matvec(M, "X=AY    ", npoin, ad, da, typdia, xm, typext, dd, 0.0, t, w); /* :256 */
+        if (st) goto done;
+        adad = pdots(dot_mode, npoin, ad, ad, nb, nt);           /* :272 */
+        ro = tgmtgm / adad;                                      /* :274 */
+        for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * dd[i];      /* :278 */
+        if (m >= nitmax) { st = m; goto fin; }                   /* :280 */
+    }
+fin:
+    if (nit_out) *nit_out = m;
+    if (relres_out) *relres_out = sqrt(rmrm / xl);
+    if (relat_out) *relat_out = relat;
+done:
+    free(r); free(dd); free(ad); free(t); free(w);
+    return st;
+}
+
+/* solve.f:387-649 for SLV=1 (GRACJG, solve.f:555-558) and SLV=3 (EQUNOR,
+ * :565-570) on a single (non-block) matrix:
  * PRECON 0 -> 1; diagonal change of variables when PRECON is divisible by
  * 2, 3 or 5 (solve.f:484-498); CG; X = X*D to undo the change of variables
  * (solve.f:637-641).  Inputs x, b, dm, typdia, xm are modified in place
@@ -743,7 +810,7 @@ static int solve_impl(const opmesh *M, int npoin, double *x, double *b, double *
                       int nitmax, double eps, int dot_mode, int nb, int nt, int *nit_out,
                       double *relres_out, int *relat_out)
 {
-    if (slv != 1) return ORC_ERR_UNSUPPORTED;
+    if (slv != 1 && slv != 3) return ORC_ERR_UNSUPPORTED;
     if (precon == 0) precon = 1;
     if (precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 ||
         precon % 17 == 0)
@@ -755,8 +822,11 @@ static int solve_impl(const opmesh *M, int npoin, double *x, double *b, double *
         int st = precd1_impl(M, npoin, precon, x, dm, typdia, xm, typext, b, d);
         if (st) { free(d); return st; }
     }
-    int st = gracjg_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode, nb,
-                         nt, nit_out, relres_out, relat_out);
+    int st = slv == 3
+                 ? equnor_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
+                               nb, nt, nit_out, relres_out, relat_out)
+                 : gracjg_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
+                               nb, nt, nit_out, relres_out, relat_out);
     if (diag) {
         for (int i = 0; i < npoin; ++i) x[i] = x[i] * d[i];
         free(d);
