@@ -92,10 +92,12 @@ int bief_set_matrix_dev(bief_handle *h, const double *dm, const double *xm,
 /* Read back the stored matrix (e.g. after a mutating solve). */
 int bief_get_matrix(bief_handle *h, double *dm, double *xm, char *typdia);
 
-/* SOLVE(X,A,B,...) for SLV=1 (GRACJG, gracjg.F) and SLV=3 (EQUNOR, CG on
- * the normal equations, equnor.f): host X (initial guess in, solution out)
- * and B.  relres_out receives SQRT(RMRM/XL) as the method prints it.  Other
- * SLV values return BIEF_ERR_UNSUPPORTED. */
+/* SOLVE(X,A,B,...) for SLV=1 (GRACJG, gracjg.F), SLV=3 (EQUNOR, CG on the
+ * normal equations, equnor.f) and SLV=7 (GMRES(KRYLOV), gmres.f, KRYLOV
+ * 1..20, NITMAX counting restarts): host X (initial guess in, solution out)
+ * and B.  relres_out receives the relative residual the method prints
+ * (SQRT(RMRM/XL), or NR0/NB for GMRES).  Other SLV values return
+ * BIEF_ERR_UNSUPPORTED. */
 int bief_solve(bief_handle *h, double *x, double *b, bief_slvcfg *cfg,
                int flags, double *relres_out);
 /* Same with device pointers, on `stream`. */

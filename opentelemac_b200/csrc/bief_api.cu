@@ -37,6 +37,9 @@ struct bief_handle {
   double2 *d_rec_c = nullptr;
   double2 *d_rec_ct = nullptr;   // transposed-operator records (EQUNOR, 'Q' storage)
   double *d_sg_ct = nullptr;     // transposed-operator segment slots
+  // GMRES: Krylov basis V and A V (2 * krylov * npoin), multi-value partials
+  double *d_gmv = nullptr, *d_gpart = nullptr;
+  int gm_k = 0;
   float *d_seg_c = nullptr, *d_s32 = nullptr;
   long long nrec = 0, nseg = 0;
   int max_nnb = 0;
@@ -168,6 +171,17 @@ void *equnor_kernel(int td, int sto) {
   return (void *)k_equnor<DIA_0, 1>;
 }
 
+void *gmres_kernel(int td, int sto) {
+  if (sto == 3) {
+    if (td == DIA_Q) return (void *)k_gmres<DIA_Q, 3>;
+    if (td == DIA_I) return (void *)k_gmres<DIA_I, 3>;
+    return (void *)k_gmres<DIA_0, 3>;
+  }
+  if (td == DIA_Q) return (void *)k_gmres<DIA_Q, 1>;
+  if (td == DIA_I) return (void *)k_gmres<DIA_I, 1>;
+  return (void *)k_gmres<DIA_0, 1>;
+}
+
 void *mixed_kernel(int td, int sto) {
   if (sto == 3) {
     if (td == DIA_Q) return (void *)k_mixed<DIA_Q, 3>;
@@ -208,7 +222,9 @@ int persistent_grid(int npoin, int nsm, int *out) {
                 cg_kernel(DIA_Q, 3), cg_kernel(DIA_I, 3), cg_kernel(DIA_0, 3),
                 mixed_kernel(DIA_Q, 3), mixed_kernel(DIA_I, 3), mixed_kernel(DIA_0, 3),
                 equnor_kernel(DIA_Q, 1), equnor_kernel(DIA_I, 1), equnor_kernel(DIA_0, 1),
-                equnor_kernel(DIA_Q, 3), equnor_kernel(DIA_I, 3), equnor_kernel(DIA_0, 3)};
+                equnor_kernel(DIA_Q, 3), equnor_kernel(DIA_I, 3), equnor_kernel(DIA_0, 3),
+                gmres_kernel(DIA_Q, 1), gmres_kernel(DIA_I, 1), gmres_kernel(DIA_0, 1),
+                gmres_kernel(DIA_Q, 3), gmres_kernel(DIA_I, 3), gmres_kernel(DIA_0, 3)};
   for (void *k : ks) {
     int bps = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, CG_THREADS, 0));
@@ -370,7 +386,8 @@ int build_transposed(bief_handle *h, const double *xm, cudaStream_t st, Sell *ou
 
 int check_cfg(const bief_slvcfg *cfg, int *precon) {
   if (!cfg) return BIEF_ERR_ARGS;
-  if (cfg->slv != 1 && cfg->slv != 3) return BIEF_ERR_UNSUPPORTED;
+  if (cfg->slv != 1 && cfg->slv != 3 && cfg->slv != 7) return BIEF_ERR_UNSUPPORTED;
+  if (cfg->slv == 7 && (cfg->krylov < 1 || cfg->krylov > GM_MAXK)) return BIEF_ERR_ARGS;
   int p = cfg->precon == 0 ? 1 : cfg->precon;
   if (p <= 0) return BIEF_ERR_ARGS;
   if (p % 7 == 0 || p % 11 == 0 || p % 13 == 0 || p % 17 == 0) return BIEF_ERR_UNSUPPORTED;
@@ -565,7 +582,7 @@ int bief_destroy(bief_handle *h) {
                   h->d_rec_idx, h->d_rec_slot, h->d_rec_c, h->d_seg_col, h->d_seg_c,
                   h->d_binst, h->d_brel, h->d_bpart, h->d_g1, h->d_g2, h->d_sg_meta,
                   h->d_sg_off, h->d_sg_sx, h->d_sg_col, h->d_segel, h->d_xa, h->d_xas,
-                  h->d_sg_c64, h->d_sg_c32, h->d_rec_ct, h->d_sg_ct};
+                  h->d_sg_c64, h->d_sg_c32, h->d_rec_ct, h->d_sg_ct, h->d_gmv, h->d_gpart};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (h->h_ctl) cudaFreeHost(h->h_ctl);
@@ -686,7 +703,36 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   }
   if ((st = seg ? build_seg_coefs(h, xm, s) : build_records(h, xm, s))) return st;
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
-  if (cfg->slv == 3) {  // EQUNOR
+  if (cfg->slv == 7) {  // GMRES
+    if (h->gm_k < cfg->krylov) {
+      if (h->d_gmv) cudaFree(h->d_gmv);
+      h->d_gmv = nullptr;
+      h->gm_k = 0;
+      if ((st = dalloc(&h->d_gmv, 2 * (size_t)cfg->krylov * h->npoin))) return st;
+      h->gm_k = cfg->krylov;
+    }
+    if (!h->d_gpart && (st = dalloc(&h->d_gpart, 2 * (size_t)h->G * (GM_MAXK + 1) + 4)))
+      return st;
+    GmP P;
+    P.npoin = h->npoin;
+    P.nitmax = cfg->nitmax;
+    P.krylov = cfg->krylov;
+    P.eps = cfg->eps;
+    P.S = sell_of(h);
+    P.da = da;
+    P.dsc = diag ? h->d_dsc : nullptr;
+    P.x = x;
+    P.b = bw;
+    P.r0 = h->d_r;
+    P.v = h->d_gmv;
+    P.av = h->d_gmv + (size_t)cfg->krylov * h->npoin;
+    P.part = h->d_part;
+    P.part_n = h->d_gpart;
+    P.ctl = h->d_ctl;
+    P.timeout_ns = h->timeout_ns;
+    CK(cudaEventRecord(h->ev[0], s));
+    if ((st = launch_coop(h, gmres_kernel(td, h->sto), &P, s))) return st;
+  } else if (cfg->slv == 3) {  // EQUNOR
     EqP P;
     P.npoin = h->npoin;
     P.nitmax = cfg->nitmax;
@@ -737,7 +783,8 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   cfg->ok = (st == BIEF_OK) ? 1 : 0;
   if (relres_out) *relres_out = c.relres;
   if (st >= 0 && ((flags & BIEF_SOLVE_INFOGR) || st > 0))
-    print_gracjg(st, c.nit, c.relres, c.relat, cfg->slv == 3 ? "EQUNOR" : "GRACJG");
+    print_gracjg(st, c.nit, c.relres, c.relat,
+                 cfg->slv == 3 ? "EQUNOR" : (cfg->slv == 7 ? "GMRES" : "GRACJG"));
   if (diag && (flags & BIEF_SOLVE_MUTATE_INPUTS) && st >= 0) {
     // SOLVE leaves B = D.B and A = D.A.D with TYPDIA from PRECD1
     CK(cudaMemcpyAsync(b, h->d_bs, sizeof(double) * h->npoin, cudaMemcpyDeviceToDevice, s));

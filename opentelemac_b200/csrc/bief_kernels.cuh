@@ -609,6 +609,263 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_equnor(EqP P) {
 }
 
 // ---------------------------------------------------------------------------
+// GMRES(KRYLOV) (gmres.f:55-213) without preconditioning matrices, as ONE
+// persistent kernel.  Columns 1..K-1 by modified Gram-Schmidt: each
+// projection's AXPY is fused with the next dot (one grid reduction per
+// dot); the normalisation of V(J+1) happens in the pass that computes
+// A V(J+1), where every thread that reads V(J+1) at a neighbour scales it
+// itself (the owner's bits) and the owner stores it.  Column K: its K+1 dots
+// in one pass and one multi-value reduction.  The small dense part (H, the
+// Givens rotations, back substitution) is computed by thread 0 of every
+// block from identical inputs, so all blocks hold the same scalars.
+// ---------------------------------------------------------------------------
+constexpr int GM_MAXK = 20;
+
+struct GmP {
+  int npoin, nitmax, krylov;
+  double eps;
+  Sell S;
+  const double *da, *dsc;
+  double *x;
+  const double *b;
+  double *r0, *v, *av;   // V(1..K), AV(1..K): K vectors of npoin each
+  double *part;          // grid_reduce partials: 4 * G doubles
+  double *part_n;        // grid_reduce_n partials: 2 * G * (GM_MAXK + 1) doubles
+  Ctl *ctl;
+  long long timeout_ns;
+};
+
+// Reduction of n <= GM_MAXK+1 binary64 values per thread (blocked order of
+// each value, as grid_reduce).  vals/out may alias.
+__device__ __noinline__ bool grid_reduce_n(Ctl *ctl, double *part, long long timeout_ns,
+                                           int &nbar, const double *vals, int n, double *out) {
+  __shared__ double smd[32];
+  __shared__ double red_sm[GM_MAXK + 1];
+  __shared__ int s_err;
+  const int G = gridDim.x, T = blockDim.x, t = threadIdx.x;
+  const unsigned long long k = (unsigned long long)(++nbar);
+  double *buf = part + (size_t)(k & 1) * (size_t)G * (GM_MAXK + 1);
+  for (int q = 0; q < n; ++q) {
+    const double bd = block_tree(vals[q], smd);
+    if (t == 0) buf[(size_t)blockIdx.x * (GM_MAXK + 1) + q] = bd;
+  }
+  if (t == 0) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> cnt(ctl->arrivals);
+    cnt.fetch_add(1ull, cuda::memory_order_release);
+    const unsigned long long target = k * (unsigned long long)G;
+    const unsigned long long t0 = global_ns();
+    s_err = 0;
+    while (cnt.load(cuda::memory_order_acquire) < target) {
+      if ((long long)(global_ns() - t0) > timeout_ns) {
+        s_err = 1;
+        atomicExch(&ctl->status, (int)ST_TIMEOUT);
+        break;
+      }
+      __nanosleep(20);
+    }
+  }
+  __syncthreads();
+  if (s_err) return false;
+  for (int q = 0; q < n; ++q) {
+    double acc = 0.0;
+    for (int bb = t; bb < G; bb += T) acc = add(acc, __ldcg(buf + (size_t)bb * (GM_MAXK + 1) + q));
+    const double tot = block_tree(acc, smd);
+    if (t == 0) red_sm[q] = tot;
+  }
+  __syncthreads();
+  for (int q = 0; q < n; ++q) out[q] = red_sm[q];
+  __syncthreads();
+  return true;
+}
+
+template <int TD, int STO>
+__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
+  const int T = blockDim.x, t = threadIdx.x;
+  const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
+  const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
+  const size_t N = (size_t)P.npoin;
+  double *x = P.x, *r0 = P.r0;
+  const double *b = P.b, *da = P.da;
+  const bool lead = (blockIdx.x == 0 && t == 0);
+  __shared__ double H[GM_MAXK + 1][GM_MAXK];
+  __shared__ double Cg[GM_MAXK], Sg[GM_MAXK], E[GM_MAXK + 1];
+  __shared__ int s_flag;
+  double vals[GM_MAXK + 1];
+  double s, red;
+  int nbar = 0;
+  const bool h1 = false;
+  double a1 = 0.0;
+  auto V = [&](int j) { return P.v + (size_t)(j - 1) * N; };    // 1-based columns
+  auto AV = [&](int j) { return P.av + (size_t)(j - 1) * N; };
+
+  int m = 0, relat = 1;
+  double prec = 0.0;
+  auto finish = [&]() {
+    if (P.dsc)  // solve.f:637-641: X = X*D
+      for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
+    if (lead) {
+      P.ctl->status = m < P.nitmax ? ST_OK : m;   // gmres.f:199-214 end messages
+      P.ctl->nit = m;
+      P.ctl->relres = prec;
+      P.ctl->relat = relat;
+    }
+  };
+
+  // NB = SQRT(B.B), absolute mode below 1 (:67-73)
+  s = 0.0;
+  for (int i = lo + t; i < hi; i += T) s = add(s, mul(b[i], b[i]));
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  double nbn = __dsqrt_rn(red);
+  if (nbn < 1.0) { nbn = 1.0; relat = 0; }
+  // R0 = A X - B, NR0 (:77-86)
+  s = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    double a0 = diag_term<TD>(x[i], da, i);
+    op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
+    const double r = sub(a0, b[i]);
+    r0[i] = r;
+    s = add(s, mul(r, r));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  double nr0 = __dsqrt_rn(red);
+  prec = __ddiv_rn(nr0, nbn);
+  if (isnan(prec)) { if (lead) P.ctl->status = ST_NAN; return; }
+  if (prec <= P.eps) { finish(); return; }   // :87
+
+  for (;;) {
+    ++m;                                      // :91
+    int K = P.krylov;
+    const double c0 = __ddiv_rn(-1.0, nr0);   // :95 V(1) = (-1/NR0) R0
+    // The vector V(j) as read at node q: V(1) = c0*R0, V(j>1) = cs*Vraw(j)
+    // when its normalisation is pending (cs != 0), else the stored value.
+    auto vread = [&](int j, double cs, int q) -> double {
+      return j == 1 ? mul(c0, r0[q]) : (cs != 0.0 ? mul(cs, V(j)[q]) : V(j)[q]);
+    };
+    double cs = 0.0;   // pending scale of the newest column
+    for (int J = 1; J <= K - 1; ++J) {
+      // AV(J) = A V(J) [storing V(J) normalised]; V(J+1) = AV(J);
+      // first MGS dot H(1,J) = V(J+1).V(1)
+      double *vj = V(J), *avj = AV(J), *vn = V(J + 1);
+      s = 0.0;
+      for (int i = lo + t; i < hi; i += T) {
+        const double vi = vread(J, cs, i);
+        double a0 = diag_term<TD>(vi, da, i);
+        op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int q) { return vread(J, cs, q); });
+        avj[i] = a0;
+        vn[i] = a0;
+        if (J == 1) vj[i] = vi;   // nobody reads V(1) from memory in this pass
+        const double v1 = J == 1 ? vi : V(1)[i];
+        s = add(s, mul(a0, v1));
+      }
+      if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+      // every block has finished reading the unscaled V(J): store it scaled
+      if (J > 1 && cs != 0.0)
+        for (int i = lo + t; i < hi; i += T) vj[i] = mul(cs, vj[i]);
+      if (t == 0) H[0][J - 1] = red;
+      double hprev = red;
+      // I = 2..J: V(J+1) -= H(I-1,J) V(I-1); H(I,J) = V(J+1).V(I)
+      for (int I = 2; I <= J + 1; ++I) {
+        const double ch = -hprev;
+        const double *vp = V(I - 1);
+        s = 0.0;
+        for (int i = lo + t; i < hi; i += T) {
+          const double u = add(vn[i], mul(ch, vp[i]));
+          vn[i] = u;
+          const double w = I <= J ? V(I)[i] : u;   // I = J+1: the norm of V(J+1)
+          s = add(s, mul(u, w));
+        }
+        if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr))
+          return;
+        if (I <= J) {
+          if (t == 0) H[I - 1][J - 1] = red;
+          hprev = red;
+        } else {
+          hprev = __dsqrt_rn(red);                // H(J+1,J)
+          if (t == 0) H[J][J - 1] = hprev;
+        }
+      }
+      if (hprev < 1.0e-20) {                       // :107-130
+        K = J;
+        cs = 0.0;
+        break;
+      }
+      cs = __ddiv_rn(1.0, hprev);                 // :131 V(J+1) = V(J+1)/H(J+1,J), deferred
+    }
+    // AV(K) = A V(K) (:145-151); H(K+1,K) = AV.AV - sum H(I,K)**2 with
+    // H(I,K) = AV(K).V(I) (:153-158)
+    {
+      double *vk = V(K), *avk = AV(K);
+      for (int q = 0; q <= K; ++q) vals[q] = 0.0;
+      for (int i = lo + t; i < hi; i += T) {
+        const double vi = vread(K, cs, i);
+        double a0 = diag_term<TD>(vi, da, i);
+        op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int q) { return vread(K, cs, q); });
+        avk[i] = a0;
+        vals[K] = add(vals[K], mul(a0, a0));
+        for (int I = 1; I <= K; ++I) {
+          const double vI = I == K ? vi : (I == 1 ? mul(c0, r0[i]) : V(I)[i]);
+          vals[I - 1] = add(vals[I - 1], mul(a0, vI));
+        }
+      }
+      if (!grid_reduce_n(P.ctl, P.part_n, P.timeout_ns, nbar, vals, K + 1, vals)) return;
+      // all reads of the unscaled V(K) are done: store it as used
+      for (int i = lo + t; i < hi; i += T) vk[i] = vread(K, cs, i);
+    }
+    if (t == 0) {
+      double hk = vals[K];
+      for (int I = 1; I <= K; ++I) {
+        H[I - 1][K - 1] = vals[I - 1];
+        hk = sub(hk, mul(vals[I - 1], vals[I - 1]));
+      }
+      H[K][K - 1] = __dsqrt_rn(hk > 0.0 ? hk : 0.0);
+      // Givens rotations (:160-183)
+      E[0] = nr0;
+      int fail = 0;
+      for (int I = 1; I <= K && !fail; ++I) {
+        for (int J = 1; J <= I - 1; ++J) {
+          const double zz = add(mul(Cg[J - 1], H[J - 1][I - 1]), mul(Sg[J - 1], H[J][I - 1]));
+          H[J][I - 1] = add(mul(-Sg[J - 1], H[J - 1][I - 1]), mul(Cg[J - 1], H[J][I - 1]));
+          H[J - 1][I - 1] = zz;
+        }
+        const double rr = __dsqrt_rn(add(mul(H[I - 1][I - 1], H[I - 1][I - 1]),
+                                         mul(H[I][I - 1], H[I][I - 1])));
+        if (fabs(rr) < 1.0e-6) { fail = 1; break; }
+        Cg[I - 1] = __ddiv_rn(H[I - 1][I - 1], rr);
+        Sg[I - 1] = __ddiv_rn(H[I][I - 1], rr);
+        H[I - 1][I - 1] = rr;
+        E[I] = mul(-Sg[I - 1], E[I - 1]);
+        E[I - 1] = mul(Cg[I - 1], E[I - 1]);
+      }
+      if (!fail) {  // back substitution (:184-190)
+        E[K - 1] = __ddiv_rn(E[K - 1], H[K - 1][K - 1]);
+        for (int J = K - 1; J >= 1; --J) {
+          for (int L = J + 1; L <= K; ++L) E[J - 1] = sub(E[J - 1], mul(H[J - 1][L - 1], E[L - 1]));
+          E[J - 1] = __ddiv_rn(E[J - 1], H[J - 1][J - 1]);
+        }
+      }
+      s_flag = fail;
+    }
+    __syncthreads();
+    if (s_flag) { finish(); return; }   // R < 1e-6: the solve ends without this update
+    // X = X + E(L) V(L), R0 = R0 + E(L) AV(L), L = 1..K (:191-194)
+    for (int i = lo + t; i < hi; i += T) {
+      double xi = x[i], ri = r0[i];
+      for (int L = 1; L <= K; ++L) {
+        xi = add(xi, mul(E[L - 1], V(L)[i]));
+        ri = add(ri, mul(E[L - 1], AV(L)[i]));
+      }
+      x[i] = xi;
+      r0[i] = ri;
+    }
+    nr0 = fabs(E[K]);                 // :195
+    prec = __ddiv_rn(nr0, nbn);
+    if (!(prec >= P.eps && m < P.nitmax)) { finish(); return; }   // :197
+    // the next restart reads R0 at neighbours
+    if (!grid_barrier(P.ctl, P.timeout_ns, nbar)) return;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Mixed precision, one launch: a binary32 CG on the binary32 edge-assembled
 // copy of the scaled operator (binary32 vectors, products and dot
 // accumulation) whose correction z is folded into the binary64 solution

@@ -50,7 +50,7 @@ def lib():
         L.orc_dot_blocked.restype = d
         L.orc_precd1.argtypes = [i, i, pi, pi, pi, i, pd, pd, P(c), pd, i, c, pd, pd]
         L.orc_solve.argtypes = [i, i, pi, pi, pi, pd, pd, pd, P(c), pd, i, c, i, i, i, d, i, i,
-                                i, pi, pd, pi]
+                                i, pi, pd, pi, i]
         L.orc_solve_mixed.argtypes = [i, i, pi, pi, pi, pd, pd, pd, c, pd, c, i, d, d, i, i, i,
                                       i, pi, pi, pd]
         _lib = L
@@ -127,7 +127,7 @@ def dot(x, y, mode=DOT_SEQUENTIAL, nblocks=1, nthreads=256):
 
 
 def solve(ikle0, dm, typdia, xm, typext, b, x0=None, precon=2, nitmax=100000, eps=1e-8,
-          slv=1, dot_mode=DOT_SEQUENTIAL, nblocks=1, nthreads=256):
+          slv=1, dot_mode=DOT_SEQUENTIAL, nblocks=1, nthreads=256, krylov=3):
     """SOLVE(X,A,B) with SLV=1.  Works on copies; returns a dict with x, the
     mutated b/dm/xm/typdia (as the reference leaves them), status, nit,
     relres, relat."""
@@ -143,7 +143,7 @@ def solve(ikle0, dm, typdia, xm, typext, b, x0=None, precon=2, nitmax=100000, ep
     st = lib().orc_solve(n, ne, _pi(a), _pi(bb), _pi(c), _pd(x), _pd(b), _pd(dm),
                          ctypes.byref(td), _pd(xm), ne, typext.encode(), slv, precon, nitmax,
                          eps, dot_mode, nblocks, nthreads, ctypes.byref(nit),
-                         ctypes.byref(relres), ctypes.byref(relat))
+                         ctypes.byref(relres), ctypes.byref(relat), krylov)
     return dict(x=x, b=b, dm=dm, xm=xm, typdia=td.value.decode(), status=st, nit=nit.value,
                 relres=relres.value, relat=relat.value)
 
@@ -233,7 +233,7 @@ def _seg_lib():
         L.orc_assex3.argtypes = [i, pi, pi, c, pd, i, i, pd]
         L.orc_mvseg.argtypes = [ctypes.c_char_p, i, i, pi, pi, pd, pd, c, pd, c, pd, d]
         L.orc_solve_seg.argtypes = [i, i, pi, pi, pd, pd, pd, P(c), pd, c, i, i, i, d, i, i, i,
-                                    pi, pd, pi]
+                                    pi, pd, pi, i]
         L.orc_solve_mixed_seg.argtypes = [i, i, pi, pi, pd, pd, pd, c, pd, c, i, d, d, i, i, i,
                                           i, pi, pi, pd]
         L._seg_ready = True
@@ -294,7 +294,7 @@ def mvseg(op, g1, g2, dm, typdia, xa, typext, y, c=0.0, x=None):
 
 
 def solve_seg(g1, g2, dm, typdia, xa, typext, b, x0=None, precon=2, nitmax=100000, eps=1e-8,
-              slv=1, dot_mode=DOT_SEQUENTIAL, nblocks=1, nthreads=256):
+              slv=1, dot_mode=DOT_SEQUENTIAL, nblocks=1, nthreads=256, krylov=3):
     """SOLVE(SLV=1) on a segment-storage matrix; same outputs as solve()
     (with 'xa' for the mutated off-diagonal terms)."""
     g1, g2 = _i32(g1), _i32(g2)
@@ -309,7 +309,7 @@ def solve_seg(g1, g2, dm, typdia, xa, typext, b, x0=None, precon=2, nitmax=10000
     st = _seg_lib().orc_solve_seg(n, g1.size, _pi(g1), _pi(g2), _pd(x), _pd(b), _pd(dm),
                                   ctypes.byref(td), _pd(xa), typext.encode(), slv, precon,
                                   nitmax, eps, dot_mode, nblocks, nthreads, ctypes.byref(nit),
-                                  ctypes.byref(relres), ctypes.byref(relat))
+                                  ctypes.byref(relres), ctypes.byref(relat), krylov)
     return dict(x=x, b=b, dm=dm, xa=xa, typdia=td.value.decode(), status=st, nit=nit.value,
                 relres=relres.value, relat=relat.value)
 

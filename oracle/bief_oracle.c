@@ -799,6 +799,120 @@ done:
     return st;
 }
 
+/* gmres.f:55-213, restarted GMRES(KRYLOV) without preconditioning
+ * matrices (PRECO false), KRYLOV <= 20 (H(21,20)):
+ *   NB = SQRT(B.B) (absolute mode below 1); R0 = A X - B; NR0 = |R0|;
+ *   stop if NR0/NB <= EPS.  Each restart M: V1 = (-1/NR0) R0; for
+ *   J = 1..K-1: AV(J) = A V(J), V(J+1) = AV(J), modified Gram-Schmidt
+ *   H(I,J) = V(J+1).V(I), V(J+1) = V(J+1) - H(I,J) V(I) for I = 1..J,
+ *   H(J+1,J) = |V(J+1)| (below 1e-20: K = J, leave the loop),
+ *   V(J+1) = (1/H(J+1,J)) V(J+1); AV(K) = A V(K); H(K+1,K) =
+ *   AV(K).AV(K) - sum of H(I,K)**2 with H(I,K) = AV(K).V(I), then
+ *   SQRT(MAX(.,0)); Givens rotations on H and E (E(1) = NR0), R below 1e-6
+ *   ends the solve before this restart's update; back substitution;
+ *   X = X + E(L) V(L), R0 = R0 + E(L) AV(L) for L = 1..K; NR0 = |E(K+1)|;
+ *   restart while NR0/NB >= EPS and M < NITMAX.
+ * Returns ORC_OK when M < NITMAX at the end, M (> 0) otherwise (the
+ * reference's two end messages); relres_out receives NR0/NB. */
+static int gmres_impl(const opmesh *M, int npoin, double *x, const double *da, char typdia,
+                      const double *xm, char typext, const double *b, int nitmax, double eps,
+                      int krylov, int dot_mode, int nb, int nt, int *nit_out,
+                      double *relres_out, int *relat_out)
+{
+    if (krylov < 1 || krylov > 20) return ORC_ERR_ARGS;
+    const int nelem = M->sto == 3 ? 0 : M->nelem;
+    size_t n = (size_t)npoin;
+    double *r0 = (double *)malloc(sizeof(double) * n);
+    double *t = (double *)malloc(sizeof(double) * n);
+    double *w = (double *)malloc(sizeof(double) * 3 * (size_t)nelem + 1);
+    double *v = (double *)malloc(sizeof(double) * n * (size_t)krylov);
+    double *av = (double *)malloc(sizeof(double) * n * (size_t)krylov);
+    double h[21][20], c[20], sn[20], e[21];
+    int m = 0, st = ORC_OK, relat = 1;
+    double nbn, nr0, prec = 0.0;
+    if (!r0 || !t || !w || !v || !av) { st = ORC_ERR_ARGS; goto done; }
+#define V(j) (v + (size_t)(j) * n)
+#define AV(j) (av + (size_t)(j) * n)
+    nbn = sqrt(pdots(dot_mode, npoin, b, b, nb, nt));           /* :67-68 */
+    if (nbn < 1.0) { nbn = 1.0; relat = 0; }                     /* :70-73 */
+    st = op_matvec(M, "X=AY    ", npoin, r0, da, typdia, xm, typext, x, 0.0, t, w); /* :77 */
+    if (st) goto done;
+    for (size_t i = 0; i < n; ++i) r0[i] = r0[i] - b[i];        /* :82 */
+    nr0 = sqrt(pdots(dot_mode, npoin, r0, r0, nb, nt));          /* :83-84 */
+    prec = nr0 / nbn;
+    if (prec <= eps) goto fin;                                   /* :87 */
+    for (;;) {
+        m = m + 1;                                               /* :91 */
+        int k = krylov;
+        double cc = -1.0 / nr0;
+        for (size_t i = 0; i < n; ++i) V(0)[i] = cc * r0[i];     /* :95 */
+        for (int j = 1; j <= k - 1; ++j) {                       /* :97-143 */
+            st = op_matvec(M, "X=AY    ", npoin, AV(j - 1), da, typdia, xm, typext, V(j - 1),
+                           0.0, t, w);
+            if (st) goto done;
+            memcpy(V(j), AV(j - 1), sizeof(double) * n);
+            for (int i = 1; i <= j; ++i) {
+                h[i - 1][j - 1] = pdots(dot_mode, npoin, V(j), V(i - 1), nb, nt);
+                double ch = -h[i - 1][j - 1];
+                for (size_t q = 0; q < n; ++q) V(j)[q] = V(j)[q] + ch * V(i - 1)[q];
+            }
+            h[j][j - 1] = sqrt(pdots(dot_mode, npoin, V(j), V(j), nb, nt));
+            if (h[j][j - 1] < 1.0e-20) { k = j; break; }
+            double ci = 1.0 / h[j][j - 1];
+            for (size_t q = 0; q < n; ++q) V(j)[q] = ci * V(j)[q];
+        }
+        st = op_matvec(M, "X=AY    ", npoin, AV(k - 1), da, typdia, xm, typext, V(k - 1), 0.0,
+                       t, w);                                    /* :151 */
+        if (st) goto done;
+        h[k][k - 1] = pdots(dot_mode, npoin, AV(k - 1), AV(k - 1), nb, nt);     /* :153 */
+        for (int i = 1; i <= k; ++i) {
+            h[i - 1][k - 1] = pdots(dot_mode, npoin, AV(k - 1), V(i - 1), nb, nt);
+            h[k][k - 1] = h[k][k - 1] - h[i - 1][k - 1] * h[i - 1][k - 1];
+        }
+        h[k][k - 1] = sqrt(h[k][k - 1] > 0.0 ? h[k][k - 1] : 0.0);              /* :158 */
+        e[0] = nr0;
+        for (int i = 1; i <= k; ++i) {                           /* :160-183 */
+            for (int j = 1; j <= i - 1; ++j) {
+                double zz = c[j - 1] * h[j - 1][i - 1] + sn[j - 1] * h[j][i - 1];
+                h[j][i - 1] = -sn[j - 1] * h[j - 1][i - 1] + c[j - 1] * h[j][i - 1];
+                h[j - 1][i - 1] = zz;
+            }
+            double rr = sqrt(h[i - 1][i - 1] * h[i - 1][i - 1] + h[i][i - 1] * h[i][i - 1]);
+            if (fabs(rr) < 1.0e-6) goto fin;
+            c[i - 1] = h[i - 1][i - 1] / rr;
+            sn[i - 1] = h[i][i - 1] / rr;
+            h[i - 1][i - 1] = rr;
+            e[i] = -sn[i - 1] * e[i - 1];
+            e[i - 1] = c[i - 1] * e[i - 1];
+        }
+        e[k - 1] = e[k - 1] / h[k - 1][k - 1];                   /* :184-190 */
+        for (int j = k - 1; j >= 1; --j) {
+            for (int l = j + 1; l <= k; ++l) e[j - 1] = e[j - 1] - h[j - 1][l - 1] * e[l - 1];
+            e[j - 1] = e[j - 1] / h[j - 1][j - 1];
+        }
+        for (int l = 1; l <= k; ++l) {                           /* :191-194 */
+            for (size_t q = 0; q < n; ++q) x[q] = x[q] + e[l - 1] * V(l - 1)[q];
+            for (size_t q = 0; q < n; ++q) r0[q] = r0[q] + e[l - 1] * AV(l - 1)[q];
+        }
+        nr0 = fabs(e[k]);                                        /* :195 */
+        prec = nr0 / nbn;
+        if (!(prec >= eps && m < nitmax)) break;                 /* :197 */
+    }
+#undef V
+#undef AV
+fin:
+    /* the reference reports success whenever M < NITMAX (:199-214), also
+     * after the R < 1e-6 failure message; at M = NITMAX it reports the
+     * iteration limit */
+    st = m < nitmax ? ORC_OK : m;
+    if (nit_out) *nit_out = m;
+    if (relres_out) *relres_out = prec;
+    if (relat_out) *relat_out = relat;
+done:
+    free(r0); free(t); free(w); free(v); free(av);
+    return st;
+}
+
 /* solve.f:387-649 for SLV=1 (GRACJG, solve.f:555-558) and SLV=3 (EQUNOR,
  * :565-570) on a single (non-block) matrix:
  * PRECON 0 -> 1; diagonal change of variables when PRECON is divisible by
@@ -807,10 +921,10 @@ done:
  * exactly as the reference modifies them. */
 static int solve_impl(const opmesh *M, int npoin, double *x, double *b, double *dm,
                       char *typdia, double *xm, char typext, int slv, int precon,
-                      int nitmax, double eps, int dot_mode, int nb, int nt, int *nit_out,
-                      double *relres_out, int *relat_out)
+                      int nitmax, double eps, int krylov, int dot_mode, int nb, int nt,
+                      int *nit_out, double *relres_out, int *relat_out)
 {
-    if (slv != 1 && slv != 3) return ORC_ERR_UNSUPPORTED;
+    if (slv != 1 && slv != 3 && slv != 7) return ORC_ERR_UNSUPPORTED;
     if (precon == 0) precon = 1;
     if (precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 ||
         precon % 17 == 0)
@@ -822,7 +936,10 @@ static int solve_impl(const opmesh *M, int npoin, double *x, double *b, double *
         int st = precd1_impl(M, npoin, precon, x, dm, typdia, xm, typext, b, d);
         if (st) { free(d); return st; }
     }
-    int st = slv == 3
+    int st = slv == 7
+                 ? gmres_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, krylov,
+                              dot_mode, nb, nt, nit_out, relres_out, relat_out)
+             : slv == 3
                  ? equnor_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
                                nb, nt, nit_out, relres_out, relat_out)
                  : gracjg_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
@@ -839,11 +956,11 @@ int orc_solve(int npoin, int nelem, const int *ik0, const int *ik1,
               char *typdia, double *xm, int ld, char typext, int slv,
               int precon, int nitmax, double eps, int dot_mode,
               int nb, int nt, int *nit_out, double *relres_out,
-              int *relat_out)
+              int *relat_out, int krylov)
 {
     opmesh M = {1, nelem, ld, ik0, ik1, ik2, 0, NULL, NULL};
     return solve_impl(&M, npoin, x, b, dm, typdia, xm, typext, slv, precon, nitmax, eps,
-                      dot_mode, nb, nt, nit_out, relres_out, relat_out);
+                      krylov, dot_mode, nb, nt, nit_out, relres_out, relat_out);
 }
 
 /* SOLVE (SLV=1) on a segment-storage matrix (STO=3): the same algorithm with
@@ -851,11 +968,11 @@ int orc_solve(int npoin, int nelem, const int *ik0, const int *ik1,
 int orc_solve_seg(int npoin, int nseg, const int *g1, const int *g2, double *x, double *b,
                   double *dm, char *typdia, double *xa, char typext, int slv, int precon,
                   int nitmax, double eps, int dot_mode, int nb, int nt, int *nit_out,
-                  double *relres_out, int *relat_out)
+                  double *relres_out, int *relat_out, int krylov)
 {
     opmesh M = {3, 0, 0, NULL, NULL, NULL, nseg, g1, g2};
     return solve_impl(&M, npoin, x, b, dm, typdia, xa, typext, slv, precon, nitmax, eps,
-                      dot_mode, nb, nt, nit_out, relres_out, relat_out);
+                      krylov, dot_mode, nb, nt, nit_out, relres_out, relat_out);
 }
 
 /* ------------------------------------------------------------------ */

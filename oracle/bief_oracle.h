@@ -96,7 +96,7 @@ int orc_solve(int npoin, int nelem, const int *ik0, const int *ik1,
               char *typdia, double *xm, int ld, char typext, int slv,
               int precon, int nitmax, double eps, int dot_mode,
               int nblocks, int nthreads, int *nit_out, double *relres_out,
-              int *relat_out);
+              int *relat_out, int krylov);
 
 int orc_solve_mixed(int npoin, int nelem, const int *ik0, const int *ik1,
                     const int *ik2, double *x, const double *b,
@@ -137,7 +137,7 @@ int orc_mvseg(const char *op, int npoin, int nseg, const int *g1, const int *g2,
 int orc_solve_seg(int npoin, int nseg, const int *g1, const int *g2, double *x, double *b,
                   double *dm, char *typdia, double *xa, char typext, int slv, int precon,
                   int nitmax, double eps, int dot_mode, int nb, int nt, int *nit_out,
-                  double *relres_out, int *relat_out);
+                  double *relres_out, int *relat_out, int krylov);
 
 int orc_solve_mixed_seg(int npoin, int nseg, const int *g1, const int *g2, double *x,
                         const double *b, const double *dm_in, char typdia_in,
