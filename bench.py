@@ -300,7 +300,7 @@ def run_batch(args, ws, rank, local):
     bs.assemble_wave(xs, ys, coefs)
     b = bs.gather(bvs)
     x = torch.zeros_like(b)
-    npt = bs.autotune(b, inner_tol=args.inner_tol, outer_tol=args.eps)
+    npt, tpb = bs.autotune(b, inner_tol=args.inner_tol, outer_tol=args.eps)
     flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     clean = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     times, kern = [], []
@@ -311,7 +311,8 @@ def run_batch(args, ws, rank, local):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        r = bs.solve_mixed(x, b, inner_tol=args.inner_tol, outer_tol=args.eps, nodes_per_thread=npt)
+        r = bs.solve_mixed(x, b, inner_tol=args.inner_tol, outer_tol=args.eps, nodes_per_thread=npt,
+                           threads_per_block=tpb)
         e1.record()
         e1.synchronize()
         if s >= args.warmup:
@@ -331,7 +332,10 @@ def run_batch(args, ws, rank, local):
                 "config": {"workload": "256 meshes, 2,000-200,000 nodes (log-uniform), one "
                                        "persistent launch per rank",
                            "nodes_this_rank": int(bs.total_nodes),
-                           "nodes_per_thread": int(npt), "parallelism": f"shards x{ws}"},
+                           "nodes_per_thread": int(npt), "threads_per_block": int(tpb),
+                           "autotune_ms_per_iteration": {f"npt{k[0]}_t{k[1]}": round(v, 4)
+                                                         for k, v in bs.tune_table.items()},
+                           "parallelism": f"shards x{ws}"},
                 "converged": ok, "kernel_ms": sum(kern) / len(kern),
                 "iterations_rank0": {"p50": float(np.percentile(inner, 50)),
                                      "p99": float(np.percentile(inner, 99)),

@@ -178,8 +178,10 @@ int bief_wave_coef_grad_dev(bief_handle *h, const double *xc,
  * i owning nodes [node_off[i], node_off[i]+npoin_inst[i]) (node_off[i] a
  * multiple of 32, no element coupling two instances).  All instances run
  * the bief_solve_mixed algorithm in ONE persistent launch, each with its own
- * scalars and convergence mask; nodes_per_thread (1, 2, 4, 8) sets the work
- * tile (1024*nodes_per_thread nodes) and the per-instance dot order.  x, b:
+ * scalars and convergence mask; nodes_per_thread (1, 2, 4, 8) and
+ * threads_per_block (256, 512 or 1024; 0 means 1024) set the work tile
+ * (threads_per_block*nodes_per_thread nodes), the block shape and the
+ * per-instance dot order.  x, b:
  * device arrays over the whole mesh; per-instance results in host arrays
  * status (0 / inner iterations when not converged / < 0 error), outer_out,
  * inner_out, relres_out. */
@@ -187,7 +189,7 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
                                const int *npoin_inst, double *x, const double *b,
                                int precon, double inner_tol, double outer_tol,
                                int max_outer, int max_inner,
-                               int nodes_per_thread, int *status,
+                               int nodes_per_thread, int threads_per_block, int *status,
                                int *outer_out, int *inner_out,
                                double *relres_out, void *stream);
 

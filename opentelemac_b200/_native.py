@@ -85,8 +85,8 @@ def lib():
             "bief_kernel_launches": ([vp], ctypes.c_longlong),
             "bief_strerror": ([i], ctypes.c_char_p),
             "bief_solve_noalloc": ([i, i, i, vp, vp, vp, c, c, vp, vp, pcfg, pd, i, vp], i),
-            "bief_batch_solve_mixed_dev": ([vp, i, vp, vp, vp, vp, i, d, d, i, i, i, vp, vp, vp,
-                                            vp, vp], i),
+            "bief_batch_solve_mixed_dev": ([vp, i, vp, vp, vp, vp, i, d, d, i, i, i, i, vp, vp,
+                                            vp, vp, vp], i),
             "bief_set_segments": ([vp, i, i, vp], i),
             "bief_set_matrix_seg": ([vp, vp, vp, c, c], i),
             "bief_set_matrix_seg_dev": ([vp, vp, vp, c, c], i),

@@ -64,12 +64,16 @@ class BatchSolver:
 
     # -- solve
     def solve_mixed(self, x, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, max_outer=1000,
-                    max_inner=1000000, nodes_per_thread=None):
+                    max_inner=1000000, nodes_per_thread=None, threads_per_block=None):
         """x (in/out), b: device vectors over the whole mesh.  Returns a dict
-        of per-instance status, inner/outer counts, relres and kernel ms."""
+        of per-instance status, inner/outer counts, relres and kernel ms.
+        Without nodes_per_thread the work tile and block shape come from
+        the autotuner."""
         import torch
         if nodes_per_thread is None:
-            nodes_per_thread = self.autotune(b, precon, inner_tol, outer_tol)
+            nodes_per_thread, threads_per_block = self.autotune(b, precon, inner_tol, outer_tol)
+        if threads_per_block is None:
+            threads_per_block = 1024
         ni = self.ninst
         st = np.zeros(ni, dtype=np.int32)
         outer = np.zeros(ni, dtype=np.int32)
@@ -80,29 +84,35 @@ class BatchSolver:
         rc = _native.lib().bief_batch_solve_mixed_dev(
             self.mesh.handle, ni, vp(self.node_off), vp(self.npoin),
             ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(b.data_ptr()), precon, inner_tol,
-            outer_tol, max_outer, max_inner, nodes_per_thread, vp(st), vp(outer), vp(inner),
-            vp(relres), s)
+            outer_tol, max_outer, max_inner, nodes_per_thread, threads_per_block, vp(st),
+            vp(outer), vp(inner), vp(relres), s)
         if rc < 0:
             raise bief.BiefError(rc, "batched solve")
         self.last = dict(status=st, outer=outer, inner=inner, relres=relres,
-                         kernel_ms=self.mesh.last_timing()[0], nodes_per_thread=nodes_per_thread)
+                         kernel_ms=self.mesh.last_timing()[0], nodes_per_thread=nodes_per_thread,
+                         threads_per_block=threads_per_block)
         return self.last
 
-    def autotune(self, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, candidates=(1, 2, 4),
-                 probe_inner=30):
-        """Pick nodes-per-thread by timing `probe_inner` inner iterations of
-        every instance with each candidate (kernel time per inner
-        iteration, summed over instances)."""
+    def autotune(self, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, candidates=(1, 2, 4, 8),
+                 block_shapes=(256, 512, 1024), probe_inner=30):
+        """Pick (nodes per thread, threads per block) by timing `probe_inner`
+        inner iterations of every instance with each pair (kernel time per
+        inner iteration of the longest-running instance).  The pair is kept
+        for later solves; self.tune_table holds every candidate's time."""
         import torch
         if self.tuned_npt is not None:
             return self.tuned_npt
         best, best_t = None, None
-        for npt in candidates:
-            x = torch.zeros_like(b)
-            r = self.solve_mixed(x, b, precon, inner_tol, outer_tol, 1000, probe_inner, npt)
-            per = r["kernel_ms"] / max(int(r["inner"].max()), 1)
-            if best_t is None or per < best_t:
-                best, best_t = npt, per
+        self.tune_table = {}
+        for threads in block_shapes:
+            for npt in candidates:
+                x = torch.zeros_like(b)
+                r = self.solve_mixed(x, b, precon, inner_tol, outer_tol, 1000, probe_inner, npt,
+                                     threads)
+                per = r["kernel_ms"] / max(int(r["inner"].max()), 1)
+                self.tune_table[(npt, threads)] = per
+                if best_t is None or per < best_t:
+                    best, best_t = (npt, threads), per
         self.tuned_npt = best
         return best
 

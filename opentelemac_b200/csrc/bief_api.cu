@@ -1016,7 +1016,8 @@ int bief_wave_coef_grad_dev(bief_handle *h, const double *xc, const double *yc,
 int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
                                const int *npoin_inst, double *x, const double *b, int precon,
                                double inner_tol, double outer_tol, int max_outer, int max_inner,
-                               int nodes_per_thread, int *status, int *outer_out,
+                               int nodes_per_thread, int threads_per_block, int *status,
+                               int *outer_out,
                                int *inner_out, double *relres_out, void *stream) {
   if (!h || !node_off || !npoin_inst || !x || !b || !status || !outer_out || !inner_out ||
       !relres_out || max_inner < 1 || max_outer < 0)
@@ -1025,6 +1026,9 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
   if (nodes_per_thread != 1 && nodes_per_thread != 2 && nodes_per_thread != 4 &&
       nodes_per_thread != 8)
     return BIEF_ERR_ARGS;
+  if (threads_per_block == 0) threads_per_block = CG_THREADS;
+  if (threads_per_block != 256 && threads_per_block != 512 && threads_per_block != 1024)
+    return BIEF_ERR_ARGS;
   if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
   if (h->typext != 'S' || h->sto != 1) return BIEF_ERR_UNSUPPORTED;
   if (h->max_nnb > MAX_NEIGHBOURS) return BIEF_ERR_SIZE;
@@ -1032,7 +1036,7 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
   if (precon < 0 || precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 || precon % 17 == 0)
     return BIEF_ERR_UNSUPPORTED;
   // instance ranges: ascending, disjoint, 32-aligned starts, inside the mesh
-  const int C = CG_THREADS * nodes_per_thread;
+  const int C = threads_per_block * nodes_per_thread;
   std::vector<int> meta(3 * BATCH_MAX_INST + 1, 0);
   int t0 = 0;
   for (int i = 0; i < ninst; ++i) {
@@ -1101,7 +1105,7 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
   void *k = td == DIA_Q ? (void *)k_batch<DIA_Q>
             : td == DIA_I ? (void *)k_batch<DIA_I> : (void *)k_batch<DIA_0>;
   int bps = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, CG_THREADS, 0));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads_per_block, 0));
   if (bps < 1) return BIEF_ERR_CUDA;
   const int G = std::max(1, std::min(bps * h->nsm, ntiles));
   BatchP P;
@@ -1135,7 +1139,7 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
   CK(cudaEventRecord(h->ev[0], s));
   void *args[] = {&P};
-  CK(cudaLaunchCooperativeKernel(k, dim3(G), dim3(CG_THREADS), args, 0, s));
+  CK(cudaLaunchCooperativeKernel(k, dim3(G), dim3(threads_per_block), args, 0, s));
   h->launches++;
   CK(cudaEventRecord(h->ev[1], s));
   CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));

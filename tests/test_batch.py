@@ -22,8 +22,8 @@ def _instances(sizes, seed0=100):
     return out
 
 
-@pytest.mark.parametrize("npt", [1, 2])
-def test_batch_bitexact_per_instance(oracle_mod, npt):
+@pytest.mark.parametrize("npt,threads", [(1, 1024), (2, 1024), (4, 256), (2, 512)])
+def test_batch_bitexact_per_instance(oracle_mod, npt, threads):
     from opentelemac_b200.batch import BatchSolver
     inst = _instances([7, 15, 23, 40, 57, 33])
     inst[3]["b"] = np.zeros_like(inst[3]["b"])               # b = 0: x = 0 at once
@@ -31,11 +31,13 @@ def test_batch_bitexact_per_instance(oracle_mod, npt):
     bs.assemble_wave([p["x"] for p in inst], [p["y"] for p in inst], [p["coef"] for p in inst])
     b = bs.gather([p["b"] for p in inst])
     x = bs.gather([np.zeros(p["x"].size) for p in inst])
-    r = bs.solve_mixed(x, b, inner_tol=1e-4, outer_tol=1e-9, nodes_per_thread=npt)
+    r = bs.solve_mixed(x, b, inner_tol=1e-4, outer_tol=1e-9, nodes_per_thread=npt,
+                       threads_per_block=threads)
     xs = [v.cpu().numpy() for v in bs.scatter(x)]
     for k, p in enumerate(inst):
         ref = oracle_mod.solve_mixed_batch(p["ik"], p["dm"], "Q", p["xm"], p["b"], precon=2,
-                                           inner_tol=1e-4, outer_tol=1e-9, npt=npt)
+                                           inner_tol=1e-4, outer_tol=1e-9, npt=npt,
+                                           nthreads=threads)
         assert r["status"][k] == ref["status"] == 0
         assert (r["inner"][k], r["outer"][k]) == (ref["inner"], ref["outer"]), k
         assert r["relres"][k] == ref["relres"]
