@@ -257,6 +257,27 @@ __device__ __forceinline__ T ebe_row(int i, T acc, const int *__restrict__ ptr,
 // in order of first appearance among the entries, the binary32 assembled
 // coefficient c_ij; product in difference form s_i y_i + sum c_ij (y_j-y_i).
 // ---------------------------------------------------------------------------
+// Gather entries of one row processed per batch: their index and
+// coefficient loads are all issued before the first of their node loads, so
+// that a thread keeps SLOT_B dependent load chains in flight (the solvers
+// are latency bound: 32 warps per SM at 64 registers).  The additions keep
+// their order, so the bits do not depend on the batch sizes.  Measured on
+// B200, per iteration at 4.0M / 1.0M nodes: binary64 GRACJG 183 / 51 us with
+// 4-entry batches against 207 / 56 us unbatched; binary32 inner CG 103 us
+// with 3-slot batches against 120 us (interior P1 nodes have 6 neighbours).
+#ifndef BIEF_SLOT_BATCH
+#define BIEF_SLOT_BATCH 4
+#endif
+#ifndef BIEF_SLOT_BATCH32
+#define BIEF_SLOT_BATCH32 3
+#endif
+#ifndef BIEF_SLOT_PRED
+#define BIEF_SLOT_PRED 0
+#endif
+constexpr int SLOT_B = BIEF_SLOT_BATCH;      // binary64 records
+constexpr int SLOT_B32 = BIEF_SLOT_BATCH32;  // binary32 slots
+constexpr bool SLOT_PRED = BIEF_SLOT_PRED;   // last batch predicated instead of serial
+
 struct Sell {
   const int *meta;        // per node: gather entries | neighbours << 16
   const int *rec_off;     // per slice: first record
@@ -269,25 +290,44 @@ struct Sell {
   const double *sg_c;     // segment storage: per slot, binary64 XA1/XA2
 };
 
-template <class V>
-__device__ __forceinline__ double rec_row(int i, double acc, const Sell &S, V vec) {
-  const int deg = __ldg(S.meta + i) & 0xffff;
-  const int base = __ldg(S.rec_off + (i >> 5)) + (i & 31);
-#pragma unroll 2
-  for (int m = 0; m < deg; ++m) {
-    const double2 c = __ldg(S.rec_c + base + 32 * m);
-    const int2 v = __ldg(S.rec_idx + base + 32 * m);
-    acc = add(acc, add(mul(c.x, vec(v.x)), mul(c.y, vec(v.y))));
-  }
-  return acc;
-}
-
 // Two rows at once (nodes i0 and, if has1, i1): independent load chains
 // interleaved so that twice as many loads are in flight per thread.  Each
 // row's additions keep their own order, so the bits equal rec_row's.
 template <class V>
 __device__ __forceinline__ void rec_row2(int i0, int i1, bool has1, double &a0, double &a1,
                                          const Sell &S, V vec) {
+  if constexpr (SLOT_B > 1) {
+    if (!has1) {
+      const int d0 = __ldg(S.meta + i0) & 0xffff;
+      const int b0 = __ldg(S.rec_off + (i0 >> 5)) + (i0 & 31);
+      int m = 0;
+      for (; SLOT_PRED ? m < d0 : m + SLOT_B <= d0; m += SLOT_B) {
+        double2 c[SLOT_B];
+        int2 v[SLOT_B];
+        double ya[SLOT_B], yb[SLOT_B];
+#pragma unroll
+        for (int q = 0; q < SLOT_B; ++q) {
+          const bool ok = !SLOT_PRED || m + q < d0;
+          c[q] = ok ? __ldg(S.rec_c + b0 + 32 * (m + q)) : make_double2(0.0, 0.0);
+          v[q] = ok ? __ldg(S.rec_idx + b0 + 32 * (m + q)) : make_int2(i0, i0);
+        }
+#pragma unroll
+        for (int q = 0; q < SLOT_B; ++q) {
+          ya[q] = vec(v[q].x);
+          yb[q] = vec(v[q].y);
+        }
+#pragma unroll
+        for (int q = 0; q < SLOT_B; ++q)
+          if (!SLOT_PRED || m + q < d0) a0 = add(a0, add(mul(c[q].x, ya[q]), mul(c[q].y, yb[q])));
+      }
+      for (; m < d0; ++m) {
+        const double2 c = __ldg(S.rec_c + b0 + 32 * m);
+        const int2 v = __ldg(S.rec_idx + b0 + 32 * m);
+        a0 = add(a0, add(mul(c.x, vec(v.x)), mul(c.y, vec(v.y))));
+      }
+      return;
+    }
+  }
   const int d0 = __ldg(S.meta + i0) & 0xffff;
   const int d1 = has1 ? (__ldg(S.meta + i1) & 0xffff) : 0;
   const int b0 = __ldg(S.rec_off + (i0 >> 5)) + (i0 & 31);
@@ -340,6 +380,36 @@ __device__ __forceinline__ void op_row2(int i0, int i1, bool has1, double &a0, d
 template <class V>
 __device__ __forceinline__ void seg_row2(int i0, int i1, bool has1, float y0, float y1,
                                          float &a0, float &a1, const Sell &S, V vec) {
+  if constexpr (SLOT_B32 > 1) {
+    if (!has1) {
+      const int n0 = __ldg(S.meta + i0) >> 16;
+      const int b0 = __ldg(S.seg_off + (i0 >> 5)) + (i0 & 31);
+      a0 = mul(y0, __ldg(S.s32 + i0));
+      a1 = 0.0f;
+      int m = 0;
+      for (; SLOT_PRED ? m < n0 : m + SLOT_B32 <= n0; m += SLOT_B32) {
+        int j[SLOT_B32];
+        float c[SLOT_B32], v[SLOT_B32];
+#pragma unroll
+        for (int q = 0; q < SLOT_B32; ++q) {
+          const bool ok = !SLOT_PRED || m + q < n0;
+          j[q] = ok ? __ldg(S.seg_col + b0 + 32 * (m + q)) : i0;
+          c[q] = ok ? __ldg(S.seg_c + b0 + 32 * (m + q)) : 0.0f;
+        }
+#pragma unroll
+        for (int q = 0; q < SLOT_B32; ++q) v[q] = vec(j[q]);
+#pragma unroll
+        for (int q = 0; q < SLOT_B32; ++q)
+          if (!SLOT_PRED || m + q < n0) a0 = add(a0, mul(c[q], sub(v[q], y0)));
+      }
+      for (; m < n0; ++m) {
+        const int jj = __ldg(S.seg_col + b0 + 32 * m);
+        const float cc = __ldg(S.seg_c + b0 + 32 * m);
+        a0 = add(a0, mul(cc, sub(vec(jj), y0)));
+      }
+      return;
+    }
+  }
   const int n0 = __ldg(S.meta + i0) >> 16;
   const int n1 = has1 ? (__ldg(S.meta + i1) >> 16) : 0;
   const int b0 = __ldg(S.seg_off + (i0 >> 5)) + (i0 & 31);
@@ -361,17 +431,19 @@ __device__ __forceinline__ void seg_row2(int i0, int i1, bool has1, float y0, fl
   }
 }
 
+// Single-row forms (the batched solver): the same additions as the
+// two-row functions.
+template <class V>
+__device__ __forceinline__ double rec_row(int i, double acc, const Sell &S, V vec) {
+  double unused = 0.0;
+  rec_row2(i, i, false, acc, unused, S, vec);
+  return acc;
+}
+
 template <class V>
 __device__ __forceinline__ float seg_row(int i, float yi, const Sell &S, V vec) {
-  const int nnb = __ldg(S.meta + i) >> 16;
-  const int base = __ldg(S.seg_off + (i >> 5)) + (i & 31);
-  float acc = mul(yi, __ldg(S.s32 + i));
-#pragma unroll 2
-  for (int m = 0; m < nnb; ++m) {
-    const int j = __ldg(S.seg_col + base + 32 * m);
-    const float c = __ldg(S.seg_c + base + 32 * m);
-    acc = add(acc, mul(c, sub(vec(j), yi)));
-  }
+  float acc, unused;
+  seg_row2(i, i, false, yi, 0.0f, acc, unused, S, vec);
   return acc;
 }
 
