@@ -355,6 +355,29 @@ __device__ __forceinline__ void rec_row2(int i0, int i1, bool has1, double &a0, 
 template <class V>
 __device__ __forceinline__ void sgr_row2(int i0, int i1, bool has1, double &a0, double &a1,
                                          const Sell &S, V vec) {
+  if constexpr (SLOT_B > 1) {
+    if (!has1) {
+      const int d0 = __ldg(S.meta + i0) & 0xffff;
+      const int b0 = __ldg(S.rec_off + (i0 >> 5)) + (i0 & 31);
+      int m = 0;
+      for (; m + SLOT_B <= d0; m += SLOT_B) {
+        double c[SLOT_B], v[SLOT_B];
+        int j[SLOT_B];
+#pragma unroll
+        for (int q = 0; q < SLOT_B; ++q) {
+          c[q] = __ldg(S.sg_c + b0 + 32 * (m + q));
+          j[q] = __ldg(S.seg_col + b0 + 32 * (m + q));
+        }
+#pragma unroll
+        for (int q = 0; q < SLOT_B; ++q) v[q] = vec(j[q]);
+#pragma unroll
+        for (int q = 0; q < SLOT_B; ++q) a0 = add(a0, mul(c[q], v[q]));
+      }
+      for (; m < d0; ++m)
+        a0 = add(a0, mul(__ldg(S.sg_c + b0 + 32 * m), vec(__ldg(S.seg_col + b0 + 32 * m))));
+      return;
+    }
+  }
   const int d0 = __ldg(S.meta + i0) & 0xffff;
   const int d1 = has1 ? (__ldg(S.meta + i1) & 0xffff) : 0;
   const int b0 = __ldg(S.rec_off + (i0 >> 5)) + (i0 & 31);
