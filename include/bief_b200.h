@@ -193,6 +193,14 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
                                int *outer_out, int *inner_out,
                                double *relres_out, void *stream);
 
+/* Self-test of the device-side bounded waits (no reference counterpart):
+ * runs one block into a grid barrier that can never complete and checks that
+ * its wait gives up after timeout_ns (1e6..5e9) with a recorded timeout.
+ * Returns BIEF_ERR_DEVICE_TIMEOUT when the wait ended as designed (the
+ * device stays usable), another status otherwise.  The solvers use the same
+ * wait with a 2 s limit. */
+int bief_selftest_timeout(int device, long long timeout_ns);
+
 /* Shape of the device dot-product tree: number of blocks and threads per
  * block of the persistent solver kernel. */
 int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads);

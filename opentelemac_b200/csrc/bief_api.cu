@@ -1153,6 +1153,24 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
   return BIEF_OK;
 }
 
+int bief_selftest_timeout(int device, long long timeout_ns) {
+  if (timeout_ns < 1000000LL || timeout_ns > 5000000000LL) return BIEF_ERR_ARGS;
+  DevGuard g(device);
+  Ctl *ctl = nullptr;
+  CK(cudaMalloc((void **)&ctl, sizeof(Ctl)));
+  Ctl host;
+  cudaError_t e = cudaMemset(ctl, 0, sizeof(Ctl));
+  if (e == cudaSuccess) {
+    k_selftest_wait<<<1, 32>>>(ctl, timeout_ns);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(&host, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost);
+  cudaFree(ctl);
+  if (e != cudaSuccess) return cuda_fail(e, "selftest", __LINE__);
+  return host.status == ST_TIMEOUT ? BIEF_ERR_DEVICE_TIMEOUT : BIEF_ERR_CUDA;
+}
+
 int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads) {
   if (!h) return BIEF_ERR_ARGS;
   if (nblocks) *nblocks = h->G;

@@ -64,6 +64,12 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+// Back-off between polls of a grid barrier's arrival counter (ns).
+#ifndef BIEF_SPIN_NS
+#define BIEF_SPIN_NS 20
+#endif
+constexpr unsigned SPIN_NS = BIEF_SPIN_NS;
+
 // Control block of one persistent solve (device memory, zeroed per launch).
 struct Ctl {
   unsigned long long arrivals;  // grid-barrier arrivals, never reset in a launch
@@ -118,7 +124,7 @@ __device__ __noinline__ bool grid_reduce(Ctl *ctl, double *part, long long timeo
         atomicExch(&ctl->status, (int)ST_TIMEOUT);
         break;
       }
-      __nanosleep(20);
+      if (SPIN_NS > 0) __nanosleep(SPIN_NS);
     }
   }
   __syncthreads();
@@ -172,7 +178,7 @@ static __device__ __noinline__ bool grid_barrier(Ctl *ctl, long long timeout_ns,
         atomicExch(&ctl->status, (int)ST_TIMEOUT);
         break;
       }
-      __nanosleep(20);
+      if (SPIN_NS > 0) __nanosleep(SPIN_NS);
     }
   }
   __syncthreads();

@@ -210,6 +210,14 @@ __global__ void k_assex3(int nseg, int nelem, int ld, const int2 *__restrict__ s
   }
 }
 
+// Self-test of the bounded waits: one block enters a grid barrier one
+// arrival short (as if another block never came), so its wait must give up
+// after timeout_ns and record ST_TIMEOUT instead of hanging.
+__global__ void k_selftest_wait(Ctl *ctl, long long timeout_ns) {
+  int nbar = 1;
+  grid_barrier(ctl, timeout_ns, nbar);
+}
+
 // ---------------------------------------------------------------------------
 // PRECD1 change of variables, DIADON=.FALSE., PREXSM=.TRUE.
 // Node part: D = A%D; [|D|]; D = SQRT(D); X = X*D; D = 1/D guarded
@@ -661,7 +669,7 @@ __device__ __noinline__ bool grid_reduce_n(Ctl *ctl, double *part, long long tim
         atomicExch(&ctl->status, (int)ST_TIMEOUT);
         break;
       }
-      __nanosleep(20);
+      if (SPIN_NS > 0) __nanosleep(SPIN_NS);
     }
   }
   __syncthreads();
