@@ -193,6 +193,21 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
                                int *outer_out, int *inner_out,
                                double *relres_out, void *stream);
 
+/* DIRI01 (diri01.f:90-130 with DIRAUX, diraux.f:70-85) for Dirichlet values
+ * on the NPTFR boundary points: nbor = MESH%NBOR (1-based), limdir = LIMDIR,
+ * points with limdir[k] == kdir get the value fbor[k].  SM (npoin) becomes
+ * SM - A W1 (W1 = the Dirichlet values) with SM = D*FBOR and F = FBOR at the
+ * Dirichlet points; with maskpt (npoin, or NULL) SM and F are masked; the
+ * stored matrix keeps its diagonal and loses the off-diagonal terms of the
+ * Dirichlet rows and columns (OM 'M=DMD'), in either storage.  Host arrays;
+ * the _dev variant takes device arrays and runs on `stream`. */
+int bief_diri01(bief_handle *h, int nptfr, const int *nbor, const int *limdir,
+                int kdir, const double *fbor, double *sm, double *f,
+                const double *maskpt);
+int bief_diri01_dev(bief_handle *h, int nptfr, const int *nbor,
+                    const int *limdir, int kdir, const double *fbor, double *sm,
+                    double *f, const double *maskpt, void *stream);
+
 /* Self-test of the device-side bounded waits (no reference counterpart):
  * runs one block into a grid barrier that can never complete and checks that
  * its wait gives up after timeout_ns (1e6..5e9) with a recorded timeout.

@@ -32,7 +32,7 @@ EXPORTS = [
     "bief_last_timing", "bief_kernel_launches", "bief_strerror", "bief_solve_noalloc",
     "bief_batch_solve_mixed_dev", "bief_set_segments", "bief_set_matrix_seg",
     "bief_set_matrix_seg_dev", "bief_ebe_to_seg", "bief_matrix_storage",
-    "bief_selftest_timeout",
+    "bief_selftest_timeout", "bief_diri01", "bief_diri01_dev",
 ]
 
 
@@ -94,6 +94,8 @@ def lib():
             "bief_ebe_to_seg": ([vp, vp], i),
             "bief_matrix_storage": ([vp], i),
             "bief_selftest_timeout": ([i, ctypes.c_longlong], i),
+            "bief_diri01": ([vp, i, vp, vp, i, vp, vp, vp, vp], i),
+            "bief_diri01_dev": ([vp, i, vp, vp, i, vp, vp, vp, vp, vp], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

@@ -253,6 +253,34 @@ def matvec(op, x, A, y, c=0.0):
     return x
 
 
+def diri01(A, nbor, limdir, kdir, fbor, sm, f, maskpt=None):
+    """DIRI01 for Dirichlet values on boundary points: nbor is MESH%NBOR
+    (1-based), points with limdir == kdir take fbor.  sm and f (and the
+    stored matrix) are modified in place; numpy arrays (host path) or torch
+    CUDA tensors (device path)."""
+    L = _native.lib()
+    if _is_torch(sm):
+        import torch
+        dev = sm.device
+        nb = torch.as_tensor(np.ascontiguousarray(nbor, dtype=np.int32), device=dev)
+        ld = torch.as_tensor(np.ascontiguousarray(limdir, dtype=np.int32), device=dev)
+        fb = torch.as_tensor(fbor, dtype=torch.float64, device=dev).contiguous()
+        st = L.bief_diri01_dev(A.mesh.handle, int(nb.numel()), _ptr(nb), _ptr(ld), int(kdir),
+                               _ptr(fb), _ptr(sm), _ptr(f),
+                               None if maskpt is None else _ptr(maskpt), _stream(sm))
+    else:
+        _host_vec(sm, A.mesh.npoin)
+        _host_vec(f, A.mesh.npoin)
+        nb = np.ascontiguousarray(nbor, dtype=np.int32)
+        ld = np.ascontiguousarray(limdir, dtype=np.int32)
+        fb = np.ascontiguousarray(fbor, dtype=np.float64)
+        mk = None if maskpt is None else np.ascontiguousarray(maskpt, dtype=np.float64)
+        st = L.bief_diri01(A.mesh.handle, int(nb.size), _ptr(nb), _ptr(ld), int(kdir), _ptr(fb),
+                           _ptr(sm), _ptr(f), None if mk is None else _ptr(mk))
+    _check(st, "DIRI01")
+    return sm, f
+
+
 def coef_grad(A, xc, yc, lam, x, grad):
     """grad[e] = -lam_e^T K_e x_e (device tensors)."""
     _check(_native.lib().bief_wave_coef_grad_dev(A.mesh.handle, _ptr(xc), _ptr(yc), _ptr(lam),

@@ -1153,6 +1153,89 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
   return BIEF_OK;
 }
 
+int bief_diri01_dev(bief_handle *h, int nptfr, const int *nbor, const int *limdir, int kdir,
+                    const double *fbor, double *sm, double *f, const double *maskpt,
+                    void *stream) {
+  if (!h || nptfr < 0 || (nptfr > 0 && (!nbor || !limdir || !fbor)) || !sm || !f)
+    return BIEF_ERR_ARGS;
+  if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
+  DevGuard g(h->dev);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int n = h->npoin, gn = grid_for(n, h->nsm), gb = grid_for(std::max(nptfr, 1), h->nsm);
+  double *w1 = h->d_t, *w2 = h->d_ad;
+  const int td = typdia_code(h->typdia);
+  const bool sym = h->typext != 'Q';
+  CK(cudaMemsetAsync(w1, 0, sizeof(double) * n, s));
+  if (nptfr > 0) k_diri_scatter<<<gb, 256, 0, s>>>(nptfr, nbor, limdir, kdir, fbor, w1);
+  // W2 = S W1 (MATVEC 'X=AY')
+  if (h->sto == 3) {
+    dispatch_mvseg(h, td, sym, false, h->typext != '0', h->d_xa, h->d_dm, w1, w2, OP_AY, 0.0, s);
+  } else {
+    const double *xm = h->d_xm;
+    if (h->typext == '0') {
+      CK(cudaMemsetAsync(h->d_xms, 0, sizeof(double) * 3 * h->nelem, s));
+      xm = h->d_xms;
+    }
+    dispatch_mv(h, td, sym, false, xm, h->d_dm, w1, w2, OP_AY, 0.0, s);
+  }
+  k_diri_nodes<<<gn, 256, 0, s>>>(n, sm, w2);
+  if (nptfr > 0) k_diri_aux<<<gb, 256, 0, s>>>(nptfr, nbor, limdir, kdir, fbor, h->d_dm, sm, w2, f);
+  if (maskpt) k_diri_mask<<<gn, 256, 0, s>>>(n, maskpt, sm, f, w2);
+  // OM 'M=DMD' with D = W2 on the off-diagonal terms only, in place
+  if (h->sto == 3) {
+    const int ncol = h->typext == 'Q' ? 2 : (h->typext == 'S' ? 1 : 0);
+    if (ncol)
+      k_precd1_segs<<<grid_for(h->nsg, h->nsm), 256, 0, s>>>(h->nsg, ncol, h->d_g1, h->d_g2, w2,
+                                                             h->d_xa, h->d_xa);
+  } else {
+    const int ndiag = h->typext == 'Q' ? 6 : (h->typext == 'S' ? 3 : 0);
+    if (ndiag)
+      k_precd1_elems<<<grid_for(h->nelem, h->nsm), 256, 0, s>>>(h->nelem, ndiag, h->d_ik, w2,
+                                                                h->d_xm, h->d_xm);
+  }
+  h->launches += 6;
+  CK(cudaGetLastError());
+  return BIEF_OK;
+}
+
+int bief_diri01(bief_handle *h, int nptfr, const int *nbor, const int *limdir, int kdir,
+                const double *fbor, double *sm, double *f, const double *maskpt) {
+  if (!h || nptfr < 0 || !sm || !f) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  const size_t nb = sizeof(double) * h->npoin;
+  int *d_i = nullptr;
+  double *d_f = nullptr, *d_m = nullptr;
+  int st = BIEF_OK;
+  if ((st = dalloc(&d_i, 2 * (size_t)nptfr)) || (st = dalloc(&d_f, (size_t)nptfr)) ||
+      (maskpt && (st = dalloc(&d_m, (size_t)h->npoin)))) {
+    cudaFree(d_i);
+    cudaFree(d_f);
+    return st;
+  }
+  cudaError_t e = cudaSuccess;
+  if (nptfr > 0) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_i, nbor, sizeof(int) * nptfr, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_i + nptfr, limdir, sizeof(int) * nptfr, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_f, fbor, sizeof(double) * nptfr, cudaMemcpyHostToDevice, h->stream);
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_x, sm, nb, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h->d_b, f, nb, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess && maskpt) e = cudaMemcpyAsync(d_m, maskpt, nb, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    st = bief_diri01_dev(h, nptfr, d_i, d_i + nptfr, kdir, d_f, h->d_x, h->d_b, d_m, h->stream);
+    if (st == BIEF_OK) {
+      e = cudaMemcpyAsync(sm, h->d_x, nb, cudaMemcpyDeviceToHost, h->stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(f, h->d_b, nb, cudaMemcpyDeviceToHost, h->stream);
+    }
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d_i);
+  cudaFree(d_f);
+  if (d_m) cudaFree(d_m);
+  if (e != cudaSuccess) return cuda_fail(e, "bief_diri01", __LINE__);
+  return st;
+}
+
 int bief_selftest_timeout(int device, long long timeout_ns) {
   if (timeout_ns < 1000000LL || timeout_ns > 5000000000LL) return BIEF_ERR_ARGS;
   DevGuard g(device);

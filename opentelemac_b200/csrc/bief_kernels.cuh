@@ -210,6 +210,45 @@ __global__ void k_assex3(int nseg, int nelem, int ld, const int2 *__restrict__ s
   }
 }
 
+// DIRI01 (diri01.f:90-130, DIRAUX diraux.f:70-85) on boundary numbering:
+// the Dirichlet values scattered to their nodes, SM corrected, the rows and
+// columns of the Dirichlet nodes masked.  nbor is 1-based (MESH%NBOR).
+__global__ void k_diri_scatter(int nptfr, const int *__restrict__ nbor,
+                               const int *__restrict__ limdir, int kdir,
+                               const double *__restrict__ fbor, double *w1) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nptfr; k += gridDim.x * blockDim.x)
+    if (limdir[k] == kdir) w1[nbor[k] - 1] = fbor[k];
+}
+
+// SM = SM - W2 ('X=X-Y'), then W2 = 1 ('X=C')
+__global__ void k_diri_nodes(int npoin, double *sm, double *w2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    sm[i] = sub(sm[i], w2[i]);
+    w2[i] = 1.0;
+  }
+}
+
+__global__ void k_diri_aux(int nptfr, const int *__restrict__ nbor, const int *__restrict__ limdir,
+                           int kdir, const double *__restrict__ fbor,
+                           const double *__restrict__ dm, double *sm, double *w2, double *f) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nptfr; k += gridDim.x * blockDim.x)
+    if (limdir[k] == kdir) {
+      const int n = nbor[k] - 1;
+      sm[n] = mul(dm[n], fbor[k]);
+      w2[n] = 0.0;
+      f[n] = fbor[k];
+    }
+}
+
+__global__ void k_diri_mask(int npoin, const double *__restrict__ mask, double *sm, double *f,
+                            double *w2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    sm[i] = mul(sm[i], mask[i]);
+    f[i] = mul(f[i], mask[i]);
+    w2[i] = mul(w2[i], mask[i]);
+  }
+}
+
 // Self-test of the bounded waits: one block enters a grid barrier one
 // arrival short (as if another block never came), so its wait must give up
 // after timeout_ns and record ST_TIMEOUT instead of hanging.

@@ -332,3 +332,54 @@ def solve_mixed_seg(g1, g2, dm, typdia, xa, b, x0=None, precon=2, inner_tol=0.1,
                                         ctypes.byref(outer), ctypes.byref(inner),
                                         ctypes.byref(relres))
     return dict(x=x, status=st, outer=outer.value, inner=inner.value, relres=relres.value)
+
+
+def diri01(ikle0, dm, typdia, xm, typext, nbor0, limdir, kdir, fbor, sm, f, maskpt=None):
+    """DIRI01 with boundary values (nbor0 0-based).  Returns (xm, sm, f) as
+    modified (copies)."""
+    L = lib()
+    if not getattr(L, "_diri_ready", False):
+        P = ctypes.POINTER
+        d, i, c = ctypes.c_double, ctypes.c_int, ctypes.c_char
+        pd, pi = P(d), P(i)
+        L.orc_diri01.argtypes = [i, i, pi, pi, pi, pd, c, pd, c, i, pi, pi, i, pd, pd, pd,
+                                 ctypes.c_void_p]
+        L.orc_diri01_seg.argtypes = [i, i, pi, pi, pd, c, pd, c, i, pi, pi, i, pd, pd, pd,
+                                     ctypes.c_void_p]
+        L._diri_ready = True
+    ik, a, b, c = _cols(ikle0)
+    ne = ik.shape[1]
+    xm = np.array(xm, dtype=np.float64).reshape(-1, ne).copy()
+    sm, f = np.array(sm, dtype=np.float64), np.array(f, dtype=np.float64)
+    nb, ld = _i32(nbor0), _i32(limdir)
+    fb = np.ascontiguousarray(fbor, dtype=np.float64)
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    mk = None if maskpt is None else np.ascontiguousarray(maskpt, dtype=np.float64)
+    st = L.orc_diri01(sm.size, ne, _pi(a), _pi(b), _pi(c), _pd(dm), typdia.encode(), _pd(xm),
+                      typext.encode(), nb.size, _pi(nb), _pi(ld), kdir, _pd(fb), _pd(sm), _pd(f),
+                      None if mk is None else mk.ctypes.data_as(ctypes.c_void_p))
+    if st:
+        raise ValueError("orc_diri01 status %d" % st)
+    return xm, sm, f
+
+
+def diri01_seg(g1, g2, dm, typdia, xa, typext, nbor0, limdir, kdir, fbor, sm, f, maskpt=None):
+    """DIRI01 on a segment-storage matrix.  Returns (xa, sm, f) (copies)."""
+    L = lib()
+    if not getattr(L, "_diri_ready", False):
+        diri01(np.zeros((1, 3), np.int32), np.ones(3), "Q", np.zeros((3, 1)), "S",
+               np.zeros(0, np.int32), np.zeros(0, np.int32), 1, np.zeros(0), np.zeros(3),
+               np.zeros(3))
+    g1, g2 = _i32(g1), _i32(g2)
+    xa = np.array(xa, dtype=np.float64).ravel().copy()
+    sm, f = np.array(sm, dtype=np.float64), np.array(f, dtype=np.float64)
+    nb, ld = _i32(nbor0), _i32(limdir)
+    fb = np.ascontiguousarray(fbor, dtype=np.float64)
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    mk = None if maskpt is None else np.ascontiguousarray(maskpt, dtype=np.float64)
+    st = L.orc_diri01_seg(sm.size, g1.size, _pi(g1), _pi(g2), _pd(dm), typdia.encode(), _pd(xa),
+                          typext.encode(), nb.size, _pi(nb), _pi(ld), kdir, _pd(fb), _pd(sm),
+                          _pd(f), None if mk is None else mk.ctypes.data_as(ctypes.c_void_p))
+    if st:
+        raise ValueError("orc_diri01_seg status %d" % st)
+    return xa, sm, f

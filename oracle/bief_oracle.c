@@ -1575,3 +1575,101 @@ int orc_assex3(int nelem, const int *eltseg, const int *oriseg, char typext,
 #undef XA
     return ORC_OK;
 }
+
+/* ------------------------------------------------------------------ */
+/* Dirichlet conditions                                                 */
+/* ------------------------------------------------------------------ */
+
+/* diri01.f:90-130 with boundary values (FBOR on the NPTFR boundary points,
+ * DIRAUX diraux.f:70-85 on boundary numbering): W1 = 0, W1(NBOR(K)) = FBOR(K)
+ * where LIMDIR(K) = KDIR (OSDBIF 'X=Y'); W2 = S W1 (MATVEC 'X=AY'); SM = SM -
+ * W2; W2 = 1; for those K, N = NBOR(K): SM(N) = S%D(N)*FBOR(K), W2(N) = 0,
+ * F(N) = FBOR(K); with a mask SM, F and W2 are multiplied by MASKPT; then
+ * OM 'M=DMD' with D = W2 on the off-diagonal terms only (TYPDIA set to '0'
+ * around the call), which zeroes the rows and columns of the Dirichlet
+ * points.  nbor is 0-based. */
+static int diri01_impl(const opmesh *M, int npoin, const double *dm, char typdia, double *xm,
+                       char typext, int nptfr, const int *nbor, const int *limdir, int kdir,
+                       const double *fbor, double *sm, double *f, const double *maskpt)
+{
+    const int nelem = M->sto == 3 ? 0 : M->nelem;
+    double *w1 = (double *)calloc((size_t)npoin, sizeof(double));
+    double *w2 = (double *)malloc(sizeof(double) * (size_t)npoin);
+    double *t = (double *)malloc(sizeof(double) * (size_t)npoin);
+    double *w = (double *)malloc(sizeof(double) * 3 * (size_t)nelem + 1);
+    int st = ORC_OK;
+    if (!w1 || !w2 || !t || !w) { st = ORC_ERR_ARGS; goto done; }
+    for (int k = 0; k < nptfr; ++k)
+        if (limdir[k] == kdir) w1[nbor[k]] = fbor[k];
+    st = op_matvec(M, "X=AY    ", npoin, w2, dm, typdia, xm, typext, w1, 0.0, t, w);
+    if (st) goto done;
+    for (int i = 0; i < npoin; ++i) sm[i] = sm[i] - w2[i];
+    for (int i = 0; i < npoin; ++i) w2[i] = 1.0;
+    for (int k = 0; k < nptfr; ++k)
+        if (limdir[k] == kdir) {
+            int n = nbor[k];
+            sm[n] = dm[n] * fbor[k];
+            w2[n] = 0.0;
+            f[n] = fbor[k];
+        }
+    if (maskpt)
+        for (int i = 0; i < npoin; ++i) {
+            sm[i] = sm[i] * maskpt[i];
+            f[i] = f[i] * maskpt[i];
+            w2[i] = w2[i] * maskpt[i];
+        }
+    {
+        /* OM 'M=DMD' with TYPDIA '0': off-diagonal part only (omseg.f:530-541,
+         * om1111.f:589-600) */
+        const double *dsc = w2;
+        if (M->sto == 3) {
+            if (typext == 'S' || typext == 'Q') {
+                for (int s = 0; s < M->nseg; ++s) xm[s] = xm[s] * dsc[M->g1[s]] * dsc[M->g2[s]];
+                if (typext == 'Q')
+                    for (int s = 0; s < M->nseg; ++s)
+                        xm[M->nseg + s] = xm[M->nseg + s] * dsc[M->g1[s]] * dsc[M->g2[s]];
+            }
+        } else if (typext == 'S' || typext == 'Q') {
+            const int ld = M->ld;
+            const int *ik0 = M->ik0, *ik1 = M->ik1, *ik2 = M->ik2;
+            double *x1 = xm, *x2 = xm + ld, *x3 = xm + 2 * (size_t)ld;
+            for (int e = 0; e < nelem; ++e) {
+                x1[e] = x1[e] * dsc[ik1[e]] * dsc[ik0[e]];
+                x2[e] = x2[e] * dsc[ik2[e]] * dsc[ik0[e]];
+                x3[e] = x3[e] * dsc[ik2[e]] * dsc[ik1[e]];
+            }
+            if (typext == 'Q') {
+                double *x4 = xm + 3 * (size_t)ld, *x5 = xm + 4 * (size_t)ld,
+                       *x6 = xm + 5 * (size_t)ld;
+                for (int e = 0; e < nelem; ++e) {
+                    x4[e] = x4[e] * dsc[ik1[e]] * dsc[ik0[e]];
+                    x5[e] = x5[e] * dsc[ik2[e]] * dsc[ik0[e]];
+                    x6[e] = x6[e] * dsc[ik2[e]] * dsc[ik1[e]];
+                }
+            }
+        }
+    }
+done:
+    free(w1); free(w2); free(t); free(w);
+    return st;
+}
+
+int orc_diri01(int npoin, int nelem, const int *ik0, const int *ik1, const int *ik2,
+               const double *dm, char typdia, double *xm, char typext, int nptfr,
+               const int *nbor, const int *limdir, int kdir, const double *fbor, double *sm,
+               double *f, const double *maskpt)
+{
+    opmesh M = {1, nelem, nelem, ik0, ik1, ik2, 0, NULL, NULL};
+    return diri01_impl(&M, npoin, dm, typdia, xm, typext, nptfr, nbor, limdir, kdir, fbor, sm,
+                       f, maskpt);
+}
+
+int orc_diri01_seg(int npoin, int nseg, const int *g1, const int *g2, const double *dm,
+                   char typdia, double *xa, char typext, int nptfr, const int *nbor,
+                   const int *limdir, int kdir, const double *fbor, double *sm, double *f,
+                   const double *maskpt)
+{
+    opmesh M = {3, 0, 0, NULL, NULL, NULL, nseg, g1, g2};
+    return diri01_impl(&M, npoin, dm, typdia, xa, typext, nptfr, nbor, limdir, kdir, fbor, sm,
+                       f, maskpt);
+}

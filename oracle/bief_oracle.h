@@ -145,6 +145,16 @@ int orc_solve_mixed_seg(int npoin, int nseg, const int *g1, const int *g2, doubl
                         double outer_tol, int max_outer, int max_inner, int nb, int nt,
                         int *outer_out, int *inner_total_out, double *relres_out);
 
+/* DIRI01 with boundary values (0-based nbor); xm/xa, sm and f modified */
+int orc_diri01(int npoin, int nelem, const int *ik0, const int *ik1, const int *ik2,
+               const double *dm, char typdia, double *xm, char typext, int nptfr,
+               const int *nbor, const int *limdir, int kdir, const double *fbor, double *sm,
+               double *f, const double *maskpt);
+int orc_diri01_seg(int npoin, int nseg, const int *g1, const int *g2, const double *dm,
+                   char typdia, double *xa, char typext, int nptfr, const int *nbor,
+                   const int *limdir, int kdir, const double *fbor, double *sm, double *f,
+                   const double *maskpt);
+
 #ifdef __cplusplus
 }
 #endif
