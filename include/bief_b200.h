@@ -93,8 +93,9 @@ int bief_set_matrix_dev(bief_handle *h, const double *dm, const double *xm,
 int bief_get_matrix(bief_handle *h, double *dm, double *xm, char *typdia);
 
 /* SOLVE(X,A,B,...) for SLV=1 (GRACJG, gracjg.F), SLV=3 (EQUNOR, CG on the
- * normal equations, equnor.f) and SLV=7 (GMRES(KRYLOV), gmres.f, KRYLOV
- * 1..20, NITMAX counting restarts): host X (initial guess in, solution out)
+ * normal equations, equnor.f), SLV=6 (CGSTAB, cgstab.f) and SLV=7
+ * (GMRES(KRYLOV), gmres.f, KRYLOV 1..20, NITMAX counting restarts): host X
+ * (initial guess in, solution out)
  * and B.  relres_out receives the relative residual the method prints
  * (SQRT(RMRM/XL), or NR0/NB for GMRES).  Other SLV values return
  * BIEF_ERR_UNSUPPORTED. */

@@ -182,6 +182,17 @@ void *gmres_kernel(int td, int sto) {
   return (void *)k_gmres<DIA_0, 1>;
 }
 
+void *cgstab_kernel(int td, int sto) {
+  if (sto == 3) {
+    if (td == DIA_Q) return (void *)k_cgstab<DIA_Q, 3>;
+    if (td == DIA_I) return (void *)k_cgstab<DIA_I, 3>;
+    return (void *)k_cgstab<DIA_0, 3>;
+  }
+  if (td == DIA_Q) return (void *)k_cgstab<DIA_Q, 1>;
+  if (td == DIA_I) return (void *)k_cgstab<DIA_I, 1>;
+  return (void *)k_cgstab<DIA_0, 1>;
+}
+
 void *mixed_kernel(int td, int sto) {
   if (sto == 3) {
     if (td == DIA_Q) return (void *)k_mixed<DIA_Q, 3>;
@@ -224,7 +235,9 @@ int persistent_grid(int npoin, int nsm, int *out) {
                 equnor_kernel(DIA_Q, 1), equnor_kernel(DIA_I, 1), equnor_kernel(DIA_0, 1),
                 equnor_kernel(DIA_Q, 3), equnor_kernel(DIA_I, 3), equnor_kernel(DIA_0, 3),
                 gmres_kernel(DIA_Q, 1), gmres_kernel(DIA_I, 1), gmres_kernel(DIA_0, 1),
-                gmres_kernel(DIA_Q, 3), gmres_kernel(DIA_I, 3), gmres_kernel(DIA_0, 3)};
+                gmres_kernel(DIA_Q, 3), gmres_kernel(DIA_I, 3), gmres_kernel(DIA_0, 3),
+                cgstab_kernel(DIA_Q, 1), cgstab_kernel(DIA_I, 1), cgstab_kernel(DIA_0, 1),
+                cgstab_kernel(DIA_Q, 3), cgstab_kernel(DIA_I, 3), cgstab_kernel(DIA_0, 3)};
   for (void *k : ks) {
     int bps = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, CG_THREADS, 0));
@@ -386,7 +399,7 @@ int build_transposed(bief_handle *h, const double *xm, cudaStream_t st, Sell *ou
 
 int check_cfg(const bief_slvcfg *cfg, int *precon) {
   if (!cfg) return BIEF_ERR_ARGS;
-  if (cfg->slv != 1 && cfg->slv != 3 && cfg->slv != 7) return BIEF_ERR_UNSUPPORTED;
+  if (cfg->slv != 1 && cfg->slv != 3 && cfg->slv != 6 && cfg->slv != 7) return BIEF_ERR_UNSUPPORTED;
   if (cfg->slv == 7 && (cfg->krylov < 1 || cfg->krylov > GM_MAXK)) return BIEF_ERR_ARGS;
   int p = cfg->precon == 0 ? 1 : cfg->precon;
   if (p <= 0) return BIEF_ERR_ARGS;
@@ -703,14 +716,39 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   }
   if ((st = seg ? build_seg_coefs(h, xm, s) : build_records(h, xm, s))) return st;
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
-  if (cfg->slv == 7) {  // GMRES
-    if (h->gm_k < cfg->krylov) {
-      if (h->d_gmv) cudaFree(h->d_gmv);
-      h->d_gmv = nullptr;
-      h->gm_k = 0;
-      if ((st = dalloc(&h->d_gmv, 2 * (size_t)cfg->krylov * h->npoin))) return st;
-      h->gm_k = cfg->krylov;
-    }
+  // work vectors beyond the handle's own: 2*KRYLOV for GMRES, 3 for CGSTAB
+  const int nextra = cfg->slv == 7 ? 2 * cfg->krylov : (cfg->slv == 6 ? 3 : 0);
+  if (nextra > 2 * h->gm_k) {
+    if (h->d_gmv) cudaFree(h->d_gmv);
+    h->d_gmv = nullptr;
+    h->gm_k = 0;
+    if ((st = dalloc(&h->d_gmv, (size_t)nextra * h->npoin))) return st;
+    h->gm_k = (nextra + 1) / 2;
+  }
+  if (cfg->slv == 6) {  // CGSTAB
+    StabP P;
+    P.npoin = h->npoin;
+    P.nitmax = cfg->nitmax;
+    P.eps = cfg->eps;
+    P.S = sell_of(h);
+    P.da = da;
+    P.dsc = diag ? h->d_dsc : nullptr;
+    P.x = x;
+    P.b = bw;
+    P.r = h->d_r;
+    P.p = h->d_d0;
+    P.q0 = h->d_d1;
+    P.q1 = h->d_ad;
+    P.v0 = h->d_t;
+    P.v1 = h->d_gmv;
+    P.s = h->d_gmv + (size_t)h->npoin;
+    P.t = h->d_gmv + 2 * (size_t)h->npoin;
+    P.part = h->d_part;
+    P.ctl = h->d_ctl;
+    P.timeout_ns = h->timeout_ns;
+    CK(cudaEventRecord(h->ev[0], s));
+    if ((st = launch_coop(h, cgstab_kernel(td, h->sto), &P, s))) return st;
+  } else if (cfg->slv == 7) {  // GMRES
     if (!h->d_gpart && (st = dalloc(&h->d_gpart, 2 * (size_t)h->G * (GM_MAXK + 1) + 4)))
       return st;
     GmP P;
@@ -784,7 +822,9 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   if (relres_out) *relres_out = c.relres;
   if (st >= 0 && ((flags & BIEF_SOLVE_INFOGR) || st > 0))
     print_gracjg(st, c.nit, c.relres, c.relat,
-                 cfg->slv == 3 ? "EQUNOR" : (cfg->slv == 7 ? "GMRES" : "GRACJG"));
+                 cfg->slv == 3 ? "EQUNOR"
+                 : cfg->slv == 6 ? "CGSTAB"
+                 : cfg->slv == 7 ? "GMRES" : "GRACJG");
   if (diag && (flags & BIEF_SOLVE_MUTATE_INPUTS) && st >= 0) {
     // SOLVE leaves B = D.B and A = D.A.D with TYPDIA from PRECD1
     CK(cudaMemcpyAsync(b, h->d_bs, sizeof(double) * h->npoin, cudaMemcpyDeviceToDevice, s));

@@ -656,6 +656,139 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_equnor(EqP P) {
 }
 
 // ---------------------------------------------------------------------------
+// CGSTAB (cgstab.f:95-200, BiCGSTAB) without Crout preconditioning, as ONE
+// persistent kernel with three grid reductions per iteration: (P.V);
+// (T.S, T.T); (R.R, R.P) -- the last pair gives the convergence test and
+// the next BETA1.  The new Q, and S, are recomputed at every node that
+// reads them (owner's bits); Q and V are double-buffered because the pass
+// that writes the new ones reads the old ones at neighbours.
+// ---------------------------------------------------------------------------
+struct StabP {
+  int npoin, nitmax;
+  double eps;
+  Sell S;
+  const double *da, *dsc;
+  double *x;
+  const double *b;
+  double *r, *p, *q0, *q1, *v0, *v1, *s, *t;
+  double *part;
+  Ctl *ctl;
+  long long timeout_ns;
+};
+
+template <int TD, int STO>
+__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgstab(StabP P) {
+  const int T = blockDim.x, t = threadIdx.x;
+  const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
+  const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
+  double *x = P.x, *r = P.r, *p = P.p, *sv = P.s, *tv = P.t;
+  const double *b = P.b, *da = P.da;
+  const bool lead = (blockIdx.x == 0 && t == 0);
+  double sd[2], rd[2];
+  int nbar = 0;
+  const bool h1 = false;
+  double a1 = 0.0;
+
+  auto finish = [&](int status, int m, double rmrm, double xl, int relat) {
+    if (P.dsc)  // solve.f:637-641: X = X*D
+      for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
+    if (lead) {
+      P.ctl->status = status;
+      P.ctl->nit = m;
+      P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
+      P.ctl->relat = relat;
+    }
+  };
+
+  // XL (:105-111); SQRT(XL) < RMIN: X = 0 (:112-116)
+  sd[0] = 0.0;
+  for (int i = lo + t; i < hi; i += T) sd[0] = add(sd[0], mul(b[i], b[i]));
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  double xl = rd[0];
+  int relat = 1;
+  if (xl < 1.0) { xl = 1.0; relat = 0; }
+  if (__dsqrt_rn(xl) < 1.0e-15) {
+    for (int i = lo + t; i < hi; i += T) x[i] = 0.0;
+    finish(ST_OK, 0, 0.0, xl, relat);
+    return;
+  }
+  const double tol = mul(xl, mul(P.eps, P.eps));
+  // V = A X, R = B - V, RMRM (:120-123); P = R, V = Q = 0 (:144-147)
+  double *qc = P.q0, *qn = P.q1, *vc = P.v0, *vn = P.v1;
+  sd[0] = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    double a0 = diag_term<TD>(x[i], da, i);
+    op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
+    const double ri = sub(b[i], a0);
+    r[i] = ri;
+    p[i] = ri;
+    qc[i] = 0.0;
+    vc[i] = 0.0;
+    sd[0] = add(sd[0], mul(ri, ri));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  double rmrm = rd[0];
+  if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
+  if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }
+  double beta1 = rmrm;  // R.P with P a copy of R: the same products and sum
+  double alfa = 1.0, beta = 1.0, omeg1 = 1.0;
+
+  for (int m = 1;; ++m) {
+    const double omeg2 = __ddiv_rn(mul(omeg1, beta1), beta);  // :156
+    const double omeg = __ddiv_rn(omeg2, alfa);
+    beta = beta1;
+    const double nomeg2 = -omeg2;
+    // Q = R + OMEG Q - OMEG2 V (:161-162), V = A Q (:163), P.V (:173)
+    auto qnew = [&](int j) { return add(add(r[j], mul(omeg, qc[j])), mul(nomeg2, vc[j])); };
+    sd[0] = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      const double qi = qnew(i);
+      double a0 = diag_term<TD>(qi, da, i);
+      op_row2<STO>(i, i, h1, a0, a1, P.S, qnew);
+      qn[i] = qi;
+      vn[i] = a0;
+      sd[0] = add(sd[0], mul(p[i], a0));
+    }
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    omeg1 = __ddiv_rn(beta1, rd[0]);  // :174
+    { double *tmp = qc; qc = qn; qn = tmp; tmp = vc; vc = vn; vn = tmp; }
+    // S = R - OMEG1 V (:176), T = A S (:177), T.S and T.T (:186-187)
+    const double nomeg1 = -omeg1;
+    auto snew = [&](int j) { return add(r[j], mul(nomeg1, vc[j])); };
+    sd[0] = 0.0;
+    sd[1] = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      const double si = snew(i);
+      double a0 = diag_term<TD>(si, da, i);
+      op_row2<STO>(i, i, h1, a0, a1, P.S, snew);
+      sv[i] = si;
+      tv[i] = a0;
+      sd[0] = add(sd[0], mul(a0, si));
+      sd[1] = add(sd[1], mul(a0, a0));
+    }
+    if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    alfa = __ddiv_rn(rd[0], rd[1]);  // :188
+    // X = X + OMEG1 Q + ALFA S (:190-191), R = S - ALFA T (:192), R.R and R.P
+    const double nalfa = -alfa;
+    sd[0] = 0.0;
+    sd[1] = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      x[i] = add(add(x[i], mul(omeg1, qc[i])), mul(alfa, sv[i]));
+      const double ri = add(sv[i], mul(nalfa, tv[i]));
+      r[i] = ri;
+      sd[0] = add(sd[0], mul(ri, ri));
+      sd[1] = add(sd[1], mul(ri, p[i]));
+    }
+    if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    rmrm = rd[0];
+    beta1 = rd[1];
+    if (isnan(rmrm)) { finish(ST_NAN, m, rmrm, xl, relat); return; }
+    if (rmrm <= tol) { finish(ST_OK, m, rmrm, xl, relat); return; }  // :194
+    if (m >= P.nitmax) { finish(m, m, rmrm, xl, relat); return; }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // GMRES(KRYLOV) (gmres.f:55-213) without preconditioning matrices, as ONE
 // persistent kernel.  Columns 1..K-1 by modified Gram-Schmidt: each
 // projection's AXPY is fused with the next dot (one grid reduction per

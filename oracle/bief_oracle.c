@@ -799,6 +799,80 @@ done:
     return st;
 }
 
+/* cgstab.f:95-200 (BiCGSTAB) without Crout preconditioning:
+ *   XL = B.B (absolute below 1); SQRT(XL) < 1e-15: X = 0; V = A X;
+ *   R = B - V; RMRM = R.R; stop if RMRM < EPS**2 XL; R = B, R = R - V
+ *   (the same values again); P = R; V = 0; Q = 0; ALFA = BETA = OMEG1 = 1;
+ *   per iteration: BETA1 = R.P; OMEG2 = OMEG1*BETA1/BETA;
+ *   OMEG = OMEG2/ALFA; BETA = BETA1; Q = R + OMEG Q; Q = Q - OMEG2 V;
+ *   V = A Q; OMEG1 = BETA1 / P.V; S = R - OMEG1 V; T = A S;
+ *   ALFA = T.S / T.T; X = X + OMEG1 Q; X = X + ALFA S; R = S - ALFA T;
+ *   RMRM = R.R; stop if RMRM <= XL EPS**2 or M = NITMAX. */
+static int cgstab_impl(const opmesh *M, int npoin, double *x, const double *da, char typdia,
+                       const double *xm, char typext, const double *b, int nitmax, double eps,
+                       int dot_mode, int nb, int nt, int *nit_out, double *relres_out,
+                       int *relat_out)
+{
+    const int nelem = M->sto == 3 ? 0 : M->nelem;
+    size_t n = (size_t)npoin;
+    double *p = (double *)malloc(sizeof(double) * n), *q = (double *)malloc(sizeof(double) * n);
+    double *r = (double *)malloc(sizeof(double) * n), *sv = (double *)malloc(sizeof(double) * n);
+    double *tv = (double *)malloc(sizeof(double) * n), *v = (double *)malloc(sizeof(double) * n);
+    double *t = (double *)malloc(sizeof(double) * n);
+    double *w = (double *)malloc(sizeof(double) * 3 * (size_t)nelem + 1);
+    int m = 0, st = ORC_OK, relat;
+    double xl, rmrm = 0.0, alfa, alfa1, beta, beta1, omeg, omeg1, omeg2;
+    if (!p || !q || !r || !sv || !tv || !v || !t || !w) { st = ORC_ERR_ARGS; goto done; }
+    xl = pdots(dot_mode, npoin, b, b, nb, nt);                       /* :105 */
+    if (xl < 1.0) { xl = 1.0; relat = 0; } else { relat = 1; }
+    if (sqrt(xl) < 1.0e-15) {                                         /* :112-116 */
+        rmrm = 0.0;
+        for (size_t i = 0; i < n; ++i) x[i] = 0.0;
+        goto fin;
+    }
+    st = op_matvec(M, "X=AY    ", npoin, v, da, typdia, xm, typext, x, 0.0, t, w);  /* :120 */
+    if (st) goto done;
+    for (size_t i = 0; i < n; ++i) r[i] = b[i] - v[i];               /* :121 */
+    rmrm = pdots(dot_mode, npoin, r, r, nb, nt);
+    if (rmrm < eps * eps * xl) goto fin;                             /* :123 */
+    for (size_t i = 0; i < n; ++i) r[i] = b[i];                      /* :132 */
+    for (size_t i = 0; i < n; ++i) r[i] = r[i] - v[i];               /* :142 */
+    for (size_t i = 0; i < n; ++i) { p[i] = r[i]; v[i] = 0.0; q[i] = 0.0; }
+    alfa = 1.0; beta = 1.0; omeg1 = 1.0;
+    for (;;) {
+        m = m + 1;                                                   /* :153 */
+        beta1 = pdots(dot_mode, npoin, r, p, nb, nt);
+        omeg2 = omeg1 * beta1 / beta;
+        omeg = omeg2 / alfa;
+        beta = beta1;
+        for (size_t i = 0; i < n; ++i) q[i] = r[i] + omeg * q[i];    /* :161 */
+        for (size_t i = 0; i < n; ++i) q[i] = q[i] + (-omeg2) * v[i];
+        st = op_matvec(M, "X=AY    ", npoin, v, da, typdia, xm, typext, q, 0.0, t, w);
+        if (st) goto done;
+        omeg1 = pdots(dot_mode, npoin, p, v, nb, nt);                /* :173 */
+        omeg1 = beta1 / omeg1;
+        for (size_t i = 0; i < n; ++i) sv[i] = r[i] + (-omeg1) * v[i];
+        st = op_matvec(M, "X=AY    ", npoin, tv, da, typdia, xm, typext, sv, 0.0, t, w);
+        if (st) goto done;
+        alfa = pdots(dot_mode, npoin, tv, sv, nb, nt);               /* :186 */
+        alfa1 = pdots(dot_mode, npoin, tv, tv, nb, nt);
+        alfa = alfa / alfa1;
+        for (size_t i = 0; i < n; ++i) x[i] = x[i] + omeg1 * q[i];   /* :190 */
+        for (size_t i = 0; i < n; ++i) x[i] = x[i] + alfa * sv[i];
+        for (size_t i = 0; i < n; ++i) r[i] = sv[i] + (-alfa) * tv[i];
+        rmrm = pdots(dot_mode, npoin, r, r, nb, nt);                 /* :193 */
+        if (rmrm <= xl * (eps * eps)) goto fin;
+        if (m >= nitmax) { st = m; goto fin; }
+    }
+fin:
+    if (nit_out) *nit_out = m;
+    if (relres_out) *relres_out = sqrt(rmrm / xl);
+    if (relat_out) *relat_out = relat;
+done:
+    free(p); free(q); free(r); free(sv); free(tv); free(v); free(t); free(w);
+    return st;
+}
+
 /* gmres.f:55-213, restarted GMRES(KRYLOV) without preconditioning
  * matrices (PRECO false), KRYLOV <= 20 (H(21,20)):
  *   NB = SQRT(B.B) (absolute mode below 1); R0 = A X - B; NR0 = |R0|;
@@ -924,7 +998,7 @@ static int solve_impl(const opmesh *M, int npoin, double *x, double *b, double *
                       int nitmax, double eps, int krylov, int dot_mode, int nb, int nt,
                       int *nit_out, double *relres_out, int *relat_out)
 {
-    if (slv != 1 && slv != 3 && slv != 7) return ORC_ERR_UNSUPPORTED;
+    if (slv != 1 && slv != 3 && slv != 6 && slv != 7) return ORC_ERR_UNSUPPORTED;
     if (precon == 0) precon = 1;
     if (precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 ||
         precon % 17 == 0)
@@ -939,6 +1013,9 @@ static int solve_impl(const opmesh *M, int npoin, double *x, double *b, double *
     int st = slv == 7
                  ? gmres_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, krylov,
                               dot_mode, nb, nt, nit_out, relres_out, relat_out)
+             : slv == 6
+                 ? cgstab_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
+                               nb, nt, nit_out, relres_out, relat_out)
              : slv == 3
                  ? equnor_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
                                nb, nt, nit_out, relres_out, relat_out)
