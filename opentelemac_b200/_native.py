@@ -22,6 +22,7 @@ BIEF_ERR_SIZE = -9
 
 BIEF_SOLVE_MUTATE_INPUTS = 1
 BIEF_SOLVE_INFOGR = 2
+BIEF_SOLVE_MODASS3 = 4
 
 # Every symbol include/bief_b200.h declares.
 EXPORTS = [

@@ -193,15 +193,18 @@ class Matrix:
         return self
 
 
-def solve(x, A, b, cfg, infogr=False, mutate=False):
-    """SOLVE(X,A,B,...,CFG,INFOGR,...) for CFG.slv = 1 (GRACJG).
+def solve(x, A, b, cfg, infogr=False, mutate=False, modass=1):
+    """SOLVE(X,A,B,...,CFG,INFOGR,...) for CFG.slv = 1 (GRACJG), 3 (EQUNOR),
+    6 (CGSTAB) or 7 (GMRES).
 
     x holds the initial guess and receives the solution.  With mutate=True
     the reference's side effects are reproduced: b becomes D.b and A is
-    replaced by D.A.D (TYPDIA 'I').  Returns (status, nit, relres)."""
+    replaced by D.A.D (TYPDIA 'I').  modass=3 selects compensated dot
+    products (GRACJG only).  Returns (status, nit, relres)."""
     L = _native.lib()
     flags = (_native.BIEF_SOLVE_MUTATE_INPUTS if mutate else 0) | (
-        _native.BIEF_SOLVE_INFOGR if infogr else 0)
+        _native.BIEF_SOLVE_INFOGR if infogr else 0) | (
+        _native.BIEF_SOLVE_MODASS3 if modass == 3 else 0)
     relres = ctypes.c_double()
     if _is_torch(x):
         st = L.bief_solve_dev(A.mesh.handle, _ptr(x), _ptr(b), ctypes.byref(cfg), flags,

@@ -149,15 +149,21 @@ void dispatch_mv(bief_handle *h, int td, bool sym, bool tr, const double *xm, co
 #undef MV_CASE
 }
 
-void *cg_kernel(int td, int sto) {
+template <bool COMP>
+void *cg_kernel_t(int td, int sto) {
   if (sto == 3) {
-    if (td == DIA_Q) return (void *)k_cg64<DIA_Q, 3>;
-    if (td == DIA_I) return (void *)k_cg64<DIA_I, 3>;
-    return (void *)k_cg64<DIA_0, 3>;
+    if (td == DIA_Q) return (void *)k_cg64<DIA_Q, 3, COMP>;
+    if (td == DIA_I) return (void *)k_cg64<DIA_I, 3, COMP>;
+    return (void *)k_cg64<DIA_0, 3, COMP>;
   }
-  if (td == DIA_Q) return (void *)k_cg64<DIA_Q, 1>;
-  if (td == DIA_I) return (void *)k_cg64<DIA_I, 1>;
-  return (void *)k_cg64<DIA_0, 1>;
+  if (td == DIA_Q) return (void *)k_cg64<DIA_Q, 1, COMP>;
+  if (td == DIA_I) return (void *)k_cg64<DIA_I, 1, COMP>;
+  return (void *)k_cg64<DIA_0, 1, COMP>;
+}
+
+// comp: MODASS = 3 (compensated dot products)
+void *cg_kernel(int td, int sto, bool comp = false) {
+  return comp ? cg_kernel_t<true>(td, sto) : cg_kernel_t<false>(td, sto);
 }
 
 void *equnor_kernel(int td, int sto) {
@@ -237,7 +243,9 @@ int persistent_grid(int npoin, int nsm, int *out) {
                 gmres_kernel(DIA_Q, 1), gmres_kernel(DIA_I, 1), gmres_kernel(DIA_0, 1),
                 gmres_kernel(DIA_Q, 3), gmres_kernel(DIA_I, 3), gmres_kernel(DIA_0, 3),
                 cgstab_kernel(DIA_Q, 1), cgstab_kernel(DIA_I, 1), cgstab_kernel(DIA_0, 1),
-                cgstab_kernel(DIA_Q, 3), cgstab_kernel(DIA_I, 3), cgstab_kernel(DIA_0, 3)};
+                cgstab_kernel(DIA_Q, 3), cgstab_kernel(DIA_I, 3), cgstab_kernel(DIA_0, 3),
+                cg_kernel(DIA_Q, 1, true), cg_kernel(DIA_I, 1, true), cg_kernel(DIA_0, 1, true),
+                cg_kernel(DIA_Q, 3, true), cg_kernel(DIA_I, 3, true), cg_kernel(DIA_0, 3, true)};
   for (void *k : ks) {
     int bps = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, CG_THREADS, 0));
@@ -694,6 +702,8 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   int precon, st = check_cfg(cfg, &precon);
   if (st) return st;
   if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
+  const bool comp = (flags & BIEF_SOLVE_MODASS3) != 0;
+  if (comp && cfg->slv != 1) return BIEF_ERR_UNSUPPORTED;
   DevGuard g(h->dev);
   cudaStream_t s = (cudaStream_t)stream;
   const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
@@ -809,7 +819,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    if ((st = launch_coop(h, cg_kernel(td, h->sto), &P, s))) return st;
+    if ((st = launch_coop(h, cg_kernel(td, h->sto, comp), &P, s))) return st;
   }
   CK(cudaEventRecord(h->ev[1], s));
   CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));

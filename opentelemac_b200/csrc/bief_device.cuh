@@ -159,6 +159,119 @@ __device__ __noinline__ bool grid_reduce(Ctl *ctl, double *part, long long timeo
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// Compensated dot products (MODASS = 3): Dot2 (dot_comp.f) per thread with
+// TWOSUM (twosum.f) and TWOPROD with Dekker's split (twoprod.f, split.f),
+// every operation separately rounded; partial results (p, s) merge as
+// (p, q) = TwoSum(p1, p2), s = (s1 + s2) + q -- commutative bit for bit, so
+// the xor-butterflies leave every lane with the same pair.  Value p + s.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void two_sum(double a, double b, double &x, double &y) {
+  const double xo = add(a, b), z = sub(xo, a);
+  y = add(sub(a, sub(xo, z)), sub(b, z));
+  x = xo;
+}
+
+__device__ __forceinline__ void split27(double a, double &hi, double &lo) {
+  const double z = mul(134217729.0, a);
+  hi = sub(z, sub(z, a));
+  lo = sub(a, hi);
+}
+
+__device__ __forceinline__ void two_prod(double a, double b, double &x, double &y) {
+  double ah, al, bh, bl;
+  x = mul(a, b);
+  split27(a, ah, al);
+  split27(b, bh, bl);
+  y = sub(mul(al, bl), sub(sub(sub(x, mul(ah, bh)), mul(al, bh)), mul(ah, bl)));
+}
+
+struct CPair {
+  double p, s;
+};
+
+__device__ __forceinline__ CPair cmerge(CPair a, CPair b) {
+  CPair r;
+  double q;
+  two_sum(a.p, b.p, r.p, q);
+  r.s = add(add(a.s, b.s), q);
+  return r;
+}
+
+// One Dot2 step: (p, s) += x*y
+__device__ __forceinline__ void cdot_add(CPair &a, double x, double y) {
+  double h, r, q;
+  two_prod(x, y, h, r);
+  two_sum(a.p, h, a.p, q);
+  a.s = add(a.s, add(q, r));
+}
+
+__device__ __forceinline__ CPair cpair_shfl_xor(CPair v, int o) {
+  const unsigned FULL = 0xffffffffu;
+  CPair r;
+  r.p = __shfl_xor_sync(FULL, v.p, o);
+  r.s = __shfl_xor_sync(FULL, v.s, o);
+  return r;
+}
+
+__device__ __forceinline__ CPair block_tree_c(CPair v, CPair *sm) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v = cmerge(v, cpair_shfl_xor(v, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) sm[w] = v;
+  __syncthreads();
+  CPair u{0.0, 0.0};
+  if (w == 0) {
+    if (lane < nw) u = sm[lane];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) u = cmerge(u, cpair_shfl_xor(u, o));
+  }
+  __syncthreads();
+  return u;
+}
+
+// Grid reduction of one compensated dot, in the order of grid_reduce:
+// block pairs (block_tree_c), thread t merging block pairs t, t+T, ...
+// from (0, 0), block_tree_c again; returns p + s in `out`.
+static __device__ __noinline__ bool grid_reduce_comp(Ctl *ctl, double *part, long long timeout_ns,
+                                              int &nbar, CPair v, double *out) {
+  __shared__ CPair smc[32];
+  __shared__ double bc;
+  __shared__ int s_err;
+  const int G = gridDim.x, T = blockDim.x, t = threadIdx.x;
+  const unsigned long long k = (unsigned long long)(++nbar);
+  double *buf = part + (size_t)(k & 1) * (size_t)G * 2;
+  const CPair bp = block_tree_c(v, smc);
+  if (t == 0) {
+    buf[(size_t)blockIdx.x * 2] = bp.p;
+    buf[(size_t)blockIdx.x * 2 + 1] = bp.s;
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> cnt(ctl->arrivals);
+    cnt.fetch_add(1ull, cuda::memory_order_release);
+    const unsigned long long target = k * (unsigned long long)G;
+    const unsigned long long t0 = global_ns();
+    s_err = 0;
+    while (cnt.load(cuda::memory_order_acquire) < target) {
+      if ((long long)(global_ns() - t0) > timeout_ns) {
+        s_err = 1;
+        atomicExch(&ctl->status, (int)ST_TIMEOUT);
+        break;
+      }
+      if (SPIN_NS > 0) __nanosleep(SPIN_NS);
+    }
+  }
+  __syncthreads();
+  if (s_err) return false;
+  CPair acc{0.0, 0.0};
+  for (int b = t; b < G; b += T)
+    acc = cmerge(acc, CPair{__ldcg(buf + (size_t)b * 2), __ldcg(buf + (size_t)b * 2 + 1)});
+  const CPair tot = block_tree_c(acc, smc);
+  if (t == 0) bc = add(tot.p, tot.s);
+  __syncthreads();
+  *out = bc;
+  __syncthreads();
+  return true;
+}
+
 // Grid barrier without values: all blocks' preceding writes are visible to
 // every block after it returns true.  Same monotonic counter and bounded
 // wait as grid_reduce (the two may be mixed in one launch).

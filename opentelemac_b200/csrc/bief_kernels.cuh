@@ -374,7 +374,11 @@ struct CgP {
   long long timeout_ns;
 };
 
-template <int TD, int STO>
+// COMP: MODASS = 3, every P_DOTS a compensated dot (Dot2, dot_comp.f) in
+// the device order (grid_reduce_comp); the vector operations are unchanged
+// (their compensated forms in the reference only fill error vectors that
+// GRACJG does not read).
+template <int TD, int STO, bool COMP>
 __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
@@ -383,7 +387,24 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
   const double *b = P.b, *da = P.da;
   const bool lead = (blockIdx.x == 0 && t == 0);
   double s, red;
+  CPair cs{0.0, 0.0};
   int nbar = 0;
+  auto dot0 = [&]() {
+    s = 0.0;
+    cs = CPair{0.0, 0.0};
+  };
+  auto dacc = [&](double u, double v) {
+    if constexpr (COMP)
+      cdot_add(cs, u, v);
+    else
+      s = add(s, mul(u, v));
+  };
+  auto dred = [&](double &out) -> bool {
+    if constexpr (COMP)
+      return grid_reduce_comp(P.ctl, P.part, P.timeout_ns, nbar, cs, &out);
+    else
+      return grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &out, nullptr);
+  };
 
   auto finish = [&](int status, int m, double rmrm, double xl, int relat) {
     if (P.dsc)  // solve.f:637-641: X = X*D
@@ -397,9 +418,9 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
   };
 
   // XL = P_DOTS(B,B) (gracjg.F:189)
-  s = 0.0;
-  for (int i = lo + t; i < hi; i += T) s = add(s, mul(b[i], b[i]));
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  dot0();
+  for (int i = lo + t; i < hi; i += T) dacc(b[i], b[i]);
+  if (!dred(red)) return;
   double xl = red;
   if (__dsqrt_rn(xl) < 1.0e-15) {  // gracjg.F:194-202: X = 0
     for (int i = lo + t; i < hi; i += T) x[i] = 0.0;
@@ -411,7 +432,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
   const double tol = mul(xl, mul(P.eps, P.eps));
 
   // R = A X - B (gracjg.F:213-216)
-  s = 0.0;
+  dot0();
   for (int i = lo + t; i < hi; i += ROW_ILP * T) {
     const int i1 = i + T;
     const bool h1 = ROW_ILP == 2 && i1 < hi;
@@ -419,21 +440,21 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
     op_row2<STO>(i, i1, h1, a0, a1, P.S, [&](int j) { return x[j]; });
     const double r0 = sub(a0, b[i]);
     r[i] = r0;
-    s = add(s, mul(r0, r0));
+    dacc(r0, r0);
     if (h1) {
       const double r1 = sub(a1, b[i1]);
       r[i1] = r1;
-      s = add(s, mul(r1, r1));
+      dacc(r1, r1);
     }
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  if (!dred(red)) return;
   double rmrm = red, rmgm = rmrm;
   if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
   if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }
 
   // D = G (= R), AD = A D, DAD, RO (gracjg.F:248-261)
   double *cur = P.d0, *nxt = P.d1;
-  s = 0.0;
+  dot0();
   for (int i = lo + t; i < hi; i += ROW_ILP * T) {
     const int i1 = i + T;
     const bool h1 = ROW_ILP == 2 && i1 < hi;
@@ -443,13 +464,13 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
     double a0 = diag_term<TD>(d0, da, i), a1 = h1 ? diag_term<TD>(d1, da, i1) : 0.0;
     op_row2<STO>(i, i1, h1, a0, a1, P.S, [&](int j) { return r[j]; });
     ad[i] = a0;
-    s = add(s, mul(d0, a0));
+    dacc(d0, a0);
     if (h1) {
       ad[i1] = a1;
-      s = add(s, mul(d1, a1));
+      dacc(d1, a1);
     }
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  if (!dred(red)) return;
   double dad = red;
   if (!(dad > 0.0)) { finish(isnan(dad) ? ST_NAN : ST_BREAKDOWN, 0, rmrm, xl, relat); return; }
   double ro = __ddiv_rn(rmgm, dad);
@@ -458,14 +479,14 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
     // X = X - RO*D (gracjg.F:268 / :387) fused with R = R - RO*AD (:290)
     // and RMRM = P_DOTS(R,R) (:295)
     const double nro = -ro;
-    s = 0.0;
+    dot0();
     for (int i = lo + t; i < hi; i += T) {
       x[i] = add(x[i], mul(nro, cur[i]));
       const double ri = add(r[i], mul(nro, ad[i]));
       r[i] = ri;
-      s = add(s, mul(ri, ri));
+      dacc(ri, ri);
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+    if (!dred(red)) return;
     const double rm1gm1 = rmgm;
     rmrm = red;
     rmgm = rmrm;
@@ -477,7 +498,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
     // DAD = P_DOTS(D,AD) (:382).  Every thread that needs D at node j
     // recomputes R(j)+BETA*D(j) from the previous direction, which gives
     // the same bits as the owner's value; the owner also stores it.
-    s = 0.0;
+    dot0();
     for (int i = lo + t; i < hi; i += ROW_ILP * T) {
       const int i1 = i + T;
       const bool h1 = ROW_ILP == 2 && i1 < hi;
@@ -488,13 +509,13 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
       double a0 = diag_term<TD>(d0, da, i), a1 = h1 ? diag_term<TD>(d1, da, i1) : 0.0;
       op_row2<STO>(i, i1, h1, a0, a1, P.S, [&](int j) { return add(r[j], mul(beta, cur[j])); });
       ad[i] = a0;
-      s = add(s, mul(d0, a0));
+      dacc(d0, a0);
       if (h1) {
         ad[i1] = a1;
-        s = add(s, mul(d1, a1));
+        dacc(d1, a1);
       }
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+    if (!dred(red)) return;
     dad = red;
     if (!(dad > 0.0)) { finish(isnan(dad) ? ST_NAN : ST_BREAKDOWN, m, rmrm, xl, relat); return; }
     ro = __ddiv_rn(rmgm, dad);  // :383 (RMDM = RMGM)
@@ -817,7 +838,7 @@ struct GmP {
 
 // Reduction of n <= GM_MAXK+1 binary64 values per thread (blocked order of
 // each value, as grid_reduce).  vals/out may alias.
-__device__ __noinline__ bool grid_reduce_n(Ctl *ctl, double *part, long long timeout_ns,
+static __device__ __noinline__ bool grid_reduce_n(Ctl *ctl, double *part, long long timeout_ns,
                                            int &nbar, const double *vals, int n, double *out) {
   __shared__ double smd[32];
   __shared__ double red_sm[GM_MAXK + 1];

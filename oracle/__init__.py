@@ -20,6 +20,8 @@ LIB = os.path.join(HERE, "_build", "libbief_oracle.so")
 
 DOT_SEQUENTIAL = 0
 DOT_BLOCKED = 1
+DOT_COMP_SEQUENTIAL = 2      # MODASS = 3 (dot_comp.f), the reference's order
+DOT_COMP_BLOCKED = 3         # MODASS = 3 in the device kernels' order
 
 _lib = None
 
@@ -121,9 +123,20 @@ def matvec(op, ikle0, dm, typdia, xm, typext, y, c=0.0, x=None):
 def dot(x, y, mode=DOT_SEQUENTIAL, nblocks=1, nthreads=256):
     x = np.ascontiguousarray(x, dtype=np.float64)
     y = np.ascontiguousarray(y, dtype=np.float64)
+    L = lib()
     if mode == DOT_BLOCKED:
-        return lib().orc_dot_blocked(x.size, _pd(x), _pd(y), nblocks, nthreads)
-    return lib().orc_dot(x.size, _pd(x), _pd(y))
+        return L.orc_dot_blocked(x.size, _pd(x), _pd(y), nblocks, nthreads)
+    if mode in (DOT_COMP_SEQUENTIAL, DOT_COMP_BLOCKED):
+        P = ctypes.POINTER
+        L.orc_dot_comp.argtypes = [ctypes.c_int, P(ctypes.c_double), P(ctypes.c_double)]
+        L.orc_dot_comp.restype = ctypes.c_double
+        L.orc_dot_blocked_comp.argtypes = [ctypes.c_int, P(ctypes.c_double),
+                                           P(ctypes.c_double), ctypes.c_int, ctypes.c_int]
+        L.orc_dot_blocked_comp.restype = ctypes.c_double
+        if mode == DOT_COMP_SEQUENTIAL:
+            return L.orc_dot_comp(x.size, _pd(x), _pd(y))
+        return L.orc_dot_blocked_comp(x.size, _pd(x), _pd(y), nblocks, nthreads)
+    return L.orc_dot(x.size, _pd(x), _pd(y))
 
 
 def solve(ikle0, dm, typdia, xm, typext, b, x0=None, precon=2, nitmax=100000, eps=1e-8,

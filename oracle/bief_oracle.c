@@ -550,6 +550,113 @@ static float dot_batch32(int n, const float *x, const float *y, int nt, int npt)
     return r;
 }
 
+/* ------------------------------------------------------------------ */
+/* compensated dot products (MODASS = 3)                                */
+/* ------------------------------------------------------------------ */
+
+/* twosum.f: X = A+B, Y = (A-(X-Z))+(B-Z) with Z = X-A (the exact error). */
+static void two_sum(double a, double b, double *x, double *y)
+{
+    double xo = a + b, z = xo - a;
+    *y = (a - (xo - z)) + (b - z);
+    *x = xo;
+}
+
+/* twoprod.f with split.f (Dekker, constant 2**27+1): X = A*B and the exact
+ * error Y of that product. */
+static void split27(double a, double *x, double *y)
+{
+    double z = 134217729.0 * a;
+    *x = z - (z - a);
+    *y = a - *x;
+}
+
+static void two_prod(double a, double b, double *x, double *y)
+{
+    double ah, al, bh, bl;
+    *x = a * b;
+    split27(a, &ah, &al);
+    split27(b, &bh, &bl);
+    *y = al * bl - (((*x - ah * bh) - al * bh) - ah * bl);
+}
+
+/* dot_comp.f:50-70 -- Dot2 in the reference's sequential order. */
+double orc_dot_comp(int n, const double *x, const double *y)
+{
+    if (n == 0) return 0.0;
+    double p, s, h, r, q;
+    two_prod(x[0], y[0], &p, &s);
+    for (int i = 1; i < n; ++i) {
+        two_prod(x[i], y[i], &h, &r);
+        two_sum(p, h, &p, &q);
+        s = s + (q + r);
+    }
+    return p + s;
+}
+
+/* The device's compensated dot (blocked order): each thread runs Dot2 over
+ * its nodes from (p, s) = (0, 0); pairs merge as (p, q) = TwoSum(p1, p2),
+ * s = (s1 + s2) + q, through the same xor-butterfly trees as the plain
+ * blocked dot; the result is p + s. */
+typedef struct { double p, s; } cpair;
+
+static cpair cmerge(cpair a, cpair b)
+{
+    cpair r;
+    double q;
+    two_sum(a.p, b.p, &r.p, &q);
+    r.s = (a.s + b.s) + q;
+    return r;
+}
+
+static cpair ctree(const cpair *v, int nt)
+{
+    cpair lanes[32], wsum[32], nxt[32];
+    int nw = nt / 32;
+    for (int w = 0; w < 32; ++w) { wsum[w].p = 0.0; wsum[w].s = 0.0; }
+    for (int w = 0; w < nw; ++w) {
+        for (int l = 0; l < 32; ++l) lanes[l] = v[w * 32 + l];
+        for (int o = 16; o >= 1; o >>= 1) {
+            for (int l = 0; l < 32; ++l) nxt[l] = cmerge(lanes[l], lanes[l ^ o]);
+            memcpy(lanes, nxt, sizeof(lanes));
+        }
+        wsum[w] = lanes[0];
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        for (int l = 0; l < 32; ++l) nxt[l] = cmerge(wsum[l], wsum[l ^ o]);
+        memcpy(wsum, nxt, sizeof(wsum));
+    }
+    return wsum[0];
+}
+
+double orc_dot_blocked_comp(int n, const double *x, const double *y, int nb, int nt)
+{
+    cpair *part = (cpair *)malloc(sizeof(cpair) * (size_t)nb);
+    cpair *v = (cpair *)malloc(sizeof(cpair) * (size_t)nt);
+    for (int b = 0; b < nb; ++b) {
+        long long lo = blk_lo(b, n, nb), hi = blk_lo(b + 1, n, nb);
+        for (int t = 0; t < nt; ++t) {
+            cpair a = {0.0, 0.0};
+            for (long long i = lo + t; i < hi; i += nt) {
+                double h, r, q;
+                two_prod(x[i], y[i], &h, &r);
+                two_sum(a.p, h, &a.p, &q);
+                a.s = a.s + (q + r);
+            }
+            v[t] = a;
+        }
+        part[b] = ctree(v, nt);
+    }
+    for (int t = 0; t < nt; ++t) {
+        cpair a = {0.0, 0.0};
+        for (int b = t; b < nb; b += nt) a = cmerge(a, part[b]);
+        v[t] = a;
+    }
+    cpair r = ctree(v, nt);
+    free(part); free(v);
+    return r.p + r.s;
+}
+
 /* Dot-product order used by the mixed-precision solvers: the persistent
  * single-mesh kernel's blocked order (nb blocks of nt threads) or the
  * batched kernel's tiled order (nt threads, npt nodes per thread). */
@@ -570,8 +677,12 @@ static float dot32s(const dotspec *ds, int n, const float *x, const float *y)
 static double pdots(int mode, int n, const double *x, const double *y,
                     int nb, int nt)
 {
-    return mode == ORC_DOT_BLOCKED ? orc_dot_blocked(n, x, y, nb, nt)
-                                   : orc_dot(n, x, y);
+    switch (mode) {
+        case ORC_DOT_BLOCKED: return orc_dot_blocked(n, x, y, nb, nt);
+        case ORC_DOT_COMP_SEQUENTIAL: return orc_dot_comp(n, x, y);
+        case ORC_DOT_COMP_BLOCKED: return orc_dot_blocked_comp(n, x, y, nb, nt);
+        default: return orc_dot(n, x, y);
+    }
 }
 
 /* ------------------------------------------------------------------ */

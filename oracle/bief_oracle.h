@@ -31,6 +31,8 @@ extern "C" {
 /* dot-product summation orders */
 #define ORC_DOT_SEQUENTIAL 0 /* dot.f:53, the reference's left-to-right sum */
 #define ORC_DOT_BLOCKED    1 /* the device kernels' fixed block/tree order   */
+#define ORC_DOT_COMP_SEQUENTIAL 2 /* MODASS=3: dot_comp.f (Dot2), sequential  */
+#define ORC_DOT_COMP_BLOCKED    3 /* MODASS=3 in the device kernels' order      */
 
 /* status codes (identical values to the product library's) */
 #define ORC_OK             0
@@ -78,6 +80,9 @@ int orc_matvec(const char *op, int npoin, int nelem,
 double orc_dot(int n, const double *x, const double *y);
 double orc_dot_blocked(int n, const double *x, const double *y,
                        int nblocks, int nthreads);
+double orc_dot_comp(int n, const double *x, const double *y);
+double orc_dot_blocked_comp(int n, const double *x, const double *y,
+                            int nblocks, int nthreads);
 
 int orc_precd1(int npoin, int nelem, const int *ik0, const int *ik1,
                const int *ik2, int precon, double *x, double *dm,
