@@ -413,6 +413,14 @@ def main():
     x_f64 = x.clone()
     nit64 = f64_res[1]
 
+    # binary64 GRACJG with MODASS = 3 (compensated dot products)
+    def run_fp64_comp():
+        x.zero_()
+        return bief.solve(x, A, b, cfg, modass=3)
+
+    c64_ms, c64_kern, c64_res = timed(run_fp64_comp, 2, 1)
+    c64_vs_f64 = float(torch.linalg.norm(x - x_f64) / torch.linalg.norm(x_f64))
+
     # standalone EBE matvec bandwidth (binary64, full diagonal)
     y = P["xt"]
     out = torch.zeros_like(y)
@@ -519,6 +527,9 @@ def main():
                                  "around the Python call",
                        "gbs": mv_gbs, "frac": mv_gbs / hbm, "bytes": by["mv64"],
                        "traffic": traffic.get("k_matvec_bytes_per_launch")},
+            "fp64_modass3": {"ms": sum(c64_ms) / len(c64_ms), "iterations": c64_res[1],
+                             "vs_fp64": c64_vs_f64,
+                             "note": "GRACJG with compensated dot products (MODASS=3)"},
             "fp64_cg": {"kernel": "k_cg64", "gbs": f64_bytes / (f64_kern_ms * 1e-3) / 1e9,
                         "frac": f64_bytes / (f64_kern_ms * 1e-3) / 1e9 / hbm,
                         "bytes_per_iteration": by["it64"], "bytes_per_launch": f64_bytes,
