@@ -56,7 +56,7 @@ extern "C" {
 
 /* Mirror of TYPE(SLVCFG) (bief_def.f:506-532). */
 typedef struct {
-    int    slv;     /* 1 = conjugate gradient; anything else is rejected  */
+    int    slv;     /* 1 CG, 2 RESCJG, 3 EQUNOR, 4 ERRMIN, 5 CGSQUA, 6 CGSTAB, 7 GMRES */
     int    nitmax;  /* maximum number of iterations                        */
     int    precon;  /* 0/1 none, 2 diagonal, 3 (=2 for one matrix), 5 |diag| */
     int    krylov;  /* unused by CG                                        */
@@ -96,9 +96,12 @@ int bief_set_matrix_dev(bief_handle *h, const double *dm, const double *xm,
 /* Read back the stored matrix (e.g. after a mutating solve). */
 int bief_get_matrix(bief_handle *h, double *dm, double *xm, char *typdia);
 
-/* SOLVE(X,A,B,...) for SLV=1 (GRACJG, gracjg.F), SLV=3 (EQUNOR, CG on the
- * normal equations, equnor.f), SLV=6 (CGSTAB, cgstab.f) and SLV=7
- * (GMRES(KRYLOV), gmres.f, KRYLOV 1..20, NITMAX counting restarts): host X
+/* SOLVE(X,A,B,...) for SLV=1 (GRACJG, gracjg.F), SLV=2 (RESCJG, conjugate
+ * residual, rescjg.f), SLV=3 (EQUNOR, CG on the normal equations,
+ * equnor.f), SLV=4 (ERRMIN, minimum error, errmin.f), SLV=5 (CGSQUA,
+ * conjugate gradient squared, cgsqua.f), SLV=6 (CGSTAB, cgstab.f) and
+ * SLV=7 (GMRES(KRYLOV), gmres.f, KRYLOV 1..20, NITMAX counting restarts):
+ * host X
  * (initial guess in, solution out)
  * and B.  relres_out receives the relative residual the method prints
  * (SQRT(RMRM/XL), or NR0/NB for GMRES).  Other SLV values return

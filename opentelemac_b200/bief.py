@@ -194,8 +194,8 @@ class Matrix:
 
 
 def solve(x, A, b, cfg, infogr=False, mutate=False, modass=1):
-    """SOLVE(X,A,B,...,CFG,INFOGR,...) for CFG.slv = 1 (GRACJG), 3 (EQUNOR),
-    6 (CGSTAB) or 7 (GMRES).
+    """SOLVE(X,A,B,...,CFG,INFOGR,...) for CFG.slv = 1 (GRACJG), 2 (RESCJG),
+    3 (EQUNOR), 4 (ERRMIN), 5 (CGSQUA), 6 (CGSTAB) or 7 (GMRES).
 
     x holds the initial guess and receives the solution.  With mutate=True
     the reference's side effects are reproduced: b becomes D.b and A is

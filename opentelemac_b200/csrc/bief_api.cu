@@ -177,6 +177,39 @@ void *equnor_kernel(int td, int sto) {
   return (void *)k_equnor<DIA_0, 1>;
 }
 
+void *rescjg_kernel(int td, int sto) {
+  if (sto == 3) {
+    if (td == DIA_Q) return (void *)k_rescjg<DIA_Q, 3>;
+    if (td == DIA_I) return (void *)k_rescjg<DIA_I, 3>;
+    return (void *)k_rescjg<DIA_0, 3>;
+  }
+  if (td == DIA_Q) return (void *)k_rescjg<DIA_Q, 1>;
+  if (td == DIA_I) return (void *)k_rescjg<DIA_I, 1>;
+  return (void *)k_rescjg<DIA_0, 1>;
+}
+
+void *errmin_kernel(int td, int sto) {
+  if (sto == 3) {
+    if (td == DIA_Q) return (void *)k_errmin<DIA_Q, 3>;
+    if (td == DIA_I) return (void *)k_errmin<DIA_I, 3>;
+    return (void *)k_errmin<DIA_0, 3>;
+  }
+  if (td == DIA_Q) return (void *)k_errmin<DIA_Q, 1>;
+  if (td == DIA_I) return (void *)k_errmin<DIA_I, 1>;
+  return (void *)k_errmin<DIA_0, 1>;
+}
+
+void *cgsqua_kernel(int td, int sto) {
+  if (sto == 3) {
+    if (td == DIA_Q) return (void *)k_cgsqua<DIA_Q, 3>;
+    if (td == DIA_I) return (void *)k_cgsqua<DIA_I, 3>;
+    return (void *)k_cgsqua<DIA_0, 3>;
+  }
+  if (td == DIA_Q) return (void *)k_cgsqua<DIA_Q, 1>;
+  if (td == DIA_I) return (void *)k_cgsqua<DIA_I, 1>;
+  return (void *)k_cgsqua<DIA_0, 1>;
+}
+
 void *gmres_kernel(int td, int sto) {
   if (sto == 3) {
     if (td == DIA_Q) return (void *)k_gmres<DIA_Q, 3>;
@@ -244,6 +277,12 @@ int persistent_grid(int npoin, int nsm, int *out) {
                 gmres_kernel(DIA_Q, 3), gmres_kernel(DIA_I, 3), gmres_kernel(DIA_0, 3),
                 cgstab_kernel(DIA_Q, 1), cgstab_kernel(DIA_I, 1), cgstab_kernel(DIA_0, 1),
                 cgstab_kernel(DIA_Q, 3), cgstab_kernel(DIA_I, 3), cgstab_kernel(DIA_0, 3),
+                rescjg_kernel(DIA_Q, 1), rescjg_kernel(DIA_I, 1), rescjg_kernel(DIA_0, 1),
+                rescjg_kernel(DIA_Q, 3), rescjg_kernel(DIA_I, 3), rescjg_kernel(DIA_0, 3),
+                errmin_kernel(DIA_Q, 1), errmin_kernel(DIA_I, 1), errmin_kernel(DIA_0, 1),
+                errmin_kernel(DIA_Q, 3), errmin_kernel(DIA_I, 3), errmin_kernel(DIA_0, 3),
+                cgsqua_kernel(DIA_Q, 1), cgsqua_kernel(DIA_I, 1), cgsqua_kernel(DIA_0, 1),
+                cgsqua_kernel(DIA_Q, 3), cgsqua_kernel(DIA_I, 3), cgsqua_kernel(DIA_0, 3),
                 cg_kernel(DIA_Q, 1, true), cg_kernel(DIA_I, 1, true), cg_kernel(DIA_0, 1, true),
                 cg_kernel(DIA_Q, 3, true), cg_kernel(DIA_I, 3, true), cg_kernel(DIA_0, 3, true)};
   for (void *k : ks) {
@@ -407,7 +446,7 @@ int build_transposed(bief_handle *h, const double *xm, cudaStream_t st, Sell *ou
 
 int check_cfg(const bief_slvcfg *cfg, int *precon) {
   if (!cfg) return BIEF_ERR_ARGS;
-  if (cfg->slv != 1 && cfg->slv != 3 && cfg->slv != 6 && cfg->slv != 7) return BIEF_ERR_UNSUPPORTED;
+  if (cfg->slv < 1 || cfg->slv > 7) return BIEF_ERR_UNSUPPORTED;
   if (cfg->slv == 7 && (cfg->krylov < 1 || cfg->krylov > GM_MAXK)) return BIEF_ERR_ARGS;
   int p = cfg->precon == 0 ? 1 : cfg->precon;
   if (p <= 0) return BIEF_ERR_ARGS;
@@ -726,8 +765,10 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   }
   if ((st = seg ? build_seg_coefs(h, xm, s) : build_records(h, xm, s))) return st;
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
-  // work vectors beyond the handle's own: 2*KRYLOV for GMRES, 3 for CGSTAB
-  const int nextra = cfg->slv == 7 ? 2 * cfg->krylov : (cfg->slv == 6 ? 3 : 0);
+  // work vectors beyond the handle's own: 2*KRYLOV for GMRES, 3 for CGSTAB,
+  // 1 for CGSQUA
+  const int nextra =
+      cfg->slv == 7 ? 2 * cfg->krylov : (cfg->slv == 6 ? 3 : (cfg->slv == 5 ? 1 : 0));
   if (nextra > 2 * h->gm_k) {
     if (h->d_gmv) cudaFree(h->d_gmv);
     h->d_gmv = nullptr;
@@ -780,6 +821,50 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
     if ((st = launch_coop(h, gmres_kernel(td, h->sto), &P, s))) return st;
+  } else if (cfg->slv == 5) {  // CGSQUA
+    SquaP P;
+    P.npoin = h->npoin;
+    P.nitmax = cfg->nitmax;
+    P.eps = cfg->eps;
+    P.S = sell_of(h);
+    P.da = da;
+    P.dsc = diag ? h->d_dsc : nullptr;
+    P.x = x;
+    P.b = bw;
+    P.g = h->d_r;
+    P.g0 = h->d_gmv;
+    P.p = h->d_d0;
+    P.k = h->d_d1;
+    P.h = h->d_ad;
+    P.hk = h->d_t;
+    P.part = h->d_part;
+    P.ctl = h->d_ctl;
+    P.timeout_ns = h->timeout_ns;
+    CK(cudaEventRecord(h->ev[0], s));
+    if ((st = launch_coop(h, cgsqua_kernel(td, h->sto), &P, s))) return st;
+  } else if (cfg->slv == 2 || cfg->slv == 4) {  // RESCJG, ERRMIN
+    Kry2P P;
+    P.npoin = h->npoin;
+    P.nitmax = cfg->nitmax;
+    P.eps = cfg->eps;
+    P.S = sell_of(h);
+    P.St = P.S;
+    if (cfg->slv == 4 && (st = build_transposed(h, xm, s, &P.St))) return st;
+    P.da = da;
+    P.dsc = diag ? h->d_dsc : nullptr;
+    P.x = x;
+    P.b = bw;
+    P.r = h->d_r;
+    P.d0 = h->d_d0;
+    P.d1 = h->d_d1;
+    P.ad = h->d_ad;
+    P.ag = h->d_t;
+    P.part = h->d_part;
+    P.ctl = h->d_ctl;
+    P.timeout_ns = h->timeout_ns;
+    CK(cudaEventRecord(h->ev[0], s));
+    void *k = cfg->slv == 2 ? rescjg_kernel(td, h->sto) : errmin_kernel(td, h->sto);
+    if ((st = launch_coop(h, k, &P, s))) return st;
   } else if (cfg->slv == 3) {  // EQUNOR
     EqP P;
     P.npoin = h->npoin;
@@ -832,7 +917,10 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   if (relres_out) *relres_out = c.relres;
   if (st >= 0 && ((flags & BIEF_SOLVE_INFOGR) || st > 0))
     print_gracjg(st, c.nit, c.relres, c.relat,
-                 cfg->slv == 3 ? "EQUNOR"
+                 cfg->slv == 2 ? "RESCJG"
+                 : cfg->slv == 3 ? "EQUNOR"
+                 : cfg->slv == 4 ? "ERRMIN"
+                 : cfg->slv == 5 ? "CGSQUA"
                  : cfg->slv == 6 ? "CGSTAB"
                  : cfg->slv == 7 ? "GMRES" : "GRACJG");
   if (diag && (flags & BIEF_SOLVE_MUTATE_INPUTS) && st >= 0) {

@@ -677,6 +677,354 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_equnor(EqP P) {
 }
 
 // ---------------------------------------------------------------------------
+// RESCJG (rescjg.f:134-315, conjugate residual) and ERRMIN (errmin.f:116-259,
+// minimum error) without preconditioning matrices (G aliases R), each as ONE
+// persistent kernel.  Same parameter block; ERRMIN also uses St (the
+// transposed operator) and t (A^T R); the new ERRMIN direction is recomputed
+// at every node that reads it (d0/d1 double-buffered).
+// ---------------------------------------------------------------------------
+struct Kry2P {
+  int npoin, nitmax;
+  double eps;
+  Sell S, St;
+  const double *da, *dsc;
+  double *x;
+  const double *b;
+  double *r, *d0, *d1, *ad, *ag;
+  double *part;
+  Ctl *ctl;
+  long long timeout_ns;
+};
+
+template <int TD, int STO>
+__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_rescjg(Kry2P P) {
+  const int T = blockDim.x, t = threadIdx.x;
+  const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
+  const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
+  double *x = P.x, *r = P.r, *d = P.d0, *ad = P.ad, *ag = P.ag;
+  const double *b = P.b, *da = P.da;
+  const bool lead = (blockIdx.x == 0 && t == 0);
+  double sd[2], rd[2];
+  int nbar = 0;
+  const bool h1 = false;
+  double a1 = 0.0;
+  auto finish = [&](int status, int m, double rmrm, double xl, int relat) {
+    if (P.dsc)
+      for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
+    if (lead) {
+      P.ctl->status = status;
+      P.ctl->nit = m;
+      P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
+      P.ctl->relat = relat;
+    }
+  };
+  sd[0] = 0.0;
+  for (int i = lo + t; i < hi; i += T) sd[0] = add(sd[0], mul(b[i], b[i]));
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  double xl = rd[0];
+  int relat = 1;
+  if (xl < 1.0) { xl = 1.0; relat = 0; }
+  const double tol = mul(xl, mul(P.eps, P.eps));
+  // R = A X - B, RMRM (:144-149)
+  sd[0] = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    double a0 = diag_term<TD>(x[i], da, i);
+    op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
+    const double ri = sub(a0, b[i]);
+    r[i] = ri;
+    sd[0] = add(sd[0], mul(ri, ri));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  double rmrm = rd[0];
+  if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
+  if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }
+  // D = R, AD = A D, D.AD and AD.AD (:178-217)
+  sd[0] = sd[1] = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    const double di = r[i];
+    double a0 = diag_term<TD>(di, da, i);
+    op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return r[j]; });
+    d[i] = di;
+    ad[i] = a0;
+    sd[0] = add(sd[0], mul(di, a0));
+    sd[1] = add(sd[1], mul(a0, a0));
+  }
+  if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  double adad = rd[1];
+  double ro = __ddiv_rn(rd[0], adad);
+  for (int m = 1;; ++m) {
+    // X = X - RO D (:223 / :313), R = R - RO AD (:235), RMRM (:239)
+    const double nro = -ro;
+    sd[0] = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      x[i] = add(x[i], mul(nro, d[i]));
+      const double ri = add(r[i], mul(nro, ad[i]));
+      r[i] = ri;
+      sd[0] = add(sd[0], mul(ri, ri));
+    }
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    rmrm = rd[0];
+    if (isnan(rmrm)) { finish(ST_NAN, m, rmrm, xl, relat); return; }
+    if (rmrm <= tol) { finish(ST_OK, m, rmrm, xl, relat); return; }  // :243
+    // AG = A R (:258), AG.AD (:267)
+    sd[0] = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      double a0 = diag_term<TD>(r[i], da, i);
+      op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return r[j]; });
+      ag[i] = a0;
+      sd[0] = add(sd[0], mul(a0, ad[i]));
+    }
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    const double beta = __ddiv_rn(-rd[0], adad);  // :269
+    // D = BETA D + R, AD = BETA AD + AG (:271-279), R.AD, AD.AD (:303-307)
+    sd[0] = sd[1] = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      d[i] = add(mul(beta, d[i]), r[i]);
+      const double adi = add(mul(beta, ad[i]), ag[i]);
+      ad[i] = adi;
+      sd[0] = add(sd[0], mul(r[i], adi));
+      sd[1] = add(sd[1], mul(adi, adi));
+    }
+    if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    adad = rd[1];
+    ro = __ddiv_rn(rd[0], adad);  // :309
+    if (m >= P.nitmax) {          // :313-315 -- last X update, then stop unconverged
+      const double nr = -ro;
+      for (int i = lo + t; i < hi; i += T) x[i] = add(x[i], mul(nr, d[i]));
+      finish(m, m, rmrm, xl, relat);
+      return;
+    }
+  }
+}
+
+template <int TD, int STO>
+__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_errmin(Kry2P P) {
+  const int T = blockDim.x, t = threadIdx.x;
+  const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
+  const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
+  double *x = P.x, *r = P.r, *ad = P.ad, *atr = P.ag;
+  const double *b = P.b, *da = P.da;
+  const bool lead = (blockIdx.x == 0 && t == 0);
+  double sd[2], rd[2];
+  int nbar = 0;
+  const bool h1 = false;
+  double a1 = 0.0;
+  auto finish = [&](int status, int m, double rmrm, double xl, int relat) {
+    if (P.dsc)
+      for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
+    if (lead) {
+      P.ctl->status = status;
+      P.ctl->nit = m;
+      P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
+      P.ctl->relat = relat;
+    }
+  };
+  sd[0] = 0.0;
+  for (int i = lo + t; i < hi; i += T) sd[0] = add(sd[0], mul(b[i], b[i]));
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  double xl = rd[0];
+  int relat = 1;
+  if (xl < 1.0) { xl = 1.0; relat = 0; }
+  const double tol = mul(xl, mul(P.eps, P.eps));
+  // R = A X - B, RMRM = GMGM (:126-132)
+  sd[0] = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    double a0 = diag_term<TD>(x[i], da, i);
+    op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
+    const double ri = sub(a0, b[i]);
+    r[i] = ri;
+    sd[0] = add(sd[0], mul(ri, ri));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  double rmrm = rd[0], gmgm = rmrm;
+  if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
+  if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }
+  // D = A^T R, D.D (:161-164)
+  double *cur = P.d0, *nxt = P.d1;
+  sd[0] = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    double a0 = diag_term<TD>(r[i], da, i);
+    op_row2<STO>(i, i, h1, a0, a1, P.St, [&](int j) { return r[j]; });
+    cur[i] = a0;
+    sd[0] = add(sd[0], mul(a0, a0));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  double ro = __ddiv_rn(gmgm, rd[0]);  // :176
+  // AD = A D (:170) with the first X and R updates (:182, :194) and RMRM
+  sd[0] = 0.0;
+  {
+    const double nro = -ro;
+    for (int i = lo + t; i < hi; i += T) {
+      double a0 = diag_term<TD>(cur[i], da, i);
+      op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return cur[j]; });
+      ad[i] = a0;
+      x[i] = add(x[i], mul(nro, cur[i]));
+      const double ri = add(r[i], mul(nro, a0));
+      r[i] = ri;
+      sd[0] = add(sd[0], mul(ri, ri));
+    }
+  }
+  for (int m = 1;; ++m) {
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    const double gm1 = gmgm;
+    rmrm = rd[0];
+    gmgm = rmrm;
+    if (isnan(rmrm)) { finish(ST_NAN, m, rmrm, xl, relat); return; }
+    if (rmrm <= tol) { finish(ST_OK, m, rmrm, xl, relat); return; }  // :204
+    // A^T R (:232), then every block needs it at neighbours
+    for (int i = lo + t; i < hi; i += T) {
+      double a0 = diag_term<TD>(r[i], da, i);
+      op_row2<STO>(i, i, h1, a0, a1, P.St, [&](int j) { return r[j]; });
+      atr[i] = a0;
+    }
+    if (!grid_barrier(P.ctl, P.timeout_ns, nbar)) return;
+    const double beta = __ddiv_rn(gmgm, gm1);  // :235
+    // D = BETA D + A^T R (:237-240) where needed, AD = A D (:246), D.D (:252)
+    auto dnew = [&](int j) { return add(mul(beta, cur[j]), atr[j]); };
+    sd[0] = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      const double di = dnew(i);
+      double a0 = diag_term<TD>(di, da, i);
+      op_row2<STO>(i, i, h1, a0, a1, P.S, dnew);
+      nxt[i] = di;
+      ad[i] = a0;
+      sd[0] = add(sd[0], mul(di, di));
+    }
+    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    ro = __ddiv_rn(gmgm, rd[0]);  // :253
+    { double *tmp = cur; cur = nxt; nxt = tmp; }
+    // X = X - RO D (:257), and for the next iteration R = R - RO AD, RMRM
+    const double nro = -ro;
+    if (m >= P.nitmax) {  // :259
+      for (int i = lo + t; i < hi; i += T) x[i] = add(x[i], mul(nro, cur[i]));
+      finish(m, m, rmrm, xl, relat);
+      return;
+    }
+    sd[0] = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      x[i] = add(x[i], mul(nro, cur[i]));
+      const double ri = add(r[i], mul(nro, ad[i]));
+      r[i] = ri;
+      sd[0] = add(sd[0], mul(ri, ri));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CGSQUA (cgsqua.f:151-282, conjugate gradient squared) as ONE persistent
+// kernel: per iteration H = A P with K.G0 and H.G0; then H+K (recomputed at
+// every node that reads it), X, A(H+K), G with G.G and G.G0; then the local
+// P and K updates and a plain grid barrier before the next gather.  GMG0 of
+// an iteration is the previous G.G0 (G does not change in between), and
+// G.G at the start (G0 = G).
+// ---------------------------------------------------------------------------
+struct SquaP {
+  int npoin, nitmax;
+  double eps;
+  Sell S;
+  const double *da, *dsc;
+  double *x;
+  const double *b;
+  double *g, *g0, *p, *k, *h, *hk;
+  double *part;
+  Ctl *ctl;
+  long long timeout_ns;
+};
+
+template <int TD, int STO>
+__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgsqua(SquaP P) {
+  const int T = blockDim.x, t = threadIdx.x;
+  const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
+  const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
+  double *x = P.x, *g = P.g, *g0 = P.g0, *pp = P.p, *kk = P.k, *h = P.h, *hk = P.hk;
+  const double *b = P.b, *da = P.da;
+  const bool lead = (blockIdx.x == 0 && t == 0);
+  double sd[2], rd[2];
+  int nbar = 0;
+  const bool h1 = false;
+  double a1 = 0.0;
+  auto finish = [&](int status, int m, double rl, double xl, int relat) {
+    if (P.dsc)
+      for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
+    if (lead) {
+      P.ctl->status = status;
+      P.ctl->nit = m;
+      P.ctl->relres = __dsqrt_rn(__ddiv_rn(rl, xl));
+      P.ctl->relat = relat;
+    }
+  };
+  sd[0] = 0.0;
+  for (int i = lo + t; i < hi; i += T) sd[0] = add(sd[0], mul(b[i], b[i]));
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  double xl = rd[0];
+  int relat = 1;
+  if (xl < 1.0) { xl = 1.0; relat = 0; }
+  const double tol = mul(mul(P.eps, P.eps), xl);
+  // G = A X - B; G0 = P = K = G (:164-190)
+  sd[0] = 0.0;
+  for (int i = lo + t; i < hi; i += T) {
+    double a0 = diag_term<TD>(x[i], da, i);
+    op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
+    const double gi = sub(a0, b[i]);
+    g[i] = gi;
+    g0[i] = gi;
+    pp[i] = gi;
+    kk[i] = gi;
+    sd[0] = add(sd[0], mul(gi, gi));
+  }
+  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  double rl = rd[0];
+  if (isnan(rl)) { finish(ST_NAN, 0, rl, xl, relat); return; }
+  if (rl < tol) { finish(ST_OK, 0, rl, xl, relat); return; }  // :172
+  double gmg0 = rl;
+  for (int m = 1;; ++m) {
+    // H = A P (:197), K.G0 and H.G0 (:201)
+    sd[0] = sd[1] = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      double a0 = diag_term<TD>(pp[i], da, i);
+      op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return pp[j]; });
+      h[i] = a0;
+      const double gi0 = g0[i];
+      sd[0] = add(sd[0], mul(kk[i], gi0));
+      sd[1] = add(sd[1], mul(a0, gi0));
+    }
+    if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    const double nro = -__ddiv_rn(rd[0], rd[1]);
+    // H+K = -RO H + 2 K (:205-206), X (:211), A(H+K) (:215), G (:224),
+    // G.G (:226) and G.G0 (:258)
+    auto hpk = [&](int j) { return add(mul(nro, h[j]), mul(2.0, kk[j])); };
+    sd[0] = sd[1] = 0.0;
+    for (int i = lo + t; i < hi; i += T) {
+      const double hki = hpk(i);
+      double a0 = diag_term<TD>(hki, da, i);
+      op_row2<STO>(i, i, h1, a0, a1, P.S, hpk);
+      hk[i] = hki;
+      x[i] = add(x[i], mul(nro, hki));
+      const double gi = add(g[i], mul(nro, a0));
+      g[i] = gi;
+      sd[0] = add(sd[0], mul(gi, gi));
+      sd[1] = add(sd[1], mul(gi, g0[i]));
+    }
+    if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    rl = rd[0];
+    if (isnan(rl)) { finish(ST_NAN, m, rl, xl, relat); return; }
+    if (!(rl > tol)) { finish(ST_OK, m, rl, xl, relat); return; }  // :227
+    if (m >= P.nitmax) { finish(m, m, rl, xl, relat); return; }     // :228
+    const double beta = __ddiv_rn(rd[1], gmg0);                      // :262
+    gmg0 = rd[1];
+    const double b2 = mul(beta, beta), tb = mul(2.0, beta);
+    // H = H - K; P = BETA**2 P + G + 2 BETA H; K = G + BETA H (:267-280)
+    for (int i = lo + t; i < hi; i += T) {
+      const double hh = sub(hk[i], kk[i]);
+      const double gi = g[i];
+      pp[i] = add(add(mul(b2, pp[i]), gi), mul(tb, hh));
+      kk[i] = add(gi, mul(beta, hh));
+    }
+    if (!grid_barrier(P.ctl, P.timeout_ns, nbar)) return;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // CGSTAB (cgstab.f:95-200, BiCGSTAB) without Crout preconditioning, as ONE
 // persistent kernel with three grid reductions per iteration: (P.V);
 // (T.S, T.T); (R.R, R.P) -- the last pair gives the convergence test and

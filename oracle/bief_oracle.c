@@ -910,6 +910,196 @@ done:
     return st;
 }
 
+/* rescjg.f:134-315 (conjugate residual) without preconditioning matrices
+ * (G aliases R):  XL = B.B (absolute below 1); R = A X - B; RMRM = R.R; stop
+ * if RMRM < EPS**2 XL; D = R; AD = A D; RO = D.AD / AD.AD; X = X - RO D; per
+ * iteration R = R - RO AD; RMRM = R.R; stop if RMRM <= XL EPS**2;
+ * AG = A R; BETA = -(AG.AD / AD.AD); D = BETA D + R, AD = BETA AD + AG (each
+ * as 'X=CX' then 'X=X+Y'); RO = R.AD / AD.AD; X = X - RO D; NITMAX. */
+static int rescjg_impl(const opmesh *M, int npoin, double *x, const double *da, char typdia,
+                       const double *xm, char typext, const double *b, int nitmax, double eps,
+                       int dot_mode, int nb, int nt, int *nit_out, double *relres_out,
+                       int *relat_out)
+{
+    const int nelem = M->sto == 3 ? 0 : M->nelem;
+    size_t n = (size_t)npoin;
+    double *r = (double *)malloc(sizeof(double) * n), *dd = (double *)malloc(sizeof(double) * n);
+    double *ad = (double *)malloc(sizeof(double) * n), *ag = (double *)malloc(sizeof(double) * n);
+    double *t = (double *)malloc(sizeof(double) * n);
+    double *w = (double *)malloc(sizeof(double) * 3 * (size_t)nelem + 1);
+    int m = 0, st = ORC_OK, relat;
+    double xl, rmrm, dad, adad, agad, gad, ro, beta;
+    if (!r || !dd || !ad || !ag || !t || !w) { st = ORC_ERR_ARGS; goto done; }
+    xl = pdots(dot_mode, npoin, b, b, nb, nt);                          /* :134 */
+    if (xl < 1.0) { xl = 1.0; relat = 0; } else { relat = 1; }
+    st = op_matvec(M, "X=AY    ", npoin, r, da, typdia, xm, typext, x, 0.0, t, w);   /* :144 */
+    if (st) goto done;
+    for (size_t i = 0; i < n; ++i) r[i] = r[i] - b[i];                 /* :146 */
+    rmrm = pdots(dot_mode, npoin, r, r, nb, nt);
+    if (rmrm < eps * eps * xl) goto fin;                                /* :149 */
+    memcpy(dd, r, sizeof(double) * n);                                  /* :178 */
+    st = op_matvec(M, "X=AY    ", npoin, ad, da, typdia, xm, typext, dd, 0.0, t, w); /* :184 */
+    if (st) goto done;
+    dad = pdots(dot_mode, npoin, dd, ad, nb, nt);                       /* :211 */
+    adad = pdots(dot_mode, npoin, ad, ad, nb, nt);                      /* :215 */
+    ro = dad / adad;
+    for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * dd[i];        /* :223 */
+    for (;;) {
+        m = m + 1;                                                      /* :229 */
+        for (size_t i = 0; i < n; ++i) r[i] = r[i] + (-ro) * ad[i];    /* :235 */
+        rmrm = pdots(dot_mode, npoin, r, r, nb, nt);
+        if (rmrm <= xl * (eps * eps)) goto fin;                         /* :243 */
+        st = op_matvec(M, "X=AY    ", npoin, ag, da, typdia, xm, typext, r, 0.0, t, w); /* :258 */
+        if (st) goto done;
+        agad = pdots(dot_mode, npoin, ag, ad, nb, nt);                  /* :267 */
+        beta = -agad / adad;                                            /* :269 */
+        for (size_t i = 0; i < n; ++i) dd[i] = beta * dd[i];           /* :271-272 */
+        for (size_t i = 0; i < n; ++i) dd[i] = dd[i] + r[i];
+        for (size_t i = 0; i < n; ++i) ad[i] = beta * ad[i];           /* :278-279 */
+        for (size_t i = 0; i < n; ++i) ad[i] = ad[i] + ag[i];
+        gad = pdots(dot_mode, npoin, r, ad, nb, nt);                    /* :303 */
+        adad = pdots(dot_mode, npoin, ad, ad, nb, nt);                  /* :307 */
+        ro = gad / adad;
+        for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * dd[i];    /* :313 */
+        if (m >= nitmax) { st = m; goto fin; }                          /* :315 */
+    }
+fin:
+    if (nit_out) *nit_out = m;
+    if (relres_out) *relres_out = sqrt(rmrm / xl);
+    if (relat_out) *relat_out = relat;
+done:
+    free(r); free(dd); free(ad); free(ag); free(t); free(w);
+    return st;
+}
+
+/* errmin.f:116-259 (minimum error) without preconditioning matrices (G
+ * aliases R): XL; R = A X - B; RMRM = GMGM = R.R; stop if RMRM < EPS**2 XL;
+ * D = A^T R; RO = GMGM / D.D; AD = A D; X = X - RO D; per iteration
+ * R = R - RO AD; GM1GM1 = GMGM; RMRM = GMGM = R.R; stop if RMRM <= XL EPS**2;
+ * AD = A^T R; BETA = GMGM/GM1GM1; D = BETA D + AD ('X=CX', 'X=X+Y');
+ * AD = A D; RO = GMGM / D.D; X = X - RO D; NITMAX. */
+static int errmin_impl(const opmesh *M, int npoin, double *x, const double *da, char typdia,
+                       const double *xm, char typext, const double *b, int nitmax, double eps,
+                       int dot_mode, int nb, int nt, int *nit_out, double *relres_out,
+                       int *relat_out)
+{
+    const int nelem = M->sto == 3 ? 0 : M->nelem;
+    size_t n = (size_t)npoin;
+    double *r = (double *)malloc(sizeof(double) * n), *dd = (double *)malloc(sizeof(double) * n);
+    double *ad = (double *)malloc(sizeof(double) * n), *t = (double *)malloc(sizeof(double) * n);
+    double *w = (double *)malloc(sizeof(double) * 3 * (size_t)nelem + 1);
+    int m = 0, st = ORC_OK, relat;
+    double xl, rmrm, gmgm, gm1gm1, tg, ddd, ro, beta;
+    if (!r || !dd || !ad || !t || !w) { st = ORC_ERR_ARGS; goto done; }
+    xl = pdots(dot_mode, npoin, b, b, nb, nt);                          /* :116 */
+    if (xl < 1.0) { xl = 1.0; relat = 0; } else { relat = 1; }
+    st = op_matvec(M, "X=AY    ", npoin, r, da, typdia, xm, typext, x, 0.0, t, w);   /* :126 */
+    if (st) goto done;
+    for (size_t i = 0; i < n; ++i) r[i] = r[i] - b[i];                 /* :128 */
+    rmrm = pdots(dot_mode, npoin, r, r, nb, nt);
+    gmgm = rmrm;
+    if (rmrm < eps * eps * xl) goto fin;                                /* :132 */
+    st = op_matvec(M, "X=TAY   ", npoin, dd, da, typdia, xm, typext, r, 0.0, t, w); /* :161 */
+    if (st) goto done;
+    tg = pdots(dot_mode, npoin, dd, dd, nb, nt);                        /* :164 */
+    st = op_matvec(M, "X=AY    ", npoin, ad, da, typdia, xm, typext, dd, 0.0, t, w); /* :170 */
+    if (st) goto done;
+    ro = gmgm / tg;                                                     /* :176 */
+    for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * dd[i];        /* :182 */
+    for (;;) {
+        m = m + 1;                                                      /* :188 */
+        for (size_t i = 0; i < n; ++i) r[i] = r[i] + (-ro) * ad[i];    /* :194 */
+        gm1gm1 = gmgm;
+        rmrm = pdots(dot_mode, npoin, r, r, nb, nt);                    /* :199 */
+        gmgm = rmrm;
+        if (rmrm <= xl * (eps * eps)) goto fin;                         /* :204 */
+        st = op_matvec(M, "X=TAY   ", npoin, ad, da, typdia, xm, typext, r, 0.0, t, w); /* :232 */
+        if (st) goto done;
+        beta = gmgm / gm1gm1;                                           /* :235 */
+        for (size_t i = 0; i < n; ++i) dd[i] = beta * dd[i];           /* :237 */
+        for (size_t i = 0; i < n; ++i) dd[i] = dd[i] + ad[i];          /* :240 */
+        st = op_matvec(M, "X=AY    ", npoin, ad, da, typdia, xm, typext, dd, 0.0, t, w); /* :246 */
+        if (st) goto done;
+        ddd = pdots(dot_mode, npoin, dd, dd, nb, nt);                   /* :252 */
+        ro = gmgm / ddd;
+        for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * dd[i];    /* :257 */
+        if (m >= nitmax) { st = m; goto fin; }                          /* :259 */
+    }
+fin:
+    if (nit_out) *nit_out = m;
+    if (relres_out) *relres_out = sqrt(rmrm / xl);
+    if (relat_out) *relat_out = relat;
+done:
+    free(r); free(dd); free(ad); free(t); free(w);
+    return st;
+}
+
+/* cgsqua.f:151-282 (conjugate gradient squared):  XL = B.B (absolute below
+ * 1); G = A X - B; RL = G.G; stop if RL < EPS**2 XL; G0 = P = K = G; per
+ * iteration (M from 1): H = A P; RO = K.G0 / H.G0; H = -RO H, H = H + 2 K;
+ * X = X - RO H; AHPK = A H; GMG0 = G.G0; G = G - RO AHPK; RL = G.G; stop if
+ * RL <= EPS**2 XL, or at NITMAX; GMP1G0 = G.G0; BETA = GMP1G0 / GMG0;
+ * H = H - K; P = BETA**2 P, P = P + G, P = P + 2 BETA H; K = G, K = K + BETA H. */
+static int cgsqua_impl(const opmesh *M, int npoin, double *x, const double *da, char typdia,
+                       const double *xm, char typext, const double *b, int nitmax, double eps,
+                       int dot_mode, int nb, int nt, int *nit_out, double *relres_out,
+                       int *relat_out)
+{
+    const int nelem = M->sto == 3 ? 0 : M->nelem;
+    size_t n = (size_t)npoin;
+    double *g = (double *)malloc(sizeof(double) * n), *g0 = (double *)malloc(sizeof(double) * n);
+    double *p = (double *)malloc(sizeof(double) * n), *k = (double *)malloc(sizeof(double) * n);
+    double *h = (double *)malloc(sizeof(double) * n), *ahpk = (double *)malloc(sizeof(double) * n);
+    double *t = (double *)malloc(sizeof(double) * n);
+    double *w = (double *)malloc(sizeof(double) * 3 * (size_t)nelem + 1);
+    int m = 0, st = ORC_OK, relat;
+    double xl, rl, ro, kg0, hg0, gmg0, gmp1g0, beta;
+    if (!g || !g0 || !p || !k || !h || !ahpk || !t || !w) { st = ORC_ERR_ARGS; goto done; }
+    xl = pdots(dot_mode, npoin, b, b, nb, nt);                          /* :151 */
+    if (xl < 1.0) { xl = 1.0; relat = 0; } else { relat = 1; }
+    st = op_matvec(M, "X=AY    ", npoin, g, da, typdia, xm, typext, x, 0.0, t, w);   /* :164 */
+    if (st) goto done;
+    for (size_t i = 0; i < n; ++i) g[i] = g[i] - b[i];                 /* :166 */
+    rl = pdots(dot_mode, npoin, g, g, nb, nt);                          /* :170 */
+    if (rl < eps * eps * xl) goto fin;                                  /* :172 */
+    memcpy(g0, g, sizeof(double) * n);                                  /* :188-190 */
+    memcpy(p, g, sizeof(double) * n);
+    memcpy(k, g, sizeof(double) * n);
+    m = 1;
+    for (;;) {
+        st = op_matvec(M, "X=AY    ", npoin, h, da, typdia, xm, typext, p, 0.0, t, w); /* :197 */
+        if (st) goto done;
+        kg0 = pdots(dot_mode, npoin, k, g0, nb, nt);                    /* :201 */
+        hg0 = pdots(dot_mode, npoin, h, g0, nb, nt);
+        ro = kg0 / hg0;
+        for (size_t i = 0; i < n; ++i) h[i] = (-ro) * h[i];            /* :205 */
+        for (size_t i = 0; i < n; ++i) h[i] = h[i] + 2.0 * k[i];       /* :206 */
+        for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * h[i];     /* :211 */
+        st = op_matvec(M, "X=AY    ", npoin, ahpk, da, typdia, xm, typext, h, 0.0, t, w); /* :215 */
+        if (st) goto done;
+        gmg0 = pdots(dot_mode, npoin, g, g0, nb, nt);                   /* :220 */
+        for (size_t i = 0; i < n; ++i) g[i] = g[i] + (-ro) * ahpk[i];  /* :224 */
+        rl = pdots(dot_mode, npoin, g, g, nb, nt);                      /* :226 */
+        if (!(rl > eps * eps * xl)) goto fin;                           /* :227 */
+        if (m >= nitmax) { st = m; goto fin; }                          /* :228 */
+        m = m + 1;
+        gmp1g0 = pdots(dot_mode, npoin, g, g0, nb, nt);                 /* :258 */
+        beta = gmp1g0 / gmg0;                                           /* :262 */
+        for (size_t i = 0; i < n; ++i) h[i] = h[i] - k[i];             /* :267 */
+        for (size_t i = 0; i < n; ++i) p[i] = (beta * beta) * p[i];    /* :272-274 */
+        for (size_t i = 0; i < n; ++i) p[i] = p[i] + g[i];
+        for (size_t i = 0; i < n; ++i) p[i] = p[i] + (2.0 * beta) * h[i];
+        for (size_t i = 0; i < n; ++i) k[i] = g[i] + beta * h[i];      /* :279-280 */
+    }
+fin:
+    if (nit_out) *nit_out = m;
+    if (relres_out) *relres_out = sqrt(rl / xl);
+    if (relat_out) *relat_out = relat;
+done:
+    free(g); free(g0); free(p); free(k); free(h); free(ahpk); free(t); free(w);
+    return st;
+}
+
 /* cgstab.f:95-200 (BiCGSTAB) without Crout preconditioning:
  *   XL = B.B (absolute below 1); SQRT(XL) < 1e-15: X = 0; V = A X;
  *   R = B - V; RMRM = R.R; stop if RMRM < EPS**2 XL; R = B, R = R - V
@@ -1109,7 +1299,7 @@ static int solve_impl(const opmesh *M, int npoin, double *x, double *b, double *
                       int nitmax, double eps, int krylov, int dot_mode, int nb, int nt,
                       int *nit_out, double *relres_out, int *relat_out)
 {
-    if (slv != 1 && slv != 3 && slv != 6 && slv != 7) return ORC_ERR_UNSUPPORTED;
+    if (slv < 1 || slv > 7) return ORC_ERR_UNSUPPORTED;
     if (precon == 0) precon = 1;
     if (precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 ||
         precon % 17 == 0)
@@ -1124,6 +1314,15 @@ static int solve_impl(const opmesh *M, int npoin, double *x, double *b, double *
     int st = slv == 7
                  ? gmres_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, krylov,
                               dot_mode, nb, nt, nit_out, relres_out, relat_out)
+             : slv == 2
+                 ? rescjg_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
+                               nb, nt, nit_out, relres_out, relat_out)
+             : slv == 4
+                 ? errmin_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
+                               nb, nt, nit_out, relres_out, relat_out)
+             : slv == 5
+                 ? cgsqua_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
+                               nb, nt, nit_out, relres_out, relat_out)
              : slv == 6
                  ? cgstab_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
                                nb, nt, nit_out, relres_out, relat_out)

@@ -169,7 +169,7 @@ def test_edge_cases(oracle_mod):
     mesh = bief.Mesh(p["ik"], n)
     A = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
     with pytest.raises(bief.BiefError) as e:           # method outside the path
-        bief.solve(np.zeros(n), A, p["b"].copy(), cfg(slv=2))
+        bief.solve(np.zeros(n), A, p["b"].copy(), cfg(slv=8))
     assert e.value.status == -5
     with pytest.raises(bief.BiefError) as e:           # Crout preconditioning
         bief.solve(np.zeros(n), A, p["b"].copy(), cfg(precon=14))

@@ -139,7 +139,7 @@ def test_edge_cases(oracle_mod):
         assert r["status"] == 0
         np.testing.assert_allclose(r["x"], p["xt"], rtol=0, atol=1e-6)
     # methods and preconditioners outside this path
-    assert oracle_mod.solve(ik, dm, "Q", xm, "S", b, slv=2)["status"] == -5
+    assert oracle_mod.solve(ik, dm, "Q", xm, "S", b, slv=8)["status"] == -5
     assert oracle_mod.solve(ik, dm, "Q", xm, "S", b, precon=14)["status"] == -5
 
 
