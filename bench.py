@@ -25,6 +25,25 @@ import time
 
 import numpy as np
 
+
+def quiet(fn):
+    """Run fn with the process's stdout (fd 1, C stdio included) discarded,
+    so that the one JSON line stays the only output."""
+    import ctypes
+    libc = ctypes.CDLL(None)
+    sys.stdout.flush()
+    libc.fflush(None)
+    saved = os.dup(1)
+    null = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(null, 1)
+    try:
+        return fn()
+    finally:
+        libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(null)
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -65,12 +84,15 @@ def parse():
 def algorithmic_bytes(npoin, nelem, nseg=None):
     """Algorithmic bytes (each input read once, each output written once)."""
     if nseg is not None:   # segment storage: XA 8 B + GLOSEG 2x4 B per segment
-        return dict(mv64=16 * nseg + 24 * npoin, it64=16 * nseg + 88 * npoin,
+        return dict(mv64=16 * nseg + 24 * npoin, mv32=12 * nseg + 12 * npoin,
+                    it64=16 * nseg + 88 * npoin,
                     it32=12 * nseg + 48 * npoin, upd=16 * nseg + 48 * npoin)
     return dict(
         # EBE matvec 'X=AY' with a full diagonal, binary64: XM 3x8 + IKLE 3x4
         # per element; DM, Y in, X out per node
         mv64=36 * nelem + 24 * npoin,
+        # the same in binary32: XM 3x4 + IKLE 3x4 per element; DM, Y, X
+        mv32=24 * nelem + 12 * npoin,
         # one binary64 GRACJG iteration on the scaled system: matvec without
         # diagonal (36/elem + 16/node) + 9 node-vector accesses (72/node)
         it64=36 * nelem + 88 * npoin,
@@ -413,6 +435,19 @@ def main():
     x_f64 = x.clone()
     nit64 = f64_res[1]
 
+    # how far the binary64 iterates move per CG step where the solve stops:
+    # the iterate one step before the returned one (NITMAX = nit - 2, since
+    # the converged exit skips the last X update) and one step after it
+    # (NITMAX = nit).  A second solution at the same relres cannot be
+    # expected closer to the binary64 one than this.
+    def fp64_at(nitmax):
+        x.zero_()
+        c = bief.SlvCfg(slv=1, nitmax=nitmax, precon=2, krylov=0, eps=1e-30, zero=0.0)
+        quiet(lambda: bief.solve(x, A, b, c))   # NITMAX reached: the message is not ours
+        return float(torch.linalg.norm(x - x_f64) / torch.linalg.norm(x_f64))
+
+    f64_step = {"before_stop": fp64_at(nit64 - 2), "after_stop": fp64_at(nit64)}
+
     # binary64 GRACJG with MODASS = 3 (compensated dot products)
     def run_fp64_comp():
         x.zero_()
@@ -438,6 +473,21 @@ def main():
             mv_lib.append(mesh.last_timing()[1])   # events around the launch itself
     mv_t = statistics.median(mv_lib)
     mv_t_call = statistics.median(mv_ms)
+
+    # the binary32 inner operator's product on the stored matrix (its copy
+    # is built by the first call, outside the timed launches)
+    y32 = y.float()
+    out32 = torch.empty_like(y32)
+    bief.matvec32(out32, A, y32)
+    mv32_lib = []
+    for s in range(args.warmup + 20):
+        flush_l2(s)
+        bief.matvec32(out32, A, y32)
+        torch.cuda.synchronize()
+        if s >= args.warmup:
+            mv32_lib.append(mesh.last_timing()[1])
+    mv32_t = statistics.median(mv32_lib)
+    mv32_err = float(torch.linalg.norm(out32.double() - out) / torch.linalg.norm(out))
 
     # headline: mixed precision, timed steps, clocks sampled meanwhile
     barrier(ws)
@@ -499,6 +549,7 @@ def main():
     achieved = mixed_bytes / (kern_ms * 1e-3) / 1e9
     f64_bytes = nit64 * by["it64"]
     mv_gbs = by["mv64"] / (mv_t * 1e-3) / 1e9
+    mv32_gbs = by["mv32"] / (mv32_t * 1e-3) / 1e9
 
     if rank == 0:
         line = {
@@ -519,7 +570,8 @@ def main():
             "iterations": {"fp64": nit64, "mixed_inner": inner, "mixed_updates": outer},
             "relres": {"mixed": relres, "fp64": f64_res[2]},
             "error": {"mixed_vs_fp64": mixed_vs_f64, "mixed_vs_xtrue": mixed_x_err,
-                      "fp64_vs_xtrue": f64_x_err},
+                      "fp64_vs_xtrue": f64_x_err,
+                      "fp64_one_step_at_stop": f64_step},
             "matvec": {"op": "X=AY binary64 TYPDIA=Q",
                        "kernel": "k_mvseg" if args.storage == "seg" else "k_matvec", "ms": mv_t,
                        "ms_call": mv_t_call,
@@ -527,6 +579,11 @@ def main():
                                  "around the Python call",
                        "gbs": mv_gbs, "frac": mv_gbs / hbm, "bytes": by["mv64"],
                        "traffic": traffic.get("k_matvec_bytes_per_launch")},
+            "matvec32": {"op": "X=AY binary32, the mixed solve's inner operator applied to the "
+                               "stored matrix (coefficients assembled per neighbour)",
+                         "kernel": "k_matvec32", "ms": mv32_t, "gbs": mv32_gbs,
+                         "frac": mv32_gbs / hbm, "bytes": by["mv32"],
+                         "vs_fp64_matvec": mv32_err},
             "fp64_modass3": {"ms": sum(c64_ms) / len(c64_ms), "iterations": c64_res[1],
                              "vs_fp64": c64_vs_f64,
                              "note": "GRACJG with compensated dot products (MODASS=3)"},

@@ -137,6 +137,16 @@ int bief_matvec(bief_handle *h, const char *op, double *x, const double *y,
 int bief_matvec_dev(bief_handle *h, const char *op, double *x,
                     const double *y, double c, void *stream);
 
+/* MATVEC 'X=AY' in binary32 (no reference counterpart: the product of the
+ * mixed-precision inner CG, on the stored matrix): device X and Y of NPOIN
+ * floats, X_i = s_i Y_i + sum_j c_ij (Y_j - Y_i) with binary32 coefficients
+ * assembled per neighbour from the EBE (or segment) matrix and s_i the
+ * binary32 row sum.  The first call after the matrix changed (or after a
+ * mixed solve, which reuses the same buffers) builds that copy; later calls
+ * only run the product.  Symmetric matrices only (BIEF_ERR_UNSUPPORTED
+ * otherwise).  X may alias Y.  Timing through bief_last_timing. */
+int bief_matvec32_dev(bief_handle *h, float *x, const float *y, void *stream);
+
 /* Wave-equation operator A = M + coef_e K_e assembled on the device the way
  * PROPAG assembles AM1 (propag.F:661-677,1407): MT01AA mass (mt01aa.f:82-
  * 103) plus MT02AA P0 diffusion (mt02aa.f:106-149), diagonals assembled by

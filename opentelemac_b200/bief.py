@@ -256,6 +256,20 @@ def matvec(op, x, A, y, c=0.0):
     return x
 
 
+def matvec32(x, A, y):
+    """X = A Y in binary32 on the binary32 copy of A that the mixed-precision
+    inner CG uses (symmetric matrices); x and y are float32 CUDA tensors,
+    x updated in place.  No reference counterpart."""
+    import torch
+    if not (_is_torch(x) and _is_torch(y)) or x.dtype != torch.float32 or y.dtype != torch.float32:
+        raise TypeError("matvec32 takes float32 CUDA tensors")
+    if x.numel() != A.mesh.npoin or y.numel() != A.mesh.npoin:
+        raise ValueError("matvec32: vectors of NPOIN values expected")
+    st = _native.lib().bief_matvec32_dev(A.mesh.handle, _ptr(x), _ptr(y), _stream(x))
+    _check(st, "MATVEC32")
+    return x
+
+
 def diri01(A, nbor, limdir, kdir, fbor, sm, f, maskpt=None):
     """DIRI01 for Dirichlet values on boundary points: nbor is MESH%NBOR
     (1-based), points with limdir == kdir take fbor.  sm and f (and the

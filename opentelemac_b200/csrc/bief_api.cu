@@ -41,6 +41,10 @@ struct bief_handle {
   double *d_gmv = nullptr, *d_gpart = nullptr;
   int gm_k = 0;
   float *d_seg_c = nullptr, *d_s32 = nullptr;
+  // the stored matrix's generation (bumped on every change) and the one the
+  // binary32 copy in d_seg_c / d_sg_c32 / d_s32 was built from (-1: that
+  // copy holds a solve's scaled operator)
+  long long mat_gen = 0, s32_gen = -1;
   long long nrec = 0, nseg = 0;
   int max_nnb = 0;
   // segment storage (STO=3): GLOSEG, per-node incident segments (sliced),
@@ -680,6 +684,7 @@ static int set_matrix_impl(bief_handle *h, const double *dm, const double *xm, c
   h->typext = typext;
   h->has_matrix = 1;
   h->sto = 1;
+  h->mat_gen++;
   return BIEF_OK;
 }
 
@@ -925,6 +930,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
                  : cfg->slv == 7 ? "GMRES" : "GRACJG");
   if (diag && (flags & BIEF_SOLVE_MUTATE_INPUTS) && st >= 0) {
     // SOLVE leaves B = D.B and A = D.A.D with TYPDIA from PRECD1
+    h->mat_gen++;
     CK(cudaMemcpyAsync(b, h->d_bs, sizeof(double) * h->npoin, cudaMemcpyDeviceToDevice, s));
     CK(cudaMemcpyAsync(h->d_dm, h->d_dms, sizeof(double) * h->npoin, cudaMemcpyDeviceToDevice, s));
     if (seg) {
@@ -995,6 +1001,7 @@ int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b, int precon,
       k_build_sg32<DIA_0><<<gn, 256, 0, s>>>(SG_ARGS);
 #undef SG_ARGS
     h->launches++;
+    h->s32_gen = -1;
     CK(cudaGetLastError());
   } else if ((st = build_records(h, xm, s))) {
     return st;
@@ -1011,6 +1018,7 @@ int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b, int precon,
       k_build_seg32<DIA_0><<<gn, 256, 0, s>>>(SEG_ARGS);
 #undef SEG_ARGS
     h->launches++;
+    h->s32_gen = -1;
     CK(cudaGetLastError());
   }
   MixP P;
@@ -1113,6 +1121,56 @@ int bief_matvec(bief_handle *h, const char *op, double *x, const double *y, doub
   return BIEF_OK;
 }
 
+int bief_matvec32_dev(bief_handle *h, float *x, const float *y, void *stream) {
+  if (!h || !x || !y) return BIEF_ERR_ARGS;
+  if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
+  if (h->typext != 'S') return BIEF_ERR_UNSUPPORTED;
+  const bool seg = h->sto == 3;
+  if (!seg && h->max_nnb > MAX_NEIGHBOURS) return BIEF_ERR_SIZE;
+  DevGuard g(h->dev);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int td = typdia_code(h->typdia), gn = grid_for(h->npoin, h->nsm);
+  if (h->s32_gen != h->mat_gen) {  // binary32 copy of the stored matrix
+    int st;
+    if (seg) {
+      if ((st = build_seg_coefs(h, h->d_xa, s))) return st;
+#define SG_ARGS h->npoin, h->d_sg_meta, h->d_sg_off, h->d_sg_c64, h->d_dm, h->d_sg_c32, h->d_s32
+      if (td == DIA_Q)
+        k_build_sg32<DIA_Q><<<gn, 256, 0, s>>>(SG_ARGS);
+      else if (td == DIA_I)
+        k_build_sg32<DIA_I><<<gn, 256, 0, s>>>(SG_ARGS);
+      else
+        k_build_sg32<DIA_0><<<gn, 256, 0, s>>>(SG_ARGS);
+#undef SG_ARGS
+    } else {
+#define SEG_ARGS                                                                               \
+  h->npoin, h->nelem, h->d_ptr, h->d_ek, h->d_xm, h->d_dm, h->d_meta, h->d_rec_off,           \
+      h->d_rec_slot, h->d_seg_off, h->d_seg_c, h->d_s32
+      if (td == DIA_Q)
+        k_build_seg32<DIA_Q><<<gn, 256, 0, s>>>(SEG_ARGS);
+      else if (td == DIA_I)
+        k_build_seg32<DIA_I><<<gn, 256, 0, s>>>(SEG_ARGS);
+      else
+        k_build_seg32<DIA_0><<<gn, 256, 0, s>>>(SEG_ARGS);
+#undef SEG_ARGS
+    }
+    h->launches++;
+    CK(cudaGetLastError());
+    h->s32_gen = h->mat_gen;
+  }
+  if (x == y) {  // as MATVEC, X may alias Y
+    CK(cudaMemcpyAsync(h->d_q, y, sizeof(float) * h->npoin, cudaMemcpyDeviceToDevice, s));
+    y = h->d_q;
+  }
+  CK(cudaEventRecord(h->ev[2], s));
+  k_matvec32<<<gn, 256, 0, s>>>(h->npoin, sell_of(h), y, x);
+  h->launches++;
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(h->ev[3], s));
+  h->mv_pending = 1;
+  return BIEF_OK;
+}
+
 int bief_assemble_wave_dev(bief_handle *h, const double *xc, const double *yc,
                            const double *coef, void *stream) {
   if (!h || !xc || !yc || !coef) return BIEF_ERR_ARGS;
@@ -1131,6 +1189,7 @@ int bief_assemble_wave_dev(bief_handle *h, const double *xc, const double *yc,
   int err = 0;
   CK(cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  h->mat_gen++;
   if (err) return BIEF_ERR_BAD_MESH;
   h->typdia = 'Q';
   h->typext = 'S';
@@ -1238,6 +1297,7 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
       k_build_seg32<DIA_0><<<gn, 256, 0, s>>>(SEG_ARGS);
 #undef SEG_ARGS
     h->launches++;
+    h->s32_gen = -1;
     CK(cudaGetLastError());
   }
   void *k = td == DIA_Q ? (void *)k_batch<DIA_Q>
@@ -1332,6 +1392,7 @@ int bief_diri01_dev(bief_handle *h, int nptfr, const int *nbor, const int *limdi
                                                                 h->d_xm, h->d_xm);
   }
   h->launches += 6;
+  h->mat_gen++;
   CK(cudaGetLastError());
   return BIEF_OK;
 }
@@ -1531,6 +1592,7 @@ static int set_matrix_seg_impl(bief_handle *h, const double *da, const double *x
   h->typext = typext;
   h->has_matrix = 1;
   h->sto = 3;
+  h->mat_gen++;
   return BIEF_OK;
 }
 
@@ -1561,6 +1623,7 @@ int bief_ebe_to_seg(bief_handle *h, void *stream) {
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(s));
   h->sto = 3;
+  h->mat_gen++;
   return BIEF_OK;
 }
 

@@ -63,6 +63,19 @@ __global__ void __launch_bounds__(256) k_matvec(int npoin, int nelem, const int 
   }
 }
 
+// MATVEC 'X=AY' in binary32 (no reference counterpart) on the binary32
+// edge-assembled copy of the operator, the product of the binary32 inner CG:
+// X_i = s_i Y_i + sum_j c_ij (Y_j - Y_i), with s_i the row sum and c_ij the
+// assembled off-diagonal coefficients, slots in sliced order.
+__global__ void __launch_bounds__(256) k_matvec32(int npoin, Sell S, const float *__restrict__ y,
+                                                  float *x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    float a0, a1;
+    seg_row2(i, i, false, __ldg(y + i), 0.0f, a0, a1, S, [&](int k) { return __ldg(y + k); });
+    x[i] = a0;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Segment storage (STO=3).  Per node, one slot per incident segment in
 // ascending segment order (sliced layout: slot m of node i at
