@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-large-matvec", action="store_true",
+                    help="skip the MATVEC measurements on the 2001x2001-node mesh")
     ap.add_argument("--workload", default="wave1m", choices=["wave1m", "batch256"],
                     help="wave1m: the 1M-node solve (default); batch256: 256 independent "
                          "meshes of 2,000-200,000 nodes in one persistent launch per rank")
@@ -489,6 +491,37 @@ def main():
     mv32_t = statistics.median(mv32_lib)
     mv32_err = float(torch.linalg.norm(out32.double() - out) / torch.linalg.norm(out))
 
+    # both MATVECs again on the 2001 x 2001-node mesh (4.0M nodes, 8.0M
+    # triangles: the mixed-precision configuration's size)
+    mv_large = None
+    if args.n < 2001 and not args.no_large_matvec:
+        PL = build_problem(2001, local, "smooth", args.storage)
+        byl = algorithmic_bytes(PL["npoin"], PL["nelem"], PL["nseg"])
+
+        def lib_median(fn, mesh_l):
+            ts = []
+            for s in range(args.warmup + 20):
+                flush_l2(s)
+                fn()
+                torch.cuda.synchronize()
+                if s >= args.warmup:
+                    ts.append(mesh_l.last_timing()[1])
+            return statistics.median(ts)
+
+        yl = PL["xt"]
+        ol = torch.zeros_like(yl)
+        t64 = lib_median(lambda: bief.matvec("X=AY    ", ol, PL["A"], yl), PL["mesh"])
+        y32l = yl.float()
+        o32l = torch.empty_like(y32l)
+        bief.matvec32(o32l, PL["A"], y32l)
+        t32 = lib_median(lambda: bief.matvec32(o32l, PL["A"], y32l), PL["mesh"])
+        mv_large = {"npoin": PL["npoin"], "nelem": PL["nelem"]}
+        for key, t_ms, nb in (("matvec64", t64, byl["mv64"]), ("matvec32", t32, byl["mv32"])):
+            g = nb / (t_ms * 1e-3) / 1e9
+            mv_large[key] = {"ms": t_ms, "bytes": nb, "gbs": g}
+        PL["mesh"].close()
+        del PL, yl, ol, y32l, o32l
+
     # headline: mixed precision, timed steps, clocks sampled meanwhile
     barrier(ws)
     launches0 = mesh.kernel_launches()
@@ -537,6 +570,9 @@ def main():
     except Exception:
         pass
     hbm = float(peaks.get("hbm_gbs", 6650.0))
+    if mv_large:
+        for key in ("matvec64", "matvec32"):
+            mv_large[key]["frac"] = mv_large[key]["gbs"] / hbm
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     traffic = {}
     try:
@@ -584,6 +620,7 @@ def main():
                          "kernel": "k_matvec32", "ms": mv32_t, "gbs": mv32_gbs,
                          "frac": mv32_gbs / hbm, "bytes": by["mv32"],
                          "vs_fp64_matvec": mv32_err},
+            "matvec_2001x2001": mv_large,
             "fp64_modass3": {"ms": sum(c64_ms) / len(c64_ms), "iterations": c64_res[1],
                              "vs_fp64": c64_vs_f64,
                              "note": "GRACJG with compensated dot products (MODASS=3)"},

@@ -155,6 +155,19 @@ int bief_matvec32_dev(bief_handle *h, float *x, const float *y, void *stream);
  * Stores the result as the handle's matrix (TYPDIA 'Q', TYPEXT 'S'). */
 int bief_assemble_wave_dev(bief_handle *h, const double *x, const double *y,
                            const double *coef, void *stream);
+
+/* The general form of the same assembly, as PROPAG's two MATRIX calls build
+ * AM1: 'M=N' MATMAS with XMUL = xmul_mass (propag.F:673-676, mt01aa.f), then
+ * 'M=M+N' with the diffusion matrix of XMUL = xmul_dif (propag.F:1407-1408):
+ *   kind 10  MATDIF, u per element (P0, mt02aa.f:106-149)
+ *   kind 11  MATDIF, u per node (P1, mt02aa.f:244-279)
+ *   kind 12  MATDIFUV, u and v per node (mt02aa.f:200-240): PROPAG's own
+ *            call, with u = DM1, v = HPROP and XMUL = -1.
+ * Device arrays; v is read for kind 12 only.  Stores the result as the
+ * handle's matrix (TYPDIA 'Q', TYPEXT 'S'). */
+int bief_assemble_mass_diff_dev(bief_handle *h, const double *x, const double *y,
+                                double xmul_mass, double xmul_dif, int kind,
+                                const double *u, const double *v, void *stream);
 /* Copy the stored matrix to device arrays dm[npoin] and xm: EBE storage
  * xm[ndiag*nelem] (leading dimension NELEM), segment storage xa[ncol*nseg]. */
 int bief_get_matrix_dev(bief_handle *h, double *dm, double *xm, void *stream);

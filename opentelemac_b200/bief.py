@@ -192,6 +192,19 @@ class Matrix:
         self.typdia, self.typext = "Q", "S"
         return self
 
+    def assemble_mass_diff(self, xc, yc, u, v=None, kind=11, xmul_mass=1.0, xmul_dif=1.0):
+        """AM1 = MT01AA(xmul_mass) + MT02AA(xmul_dif) as PROPAG builds it:
+        kind 10 MATDIF with u per element, 11 MATDIF with u per node, 12
+        MATDIFUV with u and v per node (PROPAG: u = DM1, v = HPROP,
+        xmul_dif = -1).  torch CUDA float64 tensors."""
+        if kind == 12 and v is None:
+            raise ValueError("MATDIFUV needs v")
+        _check(_native.lib().bief_assemble_mass_diff_dev(
+            self.mesh.handle, _ptr(xc), _ptr(yc), float(xmul_mass), float(xmul_dif), int(kind),
+            _ptr(u), None if v is None else _ptr(v), _stream(xc)), "bief_assemble_mass_diff_dev")
+        self.typdia, self.typext = "Q", "S"
+        return self
+
 
 def solve(x, A, b, cfg, infogr=False, mutate=False, modass=1):
     """SOLVE(X,A,B,...,CFG,INFOGR,...) for CFG.slv = 1 (GRACJG), 2 (RESCJG),

@@ -1198,6 +1198,43 @@ int bief_assemble_wave_dev(bief_handle *h, const double *xc, const double *yc,
   return BIEF_OK;
 }
 
+int bief_assemble_mass_diff_dev(bief_handle *h, const double *xc, const double *yc,
+                                double xmul_mass, double xmul_dif, int kind, const double *u,
+                                const double *v, void *stream) {
+  if (!h || !xc || !yc || !u) return BIEF_ERR_ARGS;
+  if (kind != 10 && kind != 11 && kind != 12) return BIEF_ERR_ARGS;
+  if (kind == 12 && !v) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  int st = ensure_matrix_buffers(h);
+  if (st) return st;
+  if (!h->d_ew && (st = dalloc(&h->d_ew, 4 * (size_t)h->nelem))) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(cudaMemsetAsync(h->d_err, 0, sizeof(int), s));
+  const int ge = grid_for(h->nelem, h->nsm);
+#define MD_ARGS h->nelem, h->d_ik, xc, yc, xmul_mass, xmul_dif, u, v, h->d_xm, h->d_ew, h->d_err
+  if (kind == 10)
+    k_mass_diff_elems<10><<<ge, 256, 0, s>>>(MD_ARGS);
+  else if (kind == 11)
+    k_mass_diff_elems<11><<<ge, 256, 0, s>>>(MD_ARGS);
+  else
+    k_mass_diff_elems<12><<<ge, 256, 0, s>>>(MD_ARGS);
+#undef MD_ARGS
+  k_wave_nodes<<<grid_for(h->npoin, h->nsm), 256, 0, s>>>(h->npoin, h->d_ptr, h->d_ek, h->nelem,
+                                                          h->d_ew, h->d_dm);
+  h->launches += 2;
+  CK(cudaGetLastError());
+  int err = 0;
+  CK(cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  h->mat_gen++;
+  if (err) return BIEF_ERR_BAD_MESH;
+  h->typdia = 'Q';
+  h->typext = 'S';
+  h->has_matrix = 1;
+  h->sto = 1;
+  return BIEF_OK;
+}
+
 int bief_wave_coef_grad_dev(bief_handle *h, const double *xc, const double *yc,
                             const double *lambda, const double *x, double *grad, void *stream) {
   if (!h || !xc || !yc || !lambda || !x || !grad) return BIEF_ERR_ARGS;

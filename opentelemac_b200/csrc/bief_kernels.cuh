@@ -45,11 +45,8 @@ __global__ void __launch_bounds__(256) k_matvec(int npoin, int nelem, const int 
                                                 const double *__restrict__ da,
                                                 const double *__restrict__ y, double *x, int opc,
                                                 double c) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
-    double acc = diag_term<TD>(__ldg(y + i), da, i);
-    acc = ebe_row<double, SYM, TRANS>(i, acc, ptr, ek, ik, xm, nelem,
-                                      [&](int j) { return __ldg(y + j); });
-    // OS combination of MESH%T into X (matvec.f:369-380, :329-340)
+  // OS combination of MESH%T into X (matvec.f:369-380, :329-340)
+  auto store = [&](int i, double acc) {
     double r;
     switch (opc) {
       case OP_AY: r = acc; break;
@@ -60,7 +57,12 @@ __global__ void __launch_bounds__(256) k_matvec(int npoin, int nelem, const int 
       default: r = mul(c, acc); break;
     }
     x[i] = r;
-  }
+  };
+  auto vec = [&](int j) { return __ldg(y + j); };
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += stride)
+    store(i, ebe_row<double, SYM, TRANS>(i, diag_term<TD>(__ldg(y + i), da, i), ptr, ek, ik, xm,
+                                         nelem, vec));
 }
 
 // MATVEC 'X=AY' in binary32 (no reference counterpart) on the binary32
@@ -1621,6 +1623,76 @@ __global__ void k_wave_elems(int nelem, const int *__restrict__ ik, const double
     ew[(size_t)nelem + e] = sub(add(apd, bpe), mul(2.0, cpf));
     ew[2 * (size_t)nelem + e] = bpe;
     ew[3 * (size_t)nelem + e] = apd;
+  }
+}
+
+// AM1 = MT01AA(xmul_mass) 'M=N' then 'M=M+N' with MT02AA(xmul_dif), the
+// general form of PROPAG's wave-equation operator (propag.F:673-676,
+// 1407-1408).  KIND 10: MATDIF, U per element (mt02aa.f:106-149); 11:
+// MATDIF, U per node (mt02aa.f:244-279); 12: MATDIFUV, U and V per node
+// (mt02aa.f:200-240).  Same output layout as k_wave_elems (XM summed, the
+// element diagonals of each matrix kept apart for their ASSVEC sums).
+template <int KIND>
+__global__ void k_mass_diff_elems(int nelem, const int *__restrict__ ik,
+                                  const double *__restrict__ xc, const double *__restrict__ yc,
+                                  double xmul_mass, double xmul_dif,
+                                  const double *__restrict__ u, const double *__restrict__ v,
+                                  double *xm, double *ew, int *err) {
+  const double sur12 = __ddiv_rn(xmul_mass, 12.0);  // mt01aa.f:83
+  const double xsur12 = __ddiv_rn(xmul_dif, 12.0);  // mt02aa.f:97
+  const double xsur48 = __ddiv_rn(xmul_dif, 48.0);
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
+    const int i1 = ik[e], i2 = ik[(size_t)nelem + e], i3 = ik[2 * (size_t)nelem + e];
+    const double x1 = xc[i1], y1 = yc[i1];
+    const double X2 = sub(xc[i2], x1), X3 = sub(xc[i3], x1);  // inbief.f:385-391
+    const double Y2 = sub(yc[i2], y1), Y3 = sub(yc[i3], y1);
+    const double surf = mul(0.5, sub(mul(X2, Y3), mul(X3, Y2)));  // surv11.f:63
+    if (sub(mul(X2, Y3), mul(Y2, X3)) < 1.0e-20) atomicExch(err, 1);  // geoelt.f:82
+    const double det = mul(surf, sur12);  // mt01aa.f:91
+    double a11, a22, a33, a12, a13, a23;
+    if (KIND == 10) {
+      const double s2d = __ddiv_rn(mul(xmul_dif, 0.25), surf);
+      const double visc1 = mul(u[e], s2d);
+      const double bpe = mul(visc1, add(mul(Y3, Y3), mul(X3, X3)));
+      const double cpf = mul(visc1, add(mul(Y2, Y3), mul(X2, X3)));
+      const double apd = mul(visc1, add(mul(Y2, Y2), mul(X2, X2)));
+      a11 = sub(add(apd, bpe), mul(2.0, cpf));
+      a22 = bpe;
+      a33 = apd;
+      a12 = sub(cpf, bpe);
+      a13 = sub(cpf, apd);
+      a23 = -cpf;
+    } else {
+      if (KIND == 11) {
+        const double somvx = __ddiv_rn(mul(add(add(u[i1], u[i2]), u[i3]), xsur12), surf);
+        const double x2x3 = add(mul(X2, X3), mul(Y2, Y3));
+        const double x2aux = add(mul(X2, add(-X2, X3)), mul(Y2, add(-Y2, Y3)));
+        const double x3aux = add(mul(X3, add(-X2, X3)), mul(Y3, add(-Y2, Y3)));
+        a12 = -mul(somvx, x3aux);
+        a13 = mul(somvx, x2aux);
+        a23 = -mul(somvx, x2x3);
+      } else {
+        const double g1 = v[i1], g2 = v[i2], g3 = v[i3];
+        const double coef1 = __ddiv_rn(xsur48, surf);
+        const double g123 = add(add(g1, g2), g3);
+        const double coef2 = add(add(mul(u[i1], add(g1, g123)), mul(u[i2], add(g2, g123))),
+                                 mul(u[i3], add(g3, g123)));
+        a12 = mul(mul(add(mul(Y3, sub(Y2, Y3)), mul(X3, sub(X2, X3))), coef2), coef1);
+        a13 = -mul(mul(add(mul(Y2, sub(Y2, Y3)), mul(X2, sub(X2, X3))), coef2), coef1);
+        a23 = -mul(mul(add(mul(Y2, Y3), mul(X2, X3)), coef2), coef1);
+      }
+      a11 = sub(-a12, a13);
+      a22 = sub(-a12, a23);
+      a33 = sub(-a13, a23);
+    }
+    // OM 'M=M+N': XM(mass) + XM(diffusion)
+    xm[e] = add(det, a12);
+    xm[(size_t)nelem + e] = add(det, a13);
+    xm[2 * (size_t)nelem + e] = add(det, a23);
+    ew[e] = add(det, det);
+    ew[(size_t)nelem + e] = a11;
+    ew[2 * (size_t)nelem + e] = a22;
+    ew[3 * (size_t)nelem + e] = a33;
   }
 }
 

@@ -44,6 +44,7 @@ def lib():
         pd, pi = P(d), P(i)
         L.orc_wave_matrix.argtypes = [i, i, pd, pd, pi, pi, pi, pd, pd, pd]
         L.orc_wave_matrix_parts.argtypes = [i, i, pd, pd, pi, pi, pi, pd]
+        L.orc_mass_diff_matrix.argtypes = [i, i, pd, pd, pi, pi, pi, d, d, i, pd, pd, pd, pd]
         L.orc_matvec.argtypes = [ctypes.c_char_p, i, i, pi, pi, pi, pd, pd, c, pd, i, c, pd,
                                  d, pd, pd]
         L.orc_dot.argtypes = [i, pd, pd]
@@ -87,6 +88,26 @@ def wave_matrix(x, y, ikle0, coef):
                                _pd(dm), _pd(xm))
     if st:
         raise ValueError("orc_wave_matrix status %d" % st)
+    return dm, xm
+
+
+def mass_diff_matrix(x, y, ikle0, u, v=None, kind=11, xmul_mass=1.0, xmul_dif=1.0):
+    """AM1 = MT01AA(xmul_mass) + MT02AA(xmul_dif) as PROPAG assembles it:
+    kind 10 MATDIF with u per element, 11 MATDIF with u per node, 12
+    MATDIFUV with u and v per node.  Returns dm (npoin,), xm (3, nelem)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    vv = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+    ik, a, b, c = _cols(ikle0)
+    n, ne = x.size, ik.shape[1]
+    dm = np.empty(n)
+    xm = np.empty((3, ne))
+    st = lib().orc_mass_diff_matrix(n, ne, _pd(x), _pd(y), _pi(a), _pi(b), _pi(c),
+                                    float(xmul_mass), float(xmul_dif), int(kind), _pd(u),
+                                    None if vv is None else _pd(vv), _pd(dm), _pd(xm))
+    if st:
+        raise ValueError("orc_mass_diff_matrix status %d" % st)
     return dm, xm
 
 

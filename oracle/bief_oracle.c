@@ -150,6 +150,115 @@ int orc_wave_matrix(int npoin, int nelem, const double *x, const double *y,
     return ORC_OK;
 }
 
+/* mt02aa.f:244-279: MATDIF with a P1 viscosity U (one value per node),
+ * isotropic:  SOMVX = (U1+U2+U3) XMUL/12 / SURFAC; A12 = -SOMVX X3AUX,
+ * A13 = SOMVX X2AUX, A23 = -SOMVX X2X3; diagonals minus the row's others. */
+void orc_mt02aa_p1(int nelem, double xmul, const double *u,
+                   const int *ik0, const int *ik1, const int *ik2,
+                   const double *xel2, const double *xel3,
+                   const double *yel2, const double *yel3,
+                   const double *surfac,
+                   double *a11, double *a12, double *a13,
+                   double *a22, double *a23, double *a33)
+{
+    const double xsur12 = xmul / 12.0;
+    for (int e = 0; e < nelem; ++e) {
+        double X2 = xel2[e], X3 = xel3[e], Y2 = yel2[e], Y3 = yel3[e];
+        double somvx = (u[ik0[e]] + u[ik1[e]] + u[ik2[e]]) * xsur12 / surfac[e];
+        double x2x3 = X2 * X3 + Y2 * Y3;
+        double x2aux = X2 * (-X2 + X3) + Y2 * (-Y2 + Y3);
+        double x3aux = X3 * (-X2 + X3) + Y3 * (-Y2 + Y3);
+        a12[e] = -(somvx * x3aux);
+        a13[e] = somvx * x2aux;
+        a23[e] = -(somvx * x2x3);
+        a11[e] = -a12[e] - a13[e];
+        a22[e] = -a12[e] - a23[e];
+        a33[e] = -a13[e] - a23[e];
+    }
+}
+
+/* mt02aa.f:200-240: MATDIFUV, U and V both P1:  COEF1 = XMUL/48 / SURFAC;
+ * G123 = V1+V2+V3; COEF2 = sum_k U_k (V_k + G123); off-diagonal terms
+ * geometry * COEF2 * COEF1; diagonals minus the row's others.  PROPAG adds
+ * this to the mass matrix with U = DM1, V = HPROP, XMUL = -1
+ * (propag.F:1407-1408). */
+void orc_mt02aa_uv(int nelem, double xmul, const double *u, const double *v,
+                   const int *ik0, const int *ik1, const int *ik2,
+                   const double *xel2, const double *xel3,
+                   const double *yel2, const double *yel3,
+                   const double *surfac,
+                   double *a11, double *a12, double *a13,
+                   double *a22, double *a23, double *a33)
+{
+    const double xsur48 = xmul / 48.0;
+    for (int e = 0; e < nelem; ++e) {
+        double X2 = xel2[e], X3 = xel3[e], Y2 = yel2[e], Y3 = yel3[e];
+        int i1 = ik0[e], i2 = ik1[e], i3 = ik2[e];
+        double g1 = v[i1], g2 = v[i2], g3 = v[i3];
+        double coef1 = xsur48 / surfac[e];
+        double g123 = g1 + g2 + g3;
+        double coef2 = u[i1] * (g1 + g123) + u[i2] * (g2 + g123) + u[i3] * (g3 + g123);
+        a12[e] = (Y3 * (Y2 - Y3) + X3 * (X2 - X3)) * coef2 * coef1;
+        a13[e] = -((Y2 * (Y2 - Y3) + X2 * (X2 - X3)) * coef2 * coef1);
+        a23[e] = -((Y2 * Y3 + X2 * X3) * coef2 * coef1);
+        a11[e] = -a12[e] - a13[e];
+        a22[e] = -a12[e] - a23[e];
+        a33[e] = -a13[e] - a23[e];
+    }
+}
+
+/* AM1 as PROPAG builds it (propag.F:673-676 then :1407-1408): MATRIX
+ * 'M=N' MATMAS with XMUL = xmul_mass, then 'M=M+N' with the diffusion
+ * matrix of XMUL = xmul_dif; kind 10: MATDIF with U per element
+ * (mt02aa.f:106-149), 11: MATDIF with U per node (:244-279), 12: MATDIFUV
+ * with U and V per node (:200-240).  Diagonals by ASSVEC per matrix, then
+ * OM 'M=M+N' (D and XM added term by term). */
+int orc_mass_diff_matrix(int npoin, int nelem, const double *x, const double *y,
+                         const int *ik0, const int *ik1, const int *ik2,
+                         double xmul_mass, double xmul_dif, int kind,
+                         const double *u, const double *v, double *dm, double *xm)
+{
+    if (kind != 10 && kind != 11 && kind != 12) return ORC_ERR_ARGS;
+    if (kind == 12 && !v) return ORC_ERR_ARGS;
+    double *g = (double *)malloc(sizeof(double) * 5 * (size_t)nelem);
+    double *a = (double *)malloc(sizeof(double) * 6 * (size_t)nelem);
+    double *dn = (double *)malloc(sizeof(double) * (size_t)npoin);
+    if (!g || !a || !dn) { free(g); free(a); free(dn); return ORC_ERR_ARGS; }
+    double *xel2 = g, *xel3 = g + nelem, *yel2 = g + 2 * (size_t)nelem,
+           *yel3 = g + 3 * (size_t)nelem, *surf = g + 4 * (size_t)nelem;
+    int st = orc_geometry(nelem, x, y, ik0, ik1, ik2, xel2, xel3, yel2, yel3,
+                          surf);
+    if (st) { free(g); free(a); free(dn); return st; }
+    double *a11 = a, *a12 = a + nelem, *a13 = a + 2 * (size_t)nelem,
+           *a22 = a + 3 * (size_t)nelem, *a23 = a + 4 * (size_t)nelem,
+           *a33 = a + 5 * (size_t)nelem;
+    orc_mt01aa(nelem, xmul_mass, surf, a11, a12, a13, a22, a23, a33);
+    orc_assvec(dm, npoin, nelem, ik0, ik1, ik2, a11, a22, a33, 1);
+    for (int e = 0; e < nelem; ++e) {
+        xm[e] = a12[e];
+        xm[nelem + e] = a13[e];
+        xm[2 * (size_t)nelem + e] = a23[e];
+    }
+    if (kind == 10)
+        orc_mt02aa_p0(nelem, xmul_dif, u, xel2, xel3, yel2, yel3, surf,
+                      a11, a12, a13, a22, a23, a33);
+    else if (kind == 11)
+        orc_mt02aa_p1(nelem, xmul_dif, u, ik0, ik1, ik2, xel2, xel3, yel2, yel3, surf,
+                      a11, a12, a13, a22, a23, a33);
+    else
+        orc_mt02aa_uv(nelem, xmul_dif, u, v, ik0, ik1, ik2, xel2, xel3, yel2, yel3, surf,
+                      a11, a12, a13, a22, a23, a33);
+    orc_assvec(dn, npoin, nelem, ik0, ik1, ik2, a11, a22, a33, 1);
+    for (int i = 0; i < npoin; ++i) dm[i] = dm[i] + dn[i];
+    for (int e = 0; e < nelem; ++e) {
+        xm[e] = xm[e] + a12[e];
+        xm[nelem + e] = xm[nelem + e] + a13[e];
+        xm[2 * (size_t)nelem + e] = xm[2 * (size_t)nelem + e] + a23[e];
+    }
+    free(g); free(a); free(dn);
+    return ORC_OK;
+}
+
 /* Off-diagonal terms of the unit-coefficient diffusion matrix K_e
  * (mt02aa.f:106-149 with XMUL=1, U=1): kxm[3*nelem] = K12, K13, K23.
  * Used by the adjoint gradient checks. */

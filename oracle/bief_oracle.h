@@ -67,6 +67,27 @@ int orc_wave_matrix(int npoin, int nelem, const double *x, const double *y,
                     const int *ik0, const int *ik1, const int *ik2,
                     const double *coef, double *dm, double *xm);
 
+void orc_mt02aa_p1(int nelem, double xmul, const double *u,
+                   const int *ik0, const int *ik1, const int *ik2,
+                   const double *xel2, const double *xel3,
+                   const double *yel2, const double *yel3,
+                   const double *surfac,
+                   double *a11, double *a12, double *a13,
+                   double *a22, double *a23, double *a33);
+
+void orc_mt02aa_uv(int nelem, double xmul, const double *u, const double *v,
+                   const int *ik0, const int *ik1, const int *ik2,
+                   const double *xel2, const double *xel3,
+                   const double *yel2, const double *yel3,
+                   const double *surfac,
+                   double *a11, double *a12, double *a13,
+                   double *a22, double *a23, double *a33);
+
+int orc_mass_diff_matrix(int npoin, int nelem, const double *x, const double *y,
+                         const int *ik0, const int *ik1, const int *ik2,
+                         double xmul_mass, double xmul_dif, int kind,
+                         const double *u, const double *v, double *dm, double *xm);
+
 int orc_wave_matrix_parts(int npoin, int nelem, const double *x, const double *y,
                           const int *ik0, const int *ik1, const int *ik2,
                           double *kxm);
