@@ -73,9 +73,11 @@ typedef struct bief_handle bief_handle;
                                         = D.A.D (TYPDIA 'I'), as SOLVE does */
 #define BIEF_SOLVE_INFOGR         2  /* print the method's iteration message */
 #define BIEF_SOLVE_MODASS3        4  /* MODASS = 3: compensated dot products
-                                        (dot_comp.f) in GRACJG (SLV=1); fold
-                                        the RHS error vector B%E into B first,
-                                        as SOLVE does (solve.f:546-549) */
+                                        (dot_comp.f), as P_DOTS switches to
+                                        them for every method (p_dots.f:148-
+                                        156); fold the RHS error vector B%E
+                                        into B first, as SOLVE does
+                                        (solve.f:546-549) */
 
 /* Mesh: replaces the MESH%IKLE / NPOIN / NELEM / NELMAX part of BIEF_MESH
  * (bief_def.f:205-498).  Validates IKLE and builds the node->element

@@ -213,7 +213,7 @@ def solve(x, A, b, cfg, infogr=False, mutate=False, modass=1):
     x holds the initial guess and receives the solution.  With mutate=True
     the reference's side effects are reproduced: b becomes D.b and A is
     replaced by D.A.D (TYPDIA 'I').  modass=3 selects compensated dot
-    products (GRACJG only).  Returns (status, nit, relres)."""
+    products (every method).  Returns (status, nit, relres)."""
     L = _native.lib()
     flags = (_native.BIEF_SOLVE_MUTATE_INPUTS if mutate else 0) | (
         _native.BIEF_SOLVE_INFOGR if infogr else 0) | (

@@ -170,71 +170,26 @@ void *cg_kernel(int td, int sto, bool comp = false) {
   return comp ? cg_kernel_t<true>(td, sto) : cg_kernel_t<false>(td, sto);
 }
 
-void *equnor_kernel(int td, int sto) {
-  if (sto == 3) {
-    if (td == DIA_Q) return (void *)k_equnor<DIA_Q, 3>;
-    if (td == DIA_I) return (void *)k_equnor<DIA_I, 3>;
-    return (void *)k_equnor<DIA_0, 3>;
-  }
-  if (td == DIA_Q) return (void *)k_equnor<DIA_Q, 1>;
-  if (td == DIA_I) return (void *)k_equnor<DIA_I, 1>;
-  return (void *)k_equnor<DIA_0, 1>;
-}
+// Kernel of a method for TYPDIA code td, storage sto and dot-product mode
+// (comp: MODASS = 3, compensated)
+#define KSEL1(k, STO_, C_)                                                   \
+  (td == DIA_Q ? (void *)k<DIA_Q, STO_, C_>                                   \
+               : td == DIA_I ? (void *)k<DIA_I, STO_, C_> : (void *)k<DIA_0, STO_, C_>)
+#define KSEL(k)                                                               \
+  (sto == 3 ? (comp ? KSEL1(k, 3, true) : KSEL1(k, 3, false))                 \
+            : (comp ? KSEL1(k, 1, true) : KSEL1(k, 1, false)))
 
-void *rescjg_kernel(int td, int sto) {
-  if (sto == 3) {
-    if (td == DIA_Q) return (void *)k_rescjg<DIA_Q, 3>;
-    if (td == DIA_I) return (void *)k_rescjg<DIA_I, 3>;
-    return (void *)k_rescjg<DIA_0, 3>;
-  }
-  if (td == DIA_Q) return (void *)k_rescjg<DIA_Q, 1>;
-  if (td == DIA_I) return (void *)k_rescjg<DIA_I, 1>;
-  return (void *)k_rescjg<DIA_0, 1>;
-}
+void *equnor_kernel(int td, int sto, bool comp = false) { return KSEL(k_equnor); }
 
-void *errmin_kernel(int td, int sto) {
-  if (sto == 3) {
-    if (td == DIA_Q) return (void *)k_errmin<DIA_Q, 3>;
-    if (td == DIA_I) return (void *)k_errmin<DIA_I, 3>;
-    return (void *)k_errmin<DIA_0, 3>;
-  }
-  if (td == DIA_Q) return (void *)k_errmin<DIA_Q, 1>;
-  if (td == DIA_I) return (void *)k_errmin<DIA_I, 1>;
-  return (void *)k_errmin<DIA_0, 1>;
-}
+void *rescjg_kernel(int td, int sto, bool comp = false) { return KSEL(k_rescjg); }
 
-void *cgsqua_kernel(int td, int sto) {
-  if (sto == 3) {
-    if (td == DIA_Q) return (void *)k_cgsqua<DIA_Q, 3>;
-    if (td == DIA_I) return (void *)k_cgsqua<DIA_I, 3>;
-    return (void *)k_cgsqua<DIA_0, 3>;
-  }
-  if (td == DIA_Q) return (void *)k_cgsqua<DIA_Q, 1>;
-  if (td == DIA_I) return (void *)k_cgsqua<DIA_I, 1>;
-  return (void *)k_cgsqua<DIA_0, 1>;
-}
+void *errmin_kernel(int td, int sto, bool comp = false) { return KSEL(k_errmin); }
 
-void *gmres_kernel(int td, int sto) {
-  if (sto == 3) {
-    if (td == DIA_Q) return (void *)k_gmres<DIA_Q, 3>;
-    if (td == DIA_I) return (void *)k_gmres<DIA_I, 3>;
-    return (void *)k_gmres<DIA_0, 3>;
-  }
-  if (td == DIA_Q) return (void *)k_gmres<DIA_Q, 1>;
-  if (td == DIA_I) return (void *)k_gmres<DIA_I, 1>;
-  return (void *)k_gmres<DIA_0, 1>;
-}
+void *cgsqua_kernel(int td, int sto, bool comp = false) { return KSEL(k_cgsqua); }
 
-void *cgstab_kernel(int td, int sto) {
-  if (sto == 3) {
-    if (td == DIA_Q) return (void *)k_cgstab<DIA_Q, 3>;
-    if (td == DIA_I) return (void *)k_cgstab<DIA_I, 3>;
-    return (void *)k_cgstab<DIA_0, 3>;
-  }
-  if (td == DIA_Q) return (void *)k_cgstab<DIA_Q, 1>;
-  if (td == DIA_I) return (void *)k_cgstab<DIA_I, 1>;
-  return (void *)k_cgstab<DIA_0, 1>;
-}
+void *gmres_kernel(int td, int sto, bool comp = false) { return KSEL(k_gmres); }
+
+void *cgstab_kernel(int td, int sto, bool comp = false) { return KSEL(k_cgstab); }
 
 void *mixed_kernel(int td, int sto) {
   if (sto == 3) {
@@ -288,7 +243,25 @@ int persistent_grid(int npoin, int nsm, int *out) {
                 cgsqua_kernel(DIA_Q, 1), cgsqua_kernel(DIA_I, 1), cgsqua_kernel(DIA_0, 1),
                 cgsqua_kernel(DIA_Q, 3), cgsqua_kernel(DIA_I, 3), cgsqua_kernel(DIA_0, 3),
                 cg_kernel(DIA_Q, 1, true), cg_kernel(DIA_I, 1, true), cg_kernel(DIA_0, 1, true),
-                cg_kernel(DIA_Q, 3, true), cg_kernel(DIA_I, 3, true), cg_kernel(DIA_0, 3, true)};
+                cg_kernel(DIA_Q, 3, true), cg_kernel(DIA_I, 3, true), cg_kernel(DIA_0, 3, true),
+                equnor_kernel(DIA_Q, 1, true), equnor_kernel(DIA_Q, 3, true),
+                rescjg_kernel(DIA_Q, 1, true), rescjg_kernel(DIA_Q, 3, true),
+                errmin_kernel(DIA_Q, 1, true), errmin_kernel(DIA_Q, 3, true),
+                cgsqua_kernel(DIA_Q, 1, true), cgsqua_kernel(DIA_Q, 3, true),
+                cgstab_kernel(DIA_Q, 1, true), cgstab_kernel(DIA_Q, 3, true),
+                equnor_kernel(DIA_I, 1, true), equnor_kernel(DIA_I, 3, true),
+                rescjg_kernel(DIA_I, 1, true), rescjg_kernel(DIA_I, 3, true),
+                errmin_kernel(DIA_I, 1, true), errmin_kernel(DIA_I, 3, true),
+                cgsqua_kernel(DIA_I, 1, true), cgsqua_kernel(DIA_I, 3, true),
+                cgstab_kernel(DIA_I, 1, true), cgstab_kernel(DIA_I, 3, true),
+                equnor_kernel(DIA_0, 1, true), equnor_kernel(DIA_0, 3, true),
+                rescjg_kernel(DIA_0, 1, true), rescjg_kernel(DIA_0, 3, true),
+                errmin_kernel(DIA_0, 1, true), errmin_kernel(DIA_0, 3, true),
+                cgsqua_kernel(DIA_0, 1, true), cgsqua_kernel(DIA_0, 3, true),
+                cgstab_kernel(DIA_0, 1, true), cgstab_kernel(DIA_0, 3, true),
+                gmres_kernel(DIA_Q, 1, true), gmres_kernel(DIA_Q, 3, true),
+                gmres_kernel(DIA_I, 1, true), gmres_kernel(DIA_I, 3, true),
+                gmres_kernel(DIA_0, 1, true), gmres_kernel(DIA_0, 3, true)};
   for (void *k : ks) {
     int bps = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, CG_THREADS, 0));
@@ -605,7 +578,7 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
         (st = dalloc(&h->d_seg_c, nseg)))
       return fail(st);
     if ((st = persistent_grid(npoin, h->nsm, &h->G))) return fail(st);
-    if ((st = dalloc(&h->d_part, 4 * (size_t)h->G + 4))) return fail(st);
+    if ((st = dalloc(&h->d_part, 8 * (size_t)h->G + 4))) return fail(st);
     if ((e = cudaMallocHost((void **)&h->h_ctl, sizeof(Ctl))) != cudaSuccess)
       return fail(cuda_fail(e, "cudaMallocHost", __LINE__));
     if ((e = cudaMemcpyAsync(h->d_ptr, ptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice,
@@ -747,7 +720,6 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
   if (st) return st;
   if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
   const bool comp = (flags & BIEF_SOLVE_MODASS3) != 0;
-  if (comp && cfg->slv != 1) return BIEF_ERR_UNSUPPORTED;
   DevGuard g(h->dev);
   cudaStream_t s = (cudaStream_t)stream;
   const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
@@ -803,9 +775,9 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    if ((st = launch_coop(h, cgstab_kernel(td, h->sto), &P, s))) return st;
+    if ((st = launch_coop(h, cgstab_kernel(td, h->sto, comp), &P, s))) return st;
   } else if (cfg->slv == 7) {  // GMRES
-    if (!h->d_gpart && (st = dalloc(&h->d_gpart, 2 * (size_t)h->G * (GM_MAXK + 1) + 4)))
+    if (!h->d_gpart && (st = dalloc(&h->d_gpart, 4 * (size_t)h->G * (GM_MAXK + 1) + 4)))
       return st;
     GmP P;
     P.npoin = h->npoin;
@@ -825,7 +797,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    if ((st = launch_coop(h, gmres_kernel(td, h->sto), &P, s))) return st;
+    if ((st = launch_coop(h, gmres_kernel(td, h->sto, comp), &P, s))) return st;
   } else if (cfg->slv == 5) {  // CGSQUA
     SquaP P;
     P.npoin = h->npoin;
@@ -846,7 +818,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    if ((st = launch_coop(h, cgsqua_kernel(td, h->sto), &P, s))) return st;
+    if ((st = launch_coop(h, cgsqua_kernel(td, h->sto, comp), &P, s))) return st;
   } else if (cfg->slv == 2 || cfg->slv == 4) {  // RESCJG, ERRMIN
     Kry2P P;
     P.npoin = h->npoin;
@@ -868,7 +840,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    void *k = cfg->slv == 2 ? rescjg_kernel(td, h->sto) : errmin_kernel(td, h->sto);
+    void *k = cfg->slv == 2 ? rescjg_kernel(td, h->sto, comp) : errmin_kernel(td, h->sto, comp);
     if ((st = launch_coop(h, k, &P, s))) return st;
   } else if (cfg->slv == 3) {  // EQUNOR
     EqP P;
@@ -890,7 +862,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    if ((st = launch_coop(h, equnor_kernel(td, h->sto), &P, s))) return st;
+    if ((st = launch_coop(h, equnor_kernel(td, h->sto, comp), &P, s))) return st;
   } else {
     CgP P;
     P.npoin = h->npoin;

@@ -272,6 +272,99 @@ static __device__ __noinline__ bool grid_reduce_comp(Ctl *ctl, double *part, lon
   return true;
 }
 
+// Grid reduction of N compensated dots at once (each value exactly as
+// grid_reduce_comp reduces it); `part` holds 2 halves of G * 2N doubles.
+template <int N>
+__device__ __noinline__ bool grid_reduce_comp_n(Ctl *ctl, double *part, long long timeout_ns,
+                                                int &nbar, const CPair *v, double *out) {
+  __shared__ CPair smc[32];
+  __shared__ double bc[N];
+  __shared__ int s_err;
+  const int G = gridDim.x, T = blockDim.x, t = threadIdx.x;
+  const unsigned long long k = (unsigned long long)(++nbar);
+  double *buf = part + (size_t)(k & 1) * (size_t)G * 2 * N;
+  CPair bp[N];
+#pragma unroll
+  for (int q = 0; q < N; ++q) bp[q] = block_tree_c(v[q], smc);
+  if (t == 0) {
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      buf[((size_t)blockIdx.x * N + q) * 2] = bp[q].p;
+      buf[((size_t)blockIdx.x * N + q) * 2 + 1] = bp[q].s;
+    }
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> cnt(ctl->arrivals);
+    cnt.fetch_add(1ull, cuda::memory_order_release);
+    const unsigned long long target = k * (unsigned long long)G;
+    const unsigned long long t0 = global_ns();
+    s_err = 0;
+    while (cnt.load(cuda::memory_order_acquire) < target) {
+      if ((long long)(global_ns() - t0) > timeout_ns) {
+        s_err = 1;
+        atomicExch(&ctl->status, (int)ST_TIMEOUT);
+        break;
+      }
+      if (SPIN_NS > 0) __nanosleep(SPIN_NS);
+    }
+  }
+  __syncthreads();
+  if (s_err) return false;
+#pragma unroll
+  for (int q = 0; q < N; ++q) {
+    CPair acc{0.0, 0.0};
+    for (int b = t; b < G; b += T)
+      acc = cmerge(acc, CPair{__ldcg(buf + ((size_t)b * N + q) * 2),
+                              __ldcg(buf + ((size_t)b * N + q) * 2 + 1)});
+    const CPair tot = block_tree_c(acc, smc);
+    if (t == 0) bc[q] = add(tot.p, tot.s);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < N; ++q) out[q] = bc[q];
+  __syncthreads();
+  return true;
+}
+
+// N dot products accumulated per thread: plain (MODASS = 1: v += x*y, each
+// operation rounded) or compensated (MODASS = 3: Dot2 pairs), reduced over
+// the grid by dred with the matching tree.
+template <bool COMP, int N>
+struct DotAcc {
+  double v[N];
+  CPair c[N];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int q = 0; q < N; ++q) {
+      v[q] = 0.0;
+      c[q] = CPair{0.0, 0.0};
+    }
+  }
+  __device__ __forceinline__ void acc(int q, double x, double y) {
+    if (COMP)
+      cdot_add(c[q], x, y);
+    else
+      v[q] = add(v[q], mul(x, y));
+  }
+};
+
+template <bool COMP, int N>
+__device__ __forceinline__ bool dred(Ctl *ctl, double *part, long long timeout_ns, int &nbar,
+                                     const DotAcc<COMP, N> &d, double *out) {
+  if constexpr (COMP)
+    return grid_reduce_comp_n<N>(ctl, part, timeout_ns, nbar, d.c, out);
+  else
+    return grid_reduce<N, 0>(ctl, part, timeout_ns, nbar, d.v, nullptr, out, nullptr);
+}
+
+// Only the first of an accumulator's N values.
+template <bool COMP, int N>
+__device__ __forceinline__ bool dred_first(Ctl *ctl, double *part, long long timeout_ns,
+                                           int &nbar, const DotAcc<COMP, N> &d, double *out) {
+  if constexpr (COMP)
+    return grid_reduce_comp_n<1>(ctl, part, timeout_ns, nbar, d.c, out);
+  else
+    return grid_reduce<1, 0>(ctl, part, timeout_ns, nbar, d.v, nullptr, out, nullptr);
+}
+
 // Grid barrier without values: all blocks' preceding writes are visible to
 // every block after it returns true.  Same monotonic counter and bounded
 // wait as grid_reduce (the two may be mixed in one launch).

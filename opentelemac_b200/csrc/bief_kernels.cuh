@@ -567,7 +567,7 @@ struct EqP {
   long long timeout_ns;
 };
 
-template <int TD, int STO>
+template <int TD, int STO, bool COMP>
 __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_equnor(EqP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
@@ -575,7 +575,8 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_equnor(EqP P) {
   double *x = P.x, *r = P.r, *ad = P.ad, *atr = P.t;
   const double *b = P.b, *da = P.da;
   const bool lead = (blockIdx.x == 0 && t == 0);
-  double s, red;
+  DotAcc<COMP, 1> s;
+  double red;
   int nbar = 0;
   const bool h1 = false;
 
@@ -592,48 +593,48 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_equnor(EqP P) {
   double a1 = 0.0;
 
   // XL = P_DOTS(B,B), absolute mode below 1 (equnor.f:108-114)
-  s = 0.0;
-  for (int i = lo + t; i < hi; i += T) s = add(s, mul(b[i], b[i]));
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  s.zero();
+  for (int i = lo + t; i < hi; i += T) s.acc(0, b[i], b[i]);
+  if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
   double xl = red;
   int relat = 1;
   if (xl < 1.0) { xl = 1.0; relat = 0; }
   const double tol = mul(xl, mul(P.eps, P.eps));
 
   // R = A X - B, RMRM (:118-123)
-  s = 0.0;
+  s.zero();
   for (int i = lo + t; i < hi; i += T) {
     double a0 = diag_term<TD>(x[i], da, i);
     op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
     const double r0 = sub(a0, b[i]);
     r[i] = r0;
-    s = add(s, mul(r0, r0));
+    s.acc(0, r0, r0);
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
   double rmrm = red;
   if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
   if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }  // :127
 
   // D = A^T R, TGMTGM (:160-163)
   double *cur = P.d0, *nxt = P.d1;
-  s = 0.0;
+  s.zero();
   for (int i = lo + t; i < hi; i += T) {
     double a0 = diag_term<TD>(r[i], da, i);
     op_row2<STO>(i, i, h1, a0, a1, P.St, [&](int j) { return r[j]; });
     cur[i] = a0;
-    s = add(s, mul(a0, a0));
+    s.acc(0, a0, a0);
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
   double tg = red;
   // AD = A D, ADAD, RO (:169-189)
-  s = 0.0;
+  s.zero();
   for (int i = lo + t; i < hi; i += T) {
     double a0 = diag_term<TD>(cur[i], da, i);
     op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return cur[j]; });
     ad[i] = a0;
-    s = add(s, mul(a0, a0));
+    s.acc(0, a0, a0);
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
   double adad = red;
   if (!(adad > 0.0)) { finish(isnan(adad) ? ST_NAN : ST_BREAKDOWN, 0, rmrm, xl, relat); return; }
   double ro = __ddiv_rn(tg, adad);
@@ -641,42 +642,42 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_equnor(EqP P) {
   for (int m = 1;; ++m) {
     // X = X - RO D (:195 / :278), R = R - RO AD (:207), RMRM (:211)
     const double nro = -ro;
-    s = 0.0;
+    s.zero();
     for (int i = lo + t; i < hi; i += T) {
       x[i] = add(x[i], mul(nro, cur[i]));
       const double ri = add(r[i], mul(nro, ad[i]));
       r[i] = ri;
-      s = add(s, mul(ri, ri));
+      s.acc(0, ri, ri);
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+    if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
     rmrm = red;
     if (isnan(rmrm)) { finish(ST_NAN, m, rmrm, xl, relat); return; }
     if (rmrm <= tol) { finish(ST_OK, m, rmrm, xl, relat); return; }  // :215
 
     // A^T R (:240), TGMTGM (:244)
-    s = 0.0;
+    s.zero();
     for (int i = lo + t; i < hi; i += T) {
       double a0 = diag_term<TD>(r[i], da, i);
       op_row2<STO>(i, i, h1, a0, a1, P.St, [&](int j) { return r[j]; });
       atr[i] = a0;
-      s = add(s, mul(a0, a0));
+      s.acc(0, a0, a0);
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+    if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
     const double tg1 = tg;
     tg = red;
     const double beta = __ddiv_rn(tg, tg1);  // :245
 
     // D = BETA D + A^T R (:247-250) where needed, AD = A D (:256), ADAD (:272)
-    s = 0.0;
+    s.zero();
     for (int i = lo + t; i < hi; i += T) {
       const double di = add(mul(beta, cur[i]), atr[i]);
       nxt[i] = di;
       double a0 = diag_term<TD>(di, da, i);
       op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return add(mul(beta, cur[j]), atr[j]); });
       ad[i] = a0;
-      s = add(s, mul(a0, a0));
+      s.acc(0, a0, a0);
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+    if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
     adad = red;
     if (!(adad > 0.0)) { finish(isnan(adad) ? ST_NAN : ST_BREAKDOWN, m, rmrm, xl, relat); return; }
     ro = __ddiv_rn(tg, adad);  // :274
@@ -711,7 +712,7 @@ struct Kry2P {
   long long timeout_ns;
 };
 
-template <int TD, int STO>
+template <int TD, int STO, bool COMP>
 __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_rescjg(Kry2P P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
@@ -719,7 +720,8 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_rescjg(Kry2P P) {
   double *x = P.x, *r = P.r, *d = P.d0, *ad = P.ad, *ag = P.ag;
   const double *b = P.b, *da = P.da;
   const bool lead = (blockIdx.x == 0 && t == 0);
-  double sd[2], rd[2];
+  DotAcc<COMP, 2> sd;
+  double rd[2];
   int nbar = 0;
   const bool h1 = false;
   double a1 = 0.0;
@@ -733,74 +735,74 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_rescjg(Kry2P P) {
       P.ctl->relat = relat;
     }
   };
-  sd[0] = 0.0;
-  for (int i = lo + t; i < hi; i += T) sd[0] = add(sd[0], mul(b[i], b[i]));
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  sd.zero();
+  for (int i = lo + t; i < hi; i += T) sd.acc(0, b[i], b[i]);
+  if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
   double xl = rd[0];
   int relat = 1;
   if (xl < 1.0) { xl = 1.0; relat = 0; }
   const double tol = mul(xl, mul(P.eps, P.eps));
   // R = A X - B, RMRM (:144-149)
-  sd[0] = 0.0;
+  sd.zero();
   for (int i = lo + t; i < hi; i += T) {
     double a0 = diag_term<TD>(x[i], da, i);
     op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
     const double ri = sub(a0, b[i]);
     r[i] = ri;
-    sd[0] = add(sd[0], mul(ri, ri));
+    sd.acc(0, ri, ri);
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
   double rmrm = rd[0];
   if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
   if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }
   // D = R, AD = A D, D.AD and AD.AD (:178-217)
-  sd[0] = sd[1] = 0.0;
+  sd.zero();
   for (int i = lo + t; i < hi; i += T) {
     const double di = r[i];
     double a0 = diag_term<TD>(di, da, i);
     op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return r[j]; });
     d[i] = di;
     ad[i] = a0;
-    sd[0] = add(sd[0], mul(di, a0));
-    sd[1] = add(sd[1], mul(a0, a0));
+    sd.acc(0, di, a0);
+    sd.acc(1, a0, a0);
   }
-  if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  if (!dred<COMP, 2>(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
   double adad = rd[1];
   double ro = __ddiv_rn(rd[0], adad);
   for (int m = 1;; ++m) {
     // X = X - RO D (:223 / :313), R = R - RO AD (:235), RMRM (:239)
     const double nro = -ro;
-    sd[0] = 0.0;
+    sd.zero();
     for (int i = lo + t; i < hi; i += T) {
       x[i] = add(x[i], mul(nro, d[i]));
       const double ri = add(r[i], mul(nro, ad[i]));
       r[i] = ri;
-      sd[0] = add(sd[0], mul(ri, ri));
+      sd.acc(0, ri, ri);
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
     rmrm = rd[0];
     if (isnan(rmrm)) { finish(ST_NAN, m, rmrm, xl, relat); return; }
     if (rmrm <= tol) { finish(ST_OK, m, rmrm, xl, relat); return; }  // :243
     // AG = A R (:258), AG.AD (:267)
-    sd[0] = 0.0;
+    sd.zero();
     for (int i = lo + t; i < hi; i += T) {
       double a0 = diag_term<TD>(r[i], da, i);
       op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return r[j]; });
       ag[i] = a0;
-      sd[0] = add(sd[0], mul(a0, ad[i]));
+      sd.acc(0, a0, ad[i]);
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
     const double beta = __ddiv_rn(-rd[0], adad);  // :269
     // D = BETA D + R, AD = BETA AD + AG (:271-279), R.AD, AD.AD (:303-307)
-    sd[0] = sd[1] = 0.0;
+    sd.zero();
     for (int i = lo + t; i < hi; i += T) {
       d[i] = add(mul(beta, d[i]), r[i]);
       const double adi = add(mul(beta, ad[i]), ag[i]);
       ad[i] = adi;
-      sd[0] = add(sd[0], mul(r[i], adi));
-      sd[1] = add(sd[1], mul(adi, adi));
+      sd.acc(0, r[i], adi);
+      sd.acc(1, adi, adi);
     }
-    if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    if (!dred<COMP, 2>(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
     adad = rd[1];
     ro = __ddiv_rn(rd[0], adad);  // :309
     if (m >= P.nitmax) {          // :313-315 -- last X update, then stop unconverged
@@ -812,7 +814,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_rescjg(Kry2P P) {
   }
 }
 
-template <int TD, int STO>
+template <int TD, int STO, bool COMP>
 __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_errmin(Kry2P P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
@@ -820,7 +822,8 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_errmin(Kry2P P) {
   double *x = P.x, *r = P.r, *ad = P.ad, *atr = P.ag;
   const double *b = P.b, *da = P.da;
   const bool lead = (blockIdx.x == 0 && t == 0);
-  double sd[2], rd[2];
+  DotAcc<COMP, 2> sd;
+  double rd[2];
   int nbar = 0;
   const bool h1 = false;
   double a1 = 0.0;
@@ -834,39 +837,39 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_errmin(Kry2P P) {
       P.ctl->relat = relat;
     }
   };
-  sd[0] = 0.0;
-  for (int i = lo + t; i < hi; i += T) sd[0] = add(sd[0], mul(b[i], b[i]));
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  sd.zero();
+  for (int i = lo + t; i < hi; i += T) sd.acc(0, b[i], b[i]);
+  if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
   double xl = rd[0];
   int relat = 1;
   if (xl < 1.0) { xl = 1.0; relat = 0; }
   const double tol = mul(xl, mul(P.eps, P.eps));
   // R = A X - B, RMRM = GMGM (:126-132)
-  sd[0] = 0.0;
+  sd.zero();
   for (int i = lo + t; i < hi; i += T) {
     double a0 = diag_term<TD>(x[i], da, i);
     op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
     const double ri = sub(a0, b[i]);
     r[i] = ri;
-    sd[0] = add(sd[0], mul(ri, ri));
+    sd.acc(0, ri, ri);
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
   double rmrm = rd[0], gmgm = rmrm;
   if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
   if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }
   // D = A^T R, D.D (:161-164)
   double *cur = P.d0, *nxt = P.d1;
-  sd[0] = 0.0;
+  sd.zero();
   for (int i = lo + t; i < hi; i += T) {
     double a0 = diag_term<TD>(r[i], da, i);
     op_row2<STO>(i, i, h1, a0, a1, P.St, [&](int j) { return r[j]; });
     cur[i] = a0;
-    sd[0] = add(sd[0], mul(a0, a0));
+    sd.acc(0, a0, a0);
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
   double ro = __ddiv_rn(gmgm, rd[0]);  // :176
   // AD = A D (:170) with the first X and R updates (:182, :194) and RMRM
-  sd[0] = 0.0;
+  sd.zero();
   {
     const double nro = -ro;
     for (int i = lo + t; i < hi; i += T) {
@@ -876,11 +879,11 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_errmin(Kry2P P) {
       x[i] = add(x[i], mul(nro, cur[i]));
       const double ri = add(r[i], mul(nro, a0));
       r[i] = ri;
-      sd[0] = add(sd[0], mul(ri, ri));
+      sd.acc(0, ri, ri);
     }
   }
   for (int m = 1;; ++m) {
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
     const double gm1 = gmgm;
     rmrm = rd[0];
     gmgm = rmrm;
@@ -896,16 +899,16 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_errmin(Kry2P P) {
     const double beta = __ddiv_rn(gmgm, gm1);  // :235
     // D = BETA D + A^T R (:237-240) where needed, AD = A D (:246), D.D (:252)
     auto dnew = [&](int j) { return add(mul(beta, cur[j]), atr[j]); };
-    sd[0] = 0.0;
+    sd.zero();
     for (int i = lo + t; i < hi; i += T) {
       const double di = dnew(i);
       double a0 = diag_term<TD>(di, da, i);
       op_row2<STO>(i, i, h1, a0, a1, P.S, dnew);
       nxt[i] = di;
       ad[i] = a0;
-      sd[0] = add(sd[0], mul(di, di));
+      sd.acc(0, di, di);
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
     ro = __ddiv_rn(gmgm, rd[0]);  // :253
     { double *tmp = cur; cur = nxt; nxt = tmp; }
     // X = X - RO D (:257), and for the next iteration R = R - RO AD, RMRM
@@ -915,12 +918,12 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_errmin(Kry2P P) {
       finish(m, m, rmrm, xl, relat);
       return;
     }
-    sd[0] = 0.0;
+    sd.zero();
     for (int i = lo + t; i < hi; i += T) {
       x[i] = add(x[i], mul(nro, cur[i]));
       const double ri = add(r[i], mul(nro, ad[i]));
       r[i] = ri;
-      sd[0] = add(sd[0], mul(ri, ri));
+      sd.acc(0, ri, ri);
     }
   }
 }
@@ -946,7 +949,7 @@ struct SquaP {
   long long timeout_ns;
 };
 
-template <int TD, int STO>
+template <int TD, int STO, bool COMP>
 __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgsqua(SquaP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
@@ -954,7 +957,8 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgsqua(SquaP P) {
   double *x = P.x, *g = P.g, *g0 = P.g0, *pp = P.p, *kk = P.k, *h = P.h, *hk = P.hk;
   const double *b = P.b, *da = P.da;
   const bool lead = (blockIdx.x == 0 && t == 0);
-  double sd[2], rd[2];
+  DotAcc<COMP, 2> sd;
+  double rd[2];
   int nbar = 0;
   const bool h1 = false;
   double a1 = 0.0;
@@ -968,15 +972,15 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgsqua(SquaP P) {
       P.ctl->relat = relat;
     }
   };
-  sd[0] = 0.0;
-  for (int i = lo + t; i < hi; i += T) sd[0] = add(sd[0], mul(b[i], b[i]));
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  sd.zero();
+  for (int i = lo + t; i < hi; i += T) sd.acc(0, b[i], b[i]);
+  if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
   double xl = rd[0];
   int relat = 1;
   if (xl < 1.0) { xl = 1.0; relat = 0; }
   const double tol = mul(mul(P.eps, P.eps), xl);
   // G = A X - B; G0 = P = K = G (:164-190)
-  sd[0] = 0.0;
+  sd.zero();
   for (int i = lo + t; i < hi; i += T) {
     double a0 = diag_term<TD>(x[i], da, i);
     op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
@@ -985,30 +989,30 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgsqua(SquaP P) {
     g0[i] = gi;
     pp[i] = gi;
     kk[i] = gi;
-    sd[0] = add(sd[0], mul(gi, gi));
+    sd.acc(0, gi, gi);
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
   double rl = rd[0];
   if (isnan(rl)) { finish(ST_NAN, 0, rl, xl, relat); return; }
   if (rl < tol) { finish(ST_OK, 0, rl, xl, relat); return; }  // :172
   double gmg0 = rl;
   for (int m = 1;; ++m) {
     // H = A P (:197), K.G0 and H.G0 (:201)
-    sd[0] = sd[1] = 0.0;
+    sd.zero();
     for (int i = lo + t; i < hi; i += T) {
       double a0 = diag_term<TD>(pp[i], da, i);
       op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return pp[j]; });
       h[i] = a0;
       const double gi0 = g0[i];
-      sd[0] = add(sd[0], mul(kk[i], gi0));
-      sd[1] = add(sd[1], mul(a0, gi0));
+      sd.acc(0, kk[i], gi0);
+      sd.acc(1, a0, gi0);
     }
-    if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    if (!dred<COMP, 2>(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
     const double nro = -__ddiv_rn(rd[0], rd[1]);
     // H+K = -RO H + 2 K (:205-206), X (:211), A(H+K) (:215), G (:224),
     // G.G (:226) and G.G0 (:258)
     auto hpk = [&](int j) { return add(mul(nro, h[j]), mul(2.0, kk[j])); };
-    sd[0] = sd[1] = 0.0;
+    sd.zero();
     for (int i = lo + t; i < hi; i += T) {
       const double hki = hpk(i);
       double a0 = diag_term<TD>(hki, da, i);
@@ -1017,10 +1021,10 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgsqua(SquaP P) {
       x[i] = add(x[i], mul(nro, hki));
       const double gi = add(g[i], mul(nro, a0));
       g[i] = gi;
-      sd[0] = add(sd[0], mul(gi, gi));
-      sd[1] = add(sd[1], mul(gi, g0[i]));
+      sd.acc(0, gi, gi);
+      sd.acc(1, gi, g0[i]);
     }
-    if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    if (!dred<COMP, 2>(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
     rl = rd[0];
     if (isnan(rl)) { finish(ST_NAN, m, rl, xl, relat); return; }
     if (!(rl > tol)) { finish(ST_OK, m, rl, xl, relat); return; }  // :227
@@ -1060,7 +1064,7 @@ struct StabP {
   long long timeout_ns;
 };
 
-template <int TD, int STO>
+template <int TD, int STO, bool COMP>
 __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgstab(StabP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
@@ -1068,7 +1072,8 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgstab(StabP P) {
   double *x = P.x, *r = P.r, *p = P.p, *sv = P.s, *tv = P.t;
   const double *b = P.b, *da = P.da;
   const bool lead = (blockIdx.x == 0 && t == 0);
-  double sd[2], rd[2];
+  DotAcc<COMP, 2> sd;
+  double rd[2];
   int nbar = 0;
   const bool h1 = false;
   double a1 = 0.0;
@@ -1085,9 +1090,9 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgstab(StabP P) {
   };
 
   // XL (:105-111); SQRT(XL) < RMIN: X = 0 (:112-116)
-  sd[0] = 0.0;
-  for (int i = lo + t; i < hi; i += T) sd[0] = add(sd[0], mul(b[i], b[i]));
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  sd.zero();
+  for (int i = lo + t; i < hi; i += T) sd.acc(0, b[i], b[i]);
+  if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
   double xl = rd[0];
   int relat = 1;
   if (xl < 1.0) { xl = 1.0; relat = 0; }
@@ -1099,7 +1104,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgstab(StabP P) {
   const double tol = mul(xl, mul(P.eps, P.eps));
   // V = A X, R = B - V, RMRM (:120-123); P = R, V = Q = 0 (:144-147)
   double *qc = P.q0, *qn = P.q1, *vc = P.v0, *vn = P.v1;
-  sd[0] = 0.0;
+  sd.zero();
   for (int i = lo + t; i < hi; i += T) {
     double a0 = diag_term<TD>(x[i], da, i);
     op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
@@ -1108,9 +1113,9 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgstab(StabP P) {
     p[i] = ri;
     qc[i] = 0.0;
     vc[i] = 0.0;
-    sd[0] = add(sd[0], mul(ri, ri));
+    sd.acc(0, ri, ri);
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+  if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
   double rmrm = rd[0];
   if (isnan(rmrm)) { finish(ST_NAN, 0, rmrm, xl, relat); return; }
   if (rmrm < mul(mul(P.eps, P.eps), xl)) { finish(ST_OK, 0, rmrm, xl, relat); return; }
@@ -1124,46 +1129,44 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgstab(StabP P) {
     const double nomeg2 = -omeg2;
     // Q = R + OMEG Q - OMEG2 V (:161-162), V = A Q (:163), P.V (:173)
     auto qnew = [&](int j) { return add(add(r[j], mul(omeg, qc[j])), mul(nomeg2, vc[j])); };
-    sd[0] = 0.0;
+    sd.zero();
     for (int i = lo + t; i < hi; i += T) {
       const double qi = qnew(i);
       double a0 = diag_term<TD>(qi, da, i);
       op_row2<STO>(i, i, h1, a0, a1, P.S, qnew);
       qn[i] = qi;
       vn[i] = a0;
-      sd[0] = add(sd[0], mul(p[i], a0));
+      sd.acc(0, p[i], a0);
     }
-    if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    if (!dred_first(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
     omeg1 = __ddiv_rn(beta1, rd[0]);  // :174
     { double *tmp = qc; qc = qn; qn = tmp; tmp = vc; vc = vn; vn = tmp; }
     // S = R - OMEG1 V (:176), T = A S (:177), T.S and T.T (:186-187)
     const double nomeg1 = -omeg1;
     auto snew = [&](int j) { return add(r[j], mul(nomeg1, vc[j])); };
-    sd[0] = 0.0;
-    sd[1] = 0.0;
+    sd.zero();
     for (int i = lo + t; i < hi; i += T) {
       const double si = snew(i);
       double a0 = diag_term<TD>(si, da, i);
       op_row2<STO>(i, i, h1, a0, a1, P.S, snew);
       sv[i] = si;
       tv[i] = a0;
-      sd[0] = add(sd[0], mul(a0, si));
-      sd[1] = add(sd[1], mul(a0, a0));
+      sd.acc(0, a0, si);
+      sd.acc(1, a0, a0);
     }
-    if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    if (!dred<COMP, 2>(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
     alfa = __ddiv_rn(rd[0], rd[1]);  // :188
     // X = X + OMEG1 Q + ALFA S (:190-191), R = S - ALFA T (:192), R.R and R.P
     const double nalfa = -alfa;
-    sd[0] = 0.0;
-    sd[1] = 0.0;
+    sd.zero();
     for (int i = lo + t; i < hi; i += T) {
       x[i] = add(add(x[i], mul(omeg1, qc[i])), mul(alfa, sv[i]));
       const double ri = add(sv[i], mul(nalfa, tv[i]));
       r[i] = ri;
-      sd[0] = add(sd[0], mul(ri, ri));
-      sd[1] = add(sd[1], mul(ri, p[i]));
+      sd.acc(0, ri, ri);
+      sd.acc(1, ri, p[i]);
     }
-    if (!grid_reduce<2, 0>(P.ctl, P.part, P.timeout_ns, nbar, sd, nullptr, rd, nullptr)) return;
+    if (!dred<COMP, 2>(P.ctl, P.part, P.timeout_ns, nbar, sd, rd)) return;
     rmrm = rd[0];
     beta1 = rd[1];
     if (isnan(rmrm)) { finish(ST_NAN, m, rmrm, xl, relat); return; }
@@ -1193,8 +1196,8 @@ struct GmP {
   double *x;
   const double *b;
   double *r0, *v, *av;   // V(1..K), AV(1..K): K vectors of npoin each
-  double *part;          // grid_reduce partials: 4 * G doubles
-  double *part_n;        // grid_reduce_n partials: 2 * G * (GM_MAXK + 1) doubles
+  double *part;          // grid_reduce partials: 8 * G doubles
+  double *part_n;        // grid_reduce_n(_comp) partials: 4 * G * (GM_MAXK + 1) doubles
   Ctl *ctl;
   long long timeout_ns;
 };
@@ -1242,7 +1245,57 @@ static __device__ __noinline__ bool grid_reduce_n(Ctl *ctl, double *part, long l
   return true;
 }
 
-template <int TD, int STO>
+// The same for compensated values (MODASS = 3): each of the n pairs merged
+// as grid_reduce_comp merges one; `part` holds 2 halves of
+// G * (GM_MAXK + 1) pairs.  out receives p + s of each.
+static __device__ __noinline__ bool grid_reduce_n_comp(Ctl *ctl, double *part,
+                                                long long timeout_ns, int &nbar,
+                                                const CPair *vals, int n, double *out) {
+  __shared__ CPair smc[32];
+  __shared__ double red_sm[GM_MAXK + 1];
+  __shared__ int s_err;
+  const int G = gridDim.x, T = blockDim.x, t = threadIdx.x;
+  const unsigned long long k = (unsigned long long)(++nbar);
+  double *buf = part + (size_t)(k & 1) * (size_t)G * (GM_MAXK + 1) * 2;
+  for (int q = 0; q < n; ++q) {
+    const CPair bp = block_tree_c(vals[q], smc);
+    if (t == 0) {
+      buf[((size_t)blockIdx.x * (GM_MAXK + 1) + q) * 2] = bp.p;
+      buf[((size_t)blockIdx.x * (GM_MAXK + 1) + q) * 2 + 1] = bp.s;
+    }
+  }
+  if (t == 0) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> cnt(ctl->arrivals);
+    cnt.fetch_add(1ull, cuda::memory_order_release);
+    const unsigned long long target = k * (unsigned long long)G;
+    const unsigned long long t0 = global_ns();
+    s_err = 0;
+    while (cnt.load(cuda::memory_order_acquire) < target) {
+      if ((long long)(global_ns() - t0) > timeout_ns) {
+        s_err = 1;
+        atomicExch(&ctl->status, (int)ST_TIMEOUT);
+        break;
+      }
+      if (SPIN_NS > 0) __nanosleep(SPIN_NS);
+    }
+  }
+  __syncthreads();
+  if (s_err) return false;
+  for (int q = 0; q < n; ++q) {
+    CPair acc{0.0, 0.0};
+    for (int bb = t; bb < G; bb += T)
+      acc = cmerge(acc, CPair{__ldcg(buf + ((size_t)bb * (GM_MAXK + 1) + q) * 2),
+                              __ldcg(buf + ((size_t)bb * (GM_MAXK + 1) + q) * 2 + 1)});
+    const CPair tot = block_tree_c(acc, smc);
+    if (t == 0) red_sm[q] = add(tot.p, tot.s);
+  }
+  __syncthreads();
+  for (int q = 0; q < n; ++q) out[q] = red_sm[q];
+  __syncthreads();
+  return true;
+}
+
+template <int TD, int STO, bool COMP>
 __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
@@ -1255,7 +1308,9 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
   __shared__ double Cg[GM_MAXK], Sg[GM_MAXK], E[GM_MAXK + 1];
   __shared__ int s_flag;
   double vals[GM_MAXK + 1];
-  double s, red;
+  CPair cvals[COMP ? GM_MAXK + 1 : 1];
+  DotAcc<COMP, 1> s;
+  double red;
   int nbar = 0;
   const bool h1 = false;
   double a1 = 0.0;
@@ -1276,21 +1331,21 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
   };
 
   // NB = SQRT(B.B), absolute mode below 1 (:67-73)
-  s = 0.0;
-  for (int i = lo + t; i < hi; i += T) s = add(s, mul(b[i], b[i]));
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  s.zero();
+  for (int i = lo + t; i < hi; i += T) s.acc(0, b[i], b[i]);
+  if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
   double nbn = __dsqrt_rn(red);
   if (nbn < 1.0) { nbn = 1.0; relat = 0; }
   // R0 = A X - B, NR0 (:77-86)
-  s = 0.0;
+  s.zero();
   for (int i = lo + t; i < hi; i += T) {
     double a0 = diag_term<TD>(x[i], da, i);
     op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int j) { return x[j]; });
     const double r = sub(a0, b[i]);
     r0[i] = r;
-    s = add(s, mul(r, r));
+    s.acc(0, r, r);
   }
-  if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+  if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
   double nr0 = __dsqrt_rn(red);
   prec = __ddiv_rn(nr0, nbn);
   if (isnan(prec)) { if (lead) P.ctl->status = ST_NAN; return; }
@@ -1310,7 +1365,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
       // AV(J) = A V(J) [storing V(J) normalised]; V(J+1) = AV(J);
       // first MGS dot H(1,J) = V(J+1).V(1)
       double *vj = V(J), *avj = AV(J), *vn = V(J + 1);
-      s = 0.0;
+      s.zero();
       for (int i = lo + t; i < hi; i += T) {
         const double vi = vread(J, cs, i);
         double a0 = diag_term<TD>(vi, da, i);
@@ -1319,9 +1374,9 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
         vn[i] = a0;
         if (J == 1) vj[i] = vi;   // nobody reads V(1) from memory in this pass
         const double v1 = J == 1 ? vi : V(1)[i];
-        s = add(s, mul(a0, v1));
+        s.acc(0, a0, v1);
       }
-      if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr)) return;
+      if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
       // every block has finished reading the unscaled V(J): store it scaled
       if (J > 1 && cs != 0.0)
         for (int i = lo + t; i < hi; i += T) vj[i] = mul(cs, vj[i]);
@@ -1331,14 +1386,14 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
       for (int I = 2; I <= J + 1; ++I) {
         const double ch = -hprev;
         const double *vp = V(I - 1);
-        s = 0.0;
+        s.zero();
         for (int i = lo + t; i < hi; i += T) {
           const double u = add(vn[i], mul(ch, vp[i]));
           vn[i] = u;
           const double w = I <= J ? V(I)[i] : u;   // I = J+1: the norm of V(J+1)
-          s = add(s, mul(u, w));
+          s.acc(0, u, w);
         }
-        if (!grid_reduce<1, 0>(P.ctl, P.part, P.timeout_ns, nbar, &s, nullptr, &red, nullptr))
+        if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red))
           return;
         if (I <= J) {
           if (t == 0) H[I - 1][J - 1] = red;
@@ -1359,19 +1414,34 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
     // H(I,K) = AV(K).V(I) (:153-158)
     {
       double *vk = V(K), *avk = AV(K);
-      for (int q = 0; q <= K; ++q) vals[q] = 0.0;
+      for (int q = 0; q <= K; ++q) {
+        if (COMP)
+          cvals[q] = CPair{0.0, 0.0};
+        else
+          vals[q] = 0.0;
+      }
       for (int i = lo + t; i < hi; i += T) {
         const double vi = vread(K, cs, i);
         double a0 = diag_term<TD>(vi, da, i);
         op_row2<STO>(i, i, h1, a0, a1, P.S, [&](int q) { return vread(K, cs, q); });
         avk[i] = a0;
-        vals[K] = add(vals[K], mul(a0, a0));
+        if (COMP)
+          cdot_add(cvals[K], a0, a0);
+        else
+          vals[K] = add(vals[K], mul(a0, a0));
         for (int I = 1; I <= K; ++I) {
           const double vI = I == K ? vi : (I == 1 ? mul(c0, r0[i]) : V(I)[i]);
-          vals[I - 1] = add(vals[I - 1], mul(a0, vI));
+          if (COMP)
+            cdot_add(cvals[I - 1], a0, vI);
+          else
+            vals[I - 1] = add(vals[I - 1], mul(a0, vI));
         }
       }
-      if (!grid_reduce_n(P.ctl, P.part_n, P.timeout_ns, nbar, vals, K + 1, vals)) return;
+      if (COMP) {
+        if (!grid_reduce_n_comp(P.ctl, P.part_n, P.timeout_ns, nbar, cvals, K + 1, vals)) return;
+      } else if (!grid_reduce_n(P.ctl, P.part_n, P.timeout_ns, nbar, vals, K + 1, vals)) {
+        return;
+      }
       // all reads of the unscaled V(K) are done: store it as used
       for (int i = lo + t; i < hi; i += T) vk[i] = vread(K, cs, i);
     }

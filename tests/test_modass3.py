@@ -1,8 +1,9 @@
-"""MODASS = 3 (compensated dot products, dot_comp.f): the oracle's Dot2 in
-the reference's sequential order and in the device's blocked order agree
-with the exact dot product, the compensated GRACJG gives the same bits in
-both orders, and the device's compensated solve reproduces the reference's
-sequential-order solve bit for bit (GPU)."""
+"""MODASS = 3 (compensated dot products, dot_comp.f, which P_DOTS uses for
+every method): the oracle's Dot2 in the reference's sequential order and in
+the device's blocked order agree with the exact dot product, the compensated
+solves give the same bits in both orders, and the device's compensated
+solves (GRACJG and the other six methods) reproduce the reference's
+sequential-order solves bit for bit (GPU)."""
 from fractions import Fraction
 
 import numpy as np
@@ -72,8 +73,70 @@ def test_modass3_gpu_matches_reference_order(oracle_mod, storage):
                 r = oracle_mod.solve(p["ik"], p["dm"], "Q", p["xm"], "S", p["b"], **kw)
             assert st == r["status"] == 0 and nit == r["nit"] and relres == r["relres"]
             np.testing.assert_array_equal(x, r["x"])
-    # only GRACJG has a compensated form here
-    with pytest.raises(bief.BiefError):
-        bief.solve(np.zeros(n), A, p["b"].copy(),
-                   bief.SlvCfg(slv=6, nitmax=10, precon=2, krylov=0, eps=1e-8, zero=0.0),
-                   modass=3)
+
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", ["ebe", "seg"])
+@pytest.mark.parametrize("slv", [2, 3, 4, 5, 6])
+def test_modass3_other_methods_gpu(oracle_mod, storage, slv):
+    """P_DOTS switches to DOT_COMP for every method under MODASS = 3
+    (p_dots.f:148-156): RESCJG, EQUNOR, ERRMIN, CGSQUA and CGSTAB with
+    compensated dots, converged and at NITMAX, bit for bit against the
+    oracle in the device's order and in the reference's sequential order."""
+    for p in _problems(oracle_mod)[1:]:
+        n = p["x"].size
+        mesh = bief.Mesh(p["ik"], n)
+        A = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
+        if storage == "seg":
+            g1, g2, es, ori = mg.segments(p["ik"], n)
+            mesh.set_segments(g1, g2)
+            A.to_segments()
+            xa = oracle_mod.assex3(es, ori, "S", p["xm"], g1.size)
+        G, T = mesh.launch_info()
+        for eps, nitmax in ((1e-10, 100000), (1e-14, 15)):
+            x = np.zeros(n)
+            cfg = bief.SlvCfg(slv=slv, nitmax=nitmax, precon=2, krylov=0, eps=eps, zero=0.0)
+            st, nit, relres = bief.solve(x, A, p["b"].copy(), cfg, modass=3)
+            for mode in (oracle_mod.DOT_COMP_BLOCKED, oracle_mod.DOT_COMP_SEQUENTIAL):
+                kw = dict(slv=slv, eps=eps, nitmax=nitmax, dot_mode=mode, nblocks=G, nthreads=T)
+                if storage == "seg":
+                    r = oracle_mod.solve_seg(g1, g2, p["dm"], "Q", xa, "S", p["b"], **kw)
+                else:
+                    r = oracle_mod.solve(p["ik"], p["dm"], "Q", p["xm"], "S", p["b"], **kw)
+                assert (st, nit) == (r["status"], r["nit"]) and relres == r["relres"]
+                np.testing.assert_array_equal(x, r["x"])
+            assert st == (0 if nitmax > 15 else 15)
+        mesh.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", ["ebe", "seg"])
+@pytest.mark.parametrize("krylov", [1, 5, 20])
+def test_modass3_gmres_gpu(oracle_mod, storage, krylov):
+    """GMRES with compensated dots (the Gram-Schmidt dots and the last
+    column's K+1 dots), bit for bit against the oracle in both orders."""
+    p = _problems(oracle_mod)[1]
+    n = p["x"].size
+    mesh = bief.Mesh(p["ik"], n)
+    A = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
+    if storage == "seg":
+        g1, g2, es, ori = mg.segments(p["ik"], n)
+        mesh.set_segments(g1, g2)
+        A.to_segments()
+        xa = oracle_mod.assex3(es, ori, "S", p["xm"], g1.size)
+    G, T = mesh.launch_info()
+    for eps, nitmax in ((1e-8, 3000), (1e-14, 4)):
+        x = np.zeros(n)
+        cfg = bief.SlvCfg(slv=7, nitmax=nitmax, precon=2, krylov=krylov, eps=eps, zero=0.0)
+        st, nit, relres = bief.solve(x, A, p["b"].copy(), cfg, modass=3)
+        for mode in (oracle_mod.DOT_COMP_BLOCKED, oracle_mod.DOT_COMP_SEQUENTIAL):
+            kw = dict(slv=7, krylov=krylov, eps=eps, nitmax=nitmax, dot_mode=mode, nblocks=G,
+                      nthreads=T)
+            if storage == "seg":
+                r = oracle_mod.solve_seg(g1, g2, p["dm"], "Q", xa, "S", p["b"], **kw)
+            else:
+                r = oracle_mod.solve(p["ik"], p["dm"], "Q", p["xm"], "S", p["b"], **kw)
+            assert (st, nit) == (r["status"], r["nit"]) and relres == r["relres"]
+            np.testing.assert_array_equal(x, r["x"])
+    mesh.close()
