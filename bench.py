@@ -74,9 +74,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-large-matvec", action="store_true",
                     help="skip the MATVEC measurements on the 2001x2001-node mesh")
-    ap.add_argument("--workload", default="wave1m", choices=["wave1m", "batch256"],
+    ap.add_argument("--workload", default="wave1m", choices=["wave1m", "batch256", "matvec"],
                     help="wave1m: the 1M-node solve (default); batch256: 256 independent "
-                         "meshes of 2,000-200,000 nodes in one persistent launch per rank")
+                         "meshes of 2,000-200,000 nodes in one persistent launch per rank; "
+                         "matvec: the binary64 and binary32 MATVEC 'X=AY' alone on the "
+                         "--n x --n mesh")
     args = ap.parse_args()
     if args.inner_tol is None:
         args.inner_tol = 1e-4 if args.workload == "batch256" else 0.1
@@ -368,9 +370,79 @@ def run_batch(args, ws, rank, local):
     bs.close()
 
 
+def run_matvec(args, ws, rank, local):
+    """MATVEC 'X=AY' alone: binary64 EBE (k_matvec / k_mvseg) and binary32
+    (k_matvec32) on the --n x --n mesh, --steps timed launches each after
+    --warmup, L2 flushed before every launch, library events around each
+    launch.  One line: the binary64 product's GB/s (algorithmic bytes)."""
+    import torch
+    from opentelemac_b200 import bief
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    P = build_problem(args.n, local, "smooth", args.storage)
+    by = algorithmic_bytes(P["npoin"], P["nelem"], P["nseg"])
+    flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    clean = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    y = P["xt"]
+    out = torch.zeros_like(y)
+    y32 = y.float()
+    out32 = torch.empty_like(y32)
+    bief.matvec32(out32, P["A"], y32)
+
+    def lib_times(fn):
+        ts = []
+        for s in range(args.warmup + args.steps):
+            flush.fill_(float(s))
+            clean.sum()
+            fn()
+            torch.cuda.synchronize()
+            if s >= args.warmup:
+                ts.append(P["mesh"].last_timing()[1])
+        return ts
+
+    launches0 = P["mesh"].kernel_launches()
+    barrier(ws)
+    t64 = lib_times(lambda: bief.matvec("X=AY    ", out, P["A"], y))
+    t32 = lib_times(lambda: bief.matvec32(out32, P["A"], y32))
+    launches = P["mesh"].kernel_launches() - launches0
+    m64 = max_over_ranks(statistics.median(t64), ws)
+    m32 = max_over_ranks(statistics.median(t32), ws)
+    hbm = 6650.0
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            hbm = float(json.load(fh).get("hbm_gbs", hbm))
+    except OSError:
+        pass
+    g64 = ws * by["mv64"] / (m64 * 1e-3) / 1e9
+    g32 = ws * by["mv32"] / (m32 * 1e-3) / 1e9
+    if rank == 0:
+        kern = "k_mvseg" if args.storage == "seg" else "k_matvec"
+        print(json.dumps({
+            "metric": "EBE MATVEC 'X=AY' HBM GB/s (algorithmic bytes)", "value": g64,
+            "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": m64, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"MATVEC on the {args.n}x{args.n}-node P1 mesh",
+                       "npoin": P["npoin"], "nelem": P["nelem"],
+                       "storage": "segments (STO=3)" if args.storage == "seg" else "EBE (STO=1)",
+                       "l2": "1 GiB written then 256 MB read before every timed launch"},
+            "roofline": {"bound": "hbm", "kernel": kern, "achieved": g64 / ws, "peak": hbm,
+                         "unit": "GB/s", "frac": g64 / ws / hbm, "bytes": by["mv64"]},
+            "matvec32": {"kernel": "k_matvec32", "ms": m32, "gbs": g32, "frac": g32 / ws / hbm,
+                         "bytes": by["mv32"]},
+            "gpu_launches": launches}), flush=True)
+    P["mesh"].close()
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
+    if args.impl == "b200" and args.workload == "matvec":
+        run_matvec(args, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "b200" and args.workload == "batch256":
         run_batch(args, ws, rank, local)
         if ws > 1:
