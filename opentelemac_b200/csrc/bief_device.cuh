@@ -475,20 +475,26 @@ __device__ __forceinline__ T ebe_row(int i, T acc, const int *__restrict__ ptr,
 // are latency bound: 32 warps per SM at 64 registers).  The additions keep
 // their order, so the bits do not depend on the batch sizes.  Measured on
 // B200, per iteration at 4.0M / 1.0M nodes: binary64 GRACJG 183 / 51 us with
-// 4-entry batches against 207 / 56 us unbatched; binary32 inner CG 103 us
-// with 3-slot batches against 120 us (interior P1 nodes have 6 neighbours).
+// 4-entry batches against 207 / 56 us unbatched (6-entry batches: 196 / 54);
+// binary32 inner CG 104 / 19.0 us with 6-slot batches against 105 / 20.2
+// with 3 and 118 / 21.4 with 5 (interior P1 nodes have 6 neighbours); the
+// half-size batch after the full ones takes the binary64 iteration from
+// 185 / 51.4 to 183 / 50.8 us and changes nothing on a 1M-point Delaunay
+// mesh.
 #ifndef BIEF_SLOT_BATCH
 #define BIEF_SLOT_BATCH 4
 #endif
 #ifndef BIEF_SLOT_BATCH32
-#define BIEF_SLOT_BATCH32 3
+#define BIEF_SLOT_BATCH32 6
 #endif
-#ifndef BIEF_SLOT_PRED
-#define BIEF_SLOT_PRED 0
+#ifndef BIEF_SLOT_CASCADE
+#define BIEF_SLOT_CASCADE 1
 #endif
 constexpr int SLOT_B = BIEF_SLOT_BATCH;      // binary64 records
 constexpr int SLOT_B32 = BIEF_SLOT_BATCH32;  // binary32 slots
-constexpr bool SLOT_PRED = BIEF_SLOT_PRED;   // last batch predicated instead of serial
+// after the full batches, one batch of half the size when it fits, then
+// single entries
+constexpr bool SLOT_CASCADE = BIEF_SLOT_CASCADE;
 
 struct Sell {
   const int *meta;        // per node: gather entries | neighbours << 16
@@ -505,6 +511,27 @@ struct Sell {
 // Two rows at once (nodes i0 and, if has1, i1): independent load chains
 // interleaved so that twice as many loads are in flight per thread.  Each
 // row's additions keep their own order, so the bits equal rec_row's.
+// NB consecutive gather entries m.. of a row: all index/coefficient loads,
+// then all node loads, then the additions in order.
+template <int NB, class V>
+__device__ __forceinline__ void rec_batch(double &a0, const Sell &S, int b0, int m, V vec) {
+  double2 c[NB];
+  int2 v[NB];
+  double ya[NB], yb[NB];
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    c[q] = __ldg(S.rec_c + b0 + 32 * (m + q));
+    v[q] = __ldg(S.rec_idx + b0 + 32 * (m + q));
+  }
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    ya[q] = vec(v[q].x);
+    yb[q] = vec(v[q].y);
+  }
+#pragma unroll
+  for (int q = 0; q < NB; ++q) a0 = add(a0, add(mul(c[q].x, ya[q]), mul(c[q].y, yb[q])));
+}
+
 template <class V>
 __device__ __forceinline__ void rec_row2(int i0, int i1, bool has1, double &a0, double &a1,
                                          const Sell &S, V vec) {
@@ -513,24 +540,12 @@ __device__ __forceinline__ void rec_row2(int i0, int i1, bool has1, double &a0, 
       const int d0 = __ldg(S.meta + i0) & 0xffff;
       const int b0 = __ldg(S.rec_off + (i0 >> 5)) + (i0 & 31);
       int m = 0;
-      for (; SLOT_PRED ? m < d0 : m + SLOT_B <= d0; m += SLOT_B) {
-        double2 c[SLOT_B];
-        int2 v[SLOT_B];
-        double ya[SLOT_B], yb[SLOT_B];
-#pragma unroll
-        for (int q = 0; q < SLOT_B; ++q) {
-          const bool ok = !SLOT_PRED || m + q < d0;
-          c[q] = ok ? __ldg(S.rec_c + b0 + 32 * (m + q)) : make_double2(0.0, 0.0);
-          v[q] = ok ? __ldg(S.rec_idx + b0 + 32 * (m + q)) : make_int2(i0, i0);
+      for (; m + SLOT_B <= d0; m += SLOT_B) rec_batch<SLOT_B>(a0, S, b0, m, vec);
+      if constexpr (SLOT_CASCADE && SLOT_B / 2 > 1) {
+        if (m + SLOT_B / 2 <= d0) {
+          rec_batch<SLOT_B / 2>(a0, S, b0, m, vec);
+          m += SLOT_B / 2;
         }
-#pragma unroll
-        for (int q = 0; q < SLOT_B; ++q) {
-          ya[q] = vec(v[q].x);
-          yb[q] = vec(v[q].y);
-        }
-#pragma unroll
-        for (int q = 0; q < SLOT_B; ++q)
-          if (!SLOT_PRED || m + q < d0) a0 = add(a0, add(mul(c[q].x, ya[q]), mul(c[q].y, yb[q])));
       }
       for (; m < d0; ++m) {
         const double2 c = __ldg(S.rec_c + b0 + 32 * m);
@@ -564,6 +579,21 @@ __device__ __forceinline__ void rec_row2(int i0, int i1, bool has1, double &a0, 
 // is GLOSEG1) or XA2 (GLOSEG2) and the other end, in the sliced layout of
 // the binary32 slots (meta, rec_off and seg_col then describe these
 // slots).  Row: acc + XA*Y(other) per slot, left to right.
+template <int NB, class V>
+__device__ __forceinline__ void sgr_batch(double &a0, const Sell &S, int b0, int m, V vec) {
+  double c[NB], v[NB];
+  int j[NB];
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    c[q] = __ldg(S.sg_c + b0 + 32 * (m + q));
+    j[q] = __ldg(S.seg_col + b0 + 32 * (m + q));
+  }
+#pragma unroll
+  for (int q = 0; q < NB; ++q) v[q] = vec(j[q]);
+#pragma unroll
+  for (int q = 0; q < NB; ++q) a0 = add(a0, mul(c[q], v[q]));
+}
+
 template <class V>
 __device__ __forceinline__ void sgr_row2(int i0, int i1, bool has1, double &a0, double &a1,
                                          const Sell &S, V vec) {
@@ -572,18 +602,12 @@ __device__ __forceinline__ void sgr_row2(int i0, int i1, bool has1, double &a0, 
       const int d0 = __ldg(S.meta + i0) & 0xffff;
       const int b0 = __ldg(S.rec_off + (i0 >> 5)) + (i0 & 31);
       int m = 0;
-      for (; m + SLOT_B <= d0; m += SLOT_B) {
-        double c[SLOT_B], v[SLOT_B];
-        int j[SLOT_B];
-#pragma unroll
-        for (int q = 0; q < SLOT_B; ++q) {
-          c[q] = __ldg(S.sg_c + b0 + 32 * (m + q));
-          j[q] = __ldg(S.seg_col + b0 + 32 * (m + q));
+      for (; m + SLOT_B <= d0; m += SLOT_B) sgr_batch<SLOT_B>(a0, S, b0, m, vec);
+      if constexpr (SLOT_CASCADE && SLOT_B / 2 > 1) {
+        if (m + SLOT_B / 2 <= d0) {
+          sgr_batch<SLOT_B / 2>(a0, S, b0, m, vec);
+          m += SLOT_B / 2;
         }
-#pragma unroll
-        for (int q = 0; q < SLOT_B; ++q) v[q] = vec(j[q]);
-#pragma unroll
-        for (int q = 0; q < SLOT_B; ++q) a0 = add(a0, mul(c[q], v[q]));
       }
       for (; m < d0; ++m)
         a0 = add(a0, mul(__ldg(S.sg_c + b0 + 32 * m), vec(__ldg(S.seg_col + b0 + 32 * m))));
@@ -612,6 +636,44 @@ __device__ __forceinline__ void op_row2(int i0, int i1, bool has1, double &a0, d
     rec_row2(i0, i1, has1, a0, a1, S, vec);
 }
 
+template <int NB, class V>
+__device__ __forceinline__ void seg_batch(float &a0, float y0, const Sell &S, int b0, int m,
+                                          V vec) {
+  int j[NB];
+  float c[NB], v[NB];
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    j[q] = __ldg(S.seg_col + b0 + 32 * (m + q));
+    c[q] = __ldg(S.seg_c + b0 + 32 * (m + q));
+  }
+#pragma unroll
+  for (int q = 0; q < NB; ++q) v[q] = vec(j[q]);
+#pragma unroll
+  for (int q = 0; q < NB; ++q) a0 = add(a0, mul(c[q], sub(v[q], y0)));
+}
+
+// One row of the binary32 product with the node's slot count n0, first
+// slot b0 and row sum s already loaded (batched slot loads as below).
+template <class V>
+__device__ __forceinline__ float seg_row_nb(int i0, int n0, int b0, float s, float y0,
+                                            const Sell &S, V vec) {
+  float a0 = mul(y0, s);
+  int m = 0;
+  for (; m + SLOT_B32 <= n0; m += SLOT_B32) seg_batch<SLOT_B32>(a0, y0, S, b0, m, vec);
+  if constexpr (SLOT_CASCADE && SLOT_B32 / 2 > 1) {
+    if (m + SLOT_B32 / 2 <= n0) {
+      seg_batch<SLOT_B32 / 2>(a0, y0, S, b0, m, vec);
+      m += SLOT_B32 / 2;
+    }
+  }
+  for (; m < n0; ++m) {
+    const int jj = __ldg(S.seg_col + b0 + 32 * m);
+    const float cc = __ldg(S.seg_c + b0 + 32 * m);
+    a0 = add(a0, mul(cc, sub(vec(jj), y0)));
+  }
+  return a0;
+}
+
 template <class V>
 __device__ __forceinline__ void seg_row2(int i0, int i1, bool has1, float y0, float y1,
                                          float &a0, float &a1, const Sell &S, V vec) {
@@ -619,29 +681,8 @@ __device__ __forceinline__ void seg_row2(int i0, int i1, bool has1, float y0, fl
     if (!has1) {
       const int n0 = __ldg(S.meta + i0) >> 16;
       const int b0 = __ldg(S.seg_off + (i0 >> 5)) + (i0 & 31);
-      a0 = mul(y0, __ldg(S.s32 + i0));
+      a0 = seg_row_nb(i0, n0, b0, __ldg(S.s32 + i0), y0, S, vec);
       a1 = 0.0f;
-      int m = 0;
-      for (; SLOT_PRED ? m < n0 : m + SLOT_B32 <= n0; m += SLOT_B32) {
-        int j[SLOT_B32];
-        float c[SLOT_B32], v[SLOT_B32];
-#pragma unroll
-        for (int q = 0; q < SLOT_B32; ++q) {
-          const bool ok = !SLOT_PRED || m + q < n0;
-          j[q] = ok ? __ldg(S.seg_col + b0 + 32 * (m + q)) : i0;
-          c[q] = ok ? __ldg(S.seg_c + b0 + 32 * (m + q)) : 0.0f;
-        }
-#pragma unroll
-        for (int q = 0; q < SLOT_B32; ++q) v[q] = vec(j[q]);
-#pragma unroll
-        for (int q = 0; q < SLOT_B32; ++q)
-          if (!SLOT_PRED || m + q < n0) a0 = add(a0, mul(c[q], sub(v[q], y0)));
-      }
-      for (; m < n0; ++m) {
-        const int jj = __ldg(S.seg_col + b0 + 32 * m);
-        const float cc = __ldg(S.seg_c + b0 + 32 * m);
-        a0 = add(a0, mul(cc, sub(vec(jj), y0)));
-      }
       return;
     }
   }
