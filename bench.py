@@ -352,6 +352,20 @@ def run_batch(args, ws, rank, local):
     ok = int(replicas.sum_over_ranks(int((r["status"] == 0).sum()))) if ws > 1 else int(
         (r["status"] == 0).sum())
     inner = r["inner"]
+    # algorithmic bytes of this rank's launch: every instance's inner
+    # iterations and binary64 refinements (the initial residual included)
+    alg = 0
+    for (npo, ik), ni, no in zip(meshes, r["inner"], r["outer"]):
+        by = algorithmic_bytes(npo, ik.shape[0])
+        alg += int(ni) * by["it32"] + (int(no) + 1) * by["upd"]
+    kern_ms = sum(kern) / len(kern)
+    hbm = 6650.0
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            hbm = float(json.load(fh).get("hbm_gbs", hbm))
+    except OSError:
+        pass
+    gbs = alg / (kern_ms * 1e-3) / 1e9
     if rank == 0:
         line = {"metric": "batched P1 CG solves/s (256 meshes, mixed, relres 1e-8)",
                 "value": 256 * 1000.0 / step_ms, "unit": "solves/s", "n_gpus": ws,
@@ -366,7 +380,10 @@ def run_batch(args, ws, rank, local):
                            "autotune_ms_per_iteration": {f"npt{k[0]}_t{k[1]}": round(v, 4)
                                                          for k, v in bs.tune_table.items()},
                            "parallelism": f"shards x{ws}"},
-                "converged": ok, "kernel_ms": sum(kern) / len(kern),
+                "converged": ok, "kernel_ms": kern_ms,
+                "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": gbs, "peak": hbm,
+                             "unit": "GB/s", "frac": gbs / hbm, "bytes_per_launch": alg,
+                             "note": "rank 0's instances; working set above L2"},
                 "iterations_rank0": {"p50": float(np.percentile(inner, 50)),
                                      "p99": float(np.percentile(inner, 99)),
                                      "max": int(inner.max())}}
