@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-large-matvec", action="store_true",
                     help="skip the MATVEC measurements on the 2001x2001-node mesh")
+    ap.add_argument("--batch-shape", default=None,
+                    help="batch256: nodes per thread and threads per block as NPT,TPB "
+                         "(default: the autotuner's choice)")
     ap.add_argument("--max-inner", type=int, default=200,
                     help="mixedcap: inner iterations of each bounded mixed solve")
     ap.add_argument("--workload", default="wave1m",
@@ -330,7 +333,10 @@ def run_batch(args, ws, rank, local):
     bs.assemble_wave(xs, ys, coefs)
     b = bs.gather(bvs)
     x = torch.zeros_like(b)
-    npt, tpb = bs.autotune(b, inner_tol=args.inner_tol, outer_tol=args.eps)
+    if args.batch_shape:
+        npt, tpb = (int(v) for v in args.batch_shape.split(","))
+    else:
+        npt, tpb = bs.autotune(b, inner_tol=args.inner_tol, outer_tol=args.eps)
     flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     clean = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     times, kern = [], []
@@ -378,7 +384,7 @@ def run_batch(args, ws, rank, local):
                            "nodes_this_rank": int(bs.total_nodes),
                            "nodes_per_thread": int(npt), "threads_per_block": int(tpb),
                            "autotune_ms_per_iteration": {f"npt{k[0]}_t{k[1]}": round(v, 4)
-                                                         for k, v in bs.tune_table.items()},
+                                                         for k, v in getattr(bs, "tune_table", {}).items()},
                            "parallelism": f"shards x{ws}"},
                 "converged": ok, "kernel_ms": kern_ms,
                 "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": gbs, "peak": hbm,

@@ -233,7 +233,9 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
  * Dirichlet points; with maskpt (npoin, or NULL) SM and F are masked; the
  * stored matrix keeps its diagonal and loses the off-diagonal terms of the
  * Dirichlet rows and columns (OM 'M=DMD'), in either storage.  Host arrays;
- * the _dev variant takes device arrays and runs on `stream`. */
+ * the _dev variant takes device arrays and runs on `stream`, which it
+ * synchronises when nptfr > 0 to report an NBOR entry outside 1..NPOIN
+ * (BIEF_ERR_BAD_MESH; such entries are skipped, never written through). */
 int bief_diri01(bief_handle *h, int nptfr, const int *nbor, const int *limdir,
                 int kdir, const double *fbor, double *sm, double *f,
                 const double *maskpt);

@@ -1373,7 +1373,8 @@ int bief_diri01_dev(bief_handle *h, int nptfr, const int *nbor, const int *limdi
   const int td = typdia_code(h->typdia);
   const bool sym = h->typext != 'Q';
   CK(cudaMemsetAsync(w1, 0, sizeof(double) * n, s));
-  if (nptfr > 0) k_diri_scatter<<<gb, 256, 0, s>>>(nptfr, nbor, limdir, kdir, fbor, w1);
+  CK(cudaMemsetAsync(h->d_err, 0, sizeof(int), s));
+  if (nptfr > 0) k_diri_scatter<<<gb, 256, 0, s>>>(nptfr, n, nbor, limdir, kdir, fbor, w1, h->d_err);
   // W2 = S W1 (MATVEC 'X=AY')
   if (h->sto == 3) {
     dispatch_mvseg(h, td, sym, false, h->typext != '0', h->d_xa, h->d_dm, w1, w2, OP_AY, 0.0, s);
@@ -1386,7 +1387,8 @@ int bief_diri01_dev(bief_handle *h, int nptfr, const int *nbor, const int *limdi
     dispatch_mv(h, td, sym, false, xm, h->d_dm, w1, w2, OP_AY, 0.0, s);
   }
   k_diri_nodes<<<gn, 256, 0, s>>>(n, sm, w2);
-  if (nptfr > 0) k_diri_aux<<<gb, 256, 0, s>>>(nptfr, nbor, limdir, kdir, fbor, h->d_dm, sm, w2, f);
+  if (nptfr > 0)
+    k_diri_aux<<<gb, 256, 0, s>>>(nptfr, n, nbor, limdir, kdir, fbor, h->d_dm, sm, w2, f);
   if (maskpt) k_diri_mask<<<gn, 256, 0, s>>>(n, maskpt, sm, f, w2);
   // OM 'M=DMD' with D = W2 on the off-diagonal terms only, in place
   if (h->sto == 3) {
@@ -1403,12 +1405,21 @@ int bief_diri01_dev(bief_handle *h, int nptfr, const int *nbor, const int *limdi
   h->launches += 6;
   h->mat_gen++;
   CK(cudaGetLastError());
+  if (nptfr > 0) {  // an NBOR entry outside 1..NPOIN was skipped
+    int err = 0;
+    CK(cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (err) return BIEF_ERR_BAD_MESH;
+  }
   return BIEF_OK;
 }
 
 int bief_diri01(bief_handle *h, int nptfr, const int *nbor, const int *limdir, int kdir,
                 const double *fbor, double *sm, double *f, const double *maskpt) {
   if (!h || nptfr < 0 || !sm || !f) return BIEF_ERR_ARGS;
+  if (nptfr > 0 && (!nbor || !limdir || !fbor)) return BIEF_ERR_ARGS;
+  for (int k = 0; k < nptfr; ++k)
+    if (nbor[k] < 1 || nbor[k] > h->npoin) return BIEF_ERR_BAD_MESH;
   DevGuard g(h->dev);
   const size_t nb = sizeof(double) * h->npoin;
   int *d_i = nullptr;

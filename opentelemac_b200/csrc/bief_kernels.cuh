@@ -228,11 +228,19 @@ __global__ void k_assex3(int nseg, int nelem, int ld, const int2 *__restrict__ s
 // DIRI01 (diri01.f:90-130, DIRAUX diraux.f:70-85) on boundary numbering:
 // the Dirichlet values scattered to their nodes, SM corrected, the rows and
 // columns of the Dirichlet nodes masked.  nbor is 1-based (MESH%NBOR).
-__global__ void k_diri_scatter(int nptfr, const int *__restrict__ nbor,
+// NBOR entries outside 1..NPOIN are skipped and flagged in *err.
+__global__ void k_diri_scatter(int nptfr, int npoin, const int *__restrict__ nbor,
                                const int *__restrict__ limdir, int kdir,
-                               const double *__restrict__ fbor, double *w1) {
+                               const double *__restrict__ fbor, double *w1, int *err) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nptfr; k += gridDim.x * blockDim.x)
-    if (limdir[k] == kdir) w1[nbor[k] - 1] = fbor[k];
+    if (limdir[k] == kdir) {
+      const int n = nbor[k];
+      if (n < 1 || n > npoin) {
+        atomicExch(err, 1);
+        continue;
+      }
+      w1[n - 1] = fbor[k];
+    }
 }
 
 // SM = SM - W2 ('X=X-Y'), then W2 = 1 ('X=C')
@@ -243,12 +251,14 @@ __global__ void k_diri_nodes(int npoin, double *sm, double *w2) {
   }
 }
 
-__global__ void k_diri_aux(int nptfr, const int *__restrict__ nbor, const int *__restrict__ limdir,
-                           int kdir, const double *__restrict__ fbor,
-                           const double *__restrict__ dm, double *sm, double *w2, double *f) {
+__global__ void k_diri_aux(int nptfr, int npoin, const int *__restrict__ nbor,
+                           const int *__restrict__ limdir, int kdir,
+                           const double *__restrict__ fbor, const double *__restrict__ dm,
+                           double *sm, double *w2, double *f) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nptfr; k += gridDim.x * blockDim.x)
     if (limdir[k] == kdir) {
       const int n = nbor[k] - 1;
+      if (n < 0 || n >= npoin) continue;   // flagged by k_diri_scatter
       sm[n] = mul(dm[n], fbor[k]);
       w2[n] = 0.0;
       f[n] = fbor[k];

@@ -69,3 +69,37 @@ def test_diri01_gpu_bitexact(oracle_mod, storage, typext, masked):
     np.testing.assert_array_equal(f, rf)
     _, got, _ = A.get()
     np.testing.assert_array_equal(got.ravel(), np.asarray(rx).ravel())
+
+
+@pytest.mark.gpu
+def test_diri01_rejects_nbor_out_of_range(oracle_mod):
+    """An NBOR entry outside 1..NPOIN is reported as BIEF_ERR_BAD_MESH: by the
+    host entry point before anything runs, and by the device entry point,
+    whose kernels skip the entry instead of writing through it; the
+    handle stays usable."""
+    import torch
+    p = small_problem(oracle_mod, n=21)
+    n = p["x"].size
+    nbor0, limdir, fbor = _boundary(p["ik"])
+    mesh = bief.Mesh(p["ik"], n)
+    A = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
+    for bad in (0, n + 1, -5, 10 * n):
+        nb = nbor0 + 1
+        nb[len(nb) // 2] = bad
+        lim = np.full_like(limdir, KDIR)           # every point Dirichlet: the bad one is used
+        sm, f = np.zeros(n), np.zeros(n)
+        with pytest.raises(bief.BiefError) as e:
+            bief.diri01(A, nb, lim, KDIR, fbor, sm, f)
+        assert e.value.status == -4
+        smd = torch.zeros(n, dtype=torch.float64, device="cuda")
+        fd = torch.zeros_like(smd)
+        with pytest.raises(bief.BiefError) as e:
+            bief.diri01(A, nb, lim, KDIR, fbor, smd, fd)
+        assert e.value.status == -4
+    # the handle still works
+    A2 = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
+    x = np.zeros(n)
+    cfg = bief.SlvCfg(slv=1, nitmax=10000, precon=2, krylov=0, eps=1e-8, zero=0.0)
+    st, nit, rel = bief.solve(x, A2, p["b"].copy(), cfg)
+    assert st == 0
+    mesh.close()
