@@ -740,6 +740,8 @@ def main():
                                     "mixed_kernel": kern_ms, "fp64_kernel": f64_kern_ms},
             "speedup_mixed_vs_fp64": f64_step_ms / step_ms,
             "iterations": {"fp64": nit64, "mixed_inner": inner, "mixed_updates": outer},
+            "cg_iterations_per_s": {"fp64": nit64 * 1000.0 / f64_kern_ms,
+                                    "mixed_inner": inner * 1000.0 / kern_ms},
             "relres": {"mixed": relres, "fp64": f64_res[2]},
             "error": {"mixed_vs_fp64": mixed_vs_f64, "mixed_vs_xtrue": mixed_x_err,
                       "fp64_vs_xtrue": f64_x_err,
