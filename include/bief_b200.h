@@ -206,6 +206,18 @@ int bief_wave_coef_grad_dev(bief_handle *h, const double *xc,
                             const double *yc, const double *lambda,
                             const double *x, double *grad, void *stream);
 
+/* Adjoint gradient through x = A(u, v)^-1 b with A assembled by
+ * bief_assemble_mass_diff_dev (kind 11: MATDIF with u per node; kind 12:
+ * MATDIFUV with u and v per node, PROPAG's form with u = DM1 and v = HPROP,
+ * the depth): given lambda with A^T lambda = dL/dx, writes
+ * gu[i] = dL/du_i (npoin) and, for kind 12, gv[i] = dL/dv_i, summed per
+ * node over its elements without atomics.  xmul_dif is the diffusion
+ * matrix's XMUL.  Device arrays.  No reference counterpart. */
+int bief_mass_diff_grad_dev(bief_handle *h, const double *xc, const double *yc,
+                            double xmul_dif, int kind, const double *u, const double *v,
+                            const double *lambda, const double *x, double *gu, double *gv,
+                            void *stream);
+
 /* Batched mixed-precision solve (no reference counterpart): the handle's
  * mesh is block diagonal with ninst <= 512 independent instances, instance
  * i owning nodes [node_off[i], node_off[i]+npoin_inst[i]) (node_off[i] a

@@ -29,7 +29,8 @@ EXPORTS = [
     "bief_mesh_create", "bief_destroy", "bief_set_matrix", "bief_set_matrix_dev",
     "bief_get_matrix", "bief_get_matrix_dev", "bief_solve", "bief_solve_dev",
     "bief_solve_mixed", "bief_solve_mixed_dev", "bief_matvec", "bief_matvec_dev",
-    "bief_matvec32_dev", "bief_assemble_wave_dev", "bief_assemble_mass_diff_dev", "bief_wave_coef_grad_dev", "bief_launch_info",
+    "bief_matvec32_dev", "bief_assemble_wave_dev", "bief_assemble_mass_diff_dev",
+    "bief_mass_diff_grad_dev", "bief_wave_coef_grad_dev", "bief_launch_info",
     "bief_last_timing", "bief_kernel_launches", "bief_strerror", "bief_solve_noalloc",
     "bief_batch_solve_mixed_dev", "bief_set_segments", "bief_set_matrix_seg",
     "bief_set_matrix_seg_dev", "bief_ebe_to_seg", "bief_matrix_storage",
@@ -81,6 +82,7 @@ def lib():
             "bief_matvec_dev": ([vp, ctypes.c_char_p, vp, vp, d, vp], i),
             "bief_matvec32_dev": ([vp, vp, vp, vp], i),
             "bief_assemble_mass_diff_dev": ([vp, vp, vp, d, d, i, vp, vp, vp], i),
+            "bief_mass_diff_grad_dev": ([vp, vp, vp, d, i, vp, vp, vp, vp, vp, vp, vp], i),
             "bief_assemble_wave_dev": ([vp, vp, vp, vp, vp], i),
             "bief_wave_coef_grad_dev": ([vp, vp, vp, vp, vp, vp, vp], i),
             "bief_launch_info": ([vp, pi, pi], i),

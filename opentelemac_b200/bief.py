@@ -319,6 +319,20 @@ def coef_grad(A, xc, yc, lam, x, grad):
     return grad
 
 
+def mass_diff_grad(A, xc, yc, u, v, lam, x, kind=12, xmul_dif=1.0):
+    """(dL/du, dL/dv) for x = A(u, v)^-1 b assembled by
+    Matrix.assemble_mass_diff (kind 11 or 12), given the adjoint lam
+    (A^T lam = dL/dx); dL/dv is None for kind 11.  Device tensors."""
+    import torch
+    gu = torch.empty_like(u)
+    gv = torch.empty_like(u) if kind == 12 else None
+    _check(_native.lib().bief_mass_diff_grad_dev(
+        A.mesh.handle, _ptr(xc), _ptr(yc), float(xmul_dif), int(kind), _ptr(u),
+        None if v is None else _ptr(v), _ptr(lam), _ptr(x), _ptr(gu),
+        None if gv is None else _ptr(gv), _stream(x)), "bief_mass_diff_grad_dev")
+    return gu, gv
+
+
 def _host_vec(a, n):
     if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous:
         raise ValueError("host vectors must be contiguous float64 numpy arrays")

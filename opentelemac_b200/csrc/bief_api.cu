@@ -1219,6 +1219,34 @@ int bief_wave_coef_grad_dev(bief_handle *h, const double *xc, const double *yc,
   return BIEF_OK;
 }
 
+int bief_mass_diff_grad_dev(bief_handle *h, const double *xc, const double *yc,
+                            double xmul_dif, int kind, const double *u, const double *v,
+                            const double *lambda, const double *x, double *gu, double *gv,
+                            void *stream) {
+  if (!h || !xc || !yc || !u || !lambda || !x || !gu) return BIEF_ERR_ARGS;
+  if (kind != 11 && kind != 12) return BIEF_ERR_ARGS;
+  if (kind == 12 && (!v || !gv)) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  int st;
+  if (!h->d_ew && (st = dalloc(&h->d_ew, 4 * (size_t)h->nelem))) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int ge = grid_for(h->nelem, h->nsm), gn = grid_for(h->npoin, h->nsm);
+  if (kind == 11) {
+    k_mass_diff_grad_elems<11><<<ge, 256, 0, s>>>(h->nelem, h->d_ik, xc, yc, xmul_dif, u, v,
+                                                  lambda, x, h->d_ew);
+    k_mass_diff_grad_nodes<11><<<gn, 256, 0, s>>>(h->npoin, h->d_ptr, h->d_ek, h->nelem, h->d_ew,
+                                                  u, v, gu, gv);
+  } else {
+    k_mass_diff_grad_elems<12><<<ge, 256, 0, s>>>(h->nelem, h->d_ik, xc, yc, xmul_dif, u, v,
+                                                  lambda, x, h->d_ew);
+    k_mass_diff_grad_nodes<12><<<gn, 256, 0, s>>>(h->npoin, h->d_ptr, h->d_ek, h->nelem, h->d_ew,
+                                                  u, v, gu, gv);
+  }
+  h->launches += 2;
+  CK(cudaGetLastError());
+  return BIEF_OK;
+}
+
 int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
                                const int *npoin_inst, double *x, const double *b, int precon,
                                double inner_tol, double outer_tol, int max_outer, int max_inner,

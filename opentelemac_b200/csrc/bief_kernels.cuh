@@ -1814,4 +1814,80 @@ __global__ void k_coef_grad(int nelem, const int *__restrict__ ik, const double 
   }
 }
 
+// Adjoint gradients of the node-coefficient diffusion forms (the operators
+// of k_mass_diff_elems, KIND 11 and 12).  With A^T lam = dL/dx, an
+// element's sensitivity to its scalar factor is s_e = -lam_e^T Ghat_e x_e,
+// Ghat_e the element matrix per unit factor (zero row sums, so
+// lam^T Ghat x = -sum_{k<l} Ghat_kl (lam_k - lam_l)(x_k - x_l)):
+//   KIND 11: factor SOMVX = (U1+U2+U3) XMUL/(12 S), dSOMVX/dU_k = XMUL/(12 S);
+//            ew[e] = s_e XMUL/(12 S)
+//   KIND 12: factor COEF2 * COEF1, COEF2 = sum_k U_k (V_k + G123),
+//            COEF1 = XMUL/(48 S); ew[e] = s_e COEF1, ew[ne+e] = G123 =
+//            V1+V2+V3, ew[2ne+e] = U1+U2+U3
+// The node pass then sums over the node's elements (no atomics):
+//   KIND 11: dL/dU_i = sum_e ew[e]
+//   KIND 12: dL/dU_i = sum_e ew[e] (V_i + G123_e),
+//            dL/dV_i = sum_e ew[e] (U_i + U1+U2+U3)
+template <int KIND>
+__global__ void k_mass_diff_grad_elems(int nelem, const int *__restrict__ ik,
+                                       const double *__restrict__ xc,
+                                       const double *__restrict__ yc, double xmul_dif,
+                                       const double *__restrict__ u,
+                                       const double *__restrict__ v,
+                                       const double *__restrict__ lam,
+                                       const double *__restrict__ xs, double *ew) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += gridDim.x * blockDim.x) {
+    const int i1 = ik[e], i2 = ik[(size_t)nelem + e], i3 = ik[2 * (size_t)nelem + e];
+    const double x1 = xc[i1], y1 = yc[i1];
+    const double X2 = xc[i2] - x1, X3 = xc[i3] - x1;
+    const double Y2 = yc[i2] - y1, Y3 = yc[i3] - y1;
+    const double surf = 0.5 * (X2 * Y3 - X3 * Y2);
+    double g12, g13, g23, scale;
+    if (KIND == 11) {
+      g12 = -(X3 * (X3 - X2) + Y3 * (Y3 - Y2));
+      g13 = X2 * (X3 - X2) + Y2 * (Y3 - Y2);
+      g23 = -(X2 * X3 + Y2 * Y3);
+      scale = xmul_dif / 12.0 / surf;
+    } else {
+      g12 = Y3 * (Y2 - Y3) + X3 * (X2 - X3);
+      g13 = -(Y2 * (Y2 - Y3) + X2 * (X2 - X3));
+      g23 = -(Y2 * Y3 + X2 * X3);
+      scale = xmul_dif / 48.0 / surf;
+    }
+    const double l1 = lam[i1], l2 = lam[i2], l3 = lam[i3];
+    const double w1 = xs[i1], w2 = xs[i2], w3 = xs[i3];
+    const double lgx = -(g12 * (l1 - l2) * (w1 - w2) + g13 * (l1 - l3) * (w1 - w3) +
+                         g23 * (l2 - l3) * (w2 - w3));
+    ew[e] = -lgx * scale;
+    if (KIND == 12) {
+      ew[(size_t)nelem + e] = v[i1] + v[i2] + v[i3];
+      ew[2 * (size_t)nelem + e] = u[i1] + u[i2] + u[i3];
+    }
+  }
+}
+
+template <int KIND>
+__global__ void k_mass_diff_grad_nodes(int npoin, const int *__restrict__ ptr,
+                                       const int *__restrict__ ek, int nelem,
+                                       const double *__restrict__ ew,
+                                       const double *__restrict__ u,
+                                       const double *__restrict__ v, double *gu, double *gv) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
+    double su = 0.0, sv = 0.0;
+    const double ui = KIND == 12 ? u[i] : 0.0, vi = KIND == 12 ? v[i] : 0.0;
+    for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
+      const int e = ek[j] >> 2;
+      const double se = ew[e];
+      if (KIND == 11) {
+        su += se;
+      } else {
+        su += se * (vi + ew[(size_t)nelem + e]);
+        sv += se * (ui + ew[2 * (size_t)nelem + e]);
+      }
+    }
+    gu[i] = su;
+    if (KIND == 12) gv[i] = sv;
+  }
+}
+
 }  // namespace bief
