@@ -223,6 +223,29 @@ def test_mixed_bitexact(oracle_mod, field, tol, itol):
     np.testing.assert_array_equal(x, r["x"])
 
 
+@pytest.mark.parametrize("precon", [0, 1, 5])
+def test_mixed_bitexact_precon_and_initial_guess(oracle_mod, precon):
+    """PRECON 0/1 (no scaling: the kernel's full-diagonal path) and 5
+    (|D|), from a nonzero initial guess, on a shuffled numbering."""
+    p = small_problem(oracle_mod, n=41, shuffle=True, field="loguniform")
+    n = p["x"].size
+    x0 = np.random.default_rng(precon).uniform(-1, 1, n)
+    mesh = bief.Mesh(p["ik"], n)
+    A = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
+    x = x0.copy()
+    st, outer, inner, relres = bief.solve_mixed(x, A, p["b"], precon=precon, inner_tol=0.1,
+                                                outer_tol=1e-9)
+    G, T = mesh.launch_info()
+    r = oracle_mod.solve_mixed(p["ik"], p["dm"], "Q", p["xm"], p["b"], x0=x0, precon=precon,
+                               inner_tol=0.1, outer_tol=1e-9, max_outer=1000,
+                               max_inner=1000000, nblocks=G, nthreads=T)
+    assert st == 0 == r["status"]
+    assert (outer, inner) == (r["outer"], r["inner"])
+    assert relres == r["relres"] and relres <= 1e-9
+    np.testing.assert_array_equal(x, r["x"])
+    mesh.close()
+
+
 def test_large_mesh_properties(oracle_mod):
     """501 x 501 (251,001 nodes): size-independent checks -- linearity of
     MATVEC, the returned residual equals an independent binary64 residual,
