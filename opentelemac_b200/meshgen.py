@@ -179,7 +179,8 @@ def segments(ikle0, npoin):
     ok, so = key[other], scan[other]
     idx = np.lexsort((so, ok))
     ks = ok[idx]
-    head = np.r_[True, ks[1:] != ks[:-1]]
+    # (a mesh whose every edge is on the boundary has no other edges)
+    head = np.r_[True, ks[1:] != ks[:-1]] if ks.size else np.zeros(0, dtype=bool)
     first_scan, first_key = so[idx][head], ks[head]
     keys_sorted = first_key[np.argsort(first_scan, kind="stable")]
     g1 = np.concatenate([a[bq], keys_sorted // int(npoin)])

@@ -128,3 +128,15 @@ def test_mixed_seg_converges(oracle_mod, cfg0_problem):
     assert m["status"] == 0 and m["relres"] <= 1e-10
     assert m["inner"] <= 1.3 * f["nit"] + 5
     assert np.linalg.norm(m["x"] - f["x"]) / np.linalg.norm(f["x"]) < 1e-6
+
+
+def test_single_triangle_numbering(oracle_mod):
+    """A mesh of one triangle has boundary segments only (no interior edge
+    to number): the product's numbering still equals STOSEG's."""
+    ik = np.array([[0, 1, 2]])
+    g1, g2, es, ori = mg.segments(ik, 3)
+    be, bf = mg.boundary_faces(ik)
+    o1, o2, oes, oori = oracle_mod.stoseg(ik, 3, be, bf)
+    for a, b in [(g1, o1), (g2, o2), (es, oes), (ori, oori)]:
+        np.testing.assert_array_equal(a, b)
+    assert g1.size == 3
