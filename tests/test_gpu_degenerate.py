@@ -73,3 +73,41 @@ def test_node_outside_every_element(oracle_mod, seg):
     y = np.append(y, 2.0)
     dm = np.append(dm, 2.5)
     _check(oracle_mod, x, y, ik, dm, xm, seg)
+
+
+def test_fan_node_beyond_neighbour_limit(oracle_mod):
+    """One node shared by 80 triangles (80 neighbours): the binary64 MATVEC
+    and GRACJG (any degree) stay bit-exact; the binary32 operator, which
+    holds at most 64 neighbours per node, reports BIEF_ERR_SIZE instead of
+    running."""
+    import torch
+    m = 80
+    ang = 2 * np.pi * np.arange(m) / m
+    x = np.r_[0.0, np.cos(ang)]
+    y = np.r_[0.0, np.sin(ang)]
+    ik = np.array([[0, 1 + i, 1 + (i + 1) % m] for i in range(m)])
+    dm, xm = oracle_mod.wave_matrix(x, y, ik, np.full(m, 3.0))
+    n = x.size
+    mesh = bief.Mesh(ik, n)
+    A = bief.Matrix(mesh, dm, xm, "Q", "S")
+    yv = np.random.default_rng(2).uniform(-1, 1, n)
+    got = np.zeros(n)
+    bief.matvec("X=AY    ", got, A, yv)
+    np.testing.assert_array_equal(got, oracle_mod.matvec("X=AY    ", ik, dm, "Q", xm, "S", yv))
+    b = oracle_mod.matvec("X=AY    ", ik, dm, "Q", xm, "S", yv)
+    G, T = mesh.launch_info()
+    sol = np.zeros(n)
+    cfg = bief.SlvCfg(slv=1, nitmax=10000, precon=2, krylov=0, eps=1e-12, zero=0.0)
+    st, nit, rel = bief.solve(sol, A, b.copy(), cfg)
+    r = oracle_mod.solve(ik, dm, "Q", xm, "S", b, eps=1e-12, nitmax=10000,
+                         dot_mode=oracle_mod.DOT_BLOCKED, nblocks=G, nthreads=T)
+    assert st == 0 and (nit, rel) == (r["nit"], r["relres"])
+    np.testing.assert_array_equal(sol, r["x"])
+    with pytest.raises(bief.BiefError) as e:
+        bief.solve_mixed(np.zeros(n), A, b)
+    assert e.value.status == -9
+    y32 = torch.tensor(yv, dtype=torch.float32, device="cuda")
+    with pytest.raises(bief.BiefError) as e:
+        bief.matvec32(torch.empty_like(y32), A, y32)
+    assert e.value.status == -9
+    mesh.close()
