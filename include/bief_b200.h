@@ -122,7 +122,9 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg,
  * the iteration count of binary64 CG; smaller values refine less often).
  * Stops when the binary64 residual reaches outer_tol (relative to ||D.B||,
  * absolute when that is < 1).  B is not modified.  outer_out/inner_out:
- * refinement steps and total inner iterations. */
+ * refinement steps and total inner iterations.  Symmetric matrices only;
+ * the binary32 operator holds at most 64 neighbours per node (EBE storage),
+ * BIEF_ERR_SIZE beyond (the binary64 SOLVE has no such limit). */
 int bief_solve_mixed(bief_handle *h, double *x, const double *b,
                      int precon, double inner_tol, double outer_tol,
                      int max_outer, int max_inner, int *outer_out,
