@@ -476,7 +476,7 @@ __device__ __forceinline__ T ebe_row(int i, T acc, const int *__restrict__ ptr,
 // their order, so the bits do not depend on the batch sizes.  Measured on
 // B200, per iteration at 4.0M / 1.0M nodes: binary64 GRACJG 183 / 51 us with
 // 4-entry batches against 207 / 56 us unbatched (6-entry batches: 196 / 54);
-// binary32 inner CG 104 / 19.0 us with 6-slot batches against 105 / 20.2
+// binary32 inner CG 104 / 19.0 us with 6-slot batches against 105 / 19.6
 // with 3 and 118 / 21.4 with 5 (interior P1 nodes have 6 neighbours); the
 // half-size batch after the full ones takes the binary64 iteration from
 // 185 / 51.4 to 183 / 50.8 us and changes nothing on a 1M-point Delaunay
