@@ -1,0 +1,50 @@
+"""The device entry points run on the caller's stream: MATVEC, GRACJG, the
+mixed solve and the binary32 MATVEC issued on a non-default stream, with
+their inputs produced asynchronously on that same stream just before, give
+the bits they give on the default stream."""
+import numpy as np
+import pytest
+
+from conftest import small_problem
+from opentelemac_b200 import bief
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(p, stream):
+    import torch
+    n = p["x"].size
+    mesh = bief.Mesh(p["ik"], n)
+    A = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device="cuda")
+    bh, yh = t(p["b"]), t(p["xt"])
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        # inputs produced on the stream itself, right before the calls
+        b = bh * 1.0
+        y = yh * 1.0
+        out = torch.empty_like(y)
+        bief.matvec("X=AY    ", out, A, y)
+        x = torch.zeros_like(b)
+        cfg = bief.SlvCfg(slv=1, nitmax=100000, precon=2, krylov=0, eps=1e-10, zero=0.0)
+        st, nit, rel = bief.solve(x, A, b, cfg)
+        xm = torch.zeros_like(b)
+        stm, outer, inner, relm = bief.solve_mixed(xm, A, b, precon=2, inner_tol=0.1,
+                                                   outer_tol=1e-9)
+        y32 = y.float()
+        o32 = torch.empty_like(y32)
+        bief.matvec32(o32, A, y32)
+        res = [v.cpu().numpy() for v in (out, x, xm, o32)]
+    stream.synchronize()
+    mesh.close()
+    return res, (st, nit, rel, stm, outer, inner, relm)
+
+
+def test_non_default_stream_matches_default(oracle_mod):
+    import torch
+    p = small_problem(oracle_mod, n=81, shuffle=True, field="loguniform")
+    ref, sref = _run(p, torch.cuda.current_stream())
+    got, sgot = _run(p, torch.cuda.Stream())
+    assert sref == sgot and sref[0] == 0 and sref[3] == 0
+    for a, b in zip(ref, got):
+        np.testing.assert_array_equal(a, b)
