@@ -48,3 +48,36 @@ def test_non_default_stream_matches_default(oracle_mod):
     assert sref == sgot and sref[0] == 0 and sref[3] == 0
     for a, b in zip(ref, got):
         np.testing.assert_array_equal(a, b)
+
+
+def test_two_handles_share_no_state(oracle_mod):
+    """Two meshes in one process, calls interleaved on one stream: solving
+    and re-assembling on one handle leaves the other's results unchanged."""
+    import torch
+    pa = small_problem(oracle_mod, n=41, shuffle=True)
+    pb = small_problem(oracle_mod, n=61, field="loguniform")
+    ha, hb = bief.Mesh(pa["ik"], pa["x"].size), bief.Mesh(pb["ik"], pb["x"].size)
+    A = bief.Matrix(ha, pa["dm"], pa["xm"], "Q", "S")
+    B = bief.Matrix(hb, pb["dm"], pb["xm"], "Q", "S")
+    cfg = lambda: bief.SlvCfg(slv=1, nitmax=100000, precon=2, krylov=0, eps=1e-10, zero=0.0)
+
+    def solve_a():
+        x = np.zeros(pa["x"].size)
+        st = bief.solve(x, A, pa["b"].copy(), cfg())
+        xm = np.zeros(pa["x"].size)
+        sm = bief.solve_mixed(xm, A, pa["b"], precon=2, inner_tol=0.1, outer_tol=1e-9)
+        return x, xm, st, sm
+
+    first = solve_a()
+    xb = np.zeros(pb["x"].size)
+    bief.solve(xb, B, pb["b"].copy(), cfg(), mutate=True)          # B's matrix becomes D.B.D
+    bief.solve_mixed(np.zeros(pb["x"].size), B, pb["b"], precon=2, inner_tol=1e-4,
+                     outer_tol=1e-9)
+    t = lambda a: torch.tensor(a, dtype=torch.float64, device="cuda")
+    B.assemble_wave(t(pb["x"]), t(pb["y"]), t(pb["coef"]))            # and is re-assembled
+    again = solve_a()
+    for a, b in zip(first[:2], again[:2]):
+        np.testing.assert_array_equal(a, b)
+    assert first[2:] == again[2:]
+    ha.close()
+    hb.close()
