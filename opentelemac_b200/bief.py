@@ -156,6 +156,21 @@ class Matrix:
         self.typdia = td.value.decode()
         return dm, xm[:nd], self.typdia
 
+    def get_dev(self):
+        """Stored (dm, xm) as torch CUDA float64 tensors on the mesh's device,
+        shaped as get() returns them (TYPDIA is get()'s)."""
+        import torch
+        seg = self.storage == 3
+        nd = ({"S": 1, "Q": 2, "0": 0} if seg else {"S": 3, "Q": 6, "0": 0})[self.typext]
+        dev = torch.device("cuda", self.mesh.device)
+        dm = torch.empty(self.mesh.npoin, dtype=torch.float64, device=dev)
+        xm = torch.empty((max(nd, 1), self.mesh.nseg if seg else self.mesh.nelem),
+                         dtype=torch.float64, device=dev)
+        _check(_native.lib().bief_get_matrix_dev(self.mesh.handle, _ptr(dm), _ptr(xm),
+                                                 _stream(dm)), "bief_get_matrix_dev")
+        torch.cuda.current_stream(dev).synchronize()
+        return dm, xm[:nd]
+
     def set_seg(self, da, xa, typdia="Q", typext="S"):
         """Segment storage (STO=3): DA (npoin,) and XA (nseg,) for 'S' or
         (2, nseg) for 'Q'; numpy arrays or torch CUDA tensors."""

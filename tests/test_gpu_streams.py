@@ -1,7 +1,8 @@
-"""The device entry points run on the caller's stream: MATVEC, GRACJG, the
-mixed solve and the binary32 MATVEC issued on a non-default stream, with
-their inputs produced asynchronously on that same stream just before, give
-the bits they give on the default stream."""
+"""Device-path behaviour: the entry points run on the caller's stream
+(MATVEC, GRACJG, the mixed solve and the binary32 MATVEC issued on a
+non-default stream, inputs produced asynchronously on it just before, give
+the default stream's bits); two handles in one process share no state; the
+device read-back of the stored matrix equals the host read-back."""
 import numpy as np
 import pytest
 
@@ -81,3 +82,27 @@ def test_two_handles_share_no_state(oracle_mod):
     assert first[2:] == again[2:]
     ha.close()
     hb.close()
+
+
+@pytest.mark.parametrize("seg", [False, True])
+def test_device_read_back_equals_host_read_back(oracle_mod, seg):
+    """bief_get_matrix_dev returns the bits bief_get_matrix returns, after a
+    solve that leaves D.A.D in the handle (SOLVE's side effect), in both
+    storages."""
+    from opentelemac_b200 import meshgen as mg
+    p = small_problem(oracle_mod, n=31, shuffle=True)
+    n = p["x"].size
+    mesh = bief.Mesh(p["ik"], n)
+    A = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
+    if seg:
+        g1, g2, _, _ = mg.segments(p["ik"], n)
+        mesh.set_segments(g1, g2)
+        A.to_segments()
+    cfg = bief.SlvCfg(slv=1, nitmax=100000, precon=2, krylov=0, eps=1e-10, zero=0.0)
+    bief.solve(np.zeros(n), A, p["b"].copy(), cfg, mutate=True)
+    dm_h, xm_h, td = A.get()
+    assert td == "I"
+    dm_d, xm_d = A.get_dev()
+    np.testing.assert_array_equal(dm_d.cpu().numpy(), dm_h)
+    np.testing.assert_array_equal(xm_d.cpu().numpy(), xm_h)
+    mesh.close()
