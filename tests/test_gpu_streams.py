@@ -106,3 +106,31 @@ def test_device_read_back_equals_host_read_back(oracle_mod, seg):
     np.testing.assert_array_equal(dm_d.cpu().numpy(), dm_h)
     np.testing.assert_array_equal(xm_d.cpu().numpy(), xm_h)
     mesh.close()
+
+
+def test_segment_matrix_from_device_arrays(oracle_mod):
+    """A segment-storage matrix set from device tensors
+    (bief_set_matrix_seg_dev) holds and multiplies exactly as the same
+    matrix set from host arrays."""
+    import torch
+    from opentelemac_b200 import meshgen as mg
+    p = small_problem(oracle_mod, n=31, shuffle=True)
+    n = p["x"].size
+    g1, g2, es, ori = mg.segments(p["ik"], n)
+    xa = np.ascontiguousarray(oracle_mod.assex3(es, ori, "Q",
+                                                np.concatenate([p["xm"], 1.1 * p["xm"]]),
+                                                g1.size))
+    y = np.random.default_rng(9).uniform(-1, 1, n)
+    outs = []
+    for dev in (False, True):
+        mesh = bief.Mesh(p["ik"], n)
+        mesh.set_segments(g1, g2)
+        t = (lambda a: torch.tensor(a, dtype=torch.float64, device="cuda")) if dev else (lambda a: a)
+        A = bief.Matrix(mesh).set_seg(t(p["dm"]), t(xa), "Q", "Q")
+        o = np.zeros(n)
+        bief.matvec("X=AY    ", o, A, y)
+        dm, xm, _ = A.get()
+        outs.append((o, dm, xm))
+        mesh.close()
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
