@@ -136,12 +136,27 @@ class Matrix:
         else:
             dm = np.ascontiguousarray(dm, dtype=np.float64)
             nd = {"S": 3, "Q": 6, "0": 0}[typext]
-            xm = (np.ascontiguousarray(np.asarray(xm, dtype=np.float64).reshape(nd, -1))
-                  if nd else np.zeros(1))
+            if dm.size != self.mesh.npoin:
+                raise ValueError("dm must have npoin = %d values" % self.mesh.npoin)
+            xm = self._host_xm(xm, nd) if nd else np.zeros(1)
             _check(L.bief_set_matrix(self.mesh.handle, _ptr(dm), _ptr(xm), typdia.encode(),
                                      typext.encode()), "bief_set_matrix")
         self.typdia, self.typext = typdia, typext
         return self
+
+    def _host_xm(self, xm, nd):
+        """XM as the host entry points read it, XM(NELMAX,NDIAG): (nd, nelem)
+        input is padded to the mesh's NELMAX; (nd, nelmax) is taken as is."""
+        xm = np.asarray(xm, dtype=np.float64)
+        ne, nmax = self.mesh.nelem, self.mesh.nelmax
+        if xm.size == nd * nmax:
+            return np.ascontiguousarray(xm.reshape(nd, nmax))
+        if xm.size == nd * ne:
+            out = np.zeros((nd, nmax))
+            out[:, :ne] = xm.reshape(nd, ne)
+            return out
+        raise ValueError("xm must have %d x nelem (%d) or %d x nelmax (%d) values"
+                         % (nd, ne, nd, nmax))
 
     def get(self):
         """Stored (dm, xm, typdia) as numpy arrays: xm (ndiag, nelem) for EBE
@@ -149,12 +164,13 @@ class Matrix:
         seg = self.storage == 3
         nd = ({"S": 1, "Q": 2, "0": 0} if seg else {"S": 3, "Q": 6, "0": 0})[self.typext]
         dm = np.empty(self.mesh.npoin)
-        xm = np.empty((max(nd, 1), self.mesh.nseg if seg else self.mesh.nelem))
+        # the host entry point writes EBE columns with the NELMAX pitch
+        xm = np.empty((max(nd, 1), self.mesh.nseg if seg else self.mesh.nelmax))
         td = ctypes.create_string_buffer(2)
         _check(_native.lib().bief_get_matrix(self.mesh.handle, _ptr(dm), _ptr(xm), td),
                "bief_get_matrix")
         self.typdia = td.value.decode()
-        return dm, xm[:nd], self.typdia
+        return dm, (xm[:nd] if seg else xm[:nd, :self.mesh.nelem]), self.typdia
 
     def get_dev(self):
         """Stored (dm, xm) as torch CUDA float64 tensors on the mesh's device,

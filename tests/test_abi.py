@@ -88,3 +88,22 @@ def test_depth_fields():
     assert 0.5 <= h2.min() and h2.max() <= 500.0
     nb = mg.element_neighbours(ik)
     assert ((nb >= 0).sum(axis=1) >= 1).all()
+
+
+def test_host_xm_nelmax_layout():
+    """Matrix._host_xm gives the XM(NELMAX,NDIAG) block the host entry points
+    read: (nd, nelem) input padded with zeros, (nd, nelmax) taken as is,
+    anything else refused before the library sees it."""
+    from types import SimpleNamespace
+    from opentelemac_b200 import bief
+    A = bief.Matrix.__new__(bief.Matrix)
+    A.mesh = SimpleNamespace(nelem=5, nelmax=8, npoin=6)
+    xm = np.arange(15, dtype=np.float64).reshape(3, 5)
+    out = A._host_xm(xm, 3)
+    assert out.shape == (3, 8) and out.flags.c_contiguous
+    np.testing.assert_array_equal(out[:, :5], xm)
+    assert not out[:, 5:].any()
+    full = np.arange(24.0).reshape(3, 8)
+    np.testing.assert_array_equal(A._host_xm(full.ravel(), 3), full)
+    with pytest.raises(ValueError):
+        A._host_xm(np.zeros(14), 3)

@@ -36,18 +36,24 @@ def _cfg(eps=1e-10):
     return bief.SlvCfg(slv=1, nitmax=100000, precon=2, krylov=0, eps=eps, zero=0.0)
 
 
-def _noalloc(ik, dm, xm, b, cfg):
+def _noalloc(ik, dm, xm, b, cfg, nelmax=None):
+    """nelmax > NELEM pads IKLE with node 0 (out of range) and XM with NaN."""
     import torch
     n, ne = dm.size, ik.shape[0]
-    d_ikle = torch.tensor(mg.ikle_fortran(ik), device="cuda")
+    nelmax = ne if nelmax is None else nelmax
+    fort = mg.ikle_fortran(ik, nelmax=nelmax).reshape(3, nelmax)
+    fort[:, ne:] = 0
+    xm_pad = np.full((3, nelmax), np.nan)
+    xm_pad[:, :ne] = np.asarray(xm).reshape(3, ne)
+    d_ikle = torch.tensor(fort.ravel(), device="cuda")
     d_dm = torch.tensor(dm, device="cuda")
-    d_xm = torch.tensor(np.ascontiguousarray(xm), device="cuda")
+    d_xm = torch.tensor(xm_pad, device="cuda")
     d_x = torch.zeros(n, dtype=torch.float64, device="cuda")
     d_b = torch.tensor(b, device="cuda")
     relres = ctypes.c_double()
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     st = _native.lib().bief_solve_noalloc(
-        n, ne, ne, ctypes.c_void_p(d_ikle.data_ptr()), ctypes.c_void_p(d_dm.data_ptr()),
+        n, ne, nelmax, ctypes.c_void_p(d_ikle.data_ptr()), ctypes.c_void_p(d_dm.data_ptr()),
         ctypes.c_void_p(d_xm.data_ptr()), b"Q", b"S", ctypes.c_void_p(d_x.data_ptr()),
         ctypes.c_void_p(d_b.data_ptr()), ctypes.byref(cfg), ctypes.byref(relres), 0, stream)
     torch.cuda.synchronize()
@@ -72,6 +78,26 @@ def test_noalloc_matches_handle_solve_twice():
         np.testing.assert_array_equal(dm_out, dm_ref)
         np.testing.assert_array_equal(xm_out, xm_ref)
         mesh.close()
+
+
+def test_noalloc_nelmax_padding():
+    """IKLE(NELMAX,3) and XM(NELMAX,3) with NELMAX > NELEM: the rows past
+    NELEM are neither read (node 0 and NaN there) nor written."""
+    ik, mesh, A, dm, xm, b = _problem(61, 3)
+    ne = ik.shape[0]
+    x_ref, b_ref = np.zeros(dm.size), b.copy()
+    st_ref, nit_ref, rel_ref = bief.solve(x_ref, A, b_ref, _cfg(), mutate=True)
+    dm_ref, xm_ref, _ = A.get()
+    cfg = _cfg()
+    st, x, b_out, dm_out, xm_out, rel = _noalloc(ik, dm, xm, b, cfg, nelmax=ne + 29)
+    assert st == st_ref == 0 and cfg.nit == nit_ref and rel == rel_ref
+    np.testing.assert_array_equal(x, x_ref)
+    np.testing.assert_array_equal(b_out, b_ref)
+    np.testing.assert_array_equal(dm_out, dm_ref)
+    xm_out = xm_out.reshape(3, ne + 29)
+    np.testing.assert_array_equal(xm_out[:, :ne], xm_ref)
+    assert np.isnan(xm_out[:, ne:]).all()
+    mesh.close()
 
 
 def test_noalloc_rejects_oversize_and_bad_mesh():
