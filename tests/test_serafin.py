@@ -54,7 +54,7 @@ def test_truncated_file_rejected(tmp_path):
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not present")
-def test_reference_example_files(oracle_mod):
+def test_reference_example_files(oracle_mod, tmp_path):
     files = sorted(glob.glob(os.path.join(REF_EXAMPLES, "*", "geo*.slf")))[:40]
     assert files
     for f in files:
@@ -65,10 +65,9 @@ def test_reference_example_files(oracle_mod):
     f = os.path.join(REF_EXAMPLES, "gouttedo", "f2d_gouttedo.slf")
     s = serafin.read(f)
     assert len(s.times) == 21 and s.var_names[-1] == "WATER DEPTH"
-    tmp = f"/tmp/_slf_rt_{os.getpid()}.slf"
+    tmp = tmp_path / "rt.slf"
     serafin.write(tmp, s)
     a, b = open(f, "rb").read(), open(tmp, "rb").read()
-    os.unlink(tmp)
     assert a[:len(b)] == b and len(a) - len(b) < 8
     # the real mesh through the segment numbering and the oracle's solve
     ik = s.ikle.astype(np.int32)
