@@ -56,6 +56,14 @@ def test_bad_mesh_rejected_on_host():
     st = L.bief_mesh_create(25, ik.shape[0], ik.shape[0] - 1,
                             fort.ctypes.data_as(ctypes.c_void_p), 0, ctypes.byref(h))
     assert st == _native.BIEF_ERR_ARGS
+    st = L.bief_mesh_create(25, 0, 0, fort.ctypes.data_as(ctypes.c_void_p), 0,
+                            ctypes.byref(h))                      # no elements
+    assert st == _native.BIEF_ERR_ARGS
+    # beyond the (e << 2 | k) gather encoding: refused before IKLE is read
+    big = (1 << 29) + 1
+    st = L.bief_mesh_create(25, big, big, fort.ctypes.data_as(ctypes.c_void_p), 0,
+                            ctypes.byref(h))
+    assert st == _native.BIEF_ERR_SIZE and not h.value
 
 
 def test_null_handle_calls():
