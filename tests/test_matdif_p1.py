@@ -7,7 +7,6 @@ against closed-form properties, the device assembly bit for bit against it
 import numpy as np
 import pytest
 
-from conftest import small_problem
 from opentelemac_b200 import bief, meshgen as mg
 
 
