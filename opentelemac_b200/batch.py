@@ -83,7 +83,8 @@ class BatchSolver:
         s = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
         rc = _native.lib().bief_batch_solve_mixed_dev(
             self.mesh.handle, ni, vp(self.node_off), vp(self.npoin),
-            ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(b.data_ptr()), precon, inner_tol,
+            bief._dev(x, self.total_nodes, self.mesh, "x"),
+            bief._dev(b, self.total_nodes, self.mesh, "b"), precon, inner_tol,
             outer_tol, max_outer, max_inner, nodes_per_thread, threads_per_block, vp(st),
             vp(outer), vp(inner), vp(relres), s)
         if rc < 0:

@@ -32,6 +32,31 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+def _dev(a, n, mesh, what, dtype="float64"):
+    """Pointer to a torch tensor handed to a device entry point, after the
+    checks the library cannot make on a device address: contiguous, on the
+    mesh's GPU, of the expected dtype, exactly n values."""
+    import torch
+    if not _is_torch(a) or not a.is_cuda or not a.is_contiguous():
+        raise ValueError(f"{what}: a contiguous CUDA tensor is expected")
+    if a.dtype != getattr(torch, dtype):
+        raise TypeError(f"{what}: {dtype} expected, got {a.dtype}")
+    if a.device.index != mesh.device:
+        raise ValueError(f"{what}: tensor on cuda:{a.device.index}, mesh on cuda:{mesh.device}")
+    if a.numel() != n:
+        raise ValueError(f"{what}: {a.numel()} values, {n} expected")
+    return ctypes.c_void_p(a.data_ptr())
+
+
+def _host_in(a, n, what):
+    """A host input array as the library reads it: float64, contiguous,
+    exactly n values."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.size != n:
+        raise ValueError(f"{what}: {a.size} values, {n} expected")
+    return a
+
+
 def _stream(a):
     import torch
     return ctypes.c_void_p(torch.cuda.current_stream(a.device).cuda_stream)
@@ -97,10 +122,11 @@ class Mesh:
         g1 = np.asarray(g1)
         g2 = np.asarray(g2)
         gl = np.ascontiguousarray(np.concatenate([g1, g2]).astype(np.int32) + 1)
-        self.nseg = int(g1.size)
-        _check(_native.lib().bief_set_segments(self._h, self.nseg, self.nseg,
+        nseg = int(g1.size)
+        _check(_native.lib().bief_set_segments(self._h, nseg, nseg,
                                                gl.ctypes.data_as(ctypes.c_void_p)),
                "bief_set_segments")
+        self.nseg = nseg
         return self
 
     def close(self):
@@ -131,7 +157,10 @@ class Matrix:
     def set(self, dm, xm, typdia="Q", typext="S"):
         L = _native.lib()
         if _is_torch(dm):
-            _check(L.bief_set_matrix_dev(self.mesh.handle, _ptr(dm), _ptr(xm),
+            m = self.mesh
+            nd = {"S": 3, "Q": 6, "0": 0}.get(typext, 0)
+            pxm = _dev(xm, nd * m.nelem, m, "xm") if nd else None
+            _check(L.bief_set_matrix_dev(m.handle, _dev(dm, m.npoin, m, "dm"), pxm,
                                          typdia.encode(), typext.encode()), "bief_set_matrix_dev")
         else:
             dm = np.ascontiguousarray(dm, dtype=np.float64)
@@ -191,14 +220,18 @@ class Matrix:
         """Segment storage (STO=3): DA (npoin,) and XA (nseg,) for 'S' or
         (2, nseg) for 'Q'; numpy arrays or torch CUDA tensors."""
         L = _native.lib()
+        m = self.mesh
+        nc = {"S": 1, "Q": 2, "0": 0}.get(typext, 0)
+        if getattr(m, "nseg", None) is None:      # as the library answers
+            raise BiefError(_native.BIEF_ERR_NO_MATRIX, "segment matrix without numbering")
         if _is_torch(da):
-            _check(L.bief_set_matrix_seg_dev(self.mesh.handle, _ptr(da), _ptr(xa),
+            pxa = _dev(xa, nc * m.nseg, m, "xa") if nc else None
+            _check(L.bief_set_matrix_seg_dev(m.handle, _dev(da, m.npoin, m, "da"), pxa,
                                              typdia.encode(), typext.encode()),
                    "bief_set_matrix_seg_dev")
         else:
-            da = np.ascontiguousarray(da, dtype=np.float64)
-            xa = (np.ascontiguousarray(np.asarray(xa, dtype=np.float64).ravel())
-                  if typext != "0" else np.zeros(1))
+            da = _host_in(da, m.npoin, "da")
+            xa = _host_in(np.asarray(xa).ravel(), nc * m.nseg, "xa") if nc else np.zeros(1)
             _check(L.bief_set_matrix_seg(self.mesh.handle, _ptr(da), _ptr(xa), typdia.encode(),
                                          typext.encode()), "bief_set_matrix_seg")
         self.typdia, self.typext = typdia, typext
@@ -217,9 +250,10 @@ class Matrix:
     def assemble_wave(self, xc, yc, coef):
         """A = M + coef_e K_e from device coordinates and coefficients
         (torch CUDA float64 tensors)."""
-        _check(_native.lib().bief_assemble_wave_dev(self.mesh.handle, _ptr(xc), _ptr(yc),
-                                                    _ptr(coef), _stream(xc)),
-               "bief_assemble_wave_dev")
+        m = self.mesh
+        _check(_native.lib().bief_assemble_wave_dev(
+            m.handle, _dev(xc, m.npoin, m, "x"), _dev(yc, m.npoin, m, "y"),
+            _dev(coef, m.nelem, m, "coef"), _stream(xc)), "bief_assemble_wave_dev")
         self.typdia, self.typext = "Q", "S"
         return self
 
@@ -230,9 +264,13 @@ class Matrix:
         xmul_dif = -1).  torch CUDA float64 tensors."""
         if kind == 12 and v is None:
             raise ValueError("MATDIFUV needs v")
+        m = self.mesh
+        nu = m.nelem if kind == 10 else m.npoin
         _check(_native.lib().bief_assemble_mass_diff_dev(
-            self.mesh.handle, _ptr(xc), _ptr(yc), float(xmul_mass), float(xmul_dif), int(kind),
-            _ptr(u), None if v is None else _ptr(v), _stream(xc)), "bief_assemble_mass_diff_dev")
+            m.handle, _dev(xc, m.npoin, m, "x"), _dev(yc, m.npoin, m, "y"), float(xmul_mass),
+            float(xmul_dif), int(kind), _dev(u, nu, m, "u"),
+            None if v is None else _dev(v, m.npoin, m, "v"), _stream(xc)),
+            "bief_assemble_mass_diff_dev")
         self.typdia, self.typext = "Q", "S"
         return self
 
@@ -250,9 +288,10 @@ def solve(x, A, b, cfg, infogr=False, mutate=False, modass=1):
         _native.BIEF_SOLVE_INFOGR if infogr else 0) | (
         _native.BIEF_SOLVE_MODASS3 if modass == 3 else 0)
     relres = ctypes.c_double()
+    m = A.mesh
     if _is_torch(x):
-        st = L.bief_solve_dev(A.mesh.handle, _ptr(x), _ptr(b), ctypes.byref(cfg), flags,
-                              ctypes.byref(relres), _stream(x))
+        st = L.bief_solve_dev(m.handle, _dev(x, m.npoin, m, "x"), _dev(b, m.npoin, m, "b"),
+                              ctypes.byref(cfg), flags, ctypes.byref(relres), _stream(x))
     else:
         _host_vec(x, A.mesh.npoin)
         _host_vec(b, A.mesh.npoin)
@@ -272,13 +311,15 @@ def solve_mixed(x, A, b, precon=2, inner_tol=0.1, outer_tol=1e-8, max_outer=1000
     L = _native.lib()
     o, i = ctypes.c_int(), ctypes.c_int()
     relres = ctypes.c_double()
+    m = A.mesh
     if _is_torch(x):
-        st = L.bief_solve_mixed_dev(A.mesh.handle, _ptr(x), _ptr(b), precon, inner_tol,
-                                    outer_tol, max_outer, max_inner, ctypes.byref(o),
-                                    ctypes.byref(i), ctypes.byref(relres), _stream(x))
+        st = L.bief_solve_mixed_dev(m.handle, _dev(x, m.npoin, m, "x"), _dev(b, m.npoin, m, "b"),
+                                    precon, inner_tol, outer_tol, max_outer, max_inner,
+                                    ctypes.byref(o), ctypes.byref(i), ctypes.byref(relres),
+                                    _stream(x))
     else:
         _host_vec(x, A.mesh.npoin)
-        b = np.ascontiguousarray(b, dtype=np.float64)
+        b = _host_in(b, A.mesh.npoin, "b")
         st = L.bief_solve_mixed(A.mesh.handle, _ptr(x), _ptr(b), precon, inner_tol, outer_tol,
                                 max_outer, max_inner, ctypes.byref(o), ctypes.byref(i),
                                 ctypes.byref(relres))
@@ -290,11 +331,13 @@ def matvec(op, x, A, y, c=0.0):
     """MATVEC(OP,X,A,Y,C,MESH,LEGO=.TRUE.): X updated in place."""
     L = _native.lib()
     opb = op.encode() if isinstance(op, str) else op
+    m = A.mesh
     if _is_torch(x):
-        st = L.bief_matvec_dev(A.mesh.handle, opb, _ptr(x), _ptr(y), float(c), _stream(x))
+        st = L.bief_matvec_dev(m.handle, opb, _dev(x, m.npoin, m, "x"),
+                               _dev(y, m.npoin, m, "y"), float(c), _stream(x))
     else:
         _host_vec(x, A.mesh.npoin)
-        y = np.ascontiguousarray(y, dtype=np.float64)
+        y = _host_in(y, A.mesh.npoin, "y")
         st = L.bief_matvec(A.mesh.handle, opb, _ptr(x), _ptr(y), float(c))
     _check(st, "MATVEC")
     return x
@@ -304,12 +347,11 @@ def matvec32(x, A, y):
     """X = A Y in binary32 on the binary32 copy of A that the mixed-precision
     inner CG uses (symmetric matrices); x and y are float32 CUDA tensors,
     x updated in place.  No reference counterpart."""
-    import torch
-    if not (_is_torch(x) and _is_torch(y)) or x.dtype != torch.float32 or y.dtype != torch.float32:
+    m = A.mesh
+    if not (_is_torch(x) and _is_torch(y)):
         raise TypeError("matvec32 takes float32 CUDA tensors")
-    if x.numel() != A.mesh.npoin or y.numel() != A.mesh.npoin:
-        raise ValueError("matvec32: vectors of NPOIN values expected")
-    st = _native.lib().bief_matvec32_dev(A.mesh.handle, _ptr(x), _ptr(y), _stream(x))
+    st = _native.lib().bief_matvec32_dev(m.handle, _dev(x, m.npoin, m, "x", "float32"),
+                                         _dev(y, m.npoin, m, "y", "float32"), _stream(x))
     _check(st, "MATVEC32")
     return x
 
@@ -323,19 +365,26 @@ def diri01(A, nbor, limdir, kdir, fbor, sm, f, maskpt=None):
     if _is_torch(sm):
         import torch
         dev = sm.device
+        m = A.mesh
         nb = torch.as_tensor(np.ascontiguousarray(nbor, dtype=np.int32), device=dev)
         ld = torch.as_tensor(np.ascontiguousarray(limdir, dtype=np.int32), device=dev)
         fb = torch.as_tensor(fbor, dtype=torch.float64, device=dev).contiguous()
-        st = L.bief_diri01_dev(A.mesh.handle, int(nb.numel()), _ptr(nb), _ptr(ld), int(kdir),
-                               _ptr(fb), _ptr(sm), _ptr(f),
-                               None if maskpt is None else _ptr(maskpt), _stream(sm))
+        nptfr = int(nb.numel())
+        if ld.numel() != nptfr or fb.numel() != nptfr:
+            raise ValueError("DIRI01: nbor, limdir and fbor must have NPTFR values each")
+        st = L.bief_diri01_dev(m.handle, nptfr, _ptr(nb), _ptr(ld), int(kdir), _ptr(fb),
+                               _dev(sm, m.npoin, m, "sm"), _dev(f, m.npoin, m, "f"),
+                               None if maskpt is None else _dev(maskpt, m.npoin, m, "maskpt"),
+                               _stream(sm))
     else:
         _host_vec(sm, A.mesh.npoin)
         _host_vec(f, A.mesh.npoin)
         nb = np.ascontiguousarray(nbor, dtype=np.int32)
         ld = np.ascontiguousarray(limdir, dtype=np.int32)
         fb = np.ascontiguousarray(fbor, dtype=np.float64)
-        mk = None if maskpt is None else np.ascontiguousarray(maskpt, dtype=np.float64)
+        if ld.size != nb.size or fb.size != nb.size:
+            raise ValueError("DIRI01: nbor, limdir and fbor must have NPTFR values each")
+        mk = None if maskpt is None else _host_in(maskpt, A.mesh.npoin, "maskpt")
         st = L.bief_diri01(A.mesh.handle, int(nb.size), _ptr(nb), _ptr(ld), int(kdir), _ptr(fb),
                            _ptr(sm), _ptr(f), None if mk is None else _ptr(mk))
     _check(st, "DIRI01")
@@ -344,9 +393,11 @@ def diri01(A, nbor, limdir, kdir, fbor, sm, f, maskpt=None):
 
 def coef_grad(A, xc, yc, lam, x, grad):
     """grad[e] = -lam_e^T K_e x_e (device tensors)."""
-    _check(_native.lib().bief_wave_coef_grad_dev(A.mesh.handle, _ptr(xc), _ptr(yc), _ptr(lam),
-                                                 _ptr(x), _ptr(grad), _stream(x)),
-           "bief_wave_coef_grad_dev")
+    m = A.mesh
+    _check(_native.lib().bief_wave_coef_grad_dev(
+        m.handle, _dev(xc, m.npoin, m, "x coordinates"), _dev(yc, m.npoin, m, "y coordinates"),
+        _dev(lam, m.npoin, m, "lam"), _dev(x, m.npoin, m, "x"), _dev(grad, m.nelem, m, "grad"),
+        _stream(x)), "bief_wave_coef_grad_dev")
     return grad
 
 
@@ -355,12 +406,18 @@ def mass_diff_grad(A, xc, yc, u, v, lam, x, kind=12, xmul_dif=1.0):
     Matrix.assemble_mass_diff (kind 11 or 12), given the adjoint lam
     (A^T lam = dL/dx); dL/dv is None for kind 11.  Device tensors."""
     import torch
+    m = A.mesh
+    if kind == 12 and v is None:
+        raise ValueError("MATDIFUV needs v")
     gu = torch.empty_like(u)
     gv = torch.empty_like(u) if kind == 12 else None
     _check(_native.lib().bief_mass_diff_grad_dev(
-        A.mesh.handle, _ptr(xc), _ptr(yc), float(xmul_dif), int(kind), _ptr(u),
-        None if v is None else _ptr(v), _ptr(lam), _ptr(x), _ptr(gu),
-        None if gv is None else _ptr(gv), _stream(x)), "bief_mass_diff_grad_dev")
+        m.handle, _dev(xc, m.npoin, m, "x coordinates"), _dev(yc, m.npoin, m, "y coordinates"),
+        float(xmul_dif), int(kind), _dev(u, m.npoin, m, "u"),
+        None if v is None else _dev(v, m.npoin, m, "v"), _dev(lam, m.npoin, m, "lam"),
+        _dev(x, m.npoin, m, "x"), _dev(gu, m.npoin, m, "gu"),
+        None if gv is None else _dev(gv, m.npoin, m, "gv"), _stream(x)),
+        "bief_mass_diff_grad_dev")
     return gu, gv
 
 

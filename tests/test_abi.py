@@ -115,3 +115,19 @@ def test_host_xm_nelmax_layout():
     np.testing.assert_array_equal(A._host_xm(full.ravel(), 3), full)
     with pytest.raises(ValueError):
         A._host_xm(np.zeros(14), 3)
+
+
+def test_argument_checks_before_the_library():
+    """What the library cannot check on a device address is checked in
+    Python first: a CPU tensor, a wrong size or dtype never reaches a
+    kernel.  (CUDA-tensor cases are in tests/test_gpu_validation.py.)"""
+    from types import SimpleNamespace
+    import torch
+    from opentelemac_b200 import bief
+    m = SimpleNamespace(npoin=4, nelem=2, device=0)
+    with pytest.raises(ValueError):
+        bief._dev(torch.zeros(4, dtype=torch.float64), 4, m, "x")
+    with pytest.raises(ValueError):
+        bief._host_in(np.zeros(3), 4, "b")
+    a = bief._host_in([1, 2, 3, 4], 4, "b")
+    assert a.dtype == np.float64 and a.flags.c_contiguous
