@@ -496,6 +496,17 @@ constexpr int SLOT_B32 = BIEF_SLOT_BATCH32;  // binary32 slots
 // single entries
 constexpr bool SLOT_CASCADE = BIEF_SLOT_CASCADE;
 
+// Loads of the operator streams (binary64 records or segment slots, binary32
+// slots): each value is read once per product.  When the kernel's working
+// set exceeds the L2 the host sets the stream's flag in Sell and the loads
+// are marked evict-first (ld.global.cs), so that the gathered node values,
+// reused by every neighbour, keep their place in L2; otherwise they go
+// through the read-only path and the whole operator can stay resident.
+template <class T>
+__device__ __forceinline__ T ld_op(const T *p, int evict_first) {
+  return evict_first ? __ldcs(p) : __ldg(p);
+}
+
 struct Sell {
   const int *meta;        // per node: gather entries | neighbours << 16
   const int *rec_off;     // per slice: first record
@@ -506,6 +517,8 @@ struct Sell {
   const float *seg_c;     // per slot: binary32 coefficient
   const float *s32;       // per node: binary32 row sum
   const double *sg_c;     // segment storage: per slot, binary64 XA1/XA2
+  int cs_rec;             // binary64 operator loads evict-first (ld_op)
+  int cs_seg;             // binary32 slot loads evict-first
 };
 
 // Two rows at once (nodes i0 and, if has1, i1): independent load chains
@@ -520,8 +533,8 @@ __device__ __forceinline__ void rec_batch(double &a0, const Sell &S, int b0, int
   double ya[NB], yb[NB];
 #pragma unroll
   for (int q = 0; q < NB; ++q) {
-    c[q] = __ldg(S.rec_c + b0 + 32 * (m + q));
-    v[q] = __ldg(S.rec_idx + b0 + 32 * (m + q));
+    c[q] = ld_op(S.rec_c + b0 + 32 * (m + q), S.cs_rec);
+    v[q] = ld_op(S.rec_idx + b0 + 32 * (m + q), S.cs_rec);
   }
 #pragma unroll
   for (int q = 0; q < NB; ++q) {
@@ -548,8 +561,8 @@ __device__ __forceinline__ void rec_row2(int i0, int i1, bool has1, double &a0, 
         }
       }
       for (; m < d0; ++m) {
-        const double2 c = __ldg(S.rec_c + b0 + 32 * m);
-        const int2 v = __ldg(S.rec_idx + b0 + 32 * m);
+        const double2 c = ld_op(S.rec_c + b0 + 32 * m, S.cs_rec);
+        const int2 v = ld_op(S.rec_idx + b0 + 32 * m, S.cs_rec);
         a0 = add(a0, add(mul(c.x, vec(v.x)), mul(c.y, vec(v.y))));
       }
       return;
@@ -562,13 +575,13 @@ __device__ __forceinline__ void rec_row2(int i0, int i1, bool has1, double &a0, 
   const int dm = max(d0, d1);
   for (int m = 0; m < dm; ++m) {
     if (m < d0) {
-      const double2 c = __ldg(S.rec_c + b0 + 32 * m);
-      const int2 v = __ldg(S.rec_idx + b0 + 32 * m);
+      const double2 c = ld_op(S.rec_c + b0 + 32 * m, S.cs_rec);
+      const int2 v = ld_op(S.rec_idx + b0 + 32 * m, S.cs_rec);
       a0 = add(a0, add(mul(c.x, vec(v.x)), mul(c.y, vec(v.y))));
     }
     if (m < d1) {
-      const double2 c = __ldg(S.rec_c + b1 + 32 * m);
-      const int2 v = __ldg(S.rec_idx + b1 + 32 * m);
+      const double2 c = ld_op(S.rec_c + b1 + 32 * m, S.cs_rec);
+      const int2 v = ld_op(S.rec_idx + b1 + 32 * m, S.cs_rec);
       a1 = add(a1, add(mul(c.x, vec(v.x)), mul(c.y, vec(v.y))));
     }
   }
@@ -585,8 +598,8 @@ __device__ __forceinline__ void sgr_batch(double &a0, const Sell &S, int b0, int
   int j[NB];
 #pragma unroll
   for (int q = 0; q < NB; ++q) {
-    c[q] = __ldg(S.sg_c + b0 + 32 * (m + q));
-    j[q] = __ldg(S.seg_col + b0 + 32 * (m + q));
+    c[q] = ld_op(S.sg_c + b0 + 32 * (m + q), S.cs_rec);
+    j[q] = ld_op(S.seg_col + b0 + 32 * (m + q), S.cs_rec);
   }
 #pragma unroll
   for (int q = 0; q < NB; ++q) v[q] = vec(j[q]);
@@ -610,7 +623,7 @@ __device__ __forceinline__ void sgr_row2(int i0, int i1, bool has1, double &a0, 
         }
       }
       for (; m < d0; ++m)
-        a0 = add(a0, mul(__ldg(S.sg_c + b0 + 32 * m), vec(__ldg(S.seg_col + b0 + 32 * m))));
+        a0 = add(a0, mul(ld_op(S.sg_c + b0 + 32 * m, S.cs_rec), vec(ld_op(S.seg_col + b0 + 32 * m, S.cs_rec))));
       return;
     }
   }
@@ -620,8 +633,8 @@ __device__ __forceinline__ void sgr_row2(int i0, int i1, bool has1, double &a0, 
   const int b1 = has1 ? __ldg(S.rec_off + (i1 >> 5)) + (i1 & 31) : 0;
   const int dm = max(d0, d1);
   for (int m = 0; m < dm; ++m) {
-    if (m < d0) a0 = add(a0, mul(__ldg(S.sg_c + b0 + 32 * m), vec(__ldg(S.seg_col + b0 + 32 * m))));
-    if (m < d1) a1 = add(a1, mul(__ldg(S.sg_c + b1 + 32 * m), vec(__ldg(S.seg_col + b1 + 32 * m))));
+    if (m < d0) a0 = add(a0, mul(ld_op(S.sg_c + b0 + 32 * m, S.cs_rec), vec(ld_op(S.seg_col + b0 + 32 * m, S.cs_rec))));
+    if (m < d1) a1 = add(a1, mul(ld_op(S.sg_c + b1 + 32 * m, S.cs_rec), vec(ld_op(S.seg_col + b1 + 32 * m, S.cs_rec))));
   }
 }
 
@@ -643,8 +656,8 @@ __device__ __forceinline__ void seg_batch(float &a0, float y0, const Sell &S, in
   float c[NB], v[NB];
 #pragma unroll
   for (int q = 0; q < NB; ++q) {
-    j[q] = __ldg(S.seg_col + b0 + 32 * (m + q));
-    c[q] = __ldg(S.seg_c + b0 + 32 * (m + q));
+    j[q] = ld_op(S.seg_col + b0 + 32 * (m + q), S.cs_seg);
+    c[q] = ld_op(S.seg_c + b0 + 32 * (m + q), S.cs_seg);
   }
 #pragma unroll
   for (int q = 0; q < NB; ++q) v[q] = vec(j[q]);
@@ -667,8 +680,8 @@ __device__ __forceinline__ float seg_row_nb(int i0, int n0, int b0, float s, flo
     }
   }
   for (; m < n0; ++m) {
-    const int jj = __ldg(S.seg_col + b0 + 32 * m);
-    const float cc = __ldg(S.seg_c + b0 + 32 * m);
+    const int jj = ld_op(S.seg_col + b0 + 32 * m, S.cs_seg);
+    const float cc = ld_op(S.seg_c + b0 + 32 * m, S.cs_seg);
     a0 = add(a0, mul(cc, sub(vec(jj), y0)));
   }
   return a0;
@@ -695,13 +708,13 @@ __device__ __forceinline__ void seg_row2(int i0, int i1, bool has1, float y0, fl
   const int nm = max(n0, n1);
   for (int m = 0; m < nm; ++m) {
     if (m < n0) {
-      const int j = __ldg(S.seg_col + b0 + 32 * m);
-      const float c = __ldg(S.seg_c + b0 + 32 * m);
+      const int j = ld_op(S.seg_col + b0 + 32 * m, S.cs_seg);
+      const float c = ld_op(S.seg_c + b0 + 32 * m, S.cs_seg);
       a0 = add(a0, mul(c, sub(vec(j), y0)));
     }
     if (m < n1) {
-      const int j = __ldg(S.seg_col + b1 + 32 * m);
-      const float c = __ldg(S.seg_c + b1 + 32 * m);
+      const int j = ld_op(S.seg_col + b1 + 32 * m, S.cs_seg);
+      const float c = ld_op(S.seg_c + b1 + 32 * m, S.cs_seg);
       a1 = add(a1, mul(c, sub(vec(j), y1)));
     }
   }
