@@ -292,7 +292,10 @@ const char *bief_strerror(int status);
  * nodes and 131,072 elements (NELMAX), else BIEF_ERR_SIZE.  Calls share
  * that array, so calls that overlap on the GPU race; the first call on a
  * device looks up the array's address and should come before any stream
- * capture.  TYPEXT 'S' or 'Q'. */
+ * capture.  Every call, not only the first, waits for its stream twice
+ * (the IKLE check and the result are read back to the host before it
+ * returns).  Configuration errors get bief_solve's codes; SLV other than 1
+ * is BIEF_ERR_UNSUPPORTED.  TYPEXT 'S' or 'Q'. */
 int bief_solve_noalloc(int npoin, int nelem, int nelmax, const int *ikle,
                        double *dm, double *xm, char typdia, char typext,
                        double *x, double *b, bief_slvcfg *cfg,

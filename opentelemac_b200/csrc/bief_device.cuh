@@ -80,6 +80,15 @@ struct Ctl {
   double relres;                // SQRT(RMRM/XL) at exit
 };
 
+// Final status of a launch, written by its lead thread.  A block whose
+// barrier wait ran out has already stored ST_TIMEOUT (and returned without
+// finishing its share of the work); the other blocks may still pass that
+// barrier and converge, so the lead only replaces a status that is still
+// ST_OK: the host then sees the timeout, never a silently partial result.
+__device__ __forceinline__ void set_status(Ctl *ctl, int status) {
+  atomicCAS(&ctl->status, (int)ST_OK, status);
+}
+
 // Grid-wide reduction + barrier.  Each block reduces its thread partials
 // with block_tree (ND binary64 values, NF binary32 values); thread 0 stores
 // them in this barrier's half of `part` (two halves used alternately, so a

@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
     if (P.dsc)  // solve.f:637-641: X = X*D
       for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
     if (lead) {
-      P.ctl->status = status;
+      set_status(P.ctl, status);
       P.ctl->nit = m;
       P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
       P.ctl->relat = relat;
@@ -594,7 +594,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_equnor(EqP P) {
     if (P.dsc)  // solve.f:637-641: X = X*D
       for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
     if (lead) {
-      P.ctl->status = status;
+      set_status(P.ctl, status);
       P.ctl->nit = m;
       P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
       P.ctl->relat = relat;
@@ -739,7 +739,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_rescjg(Kry2P P) {
     if (P.dsc)
       for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
     if (lead) {
-      P.ctl->status = status;
+      set_status(P.ctl, status);
       P.ctl->nit = m;
       P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
       P.ctl->relat = relat;
@@ -841,7 +841,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_errmin(Kry2P P) {
     if (P.dsc)
       for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
     if (lead) {
-      P.ctl->status = status;
+      set_status(P.ctl, status);
       P.ctl->nit = m;
       P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
       P.ctl->relat = relat;
@@ -976,7 +976,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgsqua(SquaP P) {
     if (P.dsc)
       for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
     if (lead) {
-      P.ctl->status = status;
+      set_status(P.ctl, status);
       P.ctl->nit = m;
       P.ctl->relres = __dsqrt_rn(__ddiv_rn(rl, xl));
       P.ctl->relat = relat;
@@ -1092,7 +1092,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgstab(StabP P) {
     if (P.dsc)  // solve.f:637-641: X = X*D
       for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
     if (lead) {
-      P.ctl->status = status;
+      set_status(P.ctl, status);
       P.ctl->nit = m;
       P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
       P.ctl->relat = relat;
@@ -1333,7 +1333,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
     if (P.dsc)  // solve.f:637-641: X = X*D
       for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
     if (lead) {
-      P.ctl->status = m < P.nitmax ? ST_OK : m;   // gmres.f:199-214 end messages
+      set_status(P.ctl, m < P.nitmax ? ST_OK : m);   // gmres.f:199-214 end messages
       P.ctl->nit = m;
       P.ctl->relres = prec;
       P.ctl->relat = relat;
@@ -1358,7 +1358,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
   if (!dred<COMP, 1>(P.ctl, P.part, P.timeout_ns, nbar, s, &red)) return;
   double nr0 = __dsqrt_rn(red);
   prec = __ddiv_rn(nr0, nbn);
-  if (isnan(prec)) { if (lead) P.ctl->status = ST_NAN; return; }
+  if (isnan(prec)) { if (lead) set_status(P.ctl, ST_NAN); return; }
   if (prec <= P.eps) { finish(); return; }   // :87
 
   for (;;) {
@@ -1551,7 +1551,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_mixed(MixP P) {
     if (P.dsc)
       for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
     if (lead) {
-      P.ctl->status = status;
+      set_status(P.ctl, status);
       P.ctl->nit = inner;
       P.ctl->outer = outer;
       P.ctl->relres = __dsqrt_rn(__ddiv_rn(rr, xl));

@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(NA_THREADS, 1) k_na_cg(NaP P) {
     if (P.dsc)
       for (int i = lo + t; i < hi; i += T) x[i] = mul(x[i], P.dsc[i]);
     if (lead) {
-      P.ctl->status = status;
+      set_status(P.ctl, status);
       P.ctl->nit = m;
       P.ctl->relres = __dsqrt_rn(__ddiv_rn(rmrm, xl));
       P.ctl->relat = relat;
@@ -313,10 +313,15 @@ extern "C" int bief_solve_noalloc(int npoin, int nelem, int nelmax, const int *i
   if (td_in < 0 || (typext != 'S' && typext != 'Q' && typext != '0')) return BIEF_ERR_ARGS;
   if (typext == '0') return BIEF_ERR_UNSUPPORTED;  // diagonal-only systems: use bief_solve
   if (!xm) return BIEF_ERR_ARGS;
-  if (cfg->slv != 1) return BIEF_ERR_UNSUPPORTED;
+  // the configuration checks of bief_solve, in its order and with its
+  // codes, then the one method this entry point runs
+  if (cfg->slv < 1 || cfg->slv > 7) return BIEF_ERR_UNSUPPORTED;
+  if (cfg->slv == 7 && (cfg->krylov < 1 || cfg->krylov > 20)) return BIEF_ERR_ARGS;
   const int precon = cfg->precon == 0 ? 1 : cfg->precon;
-  if (precon <= 0 || precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 || precon % 17 == 0)
+  if (precon <= 0) return BIEF_ERR_ARGS;
+  if (precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 || precon % 17 == 0)
     return BIEF_ERR_UNSUPPORTED;
+  if (cfg->slv != 1) return BIEF_ERR_UNSUPPORTED;
   if (device < 0 || device >= 256) return BIEF_ERR_ARGS;
 
   int prev = -1;

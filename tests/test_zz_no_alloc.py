@@ -36,15 +36,16 @@ def _cfg(eps=1e-10):
     return bief.SlvCfg(slv=1, nitmax=100000, precon=2, krylov=0, eps=eps, zero=0.0)
 
 
-def _noalloc(ik, dm, xm, b, cfg, nelmax=None):
+def _noalloc(ik, dm, xm, b, cfg, nelmax=None, typdia="Q", typext="S"):
     """nelmax > NELEM pads IKLE with node 0 (out of range) and XM with NaN."""
     import torch
     n, ne = dm.size, ik.shape[0]
+    nd = 6 if typext == "Q" else 3
     nelmax = ne if nelmax is None else nelmax
     fort = mg.ikle_fortran(ik, nelmax=nelmax).reshape(3, nelmax)
     fort[:, ne:] = 0
-    xm_pad = np.full((3, nelmax), np.nan)
-    xm_pad[:, :ne] = np.asarray(xm).reshape(3, ne)
+    xm_pad = np.full((nd, nelmax), np.nan)
+    xm_pad[:, :ne] = np.asarray(xm).reshape(nd, ne)
     d_ikle = torch.tensor(fort.ravel(), device="cuda")
     d_dm = torch.tensor(dm, device="cuda")
     d_xm = torch.tensor(xm_pad, device="cuda")
@@ -54,15 +55,19 @@ def _noalloc(ik, dm, xm, b, cfg, nelmax=None):
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     st = _native.lib().bief_solve_noalloc(
         n, ne, nelmax, ctypes.c_void_p(d_ikle.data_ptr()), ctypes.c_void_p(d_dm.data_ptr()),
-        ctypes.c_void_p(d_xm.data_ptr()), b"Q", b"S", ctypes.c_void_p(d_x.data_ptr()),
-        ctypes.c_void_p(d_b.data_ptr()), ctypes.byref(cfg), ctypes.byref(relres), 0, stream)
+        ctypes.c_void_p(d_xm.data_ptr()), typdia.encode(), typext.encode(),
+        ctypes.c_void_p(d_x.data_ptr()), ctypes.c_void_p(d_b.data_ptr()), ctypes.byref(cfg),
+        ctypes.byref(relres), 0, stream)
     torch.cuda.synchronize()
     return st, d_x.cpu().numpy(), d_b.cpu().numpy(), d_dm.cpu().numpy(), d_xm.cpu().numpy(), \
         relres.value
 
 
 def test_noalloc_matches_handle_solve_twice():
-    for n, seed in ((101, 4), (181, 7)):          # two calls in a row, two meshes
+    # calls in a row: a larger mesh after a smaller one, then a smaller one
+    # after the larger (whatever the previous call left in the scratch must
+    # not reach the next)
+    for n, seed in ((101, 4), (181, 7), (61, 8)):
         ik, mesh, A, dm, xm, b = _problem(n, seed)
         ref_cfg = _cfg()
         x_ref, b_ref = np.zeros(dm.size), b.copy()
@@ -123,3 +128,93 @@ def test_noalloc_rejects_oversize_and_bad_mesh():
                               b"S", ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(d.data_ptr()),
                               ctypes.byref(cfg), None, 0, None)
     assert st == _native.BIEF_ERR_BAD_MESH
+
+
+def _variant(n, seed, typdia, typext):
+    """A wave-equation matrix with the given TYPDIA, and for TYPEXT 'Q' a
+    non-symmetric copy: the lower triangle (M21, M31, M32) perturbed by up to
+    1% per element."""
+    ik, mesh, A, dm, xm, b = _problem(n, seed)
+    xm = np.asarray(xm).reshape(3, -1)
+    if typext == "Q":
+        f = np.random.default_rng(seed + 1).uniform(0.99, 1.01, xm.shape)
+        xm = np.concatenate([xm, xm * f])
+    A.set(dm, xm, typdia, typext)
+    return ik, mesh, A, dm, xm, b
+
+
+@pytest.mark.parametrize("typext", ["S", "Q"])
+@pytest.mark.parametrize("typdia", ["Q", "I"])
+@pytest.mark.parametrize("precon", [1, 2, 5])
+def test_noalloc_variants_match_handle(precon, typdia, typext):
+    """Every storage and preconditioning branch of the kernels behind the
+    entry point (the non-symmetric kernel with six off-diagonal columns, no
+    change of variables for PRECON 1, |DM| for PRECON 5, both diagonal
+    kinds): bit for bit what bief_solve_dev gives, at convergence or at
+    NITMAX, side effects included, on two meshes called in a row."""
+    for n, seed in ((81, 5), (41, 9)):
+        ik, mesh, A, dm, xm, b = _variant(n, seed, typdia, typext)
+        cfg_ref = bief.SlvCfg(slv=1, nitmax=400, precon=precon, krylov=0, eps=1e-10, zero=0.0)
+        x_ref, b_ref = np.zeros(dm.size), b.copy()
+        st_ref, nit_ref, rel_ref = bief.solve(x_ref, A, b_ref, cfg_ref, mutate=True)
+        dm_ref, xm_ref, _ = A.get()
+        cfg = bief.SlvCfg(slv=1, nitmax=400, precon=precon, krylov=0, eps=1e-10, zero=0.0)
+        st, x, b_out, dm_out, xm_out, rel = _noalloc(ik, dm, xm, b, cfg, typdia=typdia,
+                                                     typext=typext)
+        assert st == st_ref and st >= 0
+        assert cfg.nit == nit_ref and cfg.ok == cfg_ref.ok and rel == rel_ref
+        np.testing.assert_array_equal(x, x_ref)
+        np.testing.assert_array_equal(b_out, b_ref)
+        np.testing.assert_array_equal(dm_out, dm_ref)
+        np.testing.assert_array_equal(xm_out.reshape(xm_ref.shape), xm_ref)
+        mesh.close()
+
+
+def test_noalloc_valid_solve_after_bad_mesh():
+    """A call refused for a bad IKLE leaves nothing behind that changes the
+    next, valid call."""
+    import torch
+    L = _native.lib()
+    _, _, ik_bad = mg.square_mesh(11)
+    fort = mg.ikle_fortran(ik_bad)
+    fort[3] = 0
+    d_ikle = torch.tensor(fort, device="cuda")
+    d = torch.ones(121, dtype=torch.float64, device="cuda")
+    dx = torch.zeros(3 * ik_bad.shape[0], dtype=torch.float64, device="cuda")
+    cfg = _cfg()
+    st = L.bief_solve_noalloc(121, ik_bad.shape[0], ik_bad.shape[0],
+                              ctypes.c_void_p(d_ikle.data_ptr()), ctypes.c_void_p(d.data_ptr()),
+                              ctypes.c_void_p(dx.data_ptr()), b"Q", b"S",
+                              ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(d.data_ptr()),
+                              ctypes.byref(cfg), None, 0, None)
+    assert st == _native.BIEF_ERR_BAD_MESH
+    ik, mesh, A, dm, xm, b = _problem(51, 6)
+    x_ref, b_ref = np.zeros(dm.size), b.copy()
+    st_ref, nit_ref, rel_ref = bief.solve(x_ref, A, b_ref, _cfg(), mutate=True)
+    cfg = _cfg()
+    st, x, b_out, _, _, rel = _noalloc(ik, dm, xm, b, cfg)
+    assert st == st_ref == 0 and cfg.nit == nit_ref and rel == rel_ref
+    np.testing.assert_array_equal(x, x_ref)
+    np.testing.assert_array_equal(b_out, b_ref)
+    mesh.close()
+
+
+@pytest.mark.parametrize("slv,precon,krylov,want", [
+    (1, -1, 0, "ARGS"), (1, -6, 0, "ARGS"), (1, 7, 0, "UNSUPPORTED"), (1, 22, 0, "UNSUPPORTED"),
+    (8, 2, 0, "UNSUPPORTED"), (0, 2, 0, "UNSUPPORTED"), (7, 2, 0, "ARGS"), (7, 2, 5, "UNSUPPORTED"),
+    (3, 2, 0, "UNSUPPORTED")])
+def test_noalloc_config_errors_match_handle(slv, precon, krylov, want):
+    """A configuration the path does not take is refused with the code
+    bief_solve gives for it (SLV 2..7 are valid there but not here)."""
+    import torch
+    ik, mesh, A, dm, xm, b = _problem(21, 2)
+    code = getattr(_native, "BIEF_ERR_" + want)
+    cfg = bief.SlvCfg(slv=slv, nitmax=10, precon=precon, krylov=krylov, eps=1e-8, zero=0.0)
+    st, *_ = _noalloc(ik, dm, xm, b, cfg)
+    assert st == code
+    if slv not in (2, 3, 4, 5, 6) and not (slv == 7 and krylov > 0):
+        with pytest.raises(_native.BiefError) as ei:
+            bief.solve(np.zeros(dm.size), A, b.copy(), bief.SlvCfg(
+                slv=slv, nitmax=10, precon=precon, krylov=krylov, eps=1e-8, zero=0.0))
+        assert ei.value.status == code
+    mesh.close()
