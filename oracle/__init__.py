@@ -54,10 +54,33 @@ def lib():
         L.orc_precd1.argtypes = [i, i, pi, pi, pi, i, pd, pd, P(c), pd, i, c, pd, pd]
         L.orc_solve.argtypes = [i, i, pi, pi, pi, pd, pd, pd, P(c), pd, i, c, i, i, i, d, i, i,
                                 i, pi, pd, pi, i]
+        L.orc_set_threads.argtypes = [i]
         L.orc_solve_mixed.argtypes = [i, i, pi, pi, pi, pd, pd, pd, c, pd, c, i, d, d, i, i, i,
                                       i, pi, pi, pd]
         _lib = L
     return _lib
+
+
+def set_threads(n):
+    """Host threads of the restatement's large-case runs (1: the sequential
+    code).  Loops with independent iterations are shared out; every sum
+    keeps its order, so the results are the same bits with any count."""
+    lib().orc_set_threads(int(n))
+
+
+class threads:
+    """Context manager: run the enclosed oracle calls on n host threads
+    (all of the host's by default), then return to one."""
+
+    def __init__(self, n=None):
+        self.n = n or (os.cpu_count() or 1)
+
+    def __enter__(self):
+        set_threads(self.n)
+        return self
+
+    def __exit__(self, *exc):
+        set_threads(1)
 
 
 def _pd(a):

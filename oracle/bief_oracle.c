@@ -21,6 +21,27 @@
 #include <omp.h>
 #endif
 
+/* Host threads for the large-case checks (orc_set_threads).  With 1, the
+ * default, every routine runs the sequential code below.  With more, the
+ * loops whose iterations are independent (vector updates, per-node
+ * gathers, per-block dot partials) are shared out with OpenMP; each
+ * iteration computes exactly what it computes sequentially and every sum
+ * keeps its order, so the results are the same bits (checked by
+ * tests/test_oracle_threads.py). */
+static int orc_nthreads = 1;
+
+void orc_set_threads(int n)
+{
+    orc_nthreads = n < 1 ? 1 : n;
+}
+
+/* Whether a loop of n iterations is shared out. */
+#define ORC_PAR(n) (orc_nthreads > 1 && (long long)(n) >= 4096)
+#define ORC_MAX_NT 1024
+#define ORC_PRAGMA(x) _Pragma(#x)
+/* a vector loop of n independent iterations */
+#define ORC_PFOR(n) ORC_PRAGMA(omp parallel for if (ORC_PAR(n)) num_threads(orc_nthreads) schedule(static))
+
 /* ------------------------------------------------------------------ */
 /* mesh geometry                                                        */
 /* ------------------------------------------------------------------ */
@@ -449,7 +470,36 @@ typedef struct {
     const int *ik0, *ik1, *ik2;
     int nseg;
     const int *g1, *g2;
+    /* node -> (element, local point) index in ASSVEC order, set only when
+     * the solve runs on several threads (op_matvec's gather form) */
+    const int *gptr, *gek;
 } opmesh;
+
+/* MATVEC 'X=AY' for symmetric EBE storage as a per-node gather: node i
+ * starts from MATVCT's diagonal term and adds, in ASSVEC's order (local
+ * point, then element), the W(e,k) that MV0303 forms for it -- the
+ * additions orc_matvec's scatter makes into T(i), in the same order, so the
+ * same bits, but every node independent of the others. */
+static void mv_ay_gather(const opmesh *M, int npoin, double *x, const double *da,
+                         char typdia, const double *xm, const double *y)
+{
+    const int *ik[3] = {M->ik0, M->ik1, M->ik2};
+    const double *xa12 = xm, *xa13 = xm + M->ld, *xa23 = xm + 2 * (size_t)M->ld;
+    const int *ptr = M->gptr, *ek = M->gek;
+    #pragma omp parallel for if (ORC_PAR(npoin)) num_threads(orc_nthreads) schedule(static)
+    for (int i = 0; i < npoin; ++i) {
+        double t = typdia == 'Q' ? y[i] * da[i] : (typdia == 'I' ? y[i] : 0.0);
+        for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
+            int e = ek[j] >> 2, k = ek[j] & 3;
+            double w;
+            if (k == 0)      w = xa12[e] * y[ik[1][e]] + xa13[e] * y[ik[2][e]];
+            else if (k == 1) w = xa23[e] * y[ik[2][e]] + xa12[e] * y[ik[0][e]];
+            else             w = xa13[e] * y[ik[0][e]] + xa23[e] * y[ik[1][e]];
+            t = t + w;
+        }
+        x[i] = t;
+    }
+}
 
 static int op_matvec(const opmesh *M, const char *op, int npoin, double *x,
                      const double *da, char typdia, const double *xm,
@@ -457,9 +507,17 @@ static int op_matvec(const opmesh *M, const char *op, int npoin, double *x,
 {
     if (M->sto == 3)
         return orc_mvseg(op, npoin, M->nseg, M->g1, M->g2, x, da, typdia, xm, typext, y, c);
+    if (M->gptr && typext == 'S' && !strcmp(op, "X=AY    ") &&
+        (typdia == 'Q' || typdia == 'I' || typdia == '0')) {
+        mv_ay_gather(M, npoin, x, da, typdia, xm, y);
+        return ORC_OK;
+    }
     return orc_matvec(op, npoin, M->nelem, M->ik0, M->ik1, M->ik2, x, da, typdia, xm,
                       M->ld, typext, y, c, t, w);
 }
+
+static int build_gather(int npoin, int nelem, const int *ik0, const int *ik1,
+                        const int *ik2, int **ptr_out, int **ek_out);
 
 /* ------------------------------------------------------------------ */
 /* dot products                                                         */
@@ -536,16 +594,19 @@ static long long blk_lo(int b, int n, int nb)
 double orc_dot_blocked(int n, const double *x, const double *y,
                        int nb, int nt)
 {
+    if (nt < 32 || nt > ORC_MAX_NT) return NAN;
     double *part = (double *)malloc(sizeof(double) * (size_t)nb);
-    double *v = (double *)malloc(sizeof(double) * (size_t)nt);
+    double v[ORC_MAX_NT];
+    #pragma omp parallel for if (ORC_PAR(n)) num_threads(orc_nthreads) schedule(static)
     for (int b = 0; b < nb; ++b) {
+        double vb[ORC_MAX_NT];
         long long lo = blk_lo(b, n, nb), hi = blk_lo(b + 1, n, nb);
         for (int t = 0; t < nt; ++t) {
             double s = 0.0;
             for (long long i = lo + t; i < hi; i += nt) s = s + x[i] * y[i];
-            v[t] = s;
+            vb[t] = s;
         }
-        part[b] = tree64(v, nt);
+        part[b] = tree64(vb, nt);
     }
     for (int t = 0; t < nt; ++t) {
         double s = 0.0;
@@ -553,22 +614,25 @@ double orc_dot_blocked(int n, const double *x, const double *y,
         v[t] = s;
     }
     double r = tree64(v, nt);
-    free(part); free(v);
+    free(part);
     return r;
 }
 
 static float dot_blocked32(int n, const float *x, const float *y, int nb, int nt)
 {
+    if (nt < 32 || nt > ORC_MAX_NT) return NAN;
     float *part = (float *)malloc(sizeof(float) * (size_t)nb);
-    float *v = (float *)malloc(sizeof(float) * (size_t)nt);
+    float v[ORC_MAX_NT];
+    #pragma omp parallel for if (ORC_PAR(n)) num_threads(orc_nthreads) schedule(static)
     for (int b = 0; b < nb; ++b) {
+        float vb[ORC_MAX_NT];
         long long lo = blk_lo(b, n, nb), hi = blk_lo(b + 1, n, nb);
         for (int t = 0; t < nt; ++t) {
             float s = 0.0f;
             for (long long i = lo + t; i < hi; i += nt) s = s + x[i] * y[i];
-            v[t] = s;
+            vb[t] = s;
         }
-        part[b] = tree32(v, nt);
+        part[b] = tree32(vb, nt);
     }
     for (int t = 0; t < nt; ++t) {
         float s = 0.0f;
@@ -576,7 +640,7 @@ static float dot_blocked32(int n, const float *x, const float *y, int nb, int nt
         v[t] = s;
     }
     float r = tree32(v, nt);
-    free(part); free(v);
+    free(part);
     return r;
 }
 
@@ -608,9 +672,11 @@ static float warp_tree32(float *lanes)
 double orc_dot_batch(int n, const double *x, const double *y, int nt, int npt)
 {
     const int C = nt * npt, ntile = (n + C - 1) / C;
+    if (nt < 32 || nt > ORC_MAX_NT) return NAN;
     double *part = (double *)malloc(sizeof(double) * (size_t)(ntile + 1));
-    double *v = (double *)malloc(sizeof(double) * (size_t)nt);
+    #pragma omp parallel for if (ORC_PAR(n)) num_threads(orc_nthreads) schedule(static)
     for (int k = 0; k < ntile; ++k) {
+        double v[ORC_MAX_NT];
         for (int t = 0; t < nt; ++t) {
             double s = 0.0;
             for (int j = 0; j < npt; ++j) {
@@ -628,16 +694,18 @@ double orc_dot_batch(int n, const double *x, const double *y, int nt, int npt)
         lanes[l] = s;
     }
     double r = warp_tree64(lanes);
-    free(part); free(v);
+    free(part);
     return r;
 }
 
 static float dot_batch32(int n, const float *x, const float *y, int nt, int npt)
 {
     const int C = nt * npt, ntile = (n + C - 1) / C;
+    if (nt < 32 || nt > ORC_MAX_NT) return NAN;
     float *part = (float *)malloc(sizeof(float) * (size_t)(ntile + 1));
-    float *v = (float *)malloc(sizeof(float) * (size_t)nt);
+    #pragma omp parallel for if (ORC_PAR(n)) num_threads(orc_nthreads) schedule(static)
     for (int k = 0; k < ntile; ++k) {
+        float v[ORC_MAX_NT];
         for (int t = 0; t < nt; ++t) {
             float s = 0.0f;
             for (int j = 0; j < npt; ++j) {
@@ -655,7 +723,7 @@ static float dot_batch32(int n, const float *x, const float *y, int nt, int npt)
         lanes[l] = s;
     }
     float r = warp_tree32(lanes);
-    free(part); free(v);
+    free(part);
     return r;
 }
 
@@ -839,6 +907,7 @@ static int precd1_impl(const opmesh *M, int npoin, int precon, double *x, double
     } else if (typext == 'S' || typext == 'Q') {
         /* OM1111 'M=DMD': off-diagonal part (om1111.f:589-600) */
         double *x1 = xm, *x2 = xm + ld, *x3 = xm + 2 * (size_t)ld;
+        #pragma omp parallel for if (ORC_PAR(nelem)) num_threads(orc_nthreads) schedule(static)
         for (int e = 0; e < nelem; ++e) {
             x1[e] = x1[e] * d[ik1[e]] * d[ik0[e]];
             x2[e] = x2[e] * d[ik2[e]] * d[ik0[e]];
@@ -895,6 +964,7 @@ static int gracjg_impl(const opmesh *M, int npoin, double *x, const double *da,
 
     xl = pdots(dot_mode, npoin, b, b, nb, nt);            /* :189 */
     if (sqrt(xl) < 1.0e-15) {                             /* :194-202 */
+        ORC_PFOR(n)
         for (size_t i = 0; i < n; ++i) x[i] = 0.0;
         rmrm = 0.0; xl = 1.0; relat = 0;
         goto fin;
@@ -903,20 +973,24 @@ static int gracjg_impl(const opmesh *M, int npoin, double *x, const double *da,
 
     st = op_matvec(M, "X=AY    ", npoin, r, da, typdia, xm, typext, x, 0.0, t, w);  /* :213 */
     if (st) goto done;
+    ORC_PFOR(n)
     for (size_t i = 0; i < n; ++i) r[i] = r[i] - b[i];    /* :215 */
     rmrm = pdots(dot_mode, npoin, r, r, nb, nt);          /* :216 */
     rmgm = rmrm;
     if (rmrm < eps * eps * xl) goto fin;                  /* :219 */
 
+    ORC_PFOR(n)
     for (size_t i = 0; i < n; ++i) dd[i] = r[i];          /* :248 */
     st = op_matvec(M, "X=AY    ", npoin, ad, da, typdia, xm, typext, dd, 0.0, t, w); /* :254 */
     if (st) goto done;
     dad = pdots(dot_mode, npoin, dd, ad, nb, nt);         /* :260 */
     ro = rmgm / dad;                                      /* :261 */
+    ORC_PFOR(n)
     for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * dd[i];   /* :268 */
 
     for (;;) {
         m = m + 1;                                        /* :284 */
+        ORC_PFOR(n)
         for (size_t i = 0; i < n; ++i) r[i] = r[i] + (-ro) * ad[i];  /* :290 */
         rm1gm1 = rmgm;
         rmrm = pdots(dot_mode, npoin, r, r, nb, nt);      /* :295 */
@@ -924,12 +998,14 @@ static int gracjg_impl(const opmesh *M, int npoin, double *x, const double *da,
         rmgm = rmrm;
         if (rmrm <= xl * (eps * eps)) goto fin;           /* :303,324 */
         beta = rmgm / rm1gm1;                             /* :357 */
+        ORC_PFOR(n)
         for (size_t i = 0; i < n; ++i) dd[i] = r[i] + beta * dd[i];  /* :361 */
         st = op_matvec(M, "X=AY    ", npoin, ad, da, typdia, xm, typext, dd, 0.0, t,
                        w);                                /* :376 */
         if (st) goto done;
         dad = pdots(dot_mode, npoin, dd, ad, nb, nt);     /* :382 */
         ro = rmdm / dad;                                  /* :383 */
+        ORC_PFOR(n)
         for (size_t i = 0; i < n; ++i) x[i] = x[i] + (-ro) * dd[i];  /* :387 */
         if (m >= nitmax) { st = m; goto fin; }            /* :406 */
     }
@@ -1441,6 +1517,7 @@ static int solve_impl(const opmesh *M, int npoin, double *x, double *b, double *
                  : gracjg_impl(M, npoin, x, dm, *typdia, xm, typext, b, nitmax, eps, dot_mode,
                                nb, nt, nit_out, relres_out, relat_out);
     if (diag) {
+        ORC_PFOR(npoin)
         for (int i = 0; i < npoin; ++i) x[i] = x[i] * d[i];
         free(d);
     }
@@ -1454,9 +1531,16 @@ int orc_solve(int npoin, int nelem, const int *ik0, const int *ik1,
               int nb, int nt, int *nit_out, double *relres_out,
               int *relat_out, int krylov)
 {
-    opmesh M = {1, nelem, ld, ik0, ik1, ik2, 0, NULL, NULL};
-    return solve_impl(&M, npoin, x, b, dm, typdia, xm, typext, slv, precon, nitmax, eps,
-                      krylov, dot_mode, nb, nt, nit_out, relres_out, relat_out);
+    opmesh M = {1, nelem, ld, ik0, ik1, ik2, 0, NULL, NULL, NULL, NULL};
+    int *gptr = NULL, *gek = NULL;
+    if (ORC_PAR(npoin) && build_gather(npoin, nelem, ik0, ik1, ik2, &gptr, &gek) == ORC_OK) {
+        M.gptr = gptr;
+        M.gek = gek;
+    }
+    int st = solve_impl(&M, npoin, x, b, dm, typdia, xm, typext, slv, precon, nitmax, eps,
+                        krylov, dot_mode, nb, nt, nit_out, relres_out, relat_out);
+    free(gptr); free(gek);
+    return st;
 }
 
 /* SOLVE (SLV=1) on a segment-storage matrix (STO=3): the same algorithm with
@@ -1617,6 +1701,7 @@ static int seg32_build_seg(int npoin, const int *g1, const int *g2, const int *p
  * wave operator survive the binary32 copy. */
 static void seg32_mv(const seg32 *g, const float *p, float *q)
 {
+    ORC_PFOR(g->npoin)
     for (int i = 0; i < g->npoin; ++i) {
         float pi = p[i];
         float acc = pi * g->s32[i];
@@ -1664,6 +1749,7 @@ static int mixed_impl(const opmesh *M, int npoin, double *x, const double *b,
     float *q = (float *)malloc(sizeof(float) * n);
     int *gptr = NULL, *gek = NULL;
     seg32 g = {0, NULL, NULL, NULL, NULL};
+    opmesh Mg = *M;
     int st = ORC_OK, outer = 0, inner = 0, diag = 0;
     double xl = 0.0, rr = 0.0, otol = 0.0;
     float rho = 0.0f, rmax = 0.0f, itol2 = 0.0f;
@@ -1688,6 +1774,10 @@ static int mixed_impl(const opmesh *M, int npoin, double *x, const double *b,
         if ((st = build_gather(npoin, nelem, ik0, ik1, ik2, &gptr, &gek))) goto done;
         if ((st = seg32_build(npoin, nelem, ik0, ik1, ik2, gptr, gek, dm, typdia, xm, &g)))
             goto done;
+        if (ORC_PAR(npoin)) {   /* threaded: binary64 products by the gather form */
+            Mg.gptr = gptr;
+            Mg.gek = gek;
+        }
     }
 
     xl = dot64s(ds, npoin, bs, bs);
@@ -1703,9 +1793,10 @@ static int mixed_impl(const opmesh *M, int npoin, double *x, const double *b,
     /* true residual r = b - A x (binary64), its binary32 copy, both norms */
 #define TRUE_RESIDUAL()                                                         \
     do {                                                                        \
-        st = op_matvec(M, "X=AY    ", npoin, t, dm, typdia, xm, typext, x, 0.0, \
+        st = op_matvec(&Mg, "X=AY    ", npoin, t, dm, typdia, xm, typext, x, 0.0, \
                        r, w);                                                   \
         if (st) goto done;                                                      \
+        ORC_PFOR(n)                                                             \
         for (size_t i = 0; i < n; ++i) { r[i] = bs[i] - t[i]; ri[i] = (float)r[i]; } \
         rr = dot64s(ds, npoin, r, r);                                          \
         rho = dot32s(ds, npoin, ri, ri);                                       \
@@ -1715,19 +1806,23 @@ static int mixed_impl(const opmesh *M, int npoin, double *x, const double *b,
     if (isnan(rr)) { st = ORC_ERR_NAN; goto fin; }
     if (rr <= otol) goto fin;
     rmax = rho;
+    ORC_PFOR(n)
     for (size_t i = 0; i < n; ++i) { z[i] = 0.0f; p[i] = ri[i]; }
     for (;;) {
         seg32_mv(&g, p, q);
         float pq = dot32s(ds, npoin, p, q);
         if (!(pq > 0.0f)) { st = isnan(pq) ? ORC_ERR_NAN : ORC_ERR_BREAKDOWN; goto fin; }
         float alpha = rho / pq;
+        ORC_PFOR(n)
         for (size_t i = 0; i < n; ++i) z[i] = z[i] + alpha * p[i];
+        ORC_PFOR(n)
         for (size_t i = 0; i < n; ++i) ri[i] = ri[i] - alpha * q[i];
         float rho_new = dot32s(ds, npoin, ri, ri);
         float rho_rec = rho_new, rho_old = rho;
         ++inner;
         int last = inner >= max_inner;
         if (last || rho_new <= itol2 * rmax || (double)rho_new <= otol) {
+            ORC_PFOR(n)
             for (size_t i = 0; i < n; ++i) { x[i] = x[i] + (double)z[i]; z[i] = 0.0f; }
             TRUE_RESIDUAL();
             ++outer;
@@ -1739,6 +1834,7 @@ static int mixed_impl(const opmesh *M, int npoin, double *x, const double *b,
         }
         float beta = rho_rec / rho_old;
         rho = rho_new;
+        ORC_PFOR(n)
         for (size_t i = 0; i < n; ++i) p[i] = ri[i] + beta * p[i];
     }
 #undef TRUE_RESIDUAL

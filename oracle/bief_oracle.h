@@ -42,6 +42,11 @@ extern "C" {
 #define ORC_ERR_BAD_MESH  -4
 #define ORC_ERR_UNSUPPORTED -5
 
+/* Host threads for large checks (default 1: the sequential code).  Only
+ * loops with independent iterations are shared out; results are the same
+ * bits with any count. */
+void orc_set_threads(int n);
+
 int orc_geometry(int nelem, const double *x, const double *y,
                  const int *ik0, const int *ik1, const int *ik2,
                  double *xel2, double *xel3, double *yel2, double *yel3,

@@ -44,10 +44,10 @@ def test_shards_cover_and_balance():
 
 def test_two_gloo_ranks():
     sizes = [5000, 3000, 2500, 2000, 1000, 800, 600, 100]
-    with mp.Manager() as m:
+    ctx = mp.get_context("spawn")   # no fork: the oracle's OpenMP threads may be alive
+    with ctx.Manager() as m:
         out = m.dict()
         port = _free_port()
-        ctx = mp.get_context("spawn")
         procs = [ctx.Process(target=_worker, args=(r, 2, port, sizes, out)) for r in range(2)]
         for p in procs:
             p.start()
