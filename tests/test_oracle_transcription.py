@@ -30,7 +30,6 @@ The reference statements followed:
   solve.f:636-641      X = X*D after the solver
 """
 import math
-import os
 
 import numpy as np
 import pytest
@@ -280,30 +279,28 @@ def test_transcription_zero_rhs(oracle_mod):
     assert np.array_equal(py["x"], c["x"]) and not py["x"].any()
 
 
-REF_GOUTTEDO = "/root/reference/examples/telemac2d/gouttedo/geo_gouttedo.slf"
-
-
-@pytest.mark.skipif(not os.path.isfile(REF_GOUTTEDO), reason="reference examples not present")
 def test_transcription_on_the_gouttedo_mesh(oracle_mod):
     """The reference's own gouttedo mesh (4,624 nodes, its node and element
-    numbering as drawn): the matrix build, MATVEC and 40 GRACJG iterations
-    of the two restatements agree bit for bit."""
-    from opentelemac_b200 import meshgen as mg, serafin
-    s = serafin.read(REF_GOUTTEDO, values=False)
-    ik = s.ikle.astype(np.int32)
+    numbering as drawn, frozen in tests/golden/gouttedo.npz): the matrix
+    build, MATVEC and 40 GRACJG iterations of the two restatements agree
+    bit for bit."""
+    from conftest import gouttedo_mesh
+    from opentelemac_b200 import meshgen as mg
+    gx, gy, ik, _ = gouttedo_mesh()
+    npoin = gx.size
     ikle = _ikle_rows(ik)
-    x = [float(v) for v in s.x]
-    y = [float(v) for v in s.y]
-    coef = mg.wave_coef(mg.depth_smooth(s.x, s.y, ik))
+    x = [float(v) for v in gx]
+    y = [float(v) for v in gy]
+    coef = mg.wave_coef(mg.depth_smooth(gx, gy, ik))
     dm, xm = _wave_matrix(x, y, ikle, [float(v) for v in coef])
-    cdm, cxm = oracle_mod.wave_matrix(s.x, s.y, ik, coef)
+    cdm, cxm = oracle_mod.wave_matrix(gx, gy, ik, coef)
     assert np.array_equal(dm, cdm)
     assert np.array_equal(xm, np.asarray(cxm).reshape(3, -1))
-    xt = mg.random_solution(s.npoin)
+    xt = mg.random_solution(npoin)
     b = _matvec_x_ay(ikle, list(dm), "Q", list(xm[0]), list(xm[1]), list(xm[2]), list(xt))
     cb = oracle_mod.matvec("X=AY    ", ik, cdm, "Q", cxm, "S", xt)
     assert np.array_equal(np.array(b), cb)
-    py = _solve_cg_diag(ikle, dm, xm, cb, np.zeros(s.npoin), 1e-12, 40)
+    py = _solve_cg_diag(ikle, dm, xm, cb, np.zeros(npoin), 1e-12, 40)
     c = oracle_mod.solve(ik, cdm, "Q", cxm, "S", cb, eps=1e-12, nitmax=40,
                          dot_mode=oracle_mod.DOT_SEQUENTIAL)
     assert py["status"] == 1 and c["status"] != 0

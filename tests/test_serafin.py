@@ -8,9 +8,11 @@ import os
 import numpy as np
 import pytest
 
+from conftest import GOLDEN, REFERENCE
 from opentelemac_b200 import meshgen as mg, serafin
 
-REF_EXAMPLES = "/root/reference/examples/telemac2d"
+# the reference's TELEMAC-2D examples, where TELEMAC_REFERENCE names its tree
+REF_EXAMPLES = os.path.join(REFERENCE, "examples", "telemac2d") if REFERENCE else ""
 
 
 @pytest.mark.parametrize("double", [False, True])
@@ -53,7 +55,8 @@ def test_truncated_file_rejected(tmp_path):
         serafin.read(p)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not present")
+@pytest.mark.skipif(not REF_EXAMPLES or not os.path.isdir(REF_EXAMPLES),
+                    reason="TELEMAC_REFERENCE not set to the reference tree")
 def test_reference_example_files(oracle_mod, tmp_path):
     files = sorted(glob.glob(os.path.join(REF_EXAMPLES, "*", "geo*.slf")))[:40]
     assert files
@@ -80,3 +83,37 @@ def test_reference_example_files(oracle_mod, tmp_path):
     b = oracle_mod.matvec("X=AY    ", ik, dm, "Q", xm, "S", mg.random_solution(s.npoin))
     r = oracle_mod.solve(ik, dm, "Q", xm, "S", b, eps=1e-10)
     assert r["status"] == 0 and r["relres"] <= 1e-10
+
+
+@pytest.mark.skipif(not REF_EXAMPLES or not os.path.isdir(REF_EXAMPLES),
+                    reason="TELEMAC_REFERENCE not set to the reference tree")
+def test_gouttedo_fixture_is_the_reference_mesh():
+    """tests/golden/gouttedo.npz holds the reference's geo_gouttedo.slf and
+    geo_gouttedo.cli as they are (same file hashes, same mesh)."""
+    import hashlib
+    d = np.load(os.path.join(GOLDEN, "gouttedo.npz"))
+    case = os.path.join(REF_EXAMPLES, "gouttedo")
+    for name, key in (("geo_gouttedo.slf", "slf_sha256"), ("geo_gouttedo.cli", "cli_sha256")):
+        with open(os.path.join(case, name), "rb") as fh:
+            assert hashlib.sha256(fh.read()).hexdigest() == str(d[key])
+    s = serafin.read(os.path.join(case, "geo_gouttedo.slf"), values=False)
+    np.testing.assert_array_equal(s.x, d["x"])
+    np.testing.assert_array_equal(s.y, d["y"])
+    np.testing.assert_array_equal(s.ikle, d["ikle0"])
+
+
+def test_gouttedo_fixture_mesh_is_valid():
+    """The frozen mesh: 4,624 nodes, 8,978 counter-clockwise triangles,
+    every node used, 268 boundary points that are exactly the nodes on
+    boundary faces."""
+    from conftest import gouttedo_mesh
+    x, y, ik, nbor = gouttedo_mesh()
+    assert x.size == 4624 and ik.shape == (8978, 3)
+    assert np.array_equal(np.unique(ik), np.arange(x.size))
+    a = (x[ik[:, 1]] - x[ik[:, 0]]) * (y[ik[:, 2]] - y[ik[:, 0]]) - \
+        (x[ik[:, 2]] - x[ik[:, 0]]) * (y[ik[:, 1]] - y[ik[:, 0]])
+    assert (a > 0).all()
+    be, bf = mg.boundary_faces(ik)
+    on_boundary = np.unique(ik[be, bf])
+    assert nbor.size == 268
+    np.testing.assert_array_equal(np.sort(nbor), on_boundary)
