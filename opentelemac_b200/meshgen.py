@@ -131,6 +131,24 @@ def mesh_size_for_npoin(npoin):
     return max(2, int(round(np.sqrt(npoin))))
 
 
+def batch_sizes(ninst=256, lo=2000, hi=200000, seed=4):
+    """Grid sizes (nodes per side) of the batched workload: node counts drawn
+    log-uniformly in [lo, hi] with a seed, each rounded to a square grid."""
+    rng = np.random.default_rng(seed)
+    npo = np.exp(rng.uniform(np.log(lo), np.log(hi), ninst))
+    return [mesh_size_for_npoin(v) for v in npo]
+
+
+def batch_instance(k, n):
+    """Instance k of the batched workload on an n x n grid: its own mesh
+    seed, the smooth depth field and a random right-hand side.  Returns
+    x, y, ikle0, coef, b."""
+    x, y, ik = square_mesh(n, seed=1000 + k)
+    coef = wave_coef(depth_smooth(x, y, ik))
+    b = np.random.default_rng(k).uniform(-1, 1, x.size)
+    return x, y, ik, coef, b
+
+
 def boundary_faces(ikle0):
     """Boundary faces in boundary order: (elements, faces), face f joining
     local points f and f+1 mod 3.  Faces of counter-clockwise elements that

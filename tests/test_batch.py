@@ -51,17 +51,15 @@ def test_batch_256_meshes():
     own depth field seed and random right-hand side, one launch, relres 1e-8."""
     import torch
     from opentelemac_b200.batch import BatchSolver
-    rng = np.random.default_rng(4)
-    npo = np.exp(rng.uniform(np.log(2000), np.log(200000), 256))
-    sizes = [mg.mesh_size_for_npoin(v) for v in npo]
+    sizes = mg.batch_sizes()
     meshes, xs, ys, coefs, bs_ = [], [], [], [], []
     for k, n in enumerate(sizes):
-        x, y, ik = mg.square_mesh(n, seed=1000 + k)
+        x, y, ik, coef, bv = mg.batch_instance(k, n)
         meshes.append((x.size, ik))
         xs.append(x)
         ys.append(y)
-        coefs.append(mg.wave_coef(mg.depth_smooth(x, y, ik)))
-        bs_.append(np.random.default_rng(k).uniform(-1, 1, x.size))
+        coefs.append(coef)
+        bs_.append(bv)
     bs = BatchSolver(meshes)
     bs.assemble_wave(xs, ys, coefs)
     b = bs.gather(bs_)
