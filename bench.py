@@ -74,6 +74,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-large-matvec", action="store_true",
                     help="skip the MATVEC measurements on the 2001x2001-node mesh")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="wave1m: skip the 2001x2001 log-uniform solves (config2) and the "
+                         "256-mesh batch (batch256) reported beside the headline")
     ap.add_argument("--batch-shape", default=None,
                     help="batch256: nodes per thread and threads per block as NPT,TPB "
                          "(default: the autotuner's choice)")
@@ -261,9 +264,9 @@ def run_reference(args, ws, rank):
     """--impl reference: the reference algorithm's CPU implementation on the
     host cores (the Fortran cannot be compiled on these machines, so the
     oracle's port of SOLVE/GRACJG, run on every host thread with OpenMP as
-    the reference would run with one MPI rank per core), rank 0 only.  One
-    full solve (untimed) gives the iteration count; each timed step is a
-    bounded sample of CG iterations, extrapolated to a full solve."""
+    the reference would run with one MPI rank per core), rank 0 only.  Every
+    step, warm-up included, is one whole solve of the workload from x = 0 to
+    the relative residual, timed with the host clock."""
     if rank != 0:
         return
     import oracle
@@ -274,21 +277,14 @@ def run_reference(args, ws, rank):
     coef = mg.wave_coef(depth_field(args.depth, x, y, ik))
     dm, xm = oracle.wave_matrix(x, y, ik, coef)
     b = oracle.matvec("X=AY    ", ik, dm, "Q", xm, "S", mg.random_solution(x.size))
-    full = oracle.solve_omp(ik, dm, xm, b, eps=args.eps, nthreads=nthreads)
-    nit_full = full["nit"]
-    t0 = time.perf_counter()
-    oracle.solve_omp(ik, dm, xm, b, nitmax=1, eps=1e-300, nthreads=nthreads)
-    t_setup = time.perf_counter() - t0
-    k = max(2, min(200, nit_full))
-    times = []
+    times, full = [], None
     for s in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        oracle.solve_omp(ik, dm, xm, b, nitmax=k, eps=1e-300, nthreads=nthreads)
+        full = oracle.solve_omp(ik, dm, xm, b, eps=args.eps, nthreads=nthreads)
         dt = time.perf_counter() - t0
         if s >= args.warmup:
             times.append(dt)
-    per_it = max(statistics.median(times) - t_setup, 1e-9) / (k - 1)
-    per_solve = t_setup + per_it * nit_full
+    per_solve = sum(times) / len(times)
     val = 1.0 / per_solve
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -297,61 +293,70 @@ def run_reference(args, ws, rank):
             "config": {"workload": f"wave-equation SOLVE (CG, diagonal precon, relres "
                                    f"{args.eps:g}) on the {args.n}x{args.n}-node P1 mesh",
                        "npoin": int(x.size), "nelem": int(ik.shape[0])},
-            "iterations": nit_full, "relres": full["relres"],
+            "iterations": full["nit"], "relres": full["relres"],
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthreads, "kind": "port",
                              "sample": f"binary64 port of SOLVE/GRACJG on {nthreads} threads; "
-                                       f"{k} of {nit_full} CG iterations per step, "
-                                       f"extrapolated to a full solve ({per_solve:.2f} s)"},
+                                       f"every step one whole solve ({full['nit']} CG "
+                                       f"iterations, {per_solve:.2f} s)"},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args, ws, rank, local):
-    """256 meshes (node counts log-uniform in [2,000, 200,000], per-mesh
-    seeds, random right-hand sides), mixed precision to relres 1e-8, all of a
-    rank's meshes in one persistent launch.  With N ranks the meshes are
-    sharded (size-balanced) across ranks: fixed total work, strong scaling,
-    no data-path collective."""
+def hbm_peak():
+    """Measured HBM copy bandwidth (GB/s) of MEASURED_PEAKS.json and where
+    it came from."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def batch_measure(ws, rank, local, steps, warmup, inner_tol, eps, shape=None):
+    """The 256-mesh workload (node counts log-uniform in [2,000, 200,000],
+    per-mesh seeds, random right-hand sides), mixed precision to relres
+    `eps`, all of a rank's meshes in one persistent launch per step; with N
+    ranks the meshes are sharded (size-balanced) across ranks: fixed total
+    work, no data-path collective.  Returns the measurements (rank 0's
+    instances for the iteration statistics and the roofline)."""
     import torch
     from opentelemac_b200 import meshgen as mg, replicas
     from opentelemac_b200.batch import BatchSolver
     torch.cuda.set_device(local)
-    rng = np.random.default_rng(4)
-    npo = np.exp(rng.uniform(np.log(2000), np.log(200000), 256))
-    sizes = [mg.mesh_size_for_npoin(v) for v in npo]
+    sizes = mg.batch_sizes()
     mine = replicas.shard_instances([n * n for n in sizes], ws, rank)
     meshes, xs, ys, coefs, bvs = [], [], [], [], []
     for k in mine:
-        x, y, ik = mg.square_mesh(sizes[k], seed=1000 + k)
+        x, y, ik, coef, bv = mg.batch_instance(k, sizes[k])
         meshes.append((x.size, ik))
         xs.append(x)
         ys.append(y)
-        coefs.append(mg.wave_coef(mg.depth_smooth(x, y, ik)))
-        bvs.append(np.random.default_rng(k).uniform(-1, 1, x.size))
+        coefs.append(coef)
+        bvs.append(bv)
     bs = BatchSolver(meshes, device=local)
     bs.assemble_wave(xs, ys, coefs)
     b = bs.gather(bvs)
     x = torch.zeros_like(b)
-    if args.batch_shape:
-        npt, tpb = (int(v) for v in args.batch_shape.split(","))
+    if shape:
+        npt, tpb = shape
     else:
-        npt, tpb = bs.autotune(b, inner_tol=args.inner_tol, outer_tol=args.eps)
+        npt, tpb = bs.autotune(b, inner_tol=inner_tol, outer_tol=eps)
     flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     clean = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     times, kern = [], []
-    for s in range(args.warmup + args.steps):
+    for s in range(warmup + steps):
         flush.fill_(float(s))   # 1 GiB written, then 256 MB read: L2 flushed, lines clean
         clean.sum()
         x.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        r = bs.solve_mixed(x, b, inner_tol=args.inner_tol, outer_tol=args.eps, nodes_per_thread=npt,
+        r = bs.solve_mixed(x, b, inner_tol=inner_tol, outer_tol=eps, nodes_per_thread=npt,
                            threads_per_block=tpb)
         e1.record()
         e1.synchronize()
-        if s >= args.warmup:
+        if s >= warmup:
             times.append(e0.elapsed_time(e1))
             kern.append(r["kernel_ms"])
     step_ms = max_over_ranks(sum(times) / len(times), ws)
@@ -365,36 +370,111 @@ def run_batch(args, ws, rank, local):
         by = algorithmic_bytes(npo, ik.shape[0])
         alg += int(ni) * by["it32"] + (int(no) + 1) * by["upd"]
     kern_ms = sum(kern) / len(kern)
-    hbm = 6650.0
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
-            hbm = float(json.load(fh).get("hbm_gbs", hbm))
-    except OSError:
-        pass
+    hbm, src = hbm_peak()
     gbs = alg / (kern_ms * 1e-3) / 1e9
+    out = {"value": 256 * 1000.0 / step_ms, "unit": "solves/s", "ms_per_step": step_ms,
+           "kernel_ms": kern_ms, "converged": ok, "inner_tol": inner_tol,
+           "nodes_this_rank": int(bs.total_nodes), "nodes_per_thread": int(npt),
+           "threads_per_block": int(tpb),
+           "autotune_ms_per_iteration": {f"npt{k[0]}_t{k[1]}": round(v, 4)
+                                         for k, v in getattr(bs, "tune_table", {}).items()},
+           "iterations_rank0": {"p50": float(np.percentile(inner, 50)),
+                                "p99": float(np.percentile(inner, 99)),
+                                "max": int(inner.max())},
+           "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": gbs, "peak": hbm,
+                        "unit": "GB/s", "frac": gbs / hbm,
+                        "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)",
+                        "bytes_per_launch": alg,
+                        "note": "rank 0's instances; working set (13.0M nodes) far above L2"}}
+    bs.close()
+    del flush, clean, x, b
+    return out
+
+
+def run_batch(args, ws, rank, local):
+    """--workload batch256: the batched line on its own."""
+    shape = tuple(int(v) for v in args.batch_shape.split(",")) if args.batch_shape else None
+    m = batch_measure(ws, rank, local, args.steps, args.warmup, args.inner_tol, args.eps, shape)
     if rank == 0:
         line = {"metric": "batched P1 CG solves/s (256 meshes, mixed, relres 1e-8)",
-                "value": 256 * 1000.0 / step_ms, "unit": "solves/s", "n_gpus": ws,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+                "value": m["value"], "unit": "solves/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_step"],
                 "higher_is_better": True, "scaling": "strong" if ws > 1 else "weak",
                 "vs_baseline": None, "dtype": "f32 inner / f64 refinement",
                 "data": "synthetic",
                 "config": {"workload": "256 meshes, 2,000-200,000 nodes (log-uniform), one "
                                        "persistent launch per rank",
-                           "nodes_this_rank": int(bs.total_nodes),
-                           "nodes_per_thread": int(npt), "threads_per_block": int(tpb),
-                           "autotune_ms_per_iteration": {f"npt{k[0]}_t{k[1]}": round(v, 4)
-                                                         for k, v in getattr(bs, "tune_table", {}).items()},
+                           "nodes_this_rank": m["nodes_this_rank"],
+                           "nodes_per_thread": m["nodes_per_thread"],
+                           "threads_per_block": m["threads_per_block"],
+                           "autotune_ms_per_iteration": m["autotune_ms_per_iteration"],
                            "parallelism": f"shards x{ws}"},
-                "converged": ok, "kernel_ms": kern_ms,
-                "roofline": {"bound": "hbm", "kernel": "k_batch", "achieved": gbs, "peak": hbm,
-                             "unit": "GB/s", "frac": gbs / hbm, "bytes_per_launch": alg,
-                             "note": "rank 0's instances; working set above L2"},
-                "iterations_rank0": {"p50": float(np.percentile(inner, 50)),
-                                     "p99": float(np.percentile(inner, 99)),
-                                     "max": int(inner.max())}}
+                "converged": m["converged"], "kernel_ms": m["kernel_ms"],
+                "roofline": m["roofline"], "iterations_rank0": m["iterations_rank0"]}
         print(json.dumps(line), flush=True)
-    bs.close()
+
+
+def config2_measure(P2, ws, flush_l2, hbm, steps=2, warmup=1):
+    """The 2001 x 2001-node mesh with the log-uniform depth (4,004,001
+    nodes, 8,000,000 triangles), relres 1e-10: binary64 GRACJG, the mixed
+    solve with refinement threshold 1e-4 (as the workload specifies) and 0.1,
+    each timed over `steps` solves after `warmup`, L2 flushed before each;
+    a binary64 solve to relres 1e-13 is the accuracy reference both are
+    measured against."""
+    import torch
+    from opentelemac_b200 import bief
+    A, b, mesh = P2["A"], P2["b"], P2["mesh"]
+    by = algorithmic_bytes(P2["npoin"], P2["nelem"], P2["nseg"])
+    eps = 1e-10
+    x = torch.zeros_like(b)
+
+    def timed(fn):
+        ms, kern, res = [], [], None
+        for s in range(warmup + steps):
+            flush_l2(s)
+            x.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = fn()
+            e1.record()
+            e1.synchronize()
+            if s >= warmup:
+                ms.append(e0.elapsed_time(e1))
+                kern.append(mesh.last_timing()[0])
+        return (max_over_ranks(sum(ms) / len(ms), ws), sum(kern) / len(kern), res)
+
+    cfg = bief.SlvCfg(slv=1, nitmax=1000000, precon=2, krylov=0, eps=eps, zero=0.0)
+    f64_ms, f64_kern, f64_res = timed(lambda: bief.solve(x, A, b, cfg))
+    x64 = x.clone()
+    x.zero_()
+    tight = bief.SlvCfg(slv=1, nitmax=1000000, precon=2, krylov=0, eps=1e-13, zero=0.0)
+    _, nit_t, rel_t = bief.solve(x, A, b, tight)
+    x13 = x.clone()
+    nrm = lambda v: float(torch.linalg.norm(v))
+    f64_bytes = f64_res[1] * by["it64"]
+    out = {"workload": "2001x2001-node P1 mesh, log-uniform depth in [0.5, 500] m (3 "
+                       "smoothing passes), relres 1e-10",
+           "npoin": P2["npoin"], "nelem": P2["nelem"],
+           "fp64": {"ms": f64_ms, "kernel_ms": f64_kern, "iterations": f64_res[1],
+                    "relres": f64_res[2], "kernel": "k_cg64",
+                    "gbs": f64_bytes / (f64_kern * 1e-3) / 1e9,
+                    "frac": f64_bytes / (f64_kern * 1e-3) / 1e9 / hbm,
+                    "bytes_per_launch": f64_bytes},
+           "tight_fp64": {"relres": rel_t, "iterations": nit_t,
+                          "fp64_vs_tight": nrm(x64 - x13) / nrm(x13)}}
+    for key, itol in (("mixed_itol_1e-4", 1e-4), ("mixed_itol_0.1", 0.1)):
+        ms, kern, res = timed(lambda: bief.solve_mixed(x, A, b, precon=2, inner_tol=itol,
+                                                       outer_tol=eps))
+        st, outer, inner, relres = res
+        mb = inner * by["it32"] + (outer + 1) * by["upd"]
+        out[key] = {"ms": ms, "kernel_ms": kern, "inner": inner, "refinements": outer,
+                    "relres": relres, "speedup_vs_fp64": f64_ms / ms,
+                    "vs_fp64": nrm(x - x64) / nrm(x64), "vs_tight_fp64": nrm(x - x13) / nrm(x13),
+                    "kernel": "k_mixed", "gbs": mb / (kern * 1e-3) / 1e9,
+                    "frac": mb / (kern * 1e-3) / 1e9 / hbm, "bytes_per_launch": mb}
+    del x, x64, x13
+    return out
 
 
 def run_matvec(args, ws, rank, local):
@@ -586,6 +666,15 @@ def main():
 
     f64_step = {"before_stop": fp64_at(nit64 - 2), "after_stop": fp64_at(nit64)}
 
+    # a binary64 solve converged far past the stopping test (relres 1e-13):
+    # the accuracy reference the binary64 and the mixed solutions are both
+    # measured against
+    x.zero_()
+    tight_cfg = bief.SlvCfg(slv=1, nitmax=1000000, precon=2, krylov=0, eps=1e-13, zero=0.0)
+    _, nit_tight, rel_tight = bief.solve(x, A, b, tight_cfg)
+    x_tight = x.clone()
+    f64_vs_tight = float(torch.linalg.norm(x_f64 - x_tight) / torch.linalg.norm(x_tight))
+
     # binary64 GRACJG with MODASS = 3 (compensated dot products)
     def run_fp64_comp():
         x.zero_()
@@ -630,8 +719,12 @@ def main():
     # both MATVECs again on the 2001 x 2001-node mesh (4.0M nodes, 8.0M
     # triangles: the mixed-precision configuration's size)
     mv_large = None
-    if args.n < 2001 and not args.no_large_matvec:
-        PL = build_problem(2001, local, "smooth", args.storage)
+    PL = None
+    if args.n < 2001 and not (args.no_large_matvec and args.no_extras):
+        # log-uniform depth: the configuration's own operator (the values do
+        # not change the product's time); its solves follow the headline
+        PL = build_problem(2001, local, "loguniform", args.storage)
+    if PL is not None and not args.no_large_matvec:
         byl = algorithmic_bytes(PL["npoin"], PL["nelem"], PL["nseg"])
 
         def lib_median(fn, mesh_l):
@@ -655,8 +748,7 @@ def main():
         for key, t_ms, nb in (("matvec64", t64, byl["mv64"]), ("matvec32", t32, byl["mv32"])):
             g = nb / (t_ms * 1e-3) / 1e9
             mv_large[key] = {"ms": t_ms, "bytes": nb, "gbs": g}
-        PL["mesh"].close()
-        del PL, yl, ol, y32l, o32l
+        del yl, ol, y32l, o32l
 
     # headline: mixed precision, timed steps, clocks sampled meanwhile
     barrier(ws)
@@ -667,6 +759,7 @@ def main():
     st, outer, inner, relres = mx_res
     mixed_x_err = float(torch.linalg.norm(x - P["xt"]) / torch.linalg.norm(P["xt"]))
     mixed_vs_f64 = float(torch.linalg.norm(x - x_f64) / torch.linalg.norm(x_f64))
+    mixed_vs_tight = float(torch.linalg.norm(x - x_tight) / torch.linalg.norm(x_tight))
     barrier(ws)
     step_ms = max_over_ranks(sum(mx_ms) / len(mx_ms), ws)
     f64_step_ms = max_over_ranks(sum(f64_ms) / len(f64_ms), ws)
@@ -695,6 +788,38 @@ def main():
             e2e.append((t1 - t0) * 1e3)
     e2e_ms = max_over_ranks(sum(e2e) / len(e2e), ws)
 
+    # the binary64 GRACJG the same way (SOLVE through the C ABI with host
+    # buffers: matrix and right-hand side uploaded, solution read back)
+    e2e64 = []
+    for s in range(1 + max(2, args.steps // 4)):
+        x_p[:] = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if args.storage == "seg":
+            A.set_seg(dm_p, xm_p, "Q", "S")
+        else:
+            A.set(dm_p, xm_p, "Q", "S")
+        bief.solve(x_p, A, b_p, cfg)
+        t1 = time.perf_counter()
+        if s >= 1:
+            e2e64.append((t1 - t0) * 1e3)
+    e2e64_ms = max_over_ranks(sum(e2e64) / len(e2e64), ws)
+    e2e64_nsteps = len(e2e64)
+
+    # beside the headline: the 2001 x 2001 log-uniform configuration and the
+    # 256-mesh batch
+    cfg2 = None
+    hbm_b, _ = hbm_peak()
+    if PL is not None and not args.no_extras:
+        cfg2 = config2_measure(PL, ws, flush_l2, hbm_b)
+    if PL is not None:
+        PL["mesh"].close()
+        del PL
+    batch = None
+    if not args.no_extras:
+        batch = batch_measure(ws, rank, local, 2, 1, 1e-4, args.eps)
+        batch["steps"], batch["warmup"] = 2, 1
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.n, args.eps, nit64, args.cpu_seconds, args.depth)
@@ -719,6 +844,11 @@ def main():
         pass
     mixed_bytes = inner * by["it32"] + (outer + 1) * by["upd"]
     achieved = mixed_bytes / (kern_ms * 1e-3) / 1e9
+    mixed_traffic = traffic.get("k_mixed_bytes_per_launch")
+    dram_gbs = mixed_traffic / (kern_ms * 1e-3) / 1e9 if mixed_traffic else None
+    # the binary32 operator and vectors of the 1M-node solve (~96 MB) fit in
+    # the 126 MB L2: whether the launch's working set stays in L2
+    l2_resident = by["mv32"] < 126e6
     f64_bytes = nit64 * by["it64"]
     mv_gbs = by["mv64"] / (mv_t * 1e-3) / 1e9
     mv32_gbs = by["mv32"] / (mv32_t * 1e-3) / 1e9
@@ -745,7 +875,10 @@ def main():
             "relres": {"mixed": relres, "fp64": f64_res[2]},
             "error": {"mixed_vs_fp64": mixed_vs_f64, "mixed_vs_xtrue": mixed_x_err,
                       "fp64_vs_xtrue": f64_x_err,
-                      "fp64_one_step_at_stop": f64_step},
+                      "fp64_one_step_at_stop": f64_step,
+                      "vs_tight_fp64": {"mixed": mixed_vs_tight, "fp64": f64_vs_tight,
+                                        "tight_relres": rel_tight,
+                                        "tight_iterations": nit_tight}},
             "matvec": {"op": "X=AY binary64 TYPDIA=Q",
                        "kernel": "k_mvseg" if args.storage == "seg" else "k_matvec", "ms": mv_t,
                        "ms_call": mv_t_call,
@@ -770,13 +903,26 @@ def main():
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
                          "bytes_per_launch": mixed_bytes,
-                         "traffic": traffic.get("k_mixed_bytes_per_launch"),
-                         "note": "at 1M nodes the binary32 working set (~96 MB) stays mostly "
-                                 "in the 126 MB L2: traffic from HBM is far below the "
-                                 "algorithmic bytes"},
+                         "traffic": mixed_traffic,
+                         "dram_gbs": dram_gbs,
+                         "dram_frac": dram_gbs / hbm if dram_gbs else None,
+                         "working_set": ("L2-resident: the binary32 operator and vectors "
+                                         "(~96 MB) stay in the 126 MB L2, so frac is "
+                                         "algorithmic bytes over time, not DRAM traffic "
+                                         "(dram_frac); limited by L2 latency and the grid "
+                                         "barriers" if l2_resident else
+                                         "above L2: streamed from HBM")},
             "e2e": {"value": ws * 1000.0 / e2e_ms, "unit": UNIT,
                     "h2d_bytes_per_step": 8 * (npoin + int(xm_h.size)) + 16 * npoin,
                     "d2h_bytes_per_step": 8 * npoin, "ms_per_step": e2e_ms},
+            "e2e_fp64": {"value": ws * 1000.0 / e2e64_ms, "unit": UNIT,
+                         "h2d_bytes_per_step": 8 * (npoin + int(xm_h.size)) + 16 * npoin,
+                         "d2h_bytes_per_step": 8 * npoin, "ms_per_step": e2e64_ms,
+                         "steps": e2e64_nsteps,
+                         "note": "binary64 GRACJG through bief_set_matrix + bief_solve with "
+                                 "host buffers"},
+            "config2": cfg2,
+            "batch256": batch,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,

@@ -33,7 +33,7 @@ def test_reference_arm_contract():
 @pytest.mark.gpu
 def test_headline_contract_small():
     d = _run("--n", "101", "--steps", "2", "--warmup", "3", "--no-cpu-baseline",
-             "--no-large-matvec")
+             "--no-large-matvec", "--no-extras")
     assert BASE <= set(d)
     for k in ("roofline", "e2e", "gpu_launches", "clocks", "error", "matvec", "matvec32",
               "cg_iterations_per_s", "time_to_solution_ms"):
@@ -42,6 +42,9 @@ def test_headline_contract_small():
     assert r["bound"] == "hbm" and r["achieved"] > 0 and r["peak"] > 0 and r["unit"] == "GB/s"
     assert d["e2e"]["h2d_bytes_per_step"] > 0 and d["e2e"]["d2h_bytes_per_step"] > 0
     assert d["gpu_launches"] > 0 and d["relres"]["mixed"] <= 1e-8
+    assert d["e2e_fp64"]["value"] > 0 and d["config2"] is None and d["batch256"] is None
+    t = d["error"]["vs_tight_fp64"]
+    assert t["tight_relres"] <= 1e-13 and t["mixed"] > 0 and t["fp64"] > 0
 
 
 @pytest.mark.gpu
