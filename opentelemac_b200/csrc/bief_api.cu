@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -35,6 +36,13 @@ struct bief_handle {
   int *d_meta = nullptr, *d_rec_off = nullptr, *d_seg_off = nullptr, *d_seg_col = nullptr;
   int2 *d_rec_idx = nullptr;
   uchar2 *d_rec_slot = nullptr;
+  // compressed gather records of the standalone MATVEC (Mv16); mv16 = 0
+  // when some entry does not fit them (k_matvec then reads IKLE)
+  int mv16 = 0;
+  unsigned char *d_mv_deg = nullptr;
+  int *d_mv_eb = nullptr;
+  unsigned short *d_mv_ek = nullptr;
+  short2 *d_mv_dv = nullptr;
   double2 *d_rec_c = nullptr;
   double2 *d_rec_ct = nullptr;   // transposed-operator records (EQUNOR, 'Q' storage)
   double *d_sg_ct = nullptr;     // transposed-operator segment slots
@@ -114,6 +122,10 @@ int grid_for(int n, int nsm) {
   return std::max(1, std::min(g, nsm * 16));
 }
 
+// One node per thread (256-thread blocks): the blocks are scheduled as SMs
+// free up, so no thread carries a second node into the tail of the launch.
+int mv_grid(int n) { return std::max(1, (n + 255) / 256); }
+
 // Parse an 8-character MATVEC operation string (trailing blanks optional).
 int parse_op(const char *op, int *opc, bool *trans) {
   if (!op) return BIEF_ERR_ARGS;
@@ -139,6 +151,12 @@ int parse_op(const char *op, int *opc, bool *trans) {
 template <int TD, bool SYM, bool TR>
 void launch_mv(bief_handle *h, const double *xm, const double *da, const double *y, double *x,
                int opc, double c, cudaStream_t st) {
+  if (h->mv16) {
+    Mv16 M{h->d_mv_deg, h->d_rec_off, h->d_mv_eb, h->d_mv_ek, h->d_mv_dv};
+    k_matvec16<TD, SYM, TR><<<mv_grid(h->npoin), 256, 0, st>>>(h->npoin, h->nelem, M, xm, da, y,
+                                                               x, opc, c);
+    return;
+  }
   k_matvec<TD, SYM, TR><<<grid_for(h->npoin, h->nsm), 256, 0, st>>>(
       h->npoin, h->nelem, h->d_ptr, h->d_ek, h->d_ik, xm, da, y, x, opc, c);
 }
@@ -559,6 +577,47 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
     for (int q = 0; q < nnb[i]; ++q) seg_col[sb + 32 * q] = nb_list[nb_ptr[i] + q];
   }
 
+  // Compressed MATVEC records (Mv16): usable when, in every slice, the
+  // entries' element numbers lie within 2^14 of the slice's smallest, every
+  // other vertex within a 16-bit offset of its node, and no node has more
+  // than 255 entries -- true of any mesh numbered with some locality.
+  std::vector<int> mv_eb(nsl, 0);
+  bool mv16 = true;
+  for (int sgi = 0; sgi < nsl && mv16; ++sgi) {
+    int lo = INT_MAX, hi = INT_MIN;
+    for (int i = 32 * sgi; i < std::min(npoin, 32 * sgi + 32); ++i) {
+      if (ptr[i + 1] - ptr[i] > 255) mv16 = false;
+      for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
+        lo = std::min(lo, ek[j] >> 2);
+        hi = std::max(hi, ek[j] >> 2);
+        const int e = ek[j] >> 2, k = ek[j] & 3;
+        const long long da = (long long)ik[(size_t)((k + 1) % 3) * nelem + e] - i;
+        const long long db = (long long)ik[(size_t)((k + 2) % 3) * nelem + e] - i;
+        if (da < -32768 || da > 32767 || db < -32768 || db > 32767) mv16 = false;
+      }
+    }
+    if (lo != INT_MAX && hi - lo >= (1 << 14)) mv16 = false;
+    mv_eb[sgi] = lo == INT_MAX ? 0 : lo;
+  }
+  std::vector<unsigned char> mv_deg;
+  std::vector<unsigned short> mv_ek;
+  std::vector<short2> mv_dv;
+  if (mv16) {
+    mv_deg.assign(npoin, 0);
+    mv_ek.assign(nrec, 0);
+    mv_dv.assign(nrec, make_short2(0, 0));
+    for (int i = 0; i < npoin; ++i) {
+      const int rb = rec_off[i >> 5] + (i & 31), eb = mv_eb[i >> 5];
+      mv_deg[i] = (unsigned char)(ptr[i + 1] - ptr[i]);
+      for (int m = 0; m < ptr[i + 1] - ptr[i]; ++m) {
+        const int j = ptr[i] + m, e = ek[j] >> 2, k = ek[j] & 3;
+        mv_ek[rb + 32 * m] = (unsigned short)(((e - eb) << 2) | k);
+        mv_dv[rb + 32 * m] = make_short2((short)(ik[(size_t)((k + 1) % 3) * nelem + e] - i),
+                                         (short)(ik[(size_t)((k + 2) % 3) * nelem + e] - i));
+      }
+    }
+  }
+
   bief_handle *h = new (std::nothrow) bief_handle;
   if (!h) return BIEF_ERR_ARGS;
   h->dev = device;
@@ -597,6 +656,21 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
         (st = dalloc(&h->d_rec_c, nrec)) || (st = dalloc(&h->d_seg_col, nseg)) ||
         (st = dalloc(&h->d_seg_c, nseg)))
       return fail(st);
+    if (mv16) {
+      if ((st = dalloc(&h->d_mv_deg, n)) || (st = dalloc(&h->d_mv_eb, (size_t)nsl)) ||
+          (st = dalloc(&h->d_mv_ek, nrec)) || (st = dalloc(&h->d_mv_dv, nrec)))
+        return fail(st);
+      if ((e = cudaMemcpyAsync(h->d_mv_deg, mv_deg.data(), n, cudaMemcpyHostToDevice,
+                               h->stream)) != cudaSuccess ||
+          (e = cudaMemcpyAsync(h->d_mv_eb, mv_eb.data(), sizeof(int) * nsl,
+                               cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+          (e = cudaMemcpyAsync(h->d_mv_ek, mv_ek.data(), sizeof(unsigned short) * nrec,
+                               cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
+          (e = cudaMemcpyAsync(h->d_mv_dv, mv_dv.data(), sizeof(short2) * nrec,
+                               cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
+        return fail(cuda_fail(e, "mesh upload", __LINE__));
+      h->mv16 = 1;
+    }
     if ((st = persistent_grid(npoin, h->nsm, &h->G))) return fail(st);
     if ((st = dalloc(&h->d_part, 8 * (size_t)h->G + 4))) return fail(st);
     if ((e = cudaMallocHost((void **)&h->h_ctl, sizeof(Ctl))) != cudaSuccess)
@@ -637,6 +711,7 @@ int bief_destroy(bief_handle *h) {
                   h->d_ad, h->d_t, h->d_z, h->d_ri, h->d_p0, h->d_p1, h->d_q, h->d_part,
                   h->d_ew, h->d_ctl, h->d_err, h->d_meta, h->d_rec_off, h->d_seg_off,
                   h->d_rec_idx, h->d_rec_slot, h->d_rec_c, h->d_seg_col, h->d_seg_c,
+                  h->d_mv_deg, h->d_mv_eb, h->d_mv_ek, h->d_mv_dv,
                   h->d_binst, h->d_brel, h->d_bpart, h->d_g1, h->d_g2, h->d_sg_meta,
                   h->d_sg_off, h->d_sg_sx, h->d_sg_col, h->d_segel, h->d_xa, h->d_xas,
                   h->d_sg_c64, h->d_sg_c32, h->d_rec_ct, h->d_sg_ct, h->d_gmv, h->d_gpart};

@@ -65,6 +65,93 @@ __global__ void __launch_bounds__(256) k_matvec(int npoin, int nelem, const int 
                                          nelem, vec));
 }
 
+// MATVEC from the compressed gather records of the mesh (Mv16, built with
+// the mesh when every entry fits): per entry, in the 32-node sliced layout,
+// the element as (IELEM - eb) << 2 | IDP-1 in 16 bits and the element's two
+// other vertices as 16-bit offsets from the node.  The coefficient and the
+// vertex loads of an entry then depend on one coalesced index load only
+// (ebe_row goes index -> IKLE -> vertex values), IKLE is not read, and the
+// index costs 6 bytes per entry instead of the 4 of the element index plus
+// the 8 of the two IKLE values.  The index streams are loaded evict-first;
+// the additions are ebe_row's, in its order, so the bits are the same.
+struct Mv16 {
+  const unsigned char *deg;    // per node: gather entries
+  const int *off;              // per slice: first record
+  const int *eb;               // per slice: smallest element number of its entries
+  const unsigned short *ek;    // per record: (IELEM - eb) << 2 | IDP-1
+  const short2 *dv;            // per record: (a - i, b - i), a and b the other vertices
+};
+
+template <int NB, bool SYM, bool TRANS, class V>
+__device__ __forceinline__ void mv16_batch(double &acc, int i, int eb, int b0, int m,
+                                           const Mv16 &M, const double *__restrict__ xm, int ne,
+                                           V vec) {
+  unsigned short p[NB];
+  short2 d[NB];
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    p[q] = __ldcs(M.ek + b0 + 32 * (m + q));
+    d[q] = __ldcs(M.dv + b0 + 32 * (m + q));
+  }
+  double xa[NB], xb[NB], ya[NB], yb[NB];
+#pragma unroll
+  for (int q = 0; q < NB; ++q) {
+    const int e = eb + (p[q] >> 2), k = p[q] & 3;
+    const int a = (k == 2) ? 0 : k + 1;  // (k+1) mod 3
+    const int b = (k == 0) ? 2 : k - 1;  // (k+2) mod 3
+    const int ca = TRANS ? xm_col<SYM>(a, k) : xm_col<SYM>(k, a);
+    const int cb = TRANS ? xm_col<SYM>(b, k) : xm_col<SYM>(k, b);
+    xa[q] = __ldg(xm + (size_t)ca * ne + e);
+    xb[q] = __ldg(xm + (size_t)cb * ne + e);
+    ya[q] = vec(i + d[q].x);
+    yb[q] = vec(i + d[q].y);
+  }
+#pragma unroll
+  for (int q = 0; q < NB; ++q) acc = add(acc, add(mul(xa[q], ya[q]), mul(xb[q], yb[q])));
+}
+
+// Gather entries per batch of k_matvec16 (all index loads of a batch, then
+// all coefficient and vertex loads, then the additions in order).
+#ifndef BIEF_MV16_BATCH
+#define BIEF_MV16_BATCH 4
+#endif
+constexpr int MV16_B = BIEF_MV16_BATCH;
+
+template <int TD, bool SYM, bool TRANS>
+__global__ void __launch_bounds__(256) k_matvec16(int npoin, int nelem, Mv16 M,
+                                                  const double *__restrict__ xm,
+                                                  const double *__restrict__ da,
+                                                  const double *__restrict__ y, double *x, int opc,
+                                                  double c) {
+  auto vec = [&](int j) { return __ldg(y + j); };
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += stride) {
+    const int deg = __ldcs(M.deg + i);
+    const int b0 = __ldg(M.off + (i >> 5)) + (i & 31), eb = __ldg(M.eb + (i >> 5));
+    double acc = TD == DIA_Q ? mul(__ldg(y + i), __ldcs(da + i)) : diag_term<TD>(__ldg(y + i), da, i);
+    int m = 0;
+    for (; m + MV16_B <= deg; m += MV16_B)
+      mv16_batch<MV16_B, SYM, TRANS>(acc, i, eb, b0, m, M, xm, nelem, vec);
+    if constexpr (MV16_B / 2 > 1) {
+      if (m + MV16_B / 2 <= deg) {
+        mv16_batch<MV16_B / 2, SYM, TRANS>(acc, i, eb, b0, m, M, xm, nelem, vec);
+        m += MV16_B / 2;
+      }
+    }
+    for (; m < deg; ++m) mv16_batch<1, SYM, TRANS>(acc, i, eb, b0, m, M, xm, nelem, vec);
+    double r;  // OS combination of MESH%T into X (matvec.f:369-380, :329-340)
+    switch (opc) {
+      case OP_AY: r = acc; break;
+      case OP_XPAY: r = add(x[i], acc); break;
+      case OP_MAY: r = -acc; break;
+      case OP_XMAY: r = sub(x[i], acc); break;
+      case OP_XPCAY: r = add(x[i], mul(c, acc)); break;
+      default: r = mul(c, acc); break;
+    }
+    x[i] = r;
+  }
+}
+
 // MATVEC 'X=AY' in binary32 (no reference counterpart) on the binary32
 // edge-assembled copy of the operator, the product of the binary32 inner CG:
 // X_i = s_i Y_i + sum_j c_ij (Y_j - Y_i), with s_i the row sum and c_ij the

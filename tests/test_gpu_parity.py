@@ -48,6 +48,32 @@ def test_matvec_bitexact(oracle_mod, typdia, typext):
                                                          typext, v, x=v))
 
 
+@pytest.mark.parametrize("shuffle", [False, True])
+def test_matvec_bitexact_both_index_forms(oracle_mod, shuffle):
+    """MATVEC on a 201 x 201 mesh: with its row-wise numbering every gather
+    entry fits the compressed 16-bit records of the mesh, with a random
+    renumbering of its 40,401 nodes and elements none does and the product
+    reads IKLE; every operation is bit for bit the oracle's either way."""
+    rng = np.random.default_rng(8)
+    x, y, ik = mg.square_mesh(201)
+    if shuffle:
+        x, y, ik, _, _ = mg.shuffled(x, y, ik, seed=5)
+    n, ne = x.size, ik.shape[0]
+    dm = rng.uniform(1, 2, n)
+    for typext in ("S", "Q"):
+        xm = rng.uniform(-1, 1, (6 if typext == "Q" else 3, ne))
+        mesh = bief.Mesh(ik, n)
+        A = bief.Matrix(mesh, dm, xm, "Q", typext)
+        v = rng.uniform(-1, 1, n)
+        x0 = rng.uniform(-1, 1, n)
+        for op in OPS:
+            got = x0.copy()
+            bief.matvec(op, got, A, v, c=1.7)
+            ref = oracle_mod.matvec(op, ik, dm, "Q", xm, typext, v, c=1.7, x=x0)
+            np.testing.assert_array_equal(got, ref, err_msg=f"{op} {typext}")
+        mesh.close()
+
+
 def test_matvec_config0_device_path(oracle_mod, cfg0_problem):
     import torch
     p = cfg0_problem

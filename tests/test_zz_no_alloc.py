@@ -131,14 +131,24 @@ def test_noalloc_rejects_oversize_and_bad_mesh():
 
 
 def _variant(n, seed, typdia, typext):
-    """A wave-equation matrix with the given TYPDIA, and for TYPEXT 'Q' a
-    non-symmetric copy: the lower triangle (M21, M31, M32) perturbed by up to
-    1% per element."""
+    """A symmetric positive definite operator in the given storage: for
+    TYPDIA 'I' the wave-equation matrix scaled to a unit diagonal (D A D with
+    D = DM^-1/2) and DM = 1 (PRECD1 reads DM even then, and after a PRECON 2
+    scaling the solve takes the diagonal as the identity, so DM must be the
+    true diagonal); for TYPEXT 'Q' a non-symmetric copy whose upper and
+    lower terms differ by up to 1% (a skew-symmetric change, so D.AD > 0
+    stays true)."""
     ik, mesh, A, dm, xm, b = _problem(n, seed)
     xm = np.asarray(xm).reshape(3, -1)
+    rng = np.random.default_rng(seed + 1)
+    if typdia == "I":
+        d = 1.0 / np.sqrt(dm)
+        xm = np.stack([xm[0] * d[ik[:, 0]] * d[ik[:, 1]], xm[1] * d[ik[:, 0]] * d[ik[:, 2]],
+                       xm[2] * d[ik[:, 1]] * d[ik[:, 2]]])
+        dm = np.ones(dm.size)
     if typext == "Q":
-        f = np.random.default_rng(seed + 1).uniform(0.99, 1.01, xm.shape)
-        xm = np.concatenate([xm, xm * f])
+        s = 0.01 * xm * rng.uniform(-1, 1, xm.shape)
+        xm = np.concatenate([xm + s, xm - s])
     A.set(dm, xm, typdia, typext)
     return ik, mesh, A, dm, xm, b
 
