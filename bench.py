@@ -82,13 +82,21 @@ def parse():
                          "(default: the autotuner's choice)")
     ap.add_argument("--max-inner", type=int, default=200,
                     help="mixedcap: inner iterations of each bounded mixed solve")
+    ap.add_argument("--batch-max-inner", type=int, default=1000000,
+                    help="batch256: stop every instance after this many inner iterations "
+                         "(the launch then covers only the first cycles: time against cycles)")
+    ap.add_argument("--nitmax", type=int, default=1000000,
+                    help="fp64: NITMAX of the binary64 solves (a small value bounds the "
+                         "launch for profiling)")
     ap.add_argument("--workload", default="wave1m",
-                    choices=["wave1m", "batch256", "matvec", "mixedcap"],
+                    choices=["wave1m", "batch256", "matvec", "mixedcap", "fp64"],
                     help="wave1m: the 1M-node solve (default); batch256: 256 independent "
                          "meshes of 2,000-200,000 nodes in one persistent launch per rank; "
                          "matvec: the binary64 and binary32 MATVEC 'X=AY' alone on the "
                          "--n x --n mesh; mixedcap: mixed solves capped at --max-inner "
-                         "inner iterations on the --n x --n mesh (a bounded profiling target)")
+                         "inner iterations on the --n x --n mesh (a bounded profiling target); "
+                         "fp64: the binary64 GRACJG alone on the --n x --n mesh (--depth, "
+                         "--eps, --nitmax)")
     args = ap.parse_args()
     if args.inner_tol is None:
         args.inner_tol = 1e-4 if args.workload == "batch256" else 0.1
@@ -313,7 +321,8 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
-def batch_measure(ws, rank, local, steps, warmup, inner_tol, eps, shape=None):
+def batch_measure(ws, rank, local, steps, warmup, inner_tol, eps, shape=None, max_inner=1000000,
+                  storage="ebe"):
     """The 256-mesh workload (node counts log-uniform in [2,000, 200,000],
     per-mesh seeds, random right-hand sides), mixed precision to relres
     `eps`, all of a rank's meshes in one persistent launch per step; with N
@@ -336,6 +345,8 @@ def batch_measure(ws, rank, local, steps, warmup, inner_tol, eps, shape=None):
         bvs.append(bv)
     bs = BatchSolver(meshes, device=local)
     bs.assemble_wave(xs, ys, coefs)
+    if storage == "seg":   # every instance's own STOSEG numbering, ASSEX3 on the device
+        bs.set_segments([mg.segments(ik, npo)[:2] for npo, ik in meshes]).to_segments()
     b = bs.gather(bvs)
     x = torch.zeros_like(b)
     if shape:
@@ -353,7 +364,7 @@ def batch_measure(ws, rank, local, steps, warmup, inner_tol, eps, shape=None):
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
         r = bs.solve_mixed(x, b, inner_tol=inner_tol, outer_tol=eps, nodes_per_thread=npt,
-                           threads_per_block=tpb)
+                           threads_per_block=tpb, max_inner=max_inner)
         e1.record()
         e1.synchronize()
         if s >= warmup:
@@ -374,6 +385,7 @@ def batch_measure(ws, rank, local, steps, warmup, inner_tol, eps, shape=None):
     gbs = alg / (kern_ms * 1e-3) / 1e9
     out = {"value": 256 * 1000.0 / step_ms, "unit": "solves/s", "ms_per_step": step_ms,
            "kernel_ms": kern_ms, "converged": ok, "inner_tol": inner_tol,
+           "max_inner": max_inner,
            "nodes_this_rank": int(bs.total_nodes), "nodes_per_thread": int(npt),
            "threads_per_block": int(tpb),
            "autotune_ms_per_iteration": {f"npt{k[0]}_t{k[1]}": round(v, 4)
@@ -394,7 +406,8 @@ def batch_measure(ws, rank, local, steps, warmup, inner_tol, eps, shape=None):
 def run_batch(args, ws, rank, local):
     """--workload batch256: the batched line on its own."""
     shape = tuple(int(v) for v in args.batch_shape.split(",")) if args.batch_shape else None
-    m = batch_measure(ws, rank, local, args.steps, args.warmup, args.inner_tol, args.eps, shape)
+    m = batch_measure(ws, rank, local, args.steps, args.warmup, args.inner_tol, args.eps, shape,
+                      args.batch_max_inner, args.storage)
     if rank == 0:
         line = {"metric": "batched P1 CG solves/s (256 meshes, mixed, relres 1e-8)",
                 "value": m["value"], "unit": "solves/s", "n_gpus": ws,
@@ -408,8 +421,11 @@ def run_batch(args, ws, rank, local):
                            "nodes_per_thread": m["nodes_per_thread"],
                            "threads_per_block": m["threads_per_block"],
                            "autotune_ms_per_iteration": m["autotune_ms_per_iteration"],
+                           "storage": "segments (STO=3)" if args.storage == "seg"
+                                      else "EBE (STO=1)",
                            "parallelism": f"shards x{ws}"},
                 "converged": m["converged"], "kernel_ms": m["kernel_ms"],
+                "max_inner": m["max_inner"],
                 "roofline": m["roofline"], "iterations_rank0": m["iterations_rank0"]}
         print(json.dumps(line), flush=True)
 
@@ -572,9 +588,58 @@ def run_mixedcap(args, ws, rank, local):
     P["mesh"].close()
 
 
+def run_fp64_solve(args, ws, rank, local):
+    """Binary64 GRACJG alone on the --n x --n mesh (--depth, --storage,
+    --eps, --nitmax): --warmup + --steps solves from x = 0, L2 flushed before
+    each, the library's events around the solver launch.  One line: ms per
+    solve and the k_cg64 (or segment) kernel's algorithmic GB/s."""
+    import torch
+    from opentelemac_b200 import bief
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    P = build_problem(args.n, local, args.depth, args.storage)
+    by = algorithmic_bytes(P["npoin"], P["nelem"], P["nseg"])
+    flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    clean = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    x = torch.zeros_like(P["b"])
+    cfg = bief.SlvCfg(slv=1, nitmax=args.nitmax, precon=2, krylov=0, eps=args.eps, zero=0.0)
+    ts, nit, rel = [], 0, 0.0
+    for s in range(args.warmup + args.steps):
+        flush.fill_(float(s))
+        clean.sum()
+        x.zero_()
+        st, nit, rel = quiet(lambda: bief.solve(x, P["A"], P["b"], cfg))
+        if s >= args.warmup:
+            ts.append(P["mesh"].last_timing()[0])
+    m = max_over_ranks(statistics.median(ts), ws)
+    hbm, src = hbm_peak()
+    gbs = nit * by["it64"] / (m * 1e-3) / 1e9
+    if rank == 0:
+        print(json.dumps({
+            "metric": "binary64 GRACJG time-to-solution", "value": m, "unit": "ms",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": m,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"binary64 GRACJG (relres {args.eps:g}, NITMAX "
+                                   f"{args.nitmax}) on the {args.n}x{args.n}-node P1 mesh",
+                       "depth": args.depth, "storage": args.storage},
+            "iterations": nit, "relres": rel, "ms_per_iteration": m / max(nit, 1),
+            "roofline": {"bound": "hbm", "kernel": "k_cg64", "achieved": gbs, "peak": hbm,
+                         "unit": "GB/s", "frac": gbs / hbm,
+                         "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)",
+                         "bytes_per_iteration": by["it64"]}}), flush=True)
+    P["mesh"].close()
+
+
 def main():
     args = parse()
     ws, rank, local = dist_init()
+    if args.impl == "b200" and args.workload == "fp64":
+        run_fp64_solve(args, ws, rank, local)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "b200" and args.workload == "mixedcap":
         run_mixedcap(args, ws, rank, local)
         if ws > 1:

@@ -231,7 +231,9 @@ int bief_mass_diff_grad_dev(bief_handle *h, const double *xc, const double *yc,
  * per-instance dot order.  x, b:
  * device arrays over the whole mesh; per-instance results in host arrays
  * status (0 / inner iterations when not converged / < 0 error), outer_out,
- * inner_out, relres_out. */
+ * inner_out, relres_out.  Either storage: with segment storage (STO=3)
+ * the segment numbering set by bief_set_segments holds every instance's
+ * segments, each instance's in its own order. */
 int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
                                const int *npoin_inst, double *x, const double *b,
                                int precon, double inner_tol, double outer_tol,

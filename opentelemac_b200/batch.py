@@ -62,6 +62,27 @@ class BatchSolver:
                           for c in coefs])
         self.A.assemble_wave(xc, yc, coef.contiguous())
 
+    def set_segments(self, segs):
+        """Segment storage (MATRIX STORAGE 3) for every instance: segs is one
+        (g1, g2) pair of 0-based GLOSEG columns per instance, numbered as the
+        instance's own mesh numbers them (meshgen.segments gives STOSEG's
+        numbering).  The instances' segment lists are concatenated, so each
+        node keeps its segments in its own instance's order; call
+        to_segments() after assemble_wave() to convert the matrix."""
+        if len(segs) != self.ninst:
+            raise ValueError(f"{len(segs)} segment lists for {self.ninst} instances")
+        g1 = np.concatenate([np.asarray(a, np.int64) + int(o) for (a, _), o in
+                             zip(segs, self.node_off)])
+        g2 = np.concatenate([np.asarray(b, np.int64) + int(o) for (_, b), o in
+                             zip(segs, self.node_off)])
+        self.mesh.set_segments(g1, g2)
+        return self
+
+    def to_segments(self):
+        """ASSEX3 of the assembled EBE matrix into the instances' segments."""
+        self.A.to_segments()
+        return self
+
     # -- solve
     def solve_mixed(self, x, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, max_outer=1000,
                     max_inner=1000000, nodes_per_thread=None, threads_per_block=None):

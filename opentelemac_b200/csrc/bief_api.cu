@@ -1359,8 +1359,9 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
   if (threads_per_block != 256 && threads_per_block != 512 && threads_per_block != 1024)
     return BIEF_ERR_ARGS;
   if (!h->has_matrix) return BIEF_ERR_NO_MATRIX;
-  if (h->typext != 'S' || h->sto != 1) return BIEF_ERR_UNSUPPORTED;
-  if (h->max_nnb > MAX_NEIGHBOURS) return BIEF_ERR_SIZE;
+  if (h->typext != 'S') return BIEF_ERR_UNSUPPORTED;
+  const bool seg = h->sto == 3;
+  if (!seg && h->max_nnb > MAX_NEIGHBOURS) return BIEF_ERR_SIZE;
   if (precon == 0) precon = 1;
   if (precon < 0 || precon % 7 == 0 || precon % 11 == 0 || precon % 13 == 0 || precon % 17 == 0)
     return BIEF_ERR_UNSUPPORTED;
@@ -1408,15 +1409,32 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
 
   const bool diag = (precon % 2 == 0 || precon % 3 == 0 || precon % 5 == 0);
   int td = typdia_code(h->typdia);
-  const double *xm = h->d_xm, *da = h->d_dm, *bw = b;
+  const double *xm = seg ? h->d_xa : h->d_xm, *da = h->d_dm, *bw = b;
   if (diag) {
     if ((st = do_precd1(h, precon, x, b, h->d_bs, &td, s))) return st;
-    xm = h->d_xms;
+    xm = seg ? h->d_xas : h->d_xms;
     da = h->d_dms;
     bw = h->d_bs;
   }
-  if ((st = build_records(h, xm, s))) return st;
-  {
+  if (seg) {
+    // segment storage: binary64 slot coefficients, their binary32 copy and
+    // row sums, as the single-mesh mixed solve builds them
+    if ((st = build_seg_coefs(h, xm, s))) return st;
+    const int gn = grid_for(h->npoin, h->nsm);
+#define SG_ARGS h->npoin, h->d_sg_meta, h->d_sg_off, h->d_sg_c64, da, h->d_sg_c32, h->d_s32
+    if (td == DIA_Q)
+      k_build_sg32<DIA_Q><<<gn, 256, 0, s>>>(SG_ARGS);
+    else if (td == DIA_I)
+      k_build_sg32<DIA_I><<<gn, 256, 0, s>>>(SG_ARGS);
+    else
+      k_build_sg32<DIA_0><<<gn, 256, 0, s>>>(SG_ARGS);
+#undef SG_ARGS
+    h->launches++;
+    h->s32_gen = -1;
+    CK(cudaGetLastError());
+  } else if ((st = build_records(h, xm, s))) {
+    return st;
+  } else {
     const int gn = grid_for(h->npoin, h->nsm);
 #define SEG_ARGS                                                                              \
   h->npoin, h->nelem, h->d_ptr, h->d_ek, xm, da, h->d_meta, h->d_rec_off, h->d_rec_slot, \
@@ -1432,8 +1450,12 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
     h->s32_gen = -1;
     CK(cudaGetLastError());
   }
-  void *k = td == DIA_Q ? (void *)k_batch<DIA_Q>
-            : td == DIA_I ? (void *)k_batch<DIA_I> : (void *)k_batch<DIA_0>;
+  void *k = seg ? (td == DIA_Q   ? (void *)k_batch<DIA_Q, 3>
+                   : td == DIA_I ? (void *)k_batch<DIA_I, 3>
+                                 : (void *)k_batch<DIA_0, 3>)
+                : (td == DIA_Q   ? (void *)k_batch<DIA_Q, 1>
+                   : td == DIA_I ? (void *)k_batch<DIA_I, 1>
+                                 : (void *)k_batch<DIA_0, 1>);
   int bps = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads_per_block, 0));
   if (bps < 1) return BIEF_ERR_CUDA;

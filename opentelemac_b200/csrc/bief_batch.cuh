@@ -13,9 +13,9 @@
 // each block rebuilds, in shared memory, the prefix sums of the tile
 // counts of the still-active instances and takes active tiles b, b+G, ...
 // Per-instance dot products: each tile's block reduces its thread partials
-// (block_tree) into a per-tile slot; one warp per instance then adds the
-// instance's tile partials (lane l: tiles l, l+32, ...) and folds the lanes
-// with a xor-butterfly.  Every block performs these reductions and the
+// (block_tree's tree) into a per-tile slot; one warp per instance then adds
+// the instance's tile partials (lane l: tiles l, l+32, ...) and folds the
+// lanes with a xor-butterfly.  Every block performs these reductions and the
 // scalar updates of every instance itself, in the same order, so all blocks
 // hold identical copies of the per-instance state without further traffic.
 #pragma once
@@ -56,31 +56,16 @@ struct BatchState {
   double rr[BATCH_MAX_INST], xl[BATCH_MAX_INST], otol[BATCH_MAX_INST];
 };
 
-// Warp sum of instance i's tile partials (slot q): lane l adds tiles
-// l, l+32, ... left to right, then a xor-butterfly; valid in every lane.
-__device__ __forceinline__ double batch_sum64(const double *half, int t0, int t1, int q) {
-  const int lane = threadIdx.x & 31;
-  double s = 0.0;
-  for (int k = t0 + lane; k < t1; k += 32) s = add(s, __ldcg(half + 2 * (size_t)k + q));
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) s = add(s, __shfl_xor_sync(0xffffffffu, s, o));
-  return s;
+template <int STO, class V>
+__device__ __forceinline__ double op_row(int i, double acc, const Sell &S, V vec) {
+  double unused = 0.0;
+  op_row2<STO>(i, i, false, acc, unused, S, vec);
+  return acc;
 }
 
-__device__ __forceinline__ float batch_sum32(const double *half, int t0, int t1, int q) {
-  const int lane = threadIdx.x & 31;
-  float s = 0.0f;
-  for (int k = t0 + lane; k < t1; k += 32) s = add(s, (float)__ldcg(half + 2 * (size_t)k + q));
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) s = add(s, __shfl_xor_sync(0xffffffffu, s, o));
-  return s;
-}
-
-template <int TD>
+template <int TD, int STO>
 __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
   __shared__ BatchState B;
-  __shared__ double smd[32];
-  __shared__ float smf[32];
   const int T = blockDim.x, t = threadIdx.x, G = gridDim.x;
   const int warp = t >> 5, lane = t & 31, nwarps = T >> 5;
   const int C = T * P.npt;
@@ -88,16 +73,27 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
   int nbar = 0;
   const float itol2 = (float)mul(P.inner_tol, P.inner_tol);
 
-  // prefix sums of the tile counts of the active instances (thread 0)
+  // prefix sums of the tile counts of the active instances (warp 0: each
+  // lane sums a run of consecutive instances, then a warp scan)
   auto rebuild_active = [&]() {
     __syncthreads();
-    if (t == 0) {
+    if (warp == 0) {
+      const int per = (NI + 31) / 32, i0 = min(NI, lane * per), i1 = min(NI, i0 + per);
       int a = 0;
-      for (int i = 0; i < NI; ++i) {
-        B.act[i] = a;
+      for (int i = i0; i < i1; ++i)
         if (B.state[i] != BS_DONE) a += P.inst_t0[i + 1] - P.inst_t0[i];
+      int incl = a;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
       }
-      B.act[NI] = a;
+      int run = incl - a;
+      for (int i = i0; i < i1; ++i) {
+        B.act[i] = run;
+        if (B.state[i] != BS_DONE) run += P.inst_t0[i + 1] - P.inst_t0[i];
+      }
+      if (lane == 31) B.act[NI] = incl;
     }
     __syncthreads();
   };
@@ -110,7 +106,114 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
     }
     return lo;
   };
-  // for every active tile handled by this block: body(i, gtile, n0, n1)
+  // partials written before barrier k go to half (k-1)&1 (nbar = k-1 while
+  // writing, = k while reading), so one phase never overwrites the partials
+  // a slower block may still be reading from the previous barrier
+  auto half = [&]() { return P.part + (size_t)(nbar & 1) * 2 * P.ntiles; };
+  // Tile partials in two stages, the two stages of block_tree: each warp
+  // folds its lanes' partials of a tile (xor butterfly) into shared memory
+  // as the tile ends; the tiles a block handles in a phase (up to MAXT at a
+  // time) are then finished together -- per tile, the warp sums in warp
+  // order, zero-padded to 32, through a second butterfly -- after one
+  // __syncthreads, instead of two block-wide syncs per tile.  Same tree,
+  // same bits.
+  constexpr int MAXT = 16;
+  __shared__ double W[MAXT][2][32];
+  __shared__ int Wgt[MAXT];
+  __shared__ unsigned char Wk[MAXT][2];  // 0 none, 1 binary64, 2 binary32
+  int ntl = 0;                           // tiles held (uniform in the block)
+  if (t < 2 * MAXT) Wk[t >> 1][t & 1] = 0;
+  auto flush = [&]() {
+    __syncthreads();
+    for (int pr = warp; pr < 2 * ntl; pr += nwarps) {
+      const int tl = pr >> 1, q = pr & 1, kind = Wk[tl][q];
+      if (kind == 0) continue;
+      double *dst = half() + 2 * (size_t)Wgt[tl] + q;
+      if (kind == 1) {
+        double u = lane < nwarps ? W[tl][q][lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) u = add(u, __shfl_xor_sync(0xffffffffu, u, o));
+        if (lane == 0) *dst = u;
+      } else {
+        float u = lane < nwarps ? (float)W[tl][q][lane] : 0.0f;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) u = add(u, __shfl_xor_sync(0xffffffffu, u, o));
+        if (lane == 0) *dst = (double)u;
+      }
+      if (lane == 0) Wk[tl][q] = 0;
+    }
+    __syncthreads();
+    ntl = 0;
+  };
+  auto store64 = [&](double v, int gt, int q) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0) W[ntl][q][warp] = v;
+    if (t == 0) { Wgt[ntl] = gt; Wk[ntl][q] = 1; }
+  };
+  auto store32 = [&](float v, int gt, int q) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0) W[ntl][q][warp] = (double)v;
+    if (t == 0) { Wgt[ntl] = gt; Wk[ntl][q] = 2; }
+  };
+  // Per-instance sums of the tile partials of the last barrier: one warp
+  // per instance, lane l adds the instance's tiles l, l+32, ... left to
+  // right, then a xor-butterfly (offsets 16..1) -- four instances of a warp
+  // at a time, with their loads interleaved.  need(i): 1 = slot 0 in binary64, 2 = slot 0 in
+  // binary32, 4 = slot 1 in binary32 (or-ed).  Results in SA[i] (slot 0)
+  // and SB[i] (slot 1), which reuse the tile buffer (idle between phases);
+  // valid in the whole block after the closing __syncthreads.
+  double *SA = &W[0][0][0], *SB = &W[0][0][0] + BATCH_MAX_INST;
+  auto gather_sums = [&](auto need) {
+    const double *h = P.part + (size_t)((nbar - 1) & 1) * 2 * P.ntiles;
+    for (int i0 = 4 * warp; i0 < NI; i0 += 4 * nwarps) {
+      int nd[4], k0[4], k1[4];
+      double s64[4];
+      float s0[4], s1[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int i = i0 + c;
+        nd[c] = i < NI ? need(i) : 0;
+        k0[c] = nd[c] ? P.inst_t0[i] + lane : 0;
+        k1[c] = nd[c] ? P.inst_t0[i + 1] : 0;
+        s64[c] = 0.0;
+        s0[c] = 0.0f;
+        s1[c] = 0.0f;
+      }
+      for (;;) {
+        bool any = false;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (k0[c] < k1[c]) {
+            any = true;
+            const double v0 = __ldcg(h + 2 * (size_t)k0[c]);
+            if (nd[c] & 1) s64[c] = add(s64[c], v0);
+            if (nd[c] & 2) s0[c] = add(s0[c], (float)v0);
+            if (nd[c] & 4) s1[c] = add(s1[c], (float)__ldcg(h + 2 * (size_t)k0[c] + 1));
+            k0[c] += 32;
+          }
+        }
+        if (!__any_sync(0xffffffffu, any)) break;
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+          s64[c] = add(s64[c], __shfl_xor_sync(0xffffffffu, s64[c], o));
+          s0[c] = add(s0[c], __shfl_xor_sync(0xffffffffu, s0[c], o));
+          s1[c] = add(s1[c], __shfl_xor_sync(0xffffffffu, s1[c], o));
+        }
+        if (lane == 0 && nd[c]) {
+          SA[i0 + c] = (nd[c] & 1) ? s64[c] : (double)s0[c];
+          SB[i0 + c] = (double)s1[c];
+        }
+      }
+    }
+    __syncthreads();
+  };
+  // for every active tile handled by this block: body(i, gtile, n0, n1);
+  // the tiles' partials are complete in `part` when it returns
   auto for_tiles = [&](auto body) {
     const int A = B.act[NI];
     for (int a = blockIdx.x; a < A; a += G) {
@@ -119,19 +222,9 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
       const int n0 = P.inst_off[i] + k * C;
       const int n1 = P.inst_off[i] + min((k + 1) * C, P.inst_n[i]);
       body(i, P.inst_t0[i] + k, n0, n1);
+      if (++ntl == MAXT) flush();
     }
-  };
-  // partials written before barrier k go to half (k-1)&1 (nbar = k-1 while
-  // writing, = k while reading), so one phase never overwrites the partials
-  // a slower block may still be reading from the previous barrier
-  auto half = [&]() { return P.part + (size_t)(nbar & 1) * 2 * P.ntiles; };
-  auto store64 = [&](double v, int gt, int q) {
-    const double r = block_tree(v, smd);
-    if (t == 0) half()[2 * (size_t)gt + q] = r;
-  };
-  auto store32 = [&](float v, int gt, int q) {
-    const float r = block_tree(v, smf);
-    if (t == 0) half()[2 * (size_t)gt + q] = (double)r;
+    if (ntl) flush();
   };
 
   // ---- initial state
@@ -156,21 +249,17 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
     store64(s, gt, 0);
   });
   if (!grid_barrier(P.ctl, P.timeout_ns, nbar)) return;
-  {
-    const double *h = P.part + (size_t)((nbar - 1) & 1) * 2 * P.ntiles;
-    for (int i = warp; i < NI; i += nwarps) {
-      double xl = batch_sum64(h, P.inst_t0[i], P.inst_t0[i + 1], 0);
-      if (lane == 0) {
-        if (__dsqrt_rn(xl) < 1.0e-15) {
-          B.state[i] = BS_UPD;   // marker: zero solution in the next phase
-          B.last[i] = 2;
-          xl = 1.0;
-        }
-        if (xl < 1.0) xl = 1.0;
-        B.xl[i] = xl;
-        B.otol[i] = mul(xl, mul(P.outer_tol, P.outer_tol));
-      }
+  gather_sums([&](int i) { return 1; });
+  for (int i = t; i < NI; i += T) {
+    double xl = SA[i];
+    if (__dsqrt_rn(xl) < 1.0e-15) {
+      B.state[i] = BS_UPD;   // marker: zero solution in the next phase
+      B.last[i] = 2;
+      xl = 1.0;
     }
+    if (xl < 1.0) xl = 1.0;
+    B.xl[i] = xl;
+    B.otol[i] = mul(xl, mul(P.outer_tol, P.outer_tol));
   }
   __syncthreads();
 
@@ -182,7 +271,7 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
       const int v = n0 + t + j * T;
       if (v < n1) {
         double acc = diag_term<TD>(P.x[v], P.da, v);
-        acc = rec_row(v, acc, P.S, [&](int w) { return P.x[w]; });
+        acc = op_row<STO>(v, acc, P.S, [&](int w) { return P.x[w]; });
         const double rv = sub(P.b[v], acc);
         sd = add(sd, mul(rv, rv));
         const float r32 = (float)rv;
@@ -207,22 +296,20 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
     }
   });
   if (!grid_barrier(P.ctl, P.timeout_ns, nbar)) return;
-  {
-    const double *h = P.part + (size_t)((nbar - 1) & 1) * 2 * P.ntiles;
-    for (int i = warp; i < NI; i += nwarps) {
-      if (B.last[i] == 2) {
-        if (lane == 0) { B.state[i] = BS_DONE; B.rr[i] = 0.0; B.last[i] = 0; }
-        continue;
-      }
-      const double rr = batch_sum64(h, P.inst_t0[i], P.inst_t0[i + 1], 0);
-      const float rho = batch_sum32(h, P.inst_t0[i], P.inst_t0[i + 1], 1);
-      if (lane == 0) {
-        B.rr[i] = rr;
-        if (isnan(rr)) { B.state[i] = BS_DONE; B.status[i] = ST_NAN; }
-        else if (rr <= B.otol[i]) { B.state[i] = BS_DONE; }
-        else { B.rho[i] = rho; B.rmax[i] = rho; B.beta[i] = 0.0f; B.state[i] = BS_ITER; }
-      }
+  gather_sums([&](int i) { return B.last[i] == 2 ? 0 : 1 | 4; });
+  for (int i = t; i < NI; i += T) {
+    if (B.last[i] == 2) {
+      B.state[i] = BS_DONE;
+      B.rr[i] = 0.0;
+      B.last[i] = 0;
+      continue;
     }
+    const double rr = SA[i];
+    const float rho = (float)SB[i];
+    B.rr[i] = rr;
+    if (isnan(rr)) { B.state[i] = BS_DONE; B.status[i] = ST_NAN; }
+    else if (rr <= B.otol[i]) { B.state[i] = BS_DONE; }
+    else { B.rho[i] = rho; B.rmax[i] = rho; B.beta[i] = 0.0f; B.state[i] = BS_ITER; }
   }
   rebuild_active();
 
@@ -263,19 +350,15 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
       }
     });
     if (!grid_barrier(P.ctl, P.timeout_ns, nbar)) return;
-    {
-      const double *h = P.part + (size_t)((nbar - 1) & 1) * 2 * P.ntiles;
-      for (int i = warp; i < NI; i += nwarps) {
-        if (B.state[i] != BS_ITER) continue;
-        const float pq = batch_sum32(h, P.inst_t0[i], P.inst_t0[i + 1], 0);
-        if (lane == 0) {
-          if (!(pq > 0.0f)) {
-            B.state[i] = BS_DONE;
-            B.status[i] = isnan(pq) ? ST_NAN : ST_BREAKDOWN;
-          } else {
-            B.alpha[i] = __fdiv_rn(B.rho[i], pq);
-          }
-        }
+    gather_sums([&](int i) { return B.state[i] == BS_ITER ? 2 : 0; });
+    for (int i = t; i < NI; i += T) {
+      if (B.state[i] != BS_ITER) continue;
+      const float pq = (float)SA[i];
+      if (!(pq > 0.0f)) {
+        B.state[i] = BS_DONE;
+        B.status[i] = isnan(pq) ? ST_NAN : ST_BREAKDOWN;
+      } else {
+        B.alpha[i] = __fdiv_rn(B.rho[i], pq);
       }
     }
     rebuild_active();
@@ -301,49 +384,45 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
       }
     });
     if (!grid_barrier(P.ctl, P.timeout_ns, nbar)) return;
-    {
-      const double *h = P.part + (size_t)((nbar - 1) & 1) * 2 * P.ntiles;
-      for (int i = warp; i < NI; i += nwarps) {
-        if (B.state[i] == BS_ITER) {
-          const float rho_new = batch_sum32(h, P.inst_t0[i], P.inst_t0[i + 1], 0);
-          if (lane == 0) {
-            const float rho_old = B.rho[i];
-            B.inner[i] += 1;
-            B.par[i] ^= 1;
-            const bool last = B.inner[i] >= P.max_inner;
-            if (last || rho_new <= mul(itol2, B.rmax[i]) || (double)rho_new <= B.otol[i]) {
-              B.state[i] = BS_UPD;
-              B.rho_rec[i] = rho_new;
-              B.rho_old[i] = rho_old;
-              B.last[i] = last ? 1 : 0;
-            } else {
-              B.beta[i] = __fdiv_rn(rho_new, rho_old);
-              B.rho[i] = rho_new;
-              B.first[i] = 0;
-            }
-          }
-        } else if (B.state[i] == BS_UPD) {
-          const double rr = batch_sum64(h, P.inst_t0[i], P.inst_t0[i + 1], 0);
-          const float rho = batch_sum32(h, P.inst_t0[i], P.inst_t0[i + 1], 1);
-          if (lane == 0) {
-            B.rr[i] = rr;
-            B.outer[i] += 1;
-            if (isnan(rr)) {
-              B.state[i] = BS_DONE;
-              B.status[i] = ST_NAN;
-            } else if (rr <= B.otol[i]) {
-              B.state[i] = BS_DONE;
-            } else if (B.last[i] || B.outer[i] >= P.max_outer) {
-              B.state[i] = BS_DONE;
-              B.status[i] = B.inner[i];
-            } else {
-              B.rmax[i] = rho;
-              B.beta[i] = __fdiv_rn(B.rho_rec[i], B.rho_old[i]);
-              B.rho[i] = rho;
-              B.first[i] = 0;
-              B.state[i] = BS_ITER;
-            }
-          }
+    gather_sums([&](int i) {
+      return B.state[i] == BS_ITER ? 2 : (B.state[i] == BS_UPD ? 1 | 4 : 0);
+    });
+    for (int i = t; i < NI; i += T) {
+      if (B.state[i] == BS_ITER) {
+        const float rho_new = (float)SA[i];
+        const float rho_old = B.rho[i];
+        B.inner[i] += 1;
+        B.par[i] ^= 1;
+        const bool last = B.inner[i] >= P.max_inner;
+        if (last || rho_new <= mul(itol2, B.rmax[i]) || (double)rho_new <= B.otol[i]) {
+          B.state[i] = BS_UPD;
+          B.rho_rec[i] = rho_new;
+          B.rho_old[i] = rho_old;
+          B.last[i] = last ? 1 : 0;
+        } else {
+          B.beta[i] = __fdiv_rn(rho_new, rho_old);
+          B.rho[i] = rho_new;
+          B.first[i] = 0;
+        }
+      } else if (B.state[i] == BS_UPD) {
+        const double rr = SA[i];
+        const float rho = (float)SB[i];
+        B.rr[i] = rr;
+        B.outer[i] += 1;
+        if (isnan(rr)) {
+          B.state[i] = BS_DONE;
+          B.status[i] = ST_NAN;
+        } else if (rr <= B.otol[i]) {
+          B.state[i] = BS_DONE;
+        } else if (B.last[i] || B.outer[i] >= P.max_outer) {
+          B.state[i] = BS_DONE;
+          B.status[i] = B.inner[i];
+        } else {
+          B.rmax[i] = rho;
+          B.beta[i] = __fdiv_rn(B.rho_rec[i], B.rho_old[i]);
+          B.rho[i] = rho;
+          B.first[i] = 0;
+          B.state[i] = BS_ITER;
         }
       }
     }
@@ -367,7 +446,8 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
 }
 
 // Every element's three nodes belong to the same instance (binary search
-// of the instance ranges); otherwise the batch is not block diagonal.
+// of the instance ranges); otherwise the batch is not block diagonal (and
+// neither is its segment numbering, whose segments are element faces).
 __global__ void k_check_blockdiag(int nelem, const int *__restrict__ ik, int ninst,
                                   const int *__restrict__ off, const int *__restrict__ cnt,
                                   int *err) {

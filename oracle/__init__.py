@@ -258,6 +258,32 @@ def solve_mixed_batch(ikle0, dm, typdia, xm, b, x0=None, precon=2, inner_tol=0.1
     return dict(x=x, status=st, outer=outer.value, inner=inner.value, relres=relres.value)
 
 
+def solve_mixed_batch_seg(g1, g2, dm, typdia, xa, b, x0=None, precon=2, inner_tol=0.1,
+                          outer_tol=1e-8, max_outer=1000, max_inner=1000000, nthreads=1024,
+                          npt=1):
+    """One instance of the batched mixed-precision solver on a segment-storage
+    matrix (symmetric XA(NSEG)), in the batched kernel's dot order."""
+    g1, g2 = _i32(g1), _i32(g2)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    n = b.size
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    dm = np.ascontiguousarray(dm, dtype=np.float64)
+    xa = np.ascontiguousarray(xa, dtype=np.float64).ravel()
+    L = lib()
+    P = ctypes.POINTER
+    d, i, ch = ctypes.c_double, ctypes.c_int, ctypes.c_char
+    L.orc_solve_mixed_batch_seg.argtypes = [i, i, P(i), P(i), P(d), P(d), P(d), ch, P(d), ch, i,
+                                            d, d, i, i, i, i, P(i), P(i), P(d)]
+    outer, inner = ctypes.c_int(0), ctypes.c_int(0)
+    relres = ctypes.c_double(0.0)
+    st = L.orc_solve_mixed_batch_seg(n, g1.size, _pi(g1), _pi(g2), _pd(x), _pd(b), _pd(dm),
+                                     typdia.encode(), _pd(xa), b"S", precon, inner_tol,
+                                     outer_tol, max_outer, max_inner, nthreads, npt,
+                                     ctypes.byref(outer), ctypes.byref(inner),
+                                     ctypes.byref(relres))
+    return dict(x=x, status=st, outer=outer.value, inner=inner.value, relres=relres.value)
+
+
 def solve_omp(ikle0, dm, xm, b, x0=None, nitmax=1000000, eps=1e-8, nthreads=None):
     """Binary64 SOLVE (PRECON 2, symmetric) on `nthreads` host threads."""
     ik, a, bb, c = _cols(ikle0)

@@ -1899,6 +1899,21 @@ int orc_solve_mixed_batch(int npoin, int nelem, const int *ik0, const int *ik1,
 }
 
 
+/* One instance of the batched solver on a segment-storage matrix: the
+ * segment form of orc_solve_mixed_seg with the batched kernel's dot order. */
+int orc_solve_mixed_batch_seg(int npoin, int nseg, const int *g1, const int *g2, double *x,
+                              const double *b, const double *dm_in, char typdia_in,
+                              const double *xa_in, char typext, int precon, double inner_tol,
+                              double outer_tol, int max_outer, int max_inner, int nt, int npt,
+                              int *outer_out, int *inner_total_out, double *relres_out)
+{
+    dotspec ds = {1, 0, nt, npt};
+    opmesh M = {3, 0, 0, NULL, NULL, NULL, nseg, g1, g2, NULL, NULL};
+    return mixed_impl(&M, npoin, x, b, dm_in, typdia_in, xa_in, typext, precon, inner_tol,
+                      outer_tol, max_outer, max_inner, &ds, outer_out, inner_total_out,
+                      relres_out);
+}
+
 /* ------------------------------------------------------------------ */
 /* multi-threaded port (CPU baseline on all host cores)                 */
 /* ------------------------------------------------------------------ */

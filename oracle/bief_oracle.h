@@ -146,6 +146,11 @@ int orc_solve_mixed_batch(int npoin, int nelem, const int *ik0, const int *ik1,
                           double outer_tol, int max_outer, int max_inner,
                           int nt, int npt, int *outer_out, int *inner_total_out,
                           double *relres_out);
+int orc_solve_mixed_batch_seg(int npoin, int nseg, const int *g1, const int *g2, double *x,
+                              const double *b, const double *dm_in, char typdia_in,
+                              const double *xa_in, char typext, int precon, double inner_tol,
+                              double outer_tol, int max_outer, int max_inner, int nt, int npt,
+                              int *outer_out, int *inner_total_out, double *relres_out);
 
 int orc_solve_omp(int npoin, int nelem, const int *ik0, const int *ik1,
                   const int *ik2, double *x, const double *b_in,

@@ -46,6 +46,37 @@ def test_batch_bitexact_per_instance(oracle_mod, npt, threads):
     bs.close()
 
 
+@pytest.mark.parametrize("npt,threads", [(1, 1024), (4, 256)])
+def test_batch_segments_bitexact_per_instance(oracle_mod, npt, threads):
+    """Segment storage (MATRIX STORAGE 3, TELEMAC-2D's default): every
+    instance's own STOSEG numbering, the EBE matrix converted by ASSEX3 on the
+    device, each instance bit for bit the oracle's batched segment solve."""
+    from opentelemac_b200.batch import BatchSolver
+    inst = _instances([9, 17, 31, 26, 44])
+    inst[2]["b"] = np.zeros_like(inst[2]["b"])
+    bs = BatchSolver([(p["x"].size, p["ik"]) for p in inst])
+    bs.assemble_wave([p["x"] for p in inst], [p["y"] for p in inst], [p["coef"] for p in inst])
+    segs = [mg.segments(p["ik"], p["x"].size) for p in inst]
+    bs.set_segments([(g[0], g[1]) for g in segs]).to_segments()
+    assert bs.A.storage == 3
+    b = bs.gather([p["b"] for p in inst])
+    x = bs.gather([np.zeros(p["x"].size) for p in inst])
+    r = bs.solve_mixed(x, b, inner_tol=1e-4, outer_tol=1e-9, nodes_per_thread=npt,
+                       threads_per_block=threads)
+    xs = [v.cpu().numpy() for v in bs.scatter(x)]
+    for k, (p, (g1, g2, es, ori)) in enumerate(zip(inst, segs)):
+        xa = oracle_mod.assex3(es, ori, "S", p["xm"], g1.size)
+        ref = oracle_mod.solve_mixed_batch_seg(g1, g2, p["dm"], "Q", xa, p["b"], precon=2,
+                                               inner_tol=1e-4, outer_tol=1e-9, npt=npt,
+                                               nthreads=threads)
+        assert r["status"][k] == ref["status"] == 0
+        assert (r["inner"][k], r["outer"][k]) == (ref["inner"], ref["outer"]), k
+        assert r["relres"][k] == ref["relres"]
+        np.testing.assert_array_equal(xs[k], ref["x"], err_msg=f"instance {k}")
+    assert r["inner"][2] == 0 and not xs[2].any()
+    bs.close()
+
+
 def test_batch_256_meshes():
     """256 meshes, node counts log-uniform in [2,000, 200,000], each with its
     own depth field seed and random right-hand side, one launch, relres 1e-8."""
