@@ -539,7 +539,7 @@ def run_matvec(args, ws, rank, local):
     g64 = ws * by["mv64"] / (m64 * 1e-3) / 1e9
     g32 = ws * by["mv32"] / (m32 * 1e-3) / 1e9
     if rank == 0:
-        kern = "k_mvseg" if args.storage == "seg" else "k_matvec"
+        kern = "k_mvseg" if args.storage == "seg" else "k_matvec16"
         print(json.dumps({
             "metric": "EBE MATVEC 'X=AY' HBM GB/s (algorithmic bytes)", "value": g64,
             "unit": "GB/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -945,7 +945,7 @@ def main():
                                         "tight_relres": rel_tight,
                                         "tight_iterations": nit_tight}},
             "matvec": {"op": "X=AY binary64 TYPDIA=Q",
-                       "kernel": "k_mvseg" if args.storage == "seg" else "k_matvec", "ms": mv_t,
+                       "kernel": "k_mvseg" if args.storage == "seg" else "k_matvec16", "ms": mv_t,
                        "ms_call": mv_t_call,
                        "timing": "ms: library events around the launch; ms_call: torch events "
                                  "around the Python call",
