@@ -122,9 +122,9 @@ int grid_for(int n, int nsm) {
   return std::max(1, std::min(g, nsm * 16));
 }
 
-// One node per thread (256-thread blocks): the blocks are scheduled as SMs
+// One node per thread (MV16_T-thread blocks): the blocks are scheduled as SMs
 // free up, so no thread carries a second node into the tail of the launch.
-int mv_grid(int n) { return std::max(1, (n + 255) / 256); }
+int mv_grid(int n) { return std::max(1, (n + MV16_T - 1) / MV16_T); }
 
 // Parse an 8-character MATVEC operation string (trailing blanks optional).
 int parse_op(const char *op, int *opc, bool *trans) {
@@ -153,8 +153,8 @@ void launch_mv(bief_handle *h, const double *xm, const double *da, const double 
                int opc, double c, cudaStream_t st) {
   if (h->mv16) {
     Mv16 M{h->d_mv_deg, h->d_rec_off, h->d_mv_eb, h->d_mv_ek, h->d_mv_dv};
-    k_matvec16<TD, SYM, TR><<<mv_grid(h->npoin), 256, 0, st>>>(h->npoin, h->nelem, M, xm, da, y,
-                                                               x, opc, c);
+    k_matvec16<TD, SYM, TR><<<mv_grid(h->npoin), MV16_T, 0, st>>>(h->npoin, h->nelem, M, xm, da,
+                                                                  y, x, opc, c);
     return;
   }
   k_matvec<TD, SYM, TR><<<grid_for(h->npoin, h->nsm), 256, 0, st>>>(
