@@ -493,6 +493,71 @@ def config2_measure(P2, ws, flush_l2, hbm, steps=2, warmup=1):
     return out
 
 
+def config3_measure(ws, steps=3, warmup=1):
+    """The differentiation workload on the 501 x 501-node mesh (251,001
+    nodes, 500,000 triangles): per-element depth h = the smooth field +
+    N(0, 0.1^2), L = 0.5 ||x(h) - x_obs||^2 with x_obs solved from the
+    unperturbed field, solves to relres 1e-13.  Timed with CUDA events:
+    one forward + backward (assembly, forward CG, adjoint CG, per-element
+    gradient), and the 50-step unrolled loop x_{n+1} = A(h)^-1 M x_n with a
+    checkpoint every 10 steps, forward and backward (150 solves)."""
+    import torch
+    from opentelemac_b200 import autograd as ag, bief, meshgen as mg
+    x, y, ik = mg.square_mesh(501)
+    prob = ag.WaveProblem(x, y, ik, eps=1e-13)
+    h0 = torch.tensor(mg.depth_smooth(x, y, ik), device="cuda")
+    h = h0 + torch.tensor(np.random.default_rng(3).normal(0.0, 0.1, ik.shape[0]),
+                          device="cuda")
+    xt = torch.tensor(mg.random_solution(x.size), device="cuda")
+    b = torch.zeros_like(xt)
+    bief.matvec("X=AY    ", b, prob.assemble(mg.DT * mg.GRAV * h0), xt)
+    x_obs = prob.solve(mg.DT * mg.GRAV * h0, b)
+
+    def ev_time(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        out = fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    def fwd_bwd():
+        hv = h.clone().requires_grad_(True)
+        xs = ag.wave_solve(mg.DT * mg.GRAV * hv, b, prob)
+        L = 0.5 * ((xs - x_obs) ** 2).sum()
+        L.backward()
+        return hv.grad
+
+    ts = []
+    for s in range(warmup + steps):
+        t, g = ev_time(fwd_bwd)
+        if s >= warmup:
+            ts.append(t)
+    fb_ms = max_over_ranks(sum(ts) / len(ts), ws)
+
+    def loop():
+        hv = h.clone().requires_grad_(True)
+        xs = ag.unrolled_loop(mg.DT * mg.GRAV * hv, xt, prob, nsteps=50, checkpoint_every=10)
+        (0.5 * (xs * xs).sum()).backward()
+        return hv.grad
+
+    n0 = prob.solves
+    loop_ms, _ = ev_time(loop)
+    loop_solves = prob.solves - n0
+    loop_ms = max_over_ranks(loop_ms, ws)
+    prob.close()
+    return {"workload": "501x501-node P1 mesh, per-element depth, L = 0.5 ||x(h) - x_obs||^2, "
+                        "relres 1e-13",
+            "npoin": int(x.size), "nelem": int(ik.shape[0]),
+            "forward_backward_ms": fb_ms,
+            "grad_norm": float(torch.linalg.norm(g)),
+            "unrolled_loop": {"steps": 50, "checkpoint_every": 10, "ms": loop_ms,
+                              "solves": loop_solves,
+                              "ms_per_solve": loop_ms / max(loop_solves, 1)}}
+
+
 def run_matvec(args, ws, rank, local):
     """MATVEC 'X=AY' alone: binary64 EBE (k_matvec / k_mvseg) and binary32
     (k_matvec32) on the --n x --n mesh, --steps timed launches each after
@@ -881,9 +946,11 @@ def main():
         PL["mesh"].close()
         del PL
     batch = None
+    cfg3 = None
     if not args.no_extras:
         batch = batch_measure(ws, rank, local, 2, 1, 1e-4, args.eps)
         batch["steps"], batch["warmup"] = 2, 1
+        cfg3 = config3_measure(ws)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -987,6 +1054,7 @@ def main():
                          "note": "binary64 GRACJG through bief_set_matrix + bief_solve with "
                                  "host buffers"},
             "config2": cfg2,
+            "config3": cfg3,
             "batch256": batch,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
