@@ -62,3 +62,18 @@ def test_batch_contract_shape():
              timeout=1800)
     assert BASE <= set(d) and d["converged"] == 256
     assert d["roofline"]["frac"] > 0 and d["config"]["nodes_per_thread"] == 8
+
+
+@pytest.mark.gpu
+def test_fp64_and_capped_batch_contracts():
+    """The binary64-only line (with a NITMAX cap, the profiling form) and the
+    batch line stopped after a few inner iterations."""
+    d = _run("--workload", "fp64", "--n", "101", "--steps", "2", "--warmup", "1")
+    assert BASE <= set(d) and d["unit"] == "ms" and d["higher_is_better"] is False
+    assert d["relres"] <= 1e-8 and d["roofline"]["kernel"] == "k_cg64"
+    d = _run("--workload", "fp64", "--n", "101", "--nitmax", "20", "--steps", "1", "--warmup", "1")
+    assert d["iterations"] == 20 and d["relres"] > 1e-8
+    d = _run("--workload", "batch256", "--batch-shape", "4,1024", "--batch-max-inner", "40",
+             "--steps", "1", "--warmup", "1", timeout=1800)
+    assert d["max_inner"] == 40 and d["iterations_rank0"]["max"] == 40
+    assert d["converged"] == 0
