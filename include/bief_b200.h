@@ -270,6 +270,14 @@ int bief_selftest_timeout(int device, long long timeout_ns);
 /* Shape of the device dot-product tree: number of blocks and threads per
  * block of the persistent solver kernel. */
 int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads);
+/* Which gather records the standalone MATVEC (bief_matvec*) reads for this
+ * mesh, fixed when the mesh is made: the most compact its numbering allows.
+ * The bits of the product are the same in every format. */
+#define BIEF_MV_IKLE   0  /* a node in more than 255 elements: element index, then IKLE */
+#define BIEF_MV_LOCAL  1  /* 16-bit element offsets and vertex offsets: 6 B per entry  */
+#define BIEF_MV_BAND   2  /* element index, 16-bit vertex offsets: 8 B per entry       */
+#define BIEF_MV_ANY    3  /* element index and both other vertices: 12 B per entry     */
+int bief_matvec_format(bief_handle *h, int *format);
 /* Kernel time (ms, CUDA events recorded around the launch on the stream
  * the call used) of the last solve kernel and of the last matvec kernel.  For
  * bief_matvec_dev, which returns before its kernel ends, the matvec time is

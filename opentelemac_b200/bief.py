@@ -107,6 +107,16 @@ class Mesh:
         _native.lib().bief_launch_info(self._h, ctypes.byref(g), ctypes.byref(t))
         return g.value, t.value
 
+    MATVEC_FORMATS = ("ikle", "local", "band", "any")
+
+    def matvec_format(self):
+        """Gather records of the standalone MATVEC for this mesh: 'local' (6 B
+        per entry), 'band' (8 B), 'any' (12 B) or 'ikle' (a node in more than
+        255 elements: element index, then IKLE)."""
+        f = ctypes.c_int()
+        _check(_native.lib().bief_matvec_format(self._h, ctypes.byref(f)), "bief_matvec_format")
+        return self.MATVEC_FORMATS[f.value]
+
     def last_timing(self):
         s, m = ctypes.c_float(), ctypes.c_float()
         _native.lib().bief_last_timing(self._h, ctypes.byref(s), ctypes.byref(m))

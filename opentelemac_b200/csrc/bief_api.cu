@@ -36,13 +36,13 @@ struct bief_handle {
   int *d_meta = nullptr, *d_rec_off = nullptr, *d_seg_off = nullptr, *d_seg_col = nullptr;
   int2 *d_rec_idx = nullptr;
   uchar2 *d_rec_slot = nullptr;
-  // compressed gather records of the standalone MATVEC (Mv16); mv16 = 0
-  // when some entry does not fit them (k_matvec then reads IKLE)
+  // gather records of the standalone MATVEC (Mv16) in format mv16 (MV_*);
+  // MV_NONE when a node has more than 255 entries (k_matvec then reads IKLE)
   int mv16 = 0;
   unsigned char *d_mv_deg = nullptr;
   int *d_mv_eb = nullptr;
-  unsigned short *d_mv_ek = nullptr;
-  short2 *d_mv_dv = nullptr;
+  void *d_mv_ek = nullptr;  // unsigned short (MV_LOCAL) or int
+  void *d_mv_dv = nullptr;  // short2 offsets (MV_LOCAL, MV_BAND); MV_ANY reads d_rec_idx
   double2 *d_rec_c = nullptr;
   double2 *d_rec_ct = nullptr;   // transposed-operator records (EQUNOR, 'Q' storage)
   double *d_sg_ct = nullptr;     // transposed-operator segment slots
@@ -155,9 +155,17 @@ template <int TD, bool SYM, bool TR>
 void launch_mv(bief_handle *h, const double *xm, const double *da, const double *y, double *x,
                int opc, double c, cudaStream_t st) {
   if (h->mv16) {
-    Mv16 M{h->d_mv_deg, h->d_rec_off, h->d_mv_eb, h->d_mv_ek, h->d_mv_dv};
-    k_matvec16<TD, SYM, TR><<<mv_grid(h->npoin), MV16_T, 0, st>>>(h->npoin, h->nelem, M, xm, da,
-                                                                  y, x, opc, c);
+    Mv16 M{h->d_mv_deg, h->d_rec_off, h->d_mv_eb, h->d_mv_ek,
+           h->mv16 == MV_ANY ? (const void *)h->d_rec_idx : h->d_mv_dv};
+    if (h->mv16 == MV_LOCAL)
+      k_matvec16<TD, SYM, TR, MV_LOCAL><<<mv_grid(h->npoin), MV16_T, 0, st>>>(
+          h->npoin, h->nelem, M, xm, da, y, x, opc, c);
+    else if (h->mv16 == MV_BAND)
+      k_matvec16<TD, SYM, TR, MV_BAND><<<mv_grid(h->npoin), MV16_T, 0, st>>>(
+          h->npoin, h->nelem, M, xm, da, y, x, opc, c);
+    else
+      k_matvec16<TD, SYM, TR, MV_ANY><<<mv_grid(h->npoin), MV16_T, 0, st>>>(
+          h->npoin, h->nelem, M, xm, da, y, x, opc, c);
     return;
   }
   k_matvec<TD, SYM, TR><<<grid_for(h->npoin, h->nsm), 256, 0, st>>>(
@@ -580,43 +588,51 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
     for (int q = 0; q < nnb[i]; ++q) seg_col[sb + 32 * q] = nb_list[nb_ptr[i] + q];
   }
 
-  // Compressed MATVEC records (Mv16): usable when, in every slice, the
-  // entries' element numbers lie within 2^14 of the slice's smallest, every
-  // other vertex within a 16-bit offset of its node, and no node has more
-  // than 255 entries -- true of any mesh numbered with some locality.
+  // MATVEC gather records (Mv16), in the most compact of three formats the
+  // mesh allows: MV_LOCAL when, in every slice, the entries' element numbers
+  // lie within 2^14 of the slice's smallest and every other vertex within a
+  // 16-bit offset of its node (any mesh numbered with some locality: 6 B per
+  // entry); MV_BAND when only the vertex offsets fit (8 B); MV_ANY otherwise
+  // (12 B: element index and the two vertices, the latter the solver's own
+  // rec_idx records).  None when a node has more than 255 entries.
   std::vector<int> mv_eb(nsl, 0);
-  bool mv16 = true;
-  for (int sgi = 0; sgi < nsl && mv16; ++sgi) {
+  bool fit_e = true, fit_v = true, fit_deg = true;
+  for (int sgi = 0; sgi < nsl; ++sgi) {
     int lo = INT_MAX, hi = INT_MIN;
     for (int i = 32 * sgi; i < std::min(npoin, 32 * sgi + 32); ++i) {
-      if (ptr[i + 1] - ptr[i] > 255) mv16 = false;
+      if (ptr[i + 1] - ptr[i] > 255) fit_deg = false;
       for (int j = ptr[i]; j < ptr[i + 1]; ++j) {
         lo = std::min(lo, ek[j] >> 2);
         hi = std::max(hi, ek[j] >> 2);
         const int e = ek[j] >> 2, k = ek[j] & 3;
         const long long da = (long long)ik[(size_t)((k + 1) % 3) * nelem + e] - i;
         const long long db = (long long)ik[(size_t)((k + 2) % 3) * nelem + e] - i;
-        if (da < -32768 || da > 32767 || db < -32768 || db > 32767) mv16 = false;
+        if (da < -32768 || da > 32767 || db < -32768 || db > 32767) fit_v = false;
       }
     }
-    if (lo != INT_MAX && hi - lo >= (1 << 14)) mv16 = false;
+    if (lo != INT_MAX && hi - lo >= (1 << 14)) fit_e = false;
     mv_eb[sgi] = lo == INT_MAX ? 0 : lo;
   }
+  const int mvf = !fit_deg ? MV_NONE : (fit_e && fit_v) ? MV_LOCAL : fit_v ? MV_BAND : MV_ANY;
   std::vector<unsigned char> mv_deg;
-  std::vector<unsigned short> mv_ek;
-  std::vector<short2> mv_dv;
-  if (mv16) {
+  std::vector<unsigned short> mv_ek16;
+  std::vector<int> mv_ek32;
+  std::vector<short2> mv_dv16;
+  if (mvf != MV_NONE) {
     mv_deg.assign(npoin, 0);
-    mv_ek.assign(nrec, 0);
-    mv_dv.assign(nrec, make_short2(0, 0));
+    if (mvf == MV_LOCAL) mv_ek16.assign(nrec, 0); else mv_ek32.assign(nrec, 0);
+    if (mvf != MV_ANY) mv_dv16.assign(nrec, make_short2(0, 0));
     for (int i = 0; i < npoin; ++i) {
       const int rb = rec_off[i >> 5] + (i & 31), eb = mv_eb[i >> 5];
       mv_deg[i] = (unsigned char)(ptr[i + 1] - ptr[i]);
       for (int m = 0; m < ptr[i + 1] - ptr[i]; ++m) {
         const int j = ptr[i] + m, e = ek[j] >> 2, k = ek[j] & 3;
-        mv_ek[rb + 32 * m] = (unsigned short)(((e - eb) << 2) | k);
-        mv_dv[rb + 32 * m] = make_short2((short)(ik[(size_t)((k + 1) % 3) * nelem + e] - i),
-                                         (short)(ik[(size_t)((k + 2) % 3) * nelem + e] - i));
+        const int va = ik[(size_t)((k + 1) % 3) * nelem + e];
+        const int vb = ik[(size_t)((k + 2) % 3) * nelem + e];
+        const size_t r = (size_t)rb + 32 * (size_t)m;
+        if (mvf == MV_LOCAL) mv_ek16[r] = (unsigned short)(((e - eb) << 2) | k);
+        else mv_ek32[r] = ek[j];
+        if (mvf != MV_ANY) mv_dv16[r] = make_short2((short)(va - i), (short)(vb - i));
       }
     }
   }
@@ -659,20 +675,28 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
         (st = dalloc(&h->d_rec_c, nrec)) || (st = dalloc(&h->d_seg_col, nseg)) ||
         (st = dalloc(&h->d_seg_c, nseg)))
       return fail(st);
-    if (mv16) {
-      if ((st = dalloc(&h->d_mv_deg, n)) || (st = dalloc(&h->d_mv_eb, (size_t)nsl)) ||
-          (st = dalloc(&h->d_mv_ek, nrec)) || (st = dalloc(&h->d_mv_dv, nrec)))
+    if (mvf != MV_NONE) {
+      const size_t bek = mvf == MV_LOCAL ? sizeof(unsigned short) : sizeof(int);
+      const void *hek = mvf == MV_LOCAL ? (const void *)mv_ek16.data() : (const void *)mv_ek32.data();
+      unsigned char *dek = nullptr;
+      short2 *ddv = nullptr;
+      if ((st = dalloc(&h->d_mv_deg, n)) || (st = dalloc(&h->d_mv_eb, (size_t)nsl)))
         return fail(st);
+      if ((st = dalloc(&dek, bek * nrec))) return fail(st);
+      h->d_mv_ek = dek;
+      if (mvf != MV_ANY && (st = dalloc(&ddv, nrec))) return fail(st);
+      h->d_mv_dv = ddv;
       if ((e = cudaMemcpyAsync(h->d_mv_deg, mv_deg.data(), n, cudaMemcpyHostToDevice,
                                h->stream)) != cudaSuccess ||
           (e = cudaMemcpyAsync(h->d_mv_eb, mv_eb.data(), sizeof(int) * nsl,
                                cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
-          (e = cudaMemcpyAsync(h->d_mv_ek, mv_ek.data(), sizeof(unsigned short) * nrec,
-                               cudaMemcpyHostToDevice, h->stream)) != cudaSuccess ||
-          (e = cudaMemcpyAsync(h->d_mv_dv, mv_dv.data(), sizeof(short2) * nrec,
-                               cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
+          (e = cudaMemcpyAsync(dek, hek, bek * nrec, cudaMemcpyHostToDevice, h->stream)) !=
+              cudaSuccess ||
+          (mvf != MV_ANY &&
+           (e = cudaMemcpyAsync(ddv, mv_dv16.data(), sizeof(short2) * nrec,
+                                cudaMemcpyHostToDevice, h->stream)) != cudaSuccess))
         return fail(cuda_fail(e, "mesh upload", __LINE__));
-      h->mv16 = 1;
+      h->mv16 = mvf;
     }
     if ((st = persistent_grid(npoin, h->nsm, &h->G))) return fail(st);
     if ((st = dalloc(&h->d_part, 8 * (size_t)h->G + 4))) return fail(st);
@@ -1625,6 +1649,12 @@ int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads) {
   if (!h) return BIEF_ERR_ARGS;
   if (nblocks) *nblocks = h->G;
   if (nthreads) *nthreads = h->T;
+  return BIEF_OK;
+}
+
+int bief_matvec_format(bief_handle *h, int *format) {
+  if (!h || !format) return BIEF_ERR_ARGS;
+  *format = h->mv16;
   return BIEF_OK;
 }
 

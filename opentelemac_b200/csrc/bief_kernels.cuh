@@ -65,46 +65,71 @@ __global__ void __launch_bounds__(256) k_matvec(int npoin, int nelem, const int 
                                          nelem, vec));
 }
 
-// MATVEC from the compressed gather records of the mesh (Mv16, built with
-// the mesh when every entry fits): per entry, in the 32-node sliced layout,
-// the element as (IELEM - eb) << 2 | IDP-1 in 16 bits and the element's two
-// other vertices as 16-bit offsets from the node.  The coefficient and the
-// vertex loads of an entry then depend on one coalesced index load only
-// (ebe_row goes index -> IKLE -> vertex values), IKLE is not read, and the
-// index costs 6 bytes per entry instead of the 4 of the element index plus
-// the 8 of the two IKLE values.  The index streams are loaded evict-first;
-// the additions are ebe_row's, in its order, so the bits are the same.
+// MATVEC from the gather records of the mesh (Mv16, built with the mesh):
+// per entry, in the 32-node sliced layout, the element and local point and
+// the element's two other vertices, so that the coefficient and the vertex
+// loads of an entry depend on one coalesced index load only (ebe_row goes
+// index -> IKLE -> vertex values) and IKLE is not read.  Three formats, the
+// most compact the numbering allows:
+//   MV_LOCAL  (IELEM - eb) << 2 | IDP-1 in 16 bits (eb: the slice's smallest
+//             element) and the vertices as 16-bit offsets from the node: 6 B;
+//   MV_BAND   IELEM << 2 | IDP-1 in 32 bits, 16-bit vertex offsets: 8 B;
+//   MV_ANY    IELEM << 2 | IDP-1 and the two vertices, 32 bits each: 12 B
+// (against 4 B of element index plus 8 B of IKLE read through it).  The
+// index streams are loaded evict-first; the additions are ebe_row's, in its
+// order, so the bits are the same.
+enum : int { MV_NONE = 0, MV_LOCAL = 1, MV_BAND = 2, MV_ANY = 3 };
+
 struct Mv16 {
   const unsigned char *deg;    // per node: gather entries
   const int *off;              // per slice: first record
-  const int *eb;               // per slice: smallest element number of its entries
-  const unsigned short *ek;    // per record: (IELEM - eb) << 2 | IDP-1
-  const short2 *dv;            // per record: (a - i, b - i), a and b the other vertices
+  const int *eb;               // per slice: smallest element number (MV_LOCAL)
+  const void *ek;              // per record: unsigned short (MV_LOCAL) or int
+  const void *dv;              // per record: short2 offsets or int2 vertices (MV_ANY)
 };
 
-template <int NB, bool SYM, bool TRANS, class V>
+// Element, local point and the two other vertices of record r of node i.
+template <int FMT>
+__device__ __forceinline__ void mv_entry(const Mv16 &M, int i, int eb, int r, int &e, int &k,
+                                         int &a, int &b) {
+  int p;
+  if constexpr (FMT == MV_LOCAL) {
+    p = __ldcs(static_cast<const unsigned short *>(M.ek) + r);
+    e = eb + (p >> 2);
+  } else {
+    p = __ldcs(static_cast<const int *>(M.ek) + r);
+    e = p >> 2;
+  }
+  k = p & 3;
+  if constexpr (FMT == MV_ANY) {
+    const int2 v = __ldcs(static_cast<const int2 *>(M.dv) + r);
+    a = v.x;
+    b = v.y;
+  } else {
+    const short2 d = __ldcs(static_cast<const short2 *>(M.dv) + r);
+    a = i + d.x;
+    b = i + d.y;
+  }
+}
+
+template <int NB, bool SYM, bool TRANS, int FMT, class V>
 __device__ __forceinline__ void mv16_batch(double &acc, int i, int eb, int b0, int m,
                                            const Mv16 &M, const double *__restrict__ xm, int ne,
                                            V vec) {
-  unsigned short p[NB];
-  short2 d[NB];
+  int e[NB], k[NB], va[NB], vb[NB];
 #pragma unroll
-  for (int q = 0; q < NB; ++q) {
-    p[q] = __ldcs(M.ek + b0 + 32 * (m + q));
-    d[q] = __ldcs(M.dv + b0 + 32 * (m + q));
-  }
+  for (int q = 0; q < NB; ++q) mv_entry<FMT>(M, i, eb, b0 + 32 * (m + q), e[q], k[q], va[q], vb[q]);
   double xa[NB], xb[NB], ya[NB], yb[NB];
 #pragma unroll
   for (int q = 0; q < NB; ++q) {
-    const int e = eb + (p[q] >> 2), k = p[q] & 3;
-    const int a = (k == 2) ? 0 : k + 1;  // (k+1) mod 3
-    const int b = (k == 0) ? 2 : k - 1;  // (k+2) mod 3
-    const int ca = TRANS ? xm_col<SYM>(a, k) : xm_col<SYM>(k, a);
-    const int cb = TRANS ? xm_col<SYM>(b, k) : xm_col<SYM>(k, b);
-    xa[q] = __ldg(xm + (size_t)ca * ne + e);
-    xb[q] = __ldg(xm + (size_t)cb * ne + e);
-    ya[q] = vec(i + d[q].x);
-    yb[q] = vec(i + d[q].y);
+    const int a = (k[q] == 2) ? 0 : k[q] + 1;  // (k+1) mod 3
+    const int b = (k[q] == 0) ? 2 : k[q] - 1;  // (k+2) mod 3
+    const int ca = TRANS ? xm_col<SYM>(a, k[q]) : xm_col<SYM>(k[q], a);
+    const int cb = TRANS ? xm_col<SYM>(b, k[q]) : xm_col<SYM>(k[q], b);
+    xa[q] = __ldg(xm + (size_t)ca * ne + e[q]);
+    xb[q] = __ldg(xm + (size_t)cb * ne + e[q]);
+    ya[q] = vec(va[q]);
+    yb[q] = vec(vb[q]);
   }
 #pragma unroll
   for (int q = 0; q < NB; ++q) acc = add(acc, add(mul(xa[q], ya[q]), mul(xb[q], yb[q])));
@@ -123,7 +148,7 @@ constexpr int MV16_B = BIEF_MV16_BATCH;
 #endif
 constexpr int MV16_T = BIEF_MV16_THREADS;
 
-template <int TD, bool SYM, bool TRANS>
+template <int TD, bool SYM, bool TRANS, int FMT>
 __global__ void __launch_bounds__(MV16_T) k_matvec16(int npoin, int nelem, Mv16 M,
                                                   const double *__restrict__ xm,
                                                   const double *__restrict__ da,
@@ -133,18 +158,19 @@ __global__ void __launch_bounds__(MV16_T) k_matvec16(int npoin, int nelem, Mv16 
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += stride) {
     const int deg = __ldcs(M.deg + i);
-    const int b0 = __ldg(M.off + (i >> 5)) + (i & 31), eb = __ldg(M.eb + (i >> 5));
+    const int b0 = __ldg(M.off + (i >> 5)) + (i & 31);
+    const int eb = FMT == MV_LOCAL ? __ldg(M.eb + (i >> 5)) : 0;
     double acc = TD == DIA_Q ? mul(__ldg(y + i), __ldcs(da + i)) : diag_term<TD>(__ldg(y + i), da, i);
     int m = 0;
     for (; m + MV16_B <= deg; m += MV16_B)
-      mv16_batch<MV16_B, SYM, TRANS>(acc, i, eb, b0, m, M, xm, nelem, vec);
+      mv16_batch<MV16_B, SYM, TRANS, FMT>(acc, i, eb, b0, m, M, xm, nelem, vec);
     if constexpr (MV16_B / 2 > 1) {
       if (m + MV16_B / 2 <= deg) {
-        mv16_batch<MV16_B / 2, SYM, TRANS>(acc, i, eb, b0, m, M, xm, nelem, vec);
+        mv16_batch<MV16_B / 2, SYM, TRANS, FMT>(acc, i, eb, b0, m, M, xm, nelem, vec);
         m += MV16_B / 2;
       }
     }
-    for (; m < deg; ++m) mv16_batch<1, SYM, TRANS>(acc, i, eb, b0, m, M, xm, nelem, vec);
+    for (; m < deg; ++m) mv16_batch<1, SYM, TRANS, FMT>(acc, i, eb, b0, m, M, xm, nelem, vec);
     double r;  // OS combination of MESH%T into X (matvec.f:369-380, :329-340)
     switch (opc) {
       case OP_AY: r = acc; break;

@@ -48,21 +48,46 @@ def test_matvec_bitexact(oracle_mod, typdia, typext):
                                                          typext, v, x=v))
 
 
-@pytest.mark.parametrize("shuffle", [False, True])
-def test_matvec_bitexact_both_index_forms(oracle_mod, shuffle):
-    """MATVEC on a 201 x 201 mesh: with its row-wise numbering every gather
-    entry fits the compressed 16-bit records of the mesh, with a random
-    renumbering of its 40,401 nodes and elements none does and the product
-    reads IKLE; every operation is bit for bit the oracle's either way."""
-    rng = np.random.default_rng(8)
+def _fan_mesh(nfan=300):
+    """A disc of nfan triangles around node 0 inside a 41 x 41 grid's
+    numbering: node 0 is in more than 255 elements."""
+    x, y, ik = mg.square_mesh(41)
+    n = x.size
+    t = 2 * np.pi * np.arange(nfan) / nfan
+    xf = np.concatenate([x, [20.5], 20.5 + 3 * np.cos(t)])
+    yf = np.concatenate([y, [-5.0], -5.0 + 3 * np.sin(t)])
+    ring = n + 1 + np.arange(nfan)
+    fan = np.stack([np.full(nfan, n), ring, np.roll(ring, -1)], axis=1)
+    return xf, yf, np.concatenate([ik, fan]).astype(np.int32)
+
+
+def _mesh_for(form):
     x, y, ik = mg.square_mesh(201)
-    if shuffle:
+    if form == "band":      # row-wise nodes, elements in random order
+        ik = ik[np.random.default_rng(5).permutation(ik.shape[0])]
+    elif form == "any":     # nodes and elements in random order
         x, y, ik, _, _ = mg.shuffled(x, y, ik, seed=5)
+    elif form == "ikle":
+        x, y, ik = _fan_mesh()
+    return x, y, ik
+
+
+@pytest.mark.parametrize("form", ["local", "band", "any", "ikle"])
+def test_matvec_bitexact_every_record_format(oracle_mod, form):
+    """MATVEC reads the most compact gather records the numbering allows: a
+    201 x 201 mesh in row-wise numbering fits 16-bit element and vertex
+    offsets ('local'); with its elements in random order only the vertex
+    offsets fit ('band'); renumbered at random, neither ('any'); a node in
+    300 triangles leaves the product to read IKLE ('ikle').  Every operation
+    is bit for bit the oracle's in each."""
+    rng = np.random.default_rng(8)
+    x, y, ik = _mesh_for(form)
     n, ne = x.size, ik.shape[0]
     dm = rng.uniform(1, 2, n)
     for typext in ("S", "Q"):
         xm = rng.uniform(-1, 1, (6 if typext == "Q" else 3, ne))
         mesh = bief.Mesh(ik, n)
+        assert mesh.matvec_format() == form
         A = bief.Matrix(mesh, dm, xm, "Q", typext)
         v = rng.uniform(-1, 1, n)
         x0 = rng.uniform(-1, 1, n)
