@@ -268,6 +268,16 @@ def barrier(ws):
         dist.barrier()
 
 
+def solve_config(args, npoin, nelem, nseg, ws):
+    """`config` of the wave-equation SOLVE line, the same dict in both arms."""
+    return {"workload": f"wave-equation SOLVE (CG, diagonal precon, relres {args.eps:g}) on "
+                        f"the {args.n}x{args.n}-node P1 mesh",
+            "npoin": npoin, "nelem": nelem, "nseg": nseg,
+            "storage": "segments (STO=3)" if args.storage == "seg" else "EBE (STO=1)",
+            "depth": args.depth, "inner_tol": args.inner_tol, "parallelism": f"replicas x{ws}",
+            "l2": "1 GiB written then 256 MB read before every timed step"}
+
+
 def run_reference(args, ws, rank):
     """--impl reference: the reference algorithm's CPU implementation on the
     host cores (the Fortran cannot be compiled on these machines, so the
@@ -298,9 +308,10 @@ def run_reference(args, ws, rank):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": per_solve * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"wave-equation SOLVE (CG, diagonal precon, relres "
-                                   f"{args.eps:g}) on the {args.n}x{args.n}-node P1 mesh",
-                       "npoin": int(x.size), "nelem": int(ik.shape[0])},
+            "config": solve_config(args, int(x.size), int(ik.shape[0]),
+                                   int(x.size + ik.shape[0] - 1) if args.storage == "seg"
+                                   else None, ws),
+            "solver": "binary64 GRACJG, every step a whole solve from x = 0",
             "iterations": full["nit"], "relres": full["relres"],
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": nthreads, "kind": "port",
                              "sample": f"binary64 port of SOLVE/GRACJG on {nthreads} threads; "
@@ -991,13 +1002,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 inner / f64 refinement", "data": "synthetic",
-            "config": {"workload": f"wave-equation SOLVE (CG, diagonal precon, relres "
-                                   f"{args.eps:g}) on the {args.n}x{args.n}-node P1 mesh",
-                       "npoin": npoin, "nelem": nelem, "nseg": P["nseg"],
-                       "storage": "segments (STO=3)" if args.storage == "seg" else "EBE (STO=1)",
-                       "depth": args.depth,
-                       "inner_tol": args.inner_tol, "parallelism": f"replicas x{ws}",
-                       "l2": "1 GiB written then 256 MB read before every timed step"},
+            "config": solve_config(args, npoin, nelem, P["nseg"], ws),
             "time_to_solution_ms": {"mixed": step_ms, "fp64": f64_step_ms,
                                     "mixed_kernel": kern_ms, "fp64_kernel": f64_kern_ms},
             "speedup_mixed_vs_fp64": f64_step_ms / step_ms,
