@@ -78,8 +78,8 @@ def parse():
                     help="wave1m: skip the 2001x2001 log-uniform solves (config2) and the "
                          "256-mesh batch (batch256) reported beside the headline")
     ap.add_argument("--batch-shape", default=None,
-                    help="batch256: nodes per thread and threads per block as NPT,TPB "
-                         "(default: the autotuner's choice)")
+                    help="batch256: nodes per thread, threads per block and optionally "
+                         "blocks per SM as NPT,TPB[,BPS] (default: the autotuner's choice)")
     ap.add_argument("--max-inner", type=int, default=200,
                     help="mixedcap: inner iterations of each bounded mixed solve")
     ap.add_argument("--batch-max-inner", type=int, default=1000000,
@@ -361,9 +361,11 @@ def batch_measure(ws, rank, local, steps, warmup, inner_tol, eps, shape=None, ma
     b = bs.gather(bvs)
     x = torch.zeros_like(b)
     if shape:
-        npt, tpb = shape
+        npt, tpb = shape[:2]
+        if len(shape) > 2:
+            bs.mesh.set_blocks_per_sm(shape[2])
     else:
-        npt, tpb = bs.autotune(b, inner_tol=inner_tol, outer_tol=eps)
+        npt, tpb, _ = bs.autotune(b, inner_tol=inner_tol, outer_tol=eps)
     flush = torch.empty(1024 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     clean = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
     times, kern = [], []
@@ -399,7 +401,9 @@ def batch_measure(ws, rank, local, steps, warmup, inner_tol, eps, shape=None, ma
            "max_inner": max_inner,
            "nodes_this_rank": int(bs.total_nodes), "nodes_per_thread": int(npt),
            "threads_per_block": int(tpb),
-           "autotune_ms_per_iteration": {f"npt{k[0]}_t{k[1]}": round(v, 4)
+           "blocks_per_sm": int(bs.mesh.launch_info()[0]
+                                // torch.cuda.get_device_properties(local).multi_processor_count),
+           "autotune_ms_per_iteration": {f"npt{k[0]}_t{k[1]}_b{k[2]}": round(v, 4)
                                          for k, v in getattr(bs, "tune_table", {}).items()},
            "iterations_rank0": {"p50": float(np.percentile(inner, 50)),
                                 "p99": float(np.percentile(inner, 99)),
@@ -431,6 +435,7 @@ def run_batch(args, ws, rank, local):
                            "nodes_this_rank": m["nodes_this_rank"],
                            "nodes_per_thread": m["nodes_per_thread"],
                            "threads_per_block": m["threads_per_block"],
+                           "blocks_per_sm": m["blocks_per_sm"],
                            "autotune_ms_per_iteration": m["autotune_ms_per_iteration"],
                            "storage": "segments (STO=3)" if args.storage == "seg"
                                       else "EBE (STO=1)",

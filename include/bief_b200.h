@@ -270,6 +270,16 @@ int bief_selftest_timeout(int device, long long timeout_ns);
 /* Shape of the device dot-product tree: number of blocks and threads per
  * block of the persistent solver kernel. */
 int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads);
+/* Residency of the persistent solver kernels: 1 = one block per SM (every
+ * register to one 1024-thread block), 2 = two blocks per SM (half the
+ * registers each, twice the warps to hide memory latency: faster once a
+ * solve streams its operator from HBM, slower while it stays in L2),
+ * 0 = automatic, the choice bief_mesh_create makes: two when the binary32
+ * operator and vectors (about 80 B per node) exceed the L2 cache.  It sets
+ * the shape of the dot-product tree (bief_launch_info) and so the bits of
+ * the dot products; the batched solver takes it too (its dot order does not
+ * depend on it). */
+int bief_set_blocks_per_sm(bief_handle *h, int blocks_per_sm);
 /* Which gather records the standalone MATVEC (bief_matvec*) reads for this
  * mesh, fixed when the mesh is made: the most compact its numbering allows.
  * The bits of the product are the same in every format. */

@@ -31,8 +31,8 @@ EXPORTS = [
     "bief_solve_mixed", "bief_solve_mixed_dev", "bief_matvec", "bief_matvec_dev",
     "bief_matvec32_dev", "bief_assemble_wave_dev", "bief_assemble_mass_diff_dev",
     "bief_mass_diff_grad_dev", "bief_wave_coef_grad_dev", "bief_launch_info",
-    "bief_matvec_format", "bief_last_timing", "bief_kernel_launches", "bief_strerror",
-    "bief_solve_noalloc",
+    "bief_matvec_format", "bief_set_blocks_per_sm", "bief_last_timing",
+    "bief_kernel_launches", "bief_strerror", "bief_solve_noalloc",
     "bief_batch_solve_mixed_dev", "bief_set_segments", "bief_set_matrix_seg",
     "bief_set_matrix_seg_dev", "bief_ebe_to_seg", "bief_matrix_storage",
     "bief_selftest_timeout", "bief_diri01", "bief_diri01_dev",
@@ -88,6 +88,7 @@ def lib():
             "bief_wave_coef_grad_dev": ([vp, vp, vp, vp, vp, vp, vp], i),
             "bief_launch_info": ([vp, pi, pi], i),
             "bief_matvec_format": ([vp, pi], i),
+            "bief_set_blocks_per_sm": ([vp, i], i),
             "bief_last_timing": ([vp, ctypes.POINTER(ctypes.c_float),
                                   ctypes.POINTER(ctypes.c_float)], i),
             "bief_kernel_launches": ([vp], ctypes.c_longlong),

@@ -92,7 +92,8 @@ class BatchSolver:
         the autotuner."""
         import torch
         if nodes_per_thread is None:
-            nodes_per_thread, threads_per_block = self.autotune(b, precon, inner_tol, outer_tol)
+            nodes_per_thread, threads_per_block, _ = self.autotune(b, precon, inner_tol,
+                                                                   outer_tol)
         if threads_per_block is None:
             threads_per_block = 1024
         ni = self.ninst
@@ -116,25 +117,31 @@ class BatchSolver:
         return self.last
 
     def autotune(self, b, precon=2, inner_tol=1e-4, outer_tol=1e-8, candidates=(1, 2, 4, 8),
-                 block_shapes=(256, 512, 1024), probe_inner=30):
-        """Pick (nodes per thread, threads per block) by timing `probe_inner`
-        inner iterations of every instance with each pair (kernel time per
-        inner iteration of the longest-running instance).  The pair is kept
-        for later solves; self.tune_table holds every candidate's time."""
+                 block_shapes=(256, 512, 1024), residencies=(1, 2), probe_inner=30):
+        """Pick (nodes per thread, threads per block, blocks per SM) by timing
+        `probe_inner` inner iterations of every instance with each triple
+        (kernel time per inner iteration of the longest-running instance).
+        The triple is kept for later solves (the residency is set on the
+        mesh); self.tune_table holds every candidate's time.  The batched
+        dot order depends on none of the three but the nodes per thread and
+        threads per block."""
         import torch
         if self.tuned_npt is not None:
             return self.tuned_npt
         best, best_t = None, None
         self.tune_table = {}
-        for threads in block_shapes:
-            for npt in candidates:
-                x = torch.zeros_like(b)
-                r = self.solve_mixed(x, b, precon, inner_tol, outer_tol, 1000, probe_inner, npt,
-                                     threads)
-                per = r["kernel_ms"] / max(int(r["inner"].max()), 1)
-                self.tune_table[(npt, threads)] = per
-                if best_t is None or per < best_t:
-                    best, best_t = (npt, threads), per
+        for bps in residencies:
+            self.mesh.set_blocks_per_sm(bps)
+            for threads in block_shapes:
+                for npt in candidates:
+                    x = torch.zeros_like(b)
+                    r = self.solve_mixed(x, b, precon, inner_tol, outer_tol, 1000, probe_inner,
+                                         npt, threads)
+                    per = r["kernel_ms"] / max(int(r["inner"].max()), 1)
+                    self.tune_table[(npt, threads, bps)] = per
+                    if best_t is None or per < best_t:
+                        best, best_t = (npt, threads, bps), per
+        self.mesh.set_blocks_per_sm(best[2])
         self.tuned_npt = best
         return best
 

@@ -107,6 +107,12 @@ class Mesh:
         _native.lib().bief_launch_info(self._h, ctypes.byref(g), ctypes.byref(t))
         return g.value, t.value
 
+    def set_blocks_per_sm(self, n=0):
+        """Residency of the persistent solvers: 1 or 2 blocks per SM, 0 for
+        the automatic choice (2 when the binary32 working set exceeds L2).
+        Sets the dot-product tree's shape (launch_info)."""
+        _check(_native.lib().bief_set_blocks_per_sm(self._h, int(n)), "bief_set_blocks_per_sm")
+
     MATVEC_FORMATS = ("ikle", "local", "band", "any")
 
     def matvec_format(self):

@@ -39,6 +39,8 @@ struct bief_handle {
   // gather records of the standalone MATVEC (Mv16) in format mv16 (MV_*);
   // MV_NONE when a node has more than 255 entries (k_matvec then reads IKLE)
   int mv16 = 0;
+  // persistent solvers: twice the resident blocks per SM (bief_set_wide)
+  bool wide = false;
   unsigned char *d_mv_deg = nullptr;
   int *d_mv_eb = nullptr;
   void *d_mv_ek = nullptr;  // unsigned short (MV_LOCAL) or int
@@ -183,54 +185,53 @@ void dispatch_mv(bief_handle *h, int td, bool sym, bool tr, const double *xm, co
 #undef MV_CASE
 }
 
-template <bool COMP>
-void *cg_kernel_t(int td, int sto) {
-  if (sto == 3) {
-    if (td == DIA_Q) return (void *)k_cg64<DIA_Q, 3, COMP>;
-    if (td == DIA_I) return (void *)k_cg64<DIA_I, 3, COMP>;
-    return (void *)k_cg64<DIA_0, 3, COMP>;
-  }
-  if (td == DIA_Q) return (void *)k_cg64<DIA_Q, 1, COMP>;
-  if (td == DIA_I) return (void *)k_cg64<DIA_I, 1, COMP>;
-  return (void *)k_cg64<DIA_0, 1, COMP>;
+// Kernel of a method for TYPDIA code td, storage sto, dot-product mode
+// (comp: MODASS = 3, compensated) and residency (wide: twice the blocks per
+// SM, MINB = 2 CG_MIN_BLOCKS)
+#define KSEL1(k, STO_, C_, M_)                                                \
+  (td == DIA_Q ? (void *)k<DIA_Q, STO_, C_, M_>                                \
+               : td == DIA_I ? (void *)k<DIA_I, STO_, C_, M_> : (void *)k<DIA_0, STO_, C_, M_>)
+#define KSELM(k, M_)                                                          \
+  (sto == 3 ? (comp ? KSEL1(k, 3, true, M_) : KSEL1(k, 3, false, M_))         \
+            : (comp ? KSEL1(k, 1, true, M_) : KSEL1(k, 1, false, M_)))
+#define KSEL(k) (wide ? KSELM(k, 2 * CG_MIN_BLOCKS) : KSELM(k, CG_MIN_BLOCKS))
+
+void *cg_kernel(int td, int sto, bool comp = false, bool wide = false) { return KSEL(k_cg64); }
+
+void *equnor_kernel(int td, int sto, bool comp = false, bool wide = false) {
+  return KSEL(k_equnor);
 }
 
-// comp: MODASS = 3 (compensated dot products)
-void *cg_kernel(int td, int sto, bool comp = false) {
-  return comp ? cg_kernel_t<true>(td, sto) : cg_kernel_t<false>(td, sto);
+void *rescjg_kernel(int td, int sto, bool comp = false, bool wide = false) {
+  return KSEL(k_rescjg);
 }
 
-// Kernel of a method for TYPDIA code td, storage sto and dot-product mode
-// (comp: MODASS = 3, compensated)
-#define KSEL1(k, STO_, C_)                                                   \
-  (td == DIA_Q ? (void *)k<DIA_Q, STO_, C_>                                   \
-               : td == DIA_I ? (void *)k<DIA_I, STO_, C_> : (void *)k<DIA_0, STO_, C_>)
-#define KSEL(k)                                                               \
-  (sto == 3 ? (comp ? KSEL1(k, 3, true) : KSEL1(k, 3, false))                 \
-            : (comp ? KSEL1(k, 1, true) : KSEL1(k, 1, false)))
-
-void *equnor_kernel(int td, int sto, bool comp = false) { return KSEL(k_equnor); }
-
-void *rescjg_kernel(int td, int sto, bool comp = false) { return KSEL(k_rescjg); }
-
-void *errmin_kernel(int td, int sto, bool comp = false) { return KSEL(k_errmin); }
-
-void *cgsqua_kernel(int td, int sto, bool comp = false) { return KSEL(k_cgsqua); }
-
-void *gmres_kernel(int td, int sto, bool comp = false) { return KSEL(k_gmres); }
-
-void *cgstab_kernel(int td, int sto, bool comp = false) { return KSEL(k_cgstab); }
-
-void *mixed_kernel(int td, int sto) {
-  if (sto == 3) {
-    if (td == DIA_Q) return (void *)k_mixed<DIA_Q, 3>;
-    if (td == DIA_I) return (void *)k_mixed<DIA_I, 3>;
-    return (void *)k_mixed<DIA_0, 3>;
-  }
-  if (td == DIA_Q) return (void *)k_mixed<DIA_Q, 1>;
-  if (td == DIA_I) return (void *)k_mixed<DIA_I, 1>;
-  return (void *)k_mixed<DIA_0, 1>;
+void *errmin_kernel(int td, int sto, bool comp = false, bool wide = false) {
+  return KSEL(k_errmin);
 }
+
+void *cgsqua_kernel(int td, int sto, bool comp = false, bool wide = false) {
+  return KSEL(k_cgsqua);
+}
+
+void *gmres_kernel(int td, int sto, bool comp = false, bool wide = false) {
+  return KSEL(k_gmres);
+}
+
+void *cgstab_kernel(int td, int sto, bool comp = false, bool wide = false) {
+  return KSEL(k_cgstab);
+}
+
+#define MSEL1(k, STO_, M_)                                                    \
+  (td == DIA_Q ? (void *)k<DIA_Q, STO_, M_>                                    \
+               : td == DIA_I ? (void *)k<DIA_I, STO_, M_> : (void *)k<DIA_0, STO_, M_>)
+#define MSEL(k)                                                               \
+  (wide ? (sto == 3 ? MSEL1(k, 3, 2 * CG_MIN_BLOCKS) : MSEL1(k, 1, 2 * CG_MIN_BLOCKS)) \
+        : (sto == 3 ? MSEL1(k, 3, CG_MIN_BLOCKS) : MSEL1(k, 1, CG_MIN_BLOCKS)))
+
+void *mixed_kernel(int td, int sto, bool wide = false) { return MSEL(k_mixed); }
+
+void *batch_kernel(int td, int sto, bool wide = false) { return MSEL(k_batch); }
 
 template <int TD, bool SYM, bool TR>
 void launch_mvseg(bief_handle *h, bool ext, const double *xa, const double *da, const double *y,
@@ -254,44 +255,22 @@ void dispatch_mvseg(bief_handle *h, int td, bool sym, bool tr, bool ext, const d
 
 // Largest grid of the persistent kernels that is guaranteed co-resident,
 // reduced for small meshes so that each thread has at least two nodes.
-int persistent_grid(int npoin, int nsm, int *out) {
+// Cooperative grid of the persistent solvers: the blocks per SM that every
+// persistent kernel of this residency can hold at once, times the SMs, but
+// no more blocks than rows of two block-widths.
+int persistent_grid(int npoin, int nsm, bool wide, int *out) {
   int best = 1 << 30;
-  void *ks[] = {cg_kernel(DIA_Q, 1), cg_kernel(DIA_I, 1), cg_kernel(DIA_0, 1),
-                mixed_kernel(DIA_Q, 1), mixed_kernel(DIA_I, 1), mixed_kernel(DIA_0, 1),
-                cg_kernel(DIA_Q, 3), cg_kernel(DIA_I, 3), cg_kernel(DIA_0, 3),
-                mixed_kernel(DIA_Q, 3), mixed_kernel(DIA_I, 3), mixed_kernel(DIA_0, 3),
-                equnor_kernel(DIA_Q, 1), equnor_kernel(DIA_I, 1), equnor_kernel(DIA_0, 1),
-                equnor_kernel(DIA_Q, 3), equnor_kernel(DIA_I, 3), equnor_kernel(DIA_0, 3),
-                gmres_kernel(DIA_Q, 1), gmres_kernel(DIA_I, 1), gmres_kernel(DIA_0, 1),
-                gmres_kernel(DIA_Q, 3), gmres_kernel(DIA_I, 3), gmres_kernel(DIA_0, 3),
-                cgstab_kernel(DIA_Q, 1), cgstab_kernel(DIA_I, 1), cgstab_kernel(DIA_0, 1),
-                cgstab_kernel(DIA_Q, 3), cgstab_kernel(DIA_I, 3), cgstab_kernel(DIA_0, 3),
-                rescjg_kernel(DIA_Q, 1), rescjg_kernel(DIA_I, 1), rescjg_kernel(DIA_0, 1),
-                rescjg_kernel(DIA_Q, 3), rescjg_kernel(DIA_I, 3), rescjg_kernel(DIA_0, 3),
-                errmin_kernel(DIA_Q, 1), errmin_kernel(DIA_I, 1), errmin_kernel(DIA_0, 1),
-                errmin_kernel(DIA_Q, 3), errmin_kernel(DIA_I, 3), errmin_kernel(DIA_0, 3),
-                cgsqua_kernel(DIA_Q, 1), cgsqua_kernel(DIA_I, 1), cgsqua_kernel(DIA_0, 1),
-                cgsqua_kernel(DIA_Q, 3), cgsqua_kernel(DIA_I, 3), cgsqua_kernel(DIA_0, 3),
-                cg_kernel(DIA_Q, 1, true), cg_kernel(DIA_I, 1, true), cg_kernel(DIA_0, 1, true),
-                cg_kernel(DIA_Q, 3, true), cg_kernel(DIA_I, 3, true), cg_kernel(DIA_0, 3, true),
-                equnor_kernel(DIA_Q, 1, true), equnor_kernel(DIA_Q, 3, true),
-                rescjg_kernel(DIA_Q, 1, true), rescjg_kernel(DIA_Q, 3, true),
-                errmin_kernel(DIA_Q, 1, true), errmin_kernel(DIA_Q, 3, true),
-                cgsqua_kernel(DIA_Q, 1, true), cgsqua_kernel(DIA_Q, 3, true),
-                cgstab_kernel(DIA_Q, 1, true), cgstab_kernel(DIA_Q, 3, true),
-                equnor_kernel(DIA_I, 1, true), equnor_kernel(DIA_I, 3, true),
-                rescjg_kernel(DIA_I, 1, true), rescjg_kernel(DIA_I, 3, true),
-                errmin_kernel(DIA_I, 1, true), errmin_kernel(DIA_I, 3, true),
-                cgsqua_kernel(DIA_I, 1, true), cgsqua_kernel(DIA_I, 3, true),
-                cgstab_kernel(DIA_I, 1, true), cgstab_kernel(DIA_I, 3, true),
-                equnor_kernel(DIA_0, 1, true), equnor_kernel(DIA_0, 3, true),
-                rescjg_kernel(DIA_0, 1, true), rescjg_kernel(DIA_0, 3, true),
-                errmin_kernel(DIA_0, 1, true), errmin_kernel(DIA_0, 3, true),
-                cgsqua_kernel(DIA_0, 1, true), cgsqua_kernel(DIA_0, 3, true),
-                cgstab_kernel(DIA_0, 1, true), cgstab_kernel(DIA_0, 3, true),
-                gmres_kernel(DIA_Q, 1, true), gmres_kernel(DIA_Q, 3, true),
-                gmres_kernel(DIA_I, 1, true), gmres_kernel(DIA_I, 3, true),
-                gmres_kernel(DIA_0, 1, true), gmres_kernel(DIA_0, 3, true)};
+  std::vector<void *> ks;
+  for (int td : {DIA_Q, DIA_I, DIA_0})
+    for (int sto : {1, 3}) {
+      ks.push_back(mixed_kernel(td, sto, wide));
+      for (bool comp : {false, true})
+        for (void *k : {cg_kernel(td, sto, comp, wide), equnor_kernel(td, sto, comp, wide),
+                        rescjg_kernel(td, sto, comp, wide), errmin_kernel(td, sto, comp, wide),
+                        cgsqua_kernel(td, sto, comp, wide), gmres_kernel(td, sto, comp, wide),
+                        cgstab_kernel(td, sto, comp, wide)})
+          ks.push_back(k);
+    }
   for (void *k : ks) {
     int bps = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, CG_THREADS, 0));
@@ -698,7 +677,10 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
         return fail(cuda_fail(e, "mesh upload", __LINE__));
       h->mv16 = mvf;
     }
-    if ((st = persistent_grid(npoin, h->nsm, &h->G))) return fail(st);
+    // twice the resident blocks when the binary32 operator and vectors
+    // (about 80 B per node) cannot stay in L2
+    h->wide = (size_t)npoin * 80 > (size_t)h->l2_bytes;
+    if ((st = persistent_grid(npoin, h->nsm, h->wide, &h->G))) return fail(st);
     if ((st = dalloc(&h->d_part, 8 * (size_t)h->G + 4))) return fail(st);
     if ((e = cudaMallocHost((void **)&h->h_ctl, sizeof(Ctl))) != cudaSuccess)
       return fail(cuda_fail(e, "cudaMallocHost", __LINE__));
@@ -897,7 +879,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    if ((st = launch_coop(h, cgstab_kernel(td, h->sto, comp), &P, s))) return st;
+    if ((st = launch_coop(h, cgstab_kernel(td, h->sto, comp, h->wide), &P, s))) return st;
   } else if (cfg->slv == 7) {  // GMRES
     if (!h->d_gpart && (st = dalloc(&h->d_gpart, 4 * (size_t)h->G * (GM_MAXK + 1) + 4)))
       return st;
@@ -919,7 +901,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    if ((st = launch_coop(h, gmres_kernel(td, h->sto, comp), &P, s))) return st;
+    if ((st = launch_coop(h, gmres_kernel(td, h->sto, comp, h->wide), &P, s))) return st;
   } else if (cfg->slv == 5) {  // CGSQUA
     SquaP P;
     P.npoin = h->npoin;
@@ -940,7 +922,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    if ((st = launch_coop(h, cgsqua_kernel(td, h->sto, comp), &P, s))) return st;
+    if ((st = launch_coop(h, cgsqua_kernel(td, h->sto, comp, h->wide), &P, s))) return st;
   } else if (cfg->slv == 2 || cfg->slv == 4) {  // RESCJG, ERRMIN
     Kry2P P;
     P.npoin = h->npoin;
@@ -962,7 +944,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    void *k = cfg->slv == 2 ? rescjg_kernel(td, h->sto, comp) : errmin_kernel(td, h->sto, comp);
+    void *k = cfg->slv == 2 ? rescjg_kernel(td, h->sto, comp, h->wide) : errmin_kernel(td, h->sto, comp, h->wide);
     if ((st = launch_coop(h, k, &P, s))) return st;
   } else if (cfg->slv == 3) {  // EQUNOR
     EqP P;
@@ -984,7 +966,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    if ((st = launch_coop(h, equnor_kernel(td, h->sto, comp), &P, s))) return st;
+    if ((st = launch_coop(h, equnor_kernel(td, h->sto, comp, h->wide), &P, s))) return st;
   } else {
     CgP P;
     P.npoin = h->npoin;
@@ -1003,7 +985,7 @@ int bief_solve_dev(bief_handle *h, double *x, double *b, bief_slvcfg *cfg, int f
     P.ctl = h->d_ctl;
     P.timeout_ns = h->timeout_ns;
     CK(cudaEventRecord(h->ev[0], s));
-    if ((st = launch_coop(h, cg_kernel(td, h->sto, comp), &P, s))) return st;
+    if ((st = launch_coop(h, cg_kernel(td, h->sto, comp, h->wide), &P, s))) return st;
   }
   CK(cudaEventRecord(h->ev[1], s));
   CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
@@ -1136,7 +1118,7 @@ int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b, int precon,
   P.timeout_ns = h->timeout_ns;
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
   CK(cudaEventRecord(h->ev[0], s));
-  if ((st = launch_coop(h, mixed_kernel(td, h->sto), &P, s))) return st;
+  if ((st = launch_coop(h, mixed_kernel(td, h->sto, h->wide), &P, s))) return st;
   CK(cudaEventRecord(h->ev[1], s));
   CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -1477,12 +1459,7 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
     h->s32_gen = -1;
     CK(cudaGetLastError());
   }
-  void *k = seg ? (td == DIA_Q   ? (void *)k_batch<DIA_Q, 3>
-                   : td == DIA_I ? (void *)k_batch<DIA_I, 3>
-                                 : (void *)k_batch<DIA_0, 3>)
-                : (td == DIA_Q   ? (void *)k_batch<DIA_Q, 1>
-                   : td == DIA_I ? (void *)k_batch<DIA_I, 1>
-                                 : (void *)k_batch<DIA_0, 1>);
+  void *k = batch_kernel(td, seg ? 3 : 1, h->wide);
   int bps = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads_per_block, 0));
   if (bps < 1) return BIEF_ERR_CUDA;
@@ -1649,6 +1626,26 @@ int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads) {
   if (!h) return BIEF_ERR_ARGS;
   if (nblocks) *nblocks = h->G;
   if (nthreads) *nthreads = h->T;
+  return BIEF_OK;
+}
+
+int bief_set_blocks_per_sm(bief_handle *h, int blocks_per_sm) {
+  if (!h || blocks_per_sm < 0 || blocks_per_sm > 2) return BIEF_ERR_ARGS;
+  DevGuard g(h->dev);
+  const bool wide = blocks_per_sm == 0 ? (size_t)h->npoin * 80 > (size_t)h->l2_bytes
+                                       : blocks_per_sm == 2;
+  int G = 0, st;
+  if ((st = persistent_grid(h->npoin, h->nsm, wide, &G))) return st;
+  if (G != h->G) {
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaFree(h->d_part));
+    h->d_part = nullptr;
+    if (h->d_gpart) CK(cudaFree(h->d_gpart));  // sized by G at its first use
+    h->d_gpart = nullptr;
+    if ((st = dalloc(&h->d_part, 8 * (size_t)G + 4))) return st;
+    h->G = G;
+  }
+  h->wide = wide;
   return BIEF_OK;
 }
 

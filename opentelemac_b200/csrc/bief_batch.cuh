@@ -63,8 +63,8 @@ __device__ __forceinline__ double op_row(int i, double acc, const Sell &S, V vec
   return acc;
 }
 
-template <int TD, int STO>
-__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_batch(BatchP P) {
+template <int TD, int STO, int MINB = CG_MIN_BLOCKS>
+__global__ void __launch_bounds__(CG_THREADS, MINB) k_batch(BatchP P) {
   __shared__ BatchState B;
   const int T = blockDim.x, t = threadIdx.x, G = gridDim.x;
   const int warp = t >> 5, lane = t & 31, nwarps = T >> 5;

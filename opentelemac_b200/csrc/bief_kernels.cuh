@@ -20,6 +20,11 @@ namespace bief {
 
 // Shape of the persistent solver kernels: threads per block (one or more
 // blocks per SM) and rows interleaved per thread in the gather phases.
+// Every persistent kernel is also built for twice as many resident blocks
+// per SM (MINB = 2 CG_MIN_BLOCKS: half the registers per thread, some of
+// its state spilled to L1): twice the warps to hide memory latency when a
+// solve streams its operator from HBM, at the price of the spills and of
+// twice the blocks in every grid reduction.
 #ifndef BIEF_CG_THREADS
 #define BIEF_CG_THREADS 1024
 #endif
@@ -522,8 +527,8 @@ struct CgP {
 // the device order (grid_reduce_comp); the vector operations are unchanged
 // (their compensated forms in the reference only fill error vectors that
 // GRACJG does not read).
-template <int TD, int STO, bool COMP>
-__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cg64(CgP P) {
+template <int TD, int STO, bool COMP, int MINB = CG_MIN_BLOCKS>
+__global__ void __launch_bounds__(CG_THREADS, MINB) k_cg64(CgP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -696,8 +701,8 @@ struct EqP {
   long long timeout_ns;
 };
 
-template <int TD, int STO, bool COMP>
-__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_equnor(EqP P) {
+template <int TD, int STO, bool COMP, int MINB = CG_MIN_BLOCKS>
+__global__ void __launch_bounds__(CG_THREADS, MINB) k_equnor(EqP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -841,8 +846,8 @@ struct Kry2P {
   long long timeout_ns;
 };
 
-template <int TD, int STO, bool COMP>
-__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_rescjg(Kry2P P) {
+template <int TD, int STO, bool COMP, int MINB = CG_MIN_BLOCKS>
+__global__ void __launch_bounds__(CG_THREADS, MINB) k_rescjg(Kry2P P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -943,8 +948,8 @@ __global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_rescjg(Kry2P P) {
   }
 }
 
-template <int TD, int STO, bool COMP>
-__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_errmin(Kry2P P) {
+template <int TD, int STO, bool COMP, int MINB = CG_MIN_BLOCKS>
+__global__ void __launch_bounds__(CG_THREADS, MINB) k_errmin(Kry2P P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -1078,8 +1083,8 @@ struct SquaP {
   long long timeout_ns;
 };
 
-template <int TD, int STO, bool COMP>
-__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgsqua(SquaP P) {
+template <int TD, int STO, bool COMP, int MINB = CG_MIN_BLOCKS>
+__global__ void __launch_bounds__(CG_THREADS, MINB) k_cgsqua(SquaP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -1193,8 +1198,8 @@ struct StabP {
   long long timeout_ns;
 };
 
-template <int TD, int STO, bool COMP>
-__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_cgstab(StabP P) {
+template <int TD, int STO, bool COMP, int MINB = CG_MIN_BLOCKS>
+__global__ void __launch_bounds__(CG_THREADS, MINB) k_cgstab(StabP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -1424,8 +1429,8 @@ static __device__ __noinline__ bool grid_reduce_n_comp(Ctl *ctl, double *part,
   return true;
 }
 
-template <int TD, int STO, bool COMP>
-__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_gmres(GmP P) {
+template <int TD, int STO, bool COMP, int MINB = CG_MIN_BLOCKS>
+__global__ void __launch_bounds__(CG_THREADS, MINB) k_gmres(GmP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);
@@ -1653,8 +1658,8 @@ struct MixP {
   long long timeout_ns;
 };
 
-template <int TD, int STO>
-__global__ void __launch_bounds__(CG_THREADS, CG_MIN_BLOCKS) k_mixed(MixP P) {
+template <int TD, int STO, int MINB = CG_MIN_BLOCKS>
+__global__ void __launch_bounds__(CG_THREADS, MINB) k_mixed(MixP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
   const int hi = (int)blk_lo(blockIdx.x + 1, P.npoin, gridDim.x);

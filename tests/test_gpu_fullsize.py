@@ -5,7 +5,8 @@
   relres 1e-8 (1,927 iterations) and the mixed-precision solve (refinement
   threshold 0.1, the headline workload): every bit of the solution, the
   iteration counts and the residual, against the restatement run in the
-  device's dot order.
+  device's dot order -- with one block per SM (148 blocks) and with two
+  (296 blocks, the kernels built for half the registers).
 - The 256-mesh batch (node counts log-uniform in [2,000, 200,000], one
   persistent launch): the smallest, the median and the largest instance
   against the restatement of the batched algorithm in the batched dot order.
@@ -31,10 +32,11 @@ def wave1m(oracle_mod):
     return dict(x=x, y=y, ik=ik, coef=coef, dm=dm, xm=xm, xt=xt, b=b)
 
 
-def _device(p):
+def _device(p, bps=0):
     import torch
     t = lambda a: torch.tensor(a, device="cuda", dtype=torch.float64)
     mesh = bief.Mesh(p["ik"], p["x"].size)
+    mesh.set_blocks_per_sm(bps)
     A = bief.Matrix(mesh)
     A.assemble_wave(t(p["x"]), t(p["y"]), t(p["coef"]))
     return mesh, A, t
@@ -52,9 +54,10 @@ def test_1m_assembly_and_matvec_bitexact(wave1m):
     mesh.close()
 
 
-def test_1m_fp64_gracjg_bitexact(oracle_mod, wave1m):
+@pytest.mark.parametrize("bps", [1, 2])
+def test_1m_fp64_gracjg_bitexact(oracle_mod, wave1m, bps):
     import torch
-    mesh, A, t = _device(wave1m)
+    mesh, A, t = _device(wave1m, bps)
     x = torch.zeros(wave1m["x"].size, dtype=torch.float64, device="cuda")
     cfg = bief.SlvCfg(slv=1, nitmax=1000000, precon=2, krylov=0, eps=1e-8, zero=0.0)
     st, nit, relres = bief.solve(x, A, t(wave1m["b"]), cfg)
@@ -69,9 +72,10 @@ def test_1m_fp64_gracjg_bitexact(oracle_mod, wave1m):
     mesh.close()
 
 
-def test_1m_mixed_bitexact(oracle_mod, wave1m):
+@pytest.mark.parametrize("bps", [1, 2])
+def test_1m_mixed_bitexact(oracle_mod, wave1m, bps):
     import torch
-    mesh, A, t = _device(wave1m)
+    mesh, A, t = _device(wave1m, bps)
     x = torch.zeros(wave1m["x"].size, dtype=torch.float64, device="cuda")
     st, outer, inner, relres = bief.solve_mixed(x, A, t(wave1m["b"]), precon=2, inner_tol=0.1,
                                                 outer_tol=1e-8)
