@@ -22,12 +22,16 @@ def _instances(sizes, seed0=100):
     return out
 
 
+@pytest.mark.parametrize("bps", [1, 2])
 @pytest.mark.parametrize("npt,threads", [(1, 1024), (2, 1024), (4, 256), (2, 512)])
-def test_batch_bitexact_per_instance(oracle_mod, npt, threads):
+def test_batch_bitexact_per_instance(oracle_mod, npt, threads, bps):
+    """Each tile shape with the kernel built for one and for two blocks per
+    SM (the batched dot order depends on the tile shape only)."""
     from opentelemac_b200.batch import BatchSolver
     inst = _instances([7, 15, 23, 40, 57, 33])
     inst[3]["b"] = np.zeros_like(inst[3]["b"])               # b = 0: x = 0 at once
     bs = BatchSolver([(p["x"].size, p["ik"]) for p in inst])
+    bs.mesh.set_blocks_per_sm(bps)
     bs.assemble_wave([p["x"] for p in inst], [p["y"] for p in inst], [p["coef"] for p in inst])
     b = bs.gather([p["b"] for p in inst])
     x = bs.gather([np.zeros(p["x"].size) for p in inst])
@@ -46,8 +50,9 @@ def test_batch_bitexact_per_instance(oracle_mod, npt, threads):
     bs.close()
 
 
+@pytest.mark.parametrize("bps", [1, 2])
 @pytest.mark.parametrize("npt,threads", [(1, 1024), (4, 256)])
-def test_batch_segments_bitexact_per_instance(oracle_mod, npt, threads):
+def test_batch_segments_bitexact_per_instance(oracle_mod, npt, threads, bps):
     """Segment storage (MATRIX STORAGE 3, TELEMAC-2D's default): every
     instance's own STOSEG numbering, the EBE matrix converted by ASSEX3 on the
     device, each instance bit for bit the oracle's batched segment solve."""
@@ -55,6 +60,7 @@ def test_batch_segments_bitexact_per_instance(oracle_mod, npt, threads):
     inst = _instances([9, 17, 31, 26, 44])
     inst[2]["b"] = np.zeros_like(inst[2]["b"])
     bs = BatchSolver([(p["x"].size, p["ik"]) for p in inst])
+    bs.mesh.set_blocks_per_sm(bps)
     bs.assemble_wave([p["x"] for p in inst], [p["y"] for p in inst], [p["coef"] for p in inst])
     segs = [mg.segments(p["ik"], p["x"].size) for p in inst]
     bs.set_segments([(g[0], g[1]) for g in segs]).to_segments()

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import small_problem
-from opentelemac_b200 import bief
+from opentelemac_b200 import bief, meshgen as mg
 
 pytestmark = pytest.mark.gpu
 
@@ -56,6 +56,38 @@ def test_mixed_both_residencies(oracle_mod, prob, bps):
     r = oracle_mod.solve_mixed(p["ik"], p["dm"], "Q", p["xm"], p["b"], precon=2, inner_tol=1e-2,
                                outer_tol=1e-10, max_outer=1000, max_inner=1000000, nblocks=G,
                                nthreads=T)
+    assert st == r["status"] == 0 and (outer, inner) == (r["outer"], r["inner"])
+    assert relres == r["relres"]
+    np.testing.assert_array_equal(x, r["x"])
+    mesh.close()
+
+
+@pytest.mark.parametrize("bps", [1, 2])
+def test_segment_storage_both_residencies(oracle_mod, prob, bps):
+    """Segment storage (STOSEG numbering, the EBE matrix converted by ASSEX3
+    on the device): CG and the mixed solve in each residency."""
+    p = prob
+    n = p["x"].size
+    g1, g2, es, ori = mg.segments(p["ik"], n)
+    xa = oracle_mod.assex3(es, ori, "S", p["xm"], g1.size)
+    mesh = bief.Mesh(p["ik"], n)
+    mesh.set_blocks_per_sm(bps)
+    mesh.set_segments(g1, g2)
+    A = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
+    A.to_segments()
+    G, T = mesh.launch_info()
+    x = np.zeros(n)
+    cfg = bief.SlvCfg(slv=1, nitmax=3000, precon=2, krylov=0, eps=1e-10, zero=0.0)
+    st, nit, relres = bief.solve(x, A, p["b"].copy(), cfg)
+    r = oracle_mod.solve_seg(g1, g2, p["dm"], "Q", xa, "S", p["b"], eps=1e-10, nitmax=3000,
+                             dot_mode=oracle_mod.DOT_BLOCKED, nblocks=G, nthreads=T)
+    assert st == r["status"] == 0 and nit == r["nit"] and relres == r["relres"]
+    np.testing.assert_array_equal(x, r["x"])
+    x = np.zeros(n)
+    st, outer, inner, relres = bief.solve_mixed(x, A, p["b"], precon=2, inner_tol=1e-2,
+                                                outer_tol=1e-10)
+    r = oracle_mod.solve_mixed_seg(g1, g2, p["dm"], "Q", xa, p["b"], precon=2, inner_tol=1e-2,
+                                   outer_tol=1e-10, nblocks=G, nthreads=T)
     assert st == r["status"] == 0 and (outer, inner) == (r["outer"], r["inner"])
     assert relres == r["relres"]
     np.testing.assert_array_equal(x, r["x"])
