@@ -49,8 +49,9 @@ def test_matvec_bitexact(oracle_mod, typdia, typext):
 
 
 def _fan_mesh(nfan=300):
-    """A disc of nfan triangles around node 0 inside a 41 x 41 grid's
-    numbering: node 0 is in more than 255 elements."""
+    """A 41 x 41 grid plus a disc of nfan triangles around one more node
+    (numbered after the grid, its ring after it): that centre node is in
+    nfan elements."""
     x, y, ik = mg.square_mesh(41)
     n = x.size
     t = 2 * np.pi * np.arange(nfan) / nfan
@@ -62,6 +63,8 @@ def _fan_mesh(nfan=300):
 
 
 def _mesh_for(form):
+    if form.startswith("fan"):
+        return _fan_mesh(int(form[3:]))
     x, y, ik = mg.square_mesh(201)
     if form == "band":      # row-wise nodes, elements in random order
         ik = ik[np.random.default_rng(5).permutation(ik.shape[0])]
@@ -72,14 +75,17 @@ def _mesh_for(form):
     return x, y, ik
 
 
-@pytest.mark.parametrize("form", ["local", "band", "any", "ikle"])
-def test_matvec_bitexact_every_record_format(oracle_mod, form):
+@pytest.mark.parametrize("form,expect", [("local", "local"), ("band", "band"), ("any", "any"),
+                                         ("ikle", "ikle"), ("fan255", "local"),
+                                         ("fan256", "ikle")])
+def test_matvec_bitexact_every_record_format(oracle_mod, form, expect):
     """MATVEC reads the most compact gather records the numbering allows: a
     201 x 201 mesh in row-wise numbering fits 16-bit element and vertex
     offsets ('local'); with its elements in random order only the vertex
     offsets fit ('band'); renumbered at random, neither ('any'); a node in
-    300 triangles leaves the product to read IKLE ('ikle').  Every operation
-    is bit for bit the oracle's in each."""
+    300 triangles leaves the product to read IKLE ('ikle'); the limit is
+    255 entries per node (a fan of 255 triangles keeps the 6-byte records,
+    256 does not).  Every operation is bit for bit the oracle's in each."""
     rng = np.random.default_rng(8)
     x, y, ik = _mesh_for(form)
     n, ne = x.size, ik.shape[0]
@@ -87,7 +93,7 @@ def test_matvec_bitexact_every_record_format(oracle_mod, form):
     for typext in ("S", "Q"):
         xm = rng.uniform(-1, 1, (6 if typext == "Q" else 3, ne))
         mesh = bief.Mesh(ik, n)
-        assert mesh.matvec_format() == form
+        assert mesh.matvec_format() == expect
         A = bief.Matrix(mesh, dm, xm, "Q", typext)
         v = rng.uniform(-1, 1, n)
         x0 = rng.uniform(-1, 1, n)
