@@ -446,6 +446,15 @@ def run_batch(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def _grid_info(mesh, device):
+    """Blocks and threads of the persistent solvers on this mesh (the
+    dot-product tree) and the resident blocks per SM they were built for."""
+    import torch
+    G, T = mesh.launch_info()
+    nsm = torch.cuda.get_device_properties(device).multi_processor_count
+    return {"blocks": G, "threads": T, "blocks_per_sm": max(1, G // nsm)}
+
+
 def config2_measure(P2, ws, flush_l2, hbm, steps=2, warmup=1):
     """The 2001 x 2001-node mesh with the log-uniform depth (4,004,001
     nodes, 8,000,000 triangles), relres 1e-10: binary64 GRACJG, the mixed
@@ -488,6 +497,7 @@ def config2_measure(P2, ws, flush_l2, hbm, steps=2, warmup=1):
     out = {"workload": "2001x2001-node P1 mesh, log-uniform depth in [0.5, 500] m (3 "
                        "smoothing passes), relres 1e-10",
            "npoin": P2["npoin"], "nelem": P2["nelem"],
+           "persistent_grid": _grid_info(mesh, b.device),
            "fp64": {"ms": f64_ms, "kernel_ms": f64_kern, "iterations": f64_res[1],
                     "relres": f64_res[2], "kernel": "k_cg64",
                     "gbs": f64_bytes / (f64_kern * 1e-3) / 1e9,
@@ -1008,6 +1018,7 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 inner / f64 refinement", "data": "synthetic",
             "config": solve_config(args, npoin, nelem, P["nseg"], ws),
+            "persistent_grid": _grid_info(P["mesh"], local),
             "time_to_solution_ms": {"mixed": step_ms, "fp64": f64_step_ms,
                                     "mixed_kernel": kern_ms, "fp64_kernel": f64_kern_ms},
             "speedup_mixed_vs_fp64": f64_step_ms / step_ms,
