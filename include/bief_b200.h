@@ -275,7 +275,8 @@ int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads);
  * registers each, twice the warps to hide memory latency: faster once a
  * solve streams its operator from HBM, slower while it stays in L2),
  * 0 = automatic, the choice bief_mesh_create makes: two when the binary32
- * operator and vectors (about 80 B per node) exceed the L2 cache.  It sets
+ * operator and vectors (about 80 B per node) exceed 2.25 times the L2 cache
+ * (about 3.5M nodes on a B200, where the two measure the same).  It sets
  * the shape of the dot-product tree (bief_launch_info) and so the bits of
  * the dot products; the batched solver takes it too (its dot order does not
  * depend on it). */

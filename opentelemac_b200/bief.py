@@ -109,7 +109,8 @@ class Mesh:
 
     def set_blocks_per_sm(self, n=0):
         """Residency of the persistent solvers: 1 or 2 blocks per SM, 0 for
-        the automatic choice (2 when the binary32 working set exceeds L2).
+        the automatic choice (2 when the binary32 working set, about 80 B per
+        node, exceeds 2.25 times the L2: about 3.5M nodes on a B200).
         Sets the dot-product tree's shape (launch_info)."""
         _check(_native.lib().bief_set_blocks_per_sm(self._h, int(n)), "bief_set_blocks_per_sm")
 

@@ -255,6 +255,17 @@ void dispatch_mvseg(bief_handle *h, int td, bool sym, bool tr, bool ext, const d
 
 // Largest grid of the persistent kernels that is guaranteed co-resident,
 // reduced for small meshes so that each thread has at least two nodes.
+// Automatic residency: two blocks per SM once the binary32 operator and
+// vectors (about 80 B per node) exceed 2.25 times the L2.  Measured on the
+// B200 (126 MB L2), 400 capped iterations on smooth meshes, one against two
+// blocks per SM: binary64 / mixed 33.1 / 14.7 against 36.7 / 16.3 ms at
+// 2.0M nodes, 53.9 / 24.9 against 54.0 / 25.3 at 3.0M, 63.6 / 30.4 against
+// 62.7 / 30.5 at 3.5M, 71.8 / 37.6 against 71.8 / 35.2 at 4.0M and 93.1 /
+// 52.5 against 91.2 / 46.0 at 5.3M.
+static bool wide_by_size(int npoin, int l2_bytes) {
+  return (double)npoin * 80.0 > 2.25 * (double)l2_bytes;
+}
+
 // Cooperative grid of the persistent solvers: the blocks per SM that every
 // persistent kernel of this residency can hold at once, times the SMs, but
 // no more blocks than rows of two block-widths.
@@ -677,9 +688,7 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
         return fail(cuda_fail(e, "mesh upload", __LINE__));
       h->mv16 = mvf;
     }
-    // twice the resident blocks when the binary32 operator and vectors
-    // (about 80 B per node) cannot stay in L2
-    h->wide = (size_t)npoin * 80 > (size_t)h->l2_bytes;
+    h->wide = wide_by_size(npoin, h->l2_bytes);
     if ((st = persistent_grid(npoin, h->nsm, h->wide, &h->G))) return fail(st);
     if ((st = dalloc(&h->d_part, 8 * (size_t)h->G + 4))) return fail(st);
     if ((e = cudaMallocHost((void **)&h->h_ctl, sizeof(Ctl))) != cudaSuccess)
@@ -1632,7 +1641,7 @@ int bief_launch_info(bief_handle *h, int *nblocks, int *nthreads) {
 int bief_set_blocks_per_sm(bief_handle *h, int blocks_per_sm) {
   if (!h || blocks_per_sm < 0 || blocks_per_sm > 2) return BIEF_ERR_ARGS;
   DevGuard g(h->dev);
-  const bool wide = blocks_per_sm == 0 ? (size_t)h->npoin * 80 > (size_t)h->l2_bytes
+  const bool wide = blocks_per_sm == 0 ? wide_by_size(h->npoin, h->l2_bytes)
                                        : blocks_per_sm == 2;
   int G = 0, st;
   if ((st = persistent_grid(h->npoin, h->nsm, wide, &G))) return st;
