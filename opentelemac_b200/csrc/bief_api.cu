@@ -34,6 +34,10 @@ struct bief_handle {
   double *d_dms = nullptr, *d_xms = nullptr, *d_dsc = nullptr;
   // gather-ready layouts (32-node slices): records and binary32 segments
   int *d_meta = nullptr, *d_rec_off = nullptr, *d_seg_off = nullptr, *d_seg_col = nullptr;
+  // binary32 slots' neighbours as 16-bit offsets from the node, when every
+  // one fits (seg16); the binary32 kernels then read them instead of d_seg_col
+  short *d_seg_dc = nullptr;
+  bool seg16 = false;
   int2 *d_rec_idx = nullptr;
   uchar2 *d_rec_slot = nullptr;
   // gather records of the standalone MATVEC (Mv16) in format mv16 (MV_*);
@@ -222,16 +226,23 @@ void *cgstab_kernel(int td, int sto, bool comp = false, bool wide = false) {
   return KSEL(k_cgstab);
 }
 
-#define MSEL1(k, STO_, M_)                                                    \
-  (td == DIA_Q ? (void *)k<DIA_Q, STO_, M_>                                    \
-               : td == DIA_I ? (void *)k<DIA_I, STO_, M_> : (void *)k<DIA_0, STO_, M_>)
-#define MSEL(k)                                                               \
-  (wide ? (sto == 3 ? MSEL1(k, 3, 2 * CG_MIN_BLOCKS) : MSEL1(k, 1, 2 * CG_MIN_BLOCKS)) \
-        : (sto == 3 ? MSEL1(k, 3, CG_MIN_BLOCKS) : MSEL1(k, 1, CG_MIN_BLOCKS)))
+// ... and, for the binary32 kernels, c16: the slots' neighbours as 16-bit
+// offsets (EBE storage only)
+#define MSEL1(k, STO_, M_, C_)                                                \
+  (td == DIA_Q ? (void *)k<DIA_Q, STO_, M_, C_>                                \
+               : td == DIA_I ? (void *)k<DIA_I, STO_, M_, C_> : (void *)k<DIA_0, STO_, M_, C_>)
+#define MSELM(k, M_)                                                          \
+  (sto == 3 ? MSEL1(k, 3, M_, false)                                          \
+            : (c16 ? MSEL1(k, 1, M_, true) : MSEL1(k, 1, M_, false)))
+#define MSEL(k) (wide ? MSELM(k, 2 * CG_MIN_BLOCKS) : MSELM(k, CG_MIN_BLOCKS))
 
-void *mixed_kernel(int td, int sto, bool wide = false) { return MSEL(k_mixed); }
+void *mixed_kernel(int td, int sto, bool wide = false, bool c16 = false) {
+  return MSEL(k_mixed);
+}
 
-void *batch_kernel(int td, int sto, bool wide = false) { return MSEL(k_batch); }
+void *batch_kernel(int td, int sto, bool wide = false, bool c16 = false) {
+  return MSEL(k_batch);
+}
 
 template <int TD, bool SYM, bool TR>
 void launch_mvseg(bief_handle *h, bool ext, const double *xa, const double *da, const double *y,
@@ -275,6 +286,7 @@ int persistent_grid(int npoin, int nsm, bool wide, int *out) {
   for (int td : {DIA_Q, DIA_I, DIA_0})
     for (int sto : {1, 3}) {
       ks.push_back(mixed_kernel(td, sto, wide));
+      if (sto == 1) ks.push_back(mixed_kernel(td, sto, wide, true));
       for (bool comp : {false, true})
         for (void *k : {cg_kernel(td, sto, comp, wide), equnor_kernel(td, sto, comp, wide),
                         rescjg_kernel(td, sto, comp, wide), errmin_kernel(td, sto, comp, wide),
@@ -402,7 +414,8 @@ int build_transposed(bief_handle *h, const double *xm, cudaStream_t st, Sell *ou
 static void set_cache_policy(const bief_handle *h, Sell &S) {
   const double l2 = (double)h->l2_bytes, n = (double)h->npoin;
   const double op64 = h->sto == 3 ? 12.0 * (double)h->nsg_slots : 24.0 * (double)h->nrec;
-  const double op32 = 8.0 * (double)(h->sto == 3 ? h->nsg_slots : h->nseg);
+  const double op32 = h->sto == 3 ? 8.0 * (double)h->nsg_slots
+                                  : (h->seg16 ? 6.0 : 8.0) * (double)h->nseg;
   S.cs_rec = l2 > 0.0 && op64 + 56.0 * n > l2;
   S.cs_seg = l2 > 0.0 && op32 + 28.0 * n > l2;
 }
@@ -418,6 +431,7 @@ Sell sell_of(const bief_handle *h) {
     S.rec_c = nullptr;
     S.seg_off = h->d_sg_off;
     S.seg_col = h->d_sg_col;
+    S.seg_dc = nullptr;
     S.seg_c = h->d_sg_c32;
     S.s32 = h->d_s32;
     S.sg_c = h->d_sg_c64;
@@ -429,6 +443,7 @@ Sell sell_of(const bief_handle *h) {
   S.rec_c = h->d_rec_c;
   S.seg_off = h->d_seg_off;
   S.seg_col = h->d_seg_col;
+  S.seg_dc = h->seg16 ? h->d_seg_dc : nullptr;
   S.seg_c = h->d_seg_c;
   S.s32 = h->d_s32;
   return S;
@@ -567,6 +582,8 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
   std::vector<int2> rec_idx(nrec, make_int2(0, 0));
   std::vector<uchar2> rec_slot(nrec, make_uchar2(0, 0));
   std::vector<int> seg_col(nseg, 0);
+  std::vector<short> seg_dc;
+  bool seg16 = true;
   for (int i = 0; i < npoin; ++i) {
     const int rb = rec_off[i >> 5] + (i & 31), sb = seg_off[i >> 5] + (i & 31);
     for (int m = 0; m < ptr[i + 1] - ptr[i]; ++m) {
@@ -575,7 +592,19 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
                                        ik[(size_t)((k + 2) % 3) * nelem + e]);
       rec_slot[rb + 32 * m] = make_uchar2(slot_a[j], slot_b[j]);
     }
-    for (int q = 0; q < nnb[i]; ++q) seg_col[sb + 32 * q] = nb_list[nb_ptr[i] + q];
+    for (int q = 0; q < nnb[i]; ++q) {
+      const int j = nb_list[nb_ptr[i] + q];
+      seg_col[sb + 32 * q] = j;
+      if (j - i < -32768 || j - i > 32767) seg16 = false;
+    }
+  }
+  if (seg16) {  // the same slots as 16-bit offsets from their node (6 B instead of 8 per slot)
+    seg_dc.assign(nseg, 0);
+    for (int i = 0; i < npoin; ++i) {
+      const int sb = seg_off[i >> 5] + (i & 31);
+      for (int q = 0; q < nnb[i]; ++q)
+        seg_dc[sb + 32 * q] = (short)(seg_col[sb + 32 * q] - i);
+    }
   }
 
   // MATVEC gather records (Mv16), in the most compact of three formats the
@@ -688,6 +717,13 @@ int bief_mesh_create(int npoin, int nelem, int nelmax, const int *ikle, int devi
         return fail(cuda_fail(e, "mesh upload", __LINE__));
       h->mv16 = mvf;
     }
+    if (seg16) {
+      if ((st = dalloc(&h->d_seg_dc, (size_t)nseg))) return fail(st);
+      if ((e = cudaMemcpyAsync(h->d_seg_dc, seg_dc.data(), sizeof(short) * nseg,
+                               cudaMemcpyHostToDevice, h->stream)) != cudaSuccess)
+        return fail(cuda_fail(e, "mesh upload", __LINE__));
+      h->seg16 = true;
+    }
     h->wide = wide_by_size(npoin, h->l2_bytes);
     if ((st = persistent_grid(npoin, h->nsm, h->wide, &h->G))) return fail(st);
     if ((st = dalloc(&h->d_part, 8 * (size_t)h->G + 4))) return fail(st);
@@ -728,7 +764,7 @@ int bief_destroy(bief_handle *h) {
                   h->d_s32, h->d_x, h->d_b, h->d_bs, h->d_r, h->d_d0, h->d_d1,
                   h->d_ad, h->d_t, h->d_z, h->d_ri, h->d_p0, h->d_p1, h->d_q, h->d_part,
                   h->d_ew, h->d_ctl, h->d_err, h->d_meta, h->d_rec_off, h->d_seg_off,
-                  h->d_rec_idx, h->d_rec_slot, h->d_rec_c, h->d_seg_col, h->d_seg_c,
+                  h->d_rec_idx, h->d_rec_slot, h->d_rec_c, h->d_seg_col, h->d_seg_dc, h->d_seg_c,
                   h->d_mv_deg, h->d_mv_eb, h->d_mv_ek, h->d_mv_dv,
                   h->d_binst, h->d_brel, h->d_bpart, h->d_g1, h->d_g2, h->d_sg_meta,
                   h->d_sg_off, h->d_sg_sx, h->d_sg_col, h->d_segel, h->d_xa, h->d_xas,
@@ -1127,7 +1163,8 @@ int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b, int precon,
   P.timeout_ns = h->timeout_ns;
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
   CK(cudaEventRecord(h->ev[0], s));
-  if ((st = launch_coop(h, mixed_kernel(td, h->sto, h->wide), &P, s))) return st;
+  if ((st = launch_coop(h, mixed_kernel(td, h->sto, h->wide, h->sto != 3 && h->seg16), &P, s)))
+    return st;
   CK(cudaEventRecord(h->ev[1], s));
   CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -1248,7 +1285,10 @@ int bief_matvec32_dev(bief_handle *h, float *x, const float *y, void *stream) {
     y = h->d_q;
   }
   CK(cudaEventRecord(h->ev[2], s));
-  k_matvec32<<<mv_grid(h->npoin), MV16_T, 0, s>>>(h->npoin, sell_of(h), y, x);
+  if (h->sto != 3 && h->seg16)
+    k_matvec32<true><<<mv_grid(h->npoin), MV16_T, 0, s>>>(h->npoin, sell_of(h), y, x);
+  else
+    k_matvec32<false><<<mv_grid(h->npoin), MV16_T, 0, s>>>(h->npoin, sell_of(h), y, x);
   h->launches++;
   CK(cudaGetLastError());
   CK(cudaEventRecord(h->ev[3], s));
@@ -1468,7 +1508,7 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
     h->s32_gen = -1;
     CK(cudaGetLastError());
   }
-  void *k = batch_kernel(td, seg ? 3 : 1, h->wide);
+  void *k = batch_kernel(td, seg ? 3 : 1, h->wide, !seg && h->seg16);
   int bps = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads_per_block, 0));
   if (bps < 1) return BIEF_ERR_CUDA;

@@ -63,7 +63,7 @@ __device__ __forceinline__ double op_row(int i, double acc, const Sell &S, V vec
   return acc;
 }
 
-template <int TD, int STO, int MINB = CG_MIN_BLOCKS>
+template <int TD, int STO, int MINB = CG_MIN_BLOCKS, bool C16 = false>
 __global__ void __launch_bounds__(CG_THREADS, MINB) k_batch(BatchP P) {
   __shared__ BatchState B;
   const int T = blockDim.x, t = threadIdx.x, G = gridDim.x;
@@ -328,10 +328,11 @@ __global__ void __launch_bounds__(CG_THREADS, MINB) k_batch(BatchP P) {
             float pi, acc;
             if (first) {
               pi = P.ri[v];
-              acc = seg_row(v, pi, P.S, [&](int w) { return P.ri[w]; });
+              acc = seg_row<C16>(v, pi, P.S, [&](int w) { return P.ri[w]; });
             } else {
               pi = add(P.ri[v], mul(beta, cur[v]));
-              acc = seg_row(v, pi, P.S, [&](int w) { return add(P.ri[w], mul(beta, cur[w])); });
+              acc = seg_row<C16>(v, pi, P.S,
+                                 [&](int w) { return add(P.ri[w], mul(beta, cur[w])); });
             }
             nxt[v] = pi;
             P.q[v] = acc;

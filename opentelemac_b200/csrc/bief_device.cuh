@@ -523,6 +523,7 @@ struct Sell {
   const double2 *rec_c;   // per record: (XA(k,a), XA(k,b)) of the operator
   const int *seg_off;     // per slice: first segment slot
   const int *seg_col;     // per slot: neighbour
+  const short *seg_dc;    // per slot: neighbour - node in 16 bits, when every offset fits
   const float *seg_c;     // per slot: binary32 coefficient
   const float *s32;       // per node: binary32 row sum
   const double *sg_c;     // segment storage: per slot, binary64 XA1/XA2
@@ -658,14 +659,24 @@ __device__ __forceinline__ void op_row2(int i0, int i1, bool has1, double &a0, d
     rec_row2(i0, i1, has1, a0, a1, S, vec);
 }
 
-template <int NB, class V>
-__device__ __forceinline__ void seg_batch(float &a0, float y0, const Sell &S, int b0, int m,
-                                          V vec) {
+// Neighbour of binary32 slot r of node i: from the 16-bit offsets (C16, the
+// mesh's numbering allowing: 6 instead of 8 bytes per slot) or the column.
+template <bool C16>
+__device__ __forceinline__ int seg_nb(const Sell &S, int i, int r) {
+  if constexpr (C16)
+    return i + (int)ld_op(S.seg_dc + r, S.cs_seg);
+  else
+    return ld_op(S.seg_col + r, S.cs_seg);
+}
+
+template <int NB, bool C16, class V>
+__device__ __forceinline__ void seg_batch(float &a0, float y0, const Sell &S, int i0, int b0,
+                                          int m, V vec) {
   int j[NB];
   float c[NB], v[NB];
 #pragma unroll
   for (int q = 0; q < NB; ++q) {
-    j[q] = ld_op(S.seg_col + b0 + 32 * (m + q), S.cs_seg);
+    j[q] = seg_nb<C16>(S, i0, b0 + 32 * (m + q));
     c[q] = ld_op(S.seg_c + b0 + 32 * (m + q), S.cs_seg);
   }
 #pragma unroll
@@ -676,34 +687,34 @@ __device__ __forceinline__ void seg_batch(float &a0, float y0, const Sell &S, in
 
 // One row of the binary32 product with the node's slot count n0, first
 // slot b0 and row sum s already loaded (batched slot loads as below).
-template <class V>
+template <bool C16, class V>
 __device__ __forceinline__ float seg_row_nb(int i0, int n0, int b0, float s, float y0,
                                             const Sell &S, V vec) {
   float a0 = mul(y0, s);
   int m = 0;
-  for (; m + SLOT_B32 <= n0; m += SLOT_B32) seg_batch<SLOT_B32>(a0, y0, S, b0, m, vec);
+  for (; m + SLOT_B32 <= n0; m += SLOT_B32) seg_batch<SLOT_B32, C16>(a0, y0, S, i0, b0, m, vec);
   if constexpr (SLOT_CASCADE && SLOT_B32 / 2 > 1) {
     if (m + SLOT_B32 / 2 <= n0) {
-      seg_batch<SLOT_B32 / 2>(a0, y0, S, b0, m, vec);
+      seg_batch<SLOT_B32 / 2, C16>(a0, y0, S, i0, b0, m, vec);
       m += SLOT_B32 / 2;
     }
   }
   for (; m < n0; ++m) {
-    const int jj = ld_op(S.seg_col + b0 + 32 * m, S.cs_seg);
+    const int jj = seg_nb<C16>(S, i0, b0 + 32 * m);
     const float cc = ld_op(S.seg_c + b0 + 32 * m, S.cs_seg);
     a0 = add(a0, mul(cc, sub(vec(jj), y0)));
   }
   return a0;
 }
 
-template <class V>
+template <bool C16 = false, class V>
 __device__ __forceinline__ void seg_row2(int i0, int i1, bool has1, float y0, float y1,
                                          float &a0, float &a1, const Sell &S, V vec) {
   if constexpr (SLOT_B32 > 1) {
     if (!has1) {
       const int n0 = __ldg(S.meta + i0) >> 16;
       const int b0 = __ldg(S.seg_off + (i0 >> 5)) + (i0 & 31);
-      a0 = seg_row_nb(i0, n0, b0, __ldg(S.s32 + i0), y0, S, vec);
+      a0 = seg_row_nb<C16>(i0, n0, b0, __ldg(S.s32 + i0), y0, S, vec);
       a1 = 0.0f;
       return;
     }
@@ -717,12 +728,12 @@ __device__ __forceinline__ void seg_row2(int i0, int i1, bool has1, float y0, fl
   const int nm = max(n0, n1);
   for (int m = 0; m < nm; ++m) {
     if (m < n0) {
-      const int j = ld_op(S.seg_col + b0 + 32 * m, S.cs_seg);
+      const int j = seg_nb<C16>(S, i0, b0 + 32 * m);
       const float c = ld_op(S.seg_c + b0 + 32 * m, S.cs_seg);
       a0 = add(a0, mul(c, sub(vec(j), y0)));
     }
     if (m < n1) {
-      const int j = ld_op(S.seg_col + b1 + 32 * m, S.cs_seg);
+      const int j = seg_nb<C16>(S, i1, b1 + 32 * m);
       const float c = ld_op(S.seg_c + b1 + 32 * m, S.cs_seg);
       a1 = add(a1, mul(c, sub(vec(j), y1)));
     }
@@ -738,10 +749,10 @@ __device__ __forceinline__ double rec_row(int i, double acc, const Sell &S, V ve
   return acc;
 }
 
-template <class V>
+template <bool C16 = false, class V>
 __device__ __forceinline__ float seg_row(int i, float yi, const Sell &S, V vec) {
   float acc, unused;
-  seg_row2(i, i, false, yi, 0.0f, acc, unused, S, vec);
+  seg_row2<C16>(i, i, false, yi, 0.0f, acc, unused, S, vec);
   return acc;
 }
 

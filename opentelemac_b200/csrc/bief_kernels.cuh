@@ -192,12 +192,15 @@ __global__ void __launch_bounds__(MV16_T) k_matvec16(int npoin, int nelem, Mv16 
 // MATVEC 'X=AY' in binary32 (no reference counterpart) on the binary32
 // edge-assembled copy of the operator, the product of the binary32 inner CG:
 // X_i = s_i Y_i + sum_j c_ij (Y_j - Y_i), with s_i the row sum and c_ij the
-// assembled off-diagonal coefficients, slots in sliced order.
+// assembled off-diagonal coefficients, slots in sliced order (C16: their
+// neighbours as 16-bit offsets).
+template <bool C16>
 __global__ void __launch_bounds__(256) k_matvec32(int npoin, Sell S, const float *__restrict__ y,
                                                   float *x) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npoin; i += gridDim.x * blockDim.x) {
     float a0, a1;
-    seg_row2(i, i, false, __ldg(y + i), 0.0f, a0, a1, S, [&](int k) { return __ldg(y + k); });
+    seg_row2<C16>(i, i, false, __ldg(y + i), 0.0f, a0, a1, S,
+                  [&](int k) { return __ldg(y + k); });
     x[i] = a0;
   }
 }
@@ -1658,7 +1661,9 @@ struct MixP {
   long long timeout_ns;
 };
 
-template <int TD, int STO, int MINB = CG_MIN_BLOCKS>
+// C16: the binary32 slots' neighbours as 16-bit offsets (EBE meshes whose
+// numbering allows it).
+template <int TD, int STO, int MINB = CG_MIN_BLOCKS, bool C16 = false>
 __global__ void __launch_bounds__(CG_THREADS, MINB) k_mixed(MixP P) {
   const int T = blockDim.x, t = threadIdx.x;
   const int lo = (int)blk_lo(blockIdx.x, P.npoin, gridDim.x);
@@ -1740,12 +1745,12 @@ __global__ void __launch_bounds__(CG_THREADS, MINB) k_mixed(MixP P) {
       if (first) {
         p0 = ri[i];
         if (h1) p1 = ri[i1];
-        seg_row2(i, i1, h1, p0, p1, a0, a1, P.S, [&](int k) { return ri[k]; });
+        seg_row2<C16>(i, i1, h1, p0, p1, a0, a1, P.S, [&](int k) { return ri[k]; });
       } else {
         p0 = add(ri[i], mul(beta, cur[i]));
         if (h1) p1 = add(ri[i1], mul(beta, cur[i1]));
-        seg_row2(i, i1, h1, p0, p1, a0, a1, P.S,
-                 [&](int k) { return add(ri[k], mul(beta, cur[k])); });
+        seg_row2<C16>(i, i1, h1, p0, p1, a0, a1, P.S,
+                      [&](int k) { return add(ri[k], mul(beta, cur[k])); });
       }
       nxt[i] = p0;
       q[i] = a0;

@@ -115,3 +115,34 @@ def test_batch_256_meshes():
         d = 1.0 / np.sqrt(dm)
         assert np.linalg.norm(res * d) / np.linalg.norm(bs_[k] * d) <= 1.01e-8
     bs.close()
+
+
+def test_batch_slot_columns_32bit(oracle_mod):
+    """A batch with one randomly renumbered 40,401-node instance, whose
+    binary32 slots need 32-bit columns (some neighbour lies more than 32,767
+    nodes away), beside small row-wise instances: every instance bit for bit
+    the oracle's."""
+    from opentelemac_b200.batch import BatchSolver
+    inst = _instances([13, 29])
+    x, y, ik = mg.square_mesh(201, seed=77)
+    x, y, ik, _, _ = mg.shuffled(x, y, ik, seed=78)
+    e = np.concatenate([ik[:, [0, 1]], ik[:, [1, 2]], ik[:, [2, 0]]])
+    assert np.abs(e[:, 0].astype(np.int64) - e[:, 1]).max() > 32767
+    coef = mg.wave_coef(mg.depth_loguniform(ik, seed=79))
+    dm, xm = oracle_mod.wave_matrix(x, y, ik, coef)
+    inst.insert(1, dict(x=x, y=y, ik=ik, coef=coef, dm=dm, xm=xm,
+                        b=np.random.default_rng(80).uniform(-1, 1, x.size)))
+    bs = BatchSolver([(p["x"].size, p["ik"]) for p in inst])
+    bs.assemble_wave([p["x"] for p in inst], [p["y"] for p in inst], [p["coef"] for p in inst])
+    b = bs.gather([p["b"] for p in inst])
+    xb = bs.gather([np.zeros(p["x"].size) for p in inst])
+    r = bs.solve_mixed(xb, b, inner_tol=1e-4, outer_tol=1e-9, nodes_per_thread=2,
+                       threads_per_block=1024)
+    xs = [v.cpu().numpy() for v in bs.scatter(xb)]
+    for k, p in enumerate(inst):
+        ref = oracle_mod.solve_mixed_batch(p["ik"], p["dm"], "Q", p["xm"], p["b"], precon=2,
+                                           inner_tol=1e-4, outer_tol=1e-9, npt=2, nthreads=1024)
+        assert r["status"][k] == ref["status"] == 0
+        assert (r["inner"][k], r["outer"][k]) == (ref["inner"], ref["outer"]), k
+        np.testing.assert_array_equal(xs[k], ref["x"], err_msg=f"instance {k}")
+    bs.close()

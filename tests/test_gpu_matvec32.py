@@ -95,3 +95,43 @@ def test_matvec32_follows_matrix_changes(oracle_mod):
         bief.matvec32(x, MQ, yd)
     assert e.value.status == -5
     mesh.close()
+
+
+def _max_offset(ik):
+    """Largest |neighbour - node| over the mesh's edges."""
+    e = np.concatenate([ik[:, [0, 1]], ik[:, [1, 2]], ik[:, [2, 0]]])
+    return int(np.abs(e[:, 0].astype(np.int64) - e[:, 1]).max())
+
+
+@pytest.mark.parametrize("numbering", ["rowwise", "shuffled"])
+def test_slot_column_forms(oracle_mod, numbering):
+    """The binary32 slots name their neighbours as 16-bit offsets from the
+    node when every offset fits (row-wise numbering) and as 32-bit columns
+    otherwise (a random renumbering of 40,401 nodes): in both, the mixed
+    solve equals the oracle bit for bit and the binary32 MATVEC stays within
+    32 binary32 ulps of |A| |y| of the binary64 product."""
+    import torch
+    p = small_problem(oracle_mod, n=201, shuffle=numbering == "shuffled", field="loguniform")
+    n = p["x"].size
+    assert (_max_offset(p["ik"]) > 32767) == (numbering == "shuffled")
+    mesh = bief.Mesh(p["ik"], n)
+    A = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
+    G, T = mesh.launch_info()
+    x = np.zeros(n)
+    st, outer, inner, relres = bief.solve_mixed(x, A, p["b"], precon=2, inner_tol=1e-2,
+                                                outer_tol=1e-10)
+    r = oracle_mod.solve_mixed(p["ik"], p["dm"], "Q", p["xm"], p["b"], precon=2, inner_tol=1e-2,
+                               outer_tol=1e-10, max_outer=1000, max_inner=1000000, nblocks=G,
+                               nthreads=T)
+    assert st == r["status"] == 0 and (outer, inner) == (r["outer"], r["inner"])
+    np.testing.assert_array_equal(x, r["x"])
+    # the stored matrix again (the solve scaled its working copy only)
+    y = np.random.default_rng(3).uniform(-1, 1, n)
+    x32 = torch.zeros(n, dtype=torch.float32, device="cuda")
+    bief.matvec32(x32, A, torch.tensor(y, dtype=torch.float32, device="cuda"))
+    ref = oracle_mod.matvec("X=AY    ", p["ik"], p["dm"], "Q", p["xm"], "S", y)
+    scale = oracle_mod.matvec("X=AY    ", p["ik"], np.abs(p["dm"]), "Q", np.abs(p["xm"]), "S",
+                              np.abs(y))
+    err = np.abs(x32.cpu().numpy().astype(np.float64) - ref)
+    assert np.all(err <= 32 * 2.0 ** -24 * scale + 1e-30), float((err / scale).max())
+    mesh.close()
