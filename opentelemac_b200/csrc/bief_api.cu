@@ -68,6 +68,9 @@ struct bief_handle {
   long long nsg_slots = 0;
   int *d_g1 = nullptr, *d_g2 = nullptr, *d_sg_meta = nullptr, *d_sg_off = nullptr,
       *d_sg_sx = nullptr, *d_sg_col = nullptr;
+  // segment slots' neighbours as 16-bit offsets, when every one fits (sg16)
+  short *d_sg_dc = nullptr;
+  bool sg16 = false;
   int2 *d_segel = nullptr;
   double *d_xa = nullptr, *d_xas = nullptr, *d_sg_c64 = nullptr;
   float *d_sg_c32 = nullptr;
@@ -227,12 +230,12 @@ void *cgstab_kernel(int td, int sto, bool comp = false, bool wide = false) {
 }
 
 // ... and, for the binary32 kernels, c16: the slots' neighbours as 16-bit
-// offsets (EBE storage only)
+// offsets
 #define MSEL1(k, STO_, M_, C_)                                                \
   (td == DIA_Q ? (void *)k<DIA_Q, STO_, M_, C_>                                \
                : td == DIA_I ? (void *)k<DIA_I, STO_, M_, C_> : (void *)k<DIA_0, STO_, M_, C_>)
 #define MSELM(k, M_)                                                          \
-  (sto == 3 ? MSEL1(k, 3, M_, false)                                          \
+  (sto == 3 ? (c16 ? MSEL1(k, 3, M_, true) : MSEL1(k, 3, M_, false))          \
             : (c16 ? MSEL1(k, 1, M_, true) : MSEL1(k, 1, M_, false)))
 #define MSEL(k) (wide ? MSELM(k, 2 * CG_MIN_BLOCKS) : MSELM(k, CG_MIN_BLOCKS))
 
@@ -286,7 +289,7 @@ int persistent_grid(int npoin, int nsm, bool wide, int *out) {
   for (int td : {DIA_Q, DIA_I, DIA_0})
     for (int sto : {1, 3}) {
       ks.push_back(mixed_kernel(td, sto, wide));
-      if (sto == 1) ks.push_back(mixed_kernel(td, sto, wide, true));
+      ks.push_back(mixed_kernel(td, sto, wide, true));
       for (bool comp : {false, true})
         for (void *k : {cg_kernel(td, sto, comp, wide), equnor_kernel(td, sto, comp, wide),
                         rescjg_kernel(td, sto, comp, wide), errmin_kernel(td, sto, comp, wide),
@@ -414,11 +417,15 @@ int build_transposed(bief_handle *h, const double *xm, cudaStream_t st, Sell *ou
 static void set_cache_policy(const bief_handle *h, Sell &S) {
   const double l2 = (double)h->l2_bytes, n = (double)h->npoin;
   const double op64 = h->sto == 3 ? 12.0 * (double)h->nsg_slots : 24.0 * (double)h->nrec;
-  const double op32 = h->sto == 3 ? 8.0 * (double)h->nsg_slots
+  const double op32 = h->sto == 3 ? (h->sg16 ? 6.0 : 8.0) * (double)h->nsg_slots
                                   : (h->seg16 ? 6.0 : 8.0) * (double)h->nseg;
   S.cs_rec = l2 > 0.0 && op64 + 56.0 * n > l2;
   S.cs_seg = l2 > 0.0 && op32 + 28.0 * n > l2;
 }
+
+// The binary32 slots of the current storage name their neighbours as
+// 16-bit offsets.
+static bool slots16(const bief_handle *h) { return h->sto == 3 ? h->sg16 : h->seg16; }
 
 Sell sell_of(const bief_handle *h) {
   Sell S;
@@ -431,7 +438,7 @@ Sell sell_of(const bief_handle *h) {
     S.rec_c = nullptr;
     S.seg_off = h->d_sg_off;
     S.seg_col = h->d_sg_col;
-    S.seg_dc = nullptr;
+    S.seg_dc = h->sg16 ? h->d_sg_dc : nullptr;
     S.seg_c = h->d_sg_c32;
     S.s32 = h->d_s32;
     S.sg_c = h->d_sg_c64;
@@ -767,7 +774,7 @@ int bief_destroy(bief_handle *h) {
                   h->d_rec_idx, h->d_rec_slot, h->d_rec_c, h->d_seg_col, h->d_seg_dc, h->d_seg_c,
                   h->d_mv_deg, h->d_mv_eb, h->d_mv_ek, h->d_mv_dv,
                   h->d_binst, h->d_brel, h->d_bpart, h->d_g1, h->d_g2, h->d_sg_meta,
-                  h->d_sg_off, h->d_sg_sx, h->d_sg_col, h->d_segel, h->d_xa, h->d_xas,
+                  h->d_sg_off, h->d_sg_sx, h->d_sg_col, h->d_sg_dc, h->d_segel, h->d_xa, h->d_xas,
                   h->d_sg_c64, h->d_sg_c32, h->d_rec_ct, h->d_sg_ct, h->d_gmv, h->d_gpart};
   for (void *p : bufs)
     if (p) cudaFree(p);
@@ -1163,8 +1170,7 @@ int bief_solve_mixed_dev(bief_handle *h, double *x, const double *b, int precon,
   P.timeout_ns = h->timeout_ns;
   CK(cudaMemsetAsync(h->d_ctl, 0, sizeof(Ctl), s));
   CK(cudaEventRecord(h->ev[0], s));
-  if ((st = launch_coop(h, mixed_kernel(td, h->sto, h->wide, h->sto != 3 && h->seg16), &P, s)))
-    return st;
+  if ((st = launch_coop(h, mixed_kernel(td, h->sto, h->wide, slots16(h)), &P, s))) return st;
   CK(cudaEventRecord(h->ev[1], s));
   CK(cudaMemcpyAsync(h->h_ctl, h->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -1285,7 +1291,7 @@ int bief_matvec32_dev(bief_handle *h, float *x, const float *y, void *stream) {
     y = h->d_q;
   }
   CK(cudaEventRecord(h->ev[2], s));
-  if (h->sto != 3 && h->seg16)
+  if (slots16(h))
     k_matvec32<true><<<mv_grid(h->npoin), MV16_T, 0, s>>>(h->npoin, sell_of(h), y, x);
   else
     k_matvec32<false><<<mv_grid(h->npoin), MV16_T, 0, s>>>(h->npoin, sell_of(h), y, x);
@@ -1508,7 +1514,7 @@ int bief_batch_solve_mixed_dev(bief_handle *h, int ninst, const int *node_off,
     h->s32_gen = -1;
     CK(cudaGetLastError());
   }
-  void *k = batch_kernel(td, seg ? 3 : 1, h->wide, !seg && h->seg16);
+  void *k = batch_kernel(td, seg ? 3 : 1, h->wide, seg ? h->sg16 : h->seg16);
   int bps = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, threads_per_block, 0));
   if (bps < 1) return BIEF_ERR_CUDA;
@@ -1768,20 +1774,28 @@ int bief_set_segments(bief_handle *h, int nseg, int maxseg, const int *gloseg) {
   }
   const size_t nslot = (size_t)off[nsl];
   std::vector<int> sx(nslot, 0), col(nslot, 0), fill(n, 0);
+  std::vector<short> dc(nslot, 0);
+  bool fit16 = true;
   for (int s = 0; s < nseg; ++s)
     for (int side = 0; side < 2; ++side) {
       const int i = side ? g2[s] : g1[s];
       const size_t q = (size_t)off[i >> 5] + (i & 31) + 32 * (size_t)fill[i]++;
       sx[q] = (s << 1) | side;
       col[q] = side ? g1[s] : g2[s];
+      const int d = col[q] - i;
+      if (d < -32768 || d > 32767) fit16 = false;
+      dc[q] = (short)d;
     }
   DevGuard g(h->dev);
   void *old[] = {h->d_g1, h->d_g2, h->d_sg_meta, h->d_sg_off, h->d_sg_sx, h->d_sg_col,
-                 h->d_segel, h->d_xa, h->d_xas, h->d_sg_c64, h->d_sg_c32, h->d_sg_ct};
+                 h->d_sg_dc, h->d_segel, h->d_xa, h->d_xas, h->d_sg_c64, h->d_sg_c32,
+                 h->d_sg_ct};
   CK(cudaStreamSynchronize(h->stream));
   for (void *p : old)
     if (p) cudaFree(p);
   h->d_g1 = h->d_g2 = h->d_sg_meta = h->d_sg_off = h->d_sg_sx = h->d_sg_col = nullptr;
+  h->d_sg_dc = nullptr;
+  h->sg16 = false;
   h->d_segel = nullptr;
   h->d_xa = h->d_xas = h->d_sg_c64 = nullptr;
   h->d_sg_c32 = nullptr;
@@ -1811,7 +1825,13 @@ int bief_set_segments(bief_handle *h, int nseg, int maxseg, const int *gloseg) {
                      h->stream));
   CK(cudaMemsetAsync(h->d_sg_c64, 0, sizeof(double) * nslot, h->stream));
   CK(cudaMemsetAsync(h->d_sg_c32, 0, sizeof(float) * nslot, h->stream));
+  if (fit16) {  // the binary32 kernels read 2-byte offsets instead of the columns
+    if ((st = dalloc(&h->d_sg_dc, nslot))) return st;
+    CK(cudaMemcpyAsync(h->d_sg_dc, dc.data(), sizeof(short) * nslot, cudaMemcpyHostToDevice,
+                       h->stream));
+  }
   CK(cudaStreamSynchronize(h->stream));
+  h->sg16 = fit16;
   h->nsg = nseg;
   h->nsg_slots = (long long)nslot;
   h->has_segments = 1;

@@ -103,26 +103,36 @@ def _max_offset(ik):
     return int(np.abs(e[:, 0].astype(np.int64) - e[:, 1]).max())
 
 
+@pytest.mark.parametrize("storage", ["ebe", "seg"])
 @pytest.mark.parametrize("numbering", ["rowwise", "shuffled"])
-def test_slot_column_forms(oracle_mod, numbering):
-    """The binary32 slots name their neighbours as 16-bit offsets from the
-    node when every offset fits (row-wise numbering) and as 32-bit columns
-    otherwise (a random renumbering of 40,401 nodes): in both, the mixed
-    solve equals the oracle bit for bit and the binary32 MATVEC stays within
-    32 binary32 ulps of |A| |y| of the binary64 product."""
+def test_slot_column_forms(oracle_mod, numbering, storage):
+    """The binary32 slots (EBE storage, or segment storage with STOSEG's
+    numbering) name their neighbours as 16-bit offsets from the node when
+    every offset fits (row-wise numbering) and as 32-bit columns otherwise
+    (a random renumbering of 40,401 nodes): in both, the mixed solve equals
+    the oracle bit for bit and the binary32 MATVEC stays within 32 binary32
+    ulps of |A| |y| of the binary64 product."""
     import torch
     p = small_problem(oracle_mod, n=201, shuffle=numbering == "shuffled", field="loguniform")
     n = p["x"].size
     assert (_max_offset(p["ik"]) > 32767) == (numbering == "shuffled")
     mesh = bief.Mesh(p["ik"], n)
     A = bief.Matrix(mesh, p["dm"], p["xm"], "Q", "S")
+    if storage == "seg":
+        g1, g2, es, ori = mg.segments(p["ik"], n)
+        mesh.set_segments(g1, g2)
+        A.to_segments()
+        xa = oracle_mod.assex3(es, ori, "S", p["xm"], g1.size)
     G, T = mesh.launch_info()
     x = np.zeros(n)
     st, outer, inner, relres = bief.solve_mixed(x, A, p["b"], precon=2, inner_tol=1e-2,
                                                 outer_tol=1e-10)
-    r = oracle_mod.solve_mixed(p["ik"], p["dm"], "Q", p["xm"], p["b"], precon=2, inner_tol=1e-2,
-                               outer_tol=1e-10, max_outer=1000, max_inner=1000000, nblocks=G,
-                               nthreads=T)
+    kw = dict(precon=2, inner_tol=1e-2, outer_tol=1e-10, max_outer=1000, max_inner=1000000,
+              nblocks=G, nthreads=T)
+    if storage == "seg":
+        r = oracle_mod.solve_mixed_seg(g1, g2, p["dm"], "Q", xa, p["b"], **kw)
+    else:
+        r = oracle_mod.solve_mixed(p["ik"], p["dm"], "Q", p["xm"], p["b"], **kw)
     assert st == r["status"] == 0 and (outer, inner) == (r["outer"], r["inner"])
     np.testing.assert_array_equal(x, r["x"])
     # the stored matrix again (the solve scaled its working copy only)
